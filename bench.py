@@ -1,0 +1,408 @@
+"""Benchmark of the 2-D shallow-water finite-volume step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--dtype fp32|fp64]
+                    [--n 2048] [--impl ours|reference]
+
+Workload (one "step" = one SSP-RK2 step of the whole grid): 2048 x 2048
+Cartesian cells on the unit square, eta (b, h + b, u) MUSCL with the minmod
+limiter, hydrostatic-reconstruction HLL faces, SSP-RK2, wet/dry threshold
+1e-6 (dry-cell demotion) with KP hinv at 1e-6, wall boundaries, bathymetry =
+16 seeded Gaussian bumps (amplitude U[0, 0.8], width U[0.02, 0.1]), circular
+dam break (level 2 inside r = 0.2, 1 outside, plus 1e-3 seeded noise;
+h = max(level - b, 0)), u = v = 0, CFL 0.45 with the d = 2 law.  Synthetic,
+seeded inputs stand in for the reference's test cases.
+
+Under torchrun (N > 1) every rank runs its own replica of the grid (the path
+has no data-path collective: replicas only); NCCL carries only the barrier
+and the max-over-ranks of the timing.
+
+--impl reference times the CPU restatement of the path (the reference itself
+cannot be installed: it needs jax and zoomy_core, absent here) on the host's
+cores: one process per core, each stepping a 256 x 256 sample of the same
+workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "zoomy-jax_b200"))
+
+METRIC = "cell-updates/s per B200 (2-D SWE SSP-RK2 step)"
+UNIT = "cell-updates/s"
+CPU_SAMPLE_N = 256
+
+
+def workload_state(n, seed=0):
+    """Host float64 (4, n*n) initial state of the 2048^2 configuration."""
+    from zoomy_b200.workloads import dam_break_2048
+    return dam_break_2048(n, seed)
+
+
+def workload_desc(n):
+    return (f"2-D SWE {n}x{n} unit square: eta-MUSCL minmod + hydrostatic "
+            f"reconstruction + HLL, SSP-RK2, wet/dry 1e-6, walls, 16 seeded "
+            f"Gaussian bumps, circular dam break + 1e-3 noise, CFL 0.45")
+
+
+# ── CPU leg (oracle restatement) ─────────────────────────────────────────────
+def _cpu_worker(args):
+    """One process: oracle SSP-RK2 steps on an n x n sample; returns the
+    per-step wall times.  Single-threaded BLAS/NumPy."""
+    n, warmup, steps, seed = args
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "zoomy-jax_b200"))
+    from oracle import mesh as OM
+    from oracle import swe as OS
+    m = OM.create_2d(0.0, 1.0, 0.0, 1.0, n, n)
+    Q = workload_state(n, seed)
+    params = OS.Params(wet_dry_eps=1e-6)
+    scheme = OS.Scheme(order=2, limiter="minmod", recon="eta", riemann="hll_hr",
+                       eps_wet=1e-6, cfl=0.45,
+                       bc={t: "wall" for t in ("left", "right", "bottom", "top")})
+    kind = OS.bc_kinds(m, scheme)
+    times = []
+    for it in range(warmup + steps):
+        t0 = time.perf_counter()
+        dt = OS.compute_dt(m, Q, params, scheme)
+        Q = OS.step(m, Q, dt, params, scheme, kind)
+        t1 = time.perf_counter()
+        if it >= warmup:
+            times.append(t1 - t0)
+    return times
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_cpu(warmup, steps, n=CPU_SAMPLE_N, procs=None):
+    """All host cores, one oracle process each (spawn context).  Returns
+    (cell-updates/s, cores, per-step seconds, sample text)."""
+    import multiprocessing as mp
+    procs = procs or min(cpu_cores(), 128)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, [(n, warmup, steps, 100 + r) for r in range(procs)])
+    # aggregate: all processes step concurrently; a step of the job = one step
+    # of every process, bounded by the slowest
+    per_step = [max(r[k] for r in res) for k in range(steps)]
+    mean_step = sum(per_step) / len(per_step)
+    value = procs * n * n / mean_step
+    sample = (f"{procs} independent {n}x{n} replicas of the workload (one per "
+              f"core), {warmup} warm-up + {steps} timed SSP-RK2 steps each, "
+              f"float64 NumPy oracle")
+    return value, procs, mean_step, sample
+
+
+# ── clocks ──────────────────────────────────────────────────────────────────
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index, path=None):
+        self.index = index
+        self.path = path
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            if self.path:
+                pathlib.Path(self.path).write_text("\n".join(self.lines) + "\n")
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ── GPU leg ──────────────────────────────────────────────────────────────────
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_gpu(args, rank, world, local_rank):
+    import ctypes as C
+    import numpy as np
+    import torch
+    import zoomy_b200 as zb
+    from zoomy_b200 import _lib as L
+    from zoomy_b200.fvm.solver import HyperbolicSolver
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.n
+    C_cells = n * n
+    dtype = "float32" if args.dtype == "fp32" else "float64"
+    es = 4 if dtype == "float32" else 8
+    Q_host = workload_state(n, seed=0)
+    model = zb.ShallowWater2D(wet_dry_eps=1e-6, initial_conditions=Q_host,
+                              boundary_conditions={t: "wall" for t in
+                                                   ("left", "right", "bottom", "top")})
+    nsm = zb.NumericalSystemModel.from_system_model(
+        model, zb.ReconstructionSpec(2, "minmod"), "hll_hr")
+    mesh = zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n)
+    solver = HyperbolicSolver(time_end=math.inf,
+                              compute_dt=zb.timestepping.adaptive(0.45, 2),
+                              reconstruction_variables="eta", free_surface_h_index=1,
+                              eps_wet=1e-6, dtype=dtype, device=f"cuda:{local_rank}")
+    Q, Qaux = solver.setup_simulation(mesh, nsm)
+    lib = solver.lib
+    cfg = C.byref(solver.cfg)
+    ws, wsb = L.ptr(solver._ws), C.c_size_t(solver._ws_bytes)
+    ctrl = L.ptr(solver._ctrl)
+    stream = torch.cuda.current_stream(dev)
+    sp = L.stream_ptr(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def part(k, which):
+        rc = lib.zb_swe2d_step_part(cfg, L.ptr(Q), ws, wsb, ctrl, k % 3, which, sp)
+        if rc != 0:
+            L.check(rc, "zb_swe2d_step_part")
+
+    # warm-up
+    solver.init_march(Q, 0.0)
+    for k in range(args.warmup):
+        part(k, 0)
+        part(k, 1)
+    torch.cuda.synchronize(dev)
+    k0 = args.warmup
+
+    # timed region: K steps, L2 flushed before each, events around each kernel
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    wall0 = time.perf_counter()
+    with ClockSampler(local_rank, path=str(ROOT / "gpurun_out" / f"clocks_rank{rank}.csv")
+                      if (ROOT / "gpurun_out").exists() else None) as clk:
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record(stream)
+            part(k0 + k, 0)
+            ev[k][1].record(stream)
+            part(k0 + k, 1)
+            ev[k][2].record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    wall = time.perf_counter() - wall0
+    st1 = [ev[k][0].elapsed_time(ev[k][1]) * 1e-3 for k in range(K)]
+    st2 = [ev[k][1].elapsed_time(ev[k][2]) * 1e-3 for k in range(K)]
+    step_s = sum(st1) + sum(st2)
+    c = solver.read_ctrl()
+    status_ok = c.status == 0
+    # max over ranks
+    tmax = step_s
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([step_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tmax = float(t.item())
+    value = world * C_cells * K / tmax
+
+    # roofline of the dominant kernel (stage 2: reads Q1 h/qx/qy + b + Q0
+    # h/qx/qy = 7 planes, writes 3 planes), algorithmic bytes per launch
+    hbm_peak, peak_kind = peaks()
+    mean2 = sum(st2) / K
+    mean1 = sum(st1) / K
+    bytes2 = 10 * C_cells * es
+    bytes1 = 7 * C_cells * es
+    achieved = bytes2 / mean2 / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+            "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+            "traffic": None, "kernel": "swe2d_stage_kernel<MODE_STEP2>",
+            "algorithmic_bytes_per_launch": bytes2,
+            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "stage1": {"ms": round(mean1 * 1e3, 4),
+                       "achieved": round(bytes1 / mean1 / 1e9, 1),
+                       "algorithmic_bytes_per_launch": bytes1},
+            "stage2_ms": round(mean2 * 1e3, 4),
+            "step_bytes_per_cell_update": 17 * es,
+            "step_achieved": round(17 * es * C_cells * K / step_s / 1e9, 1)}
+    traffic_file = ROOT / "profiles" / f"traffic_{args.dtype}.json"
+    if traffic_file.exists():
+        try:
+            roof["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch")
+        except ValueError:
+            pass
+
+    # e2e through the public C ABI with host buffers: upload the state from
+    # pinned host memory, K fused steps each followed by a device->host read
+    # of the step's control block (dt, time, status) that the host checks,
+    # then the state back to pinned host memory
+    td = torch.float32 if dtype == "float32" else torch.float64
+    host_in = torch.as_tensor(Q_host, dtype=td).contiguous().pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    ctrl_host = torch.empty(L.CTRL_BYTES, dtype=torch.uint8).pin_memory()
+    Qd = torch.empty_like(Q)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    Qd.copy_(host_in, non_blocking=True)
+    lib.zb_swe2d_init(cfg, L.ptr(Qd), ctrl, 0, 0.0, sp)
+    for k in range(K):
+        rc = lib.zb_swe2d_step(cfg, L.ptr(Qd), ws, wsb, ctrl, k % 3, sp)
+        L.check(rc, "zb_swe2d_step")
+        ctrl_host.copy_(solver._ctrl, non_blocking=True)
+        stream.synchronize()
+        cc = L.ZbCtrl.from_buffer_copy(ctrl_host.numpy().tobytes())
+        if cc.status & L.ZB_ST_DT_INVALID:
+            raise FloatingPointError("dt invalid during the e2e run")
+    host_out.copy_(Qd, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_s = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = 4 * C_cells * es
+    e2e = {"value": world * C_cells * K / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes // K,
+           "d2h_bytes_per_step": L.CTRL_BYTES + state_bytes // K,
+           "how": ("public C ABI (zb_swe2d_init/zb_swe2d_step) with pinned host "
+                   "buffers: state upload, K steps each followed by a D2H read and "
+                   "host check of the step's control block, state download")}
+    return {
+        "value": value, "ms_per_step": tmax / K * 1e3, "roofline": roof, "e2e": e2e,
+        "clocks": clk.summary(), "gpu_launches": 2 * K, "status_ok": status_ok,
+        "sim_time": float(c.t[(k0 + K) % 3]), "wall_s": wall,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--dtype", choices=("fp32", "fp64"), default="fp32")
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": workload_desc(args.n), "grid": [args.n, args.n],
+              "global_batch": world * args.n * args.n, "seq_len": None,
+              "parallelism": f"replicas x{world}",
+              "l2": "flushed between timed steps (256 MiB write, outside the events)",
+              "bc": "wall", "seed": 0}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        value, cores, mean_step, sample = run_cpu(max(1, min(args.warmup, 1)),
+                                                  max(1, min(args.steps, 3)))
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": mean_step * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config, "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                                 "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "note": ("the reference (jax + zoomy_core) cannot be installed here; "
+                         "this arm times the float64 oracle restatement of its path")}
+        print(json.dumps(line), flush=True)
+        return
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        # before any CUDA call: spawn-context pool of oracle processes
+        v, cores, mean_step, sample = run_cpu(1, args.cpu_steps)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": sample}
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    res = run_gpu(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.dtype == "fp32" else "f64",
+            "data": "synthetic", "config": config, "roofline": res["roofline"],
+            "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
+            "gpu_launches": res["gpu_launches"], "status_ok": res["status_ok"],
+            "sim_time": res["sim_time"]}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,182 @@
+/*
+ * zb.h -- C ABI of libzb, the B200 (sm_100a) finite-volume kernels behind the
+ * zoomy-b200 host package.
+ *
+ * Conventions
+ *   - All array arguments are DEVICE pointers unless a name ends in _host.
+ *   - State arrays use the reference layout (n_state, n_cells), cell axis last,
+ *     one contiguous plane per state row: Q = [b | h | q_x | q_y] for 2-D SWE.
+ *     Cartesian cell (i, j) (i along x, j along y) is cell i*ny + j.
+ *   - dtype: ZB_F32 or ZB_F64, for every floating array of the call.
+ *   - Every call takes the CUDA stream to launch on and returns 0 on success,
+ *     a negative ZB_E* code for a rejected argument or a CUDA launch error.
+ *     Device-side findings (non-finite or non-positive dt, troubled cells,
+ *     unconverged solves) are written to the status word of the caller's
+ *     zb_ctrl block and read by the host after the stream is synchronised.
+ *   - No call allocates device memory.  Scratch lives in caller-provided
+ *     workspace whose size the matching *_workspace_bytes call returns.
+ *
+ * Reference interfaces replaced (paths inside ZoomyLab/zoomy-jax):
+ *   zoomy_jax/fvm/solver2/blocks.py:36-95    dt_pass + reduce_dt
+ *   zoomy_jax/fvm/solver2/blocks.py:98-124   assert_dt_admissible (status bits)
+ *   zoomy_jax/fvm/solver2/blocks.py:129-287  halo_bc, reconstruct, flux_pass,
+ *                                            gather_update (one fused stage)
+ *   zoomy_jax/fvm/solver2/march.py:126-157   stage_loop (SSP-RK2 Shu-Osher)
+ *   zoomy_jax/fvm/solver_jax.py:990-1131     _explicit_hyperbolic_step + step
+ *   zoomy_jax/fvm/solver_jax.py:284-369      update_qaux (KP hinv + LSQ rows)
+ */
+#ifndef ZB_H
+#define ZB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* zb_stream_t; /* a cudaStream_t */
+
+enum { ZB_F32 = 0, ZB_F64 = 1 };
+
+enum {
+  ZB_OK = 0,
+  ZB_E_ARG = -1,      /* invalid argument (size, enum, null pointer) */
+  ZB_E_CUDA = -2,     /* CUDA launch / runtime error */
+  ZB_E_UNSUPPORTED = -3
+};
+
+/* status bits written by the kernels into zb_ctrl.status */
+enum {
+  ZB_ST_DT_INVALID = 1u,   /* dt non-finite or <= 0 before t_end (fatal) */
+  ZB_ST_TROUBLED = 2u,     /* a cell left h >= 0 or became non-finite */
+  ZB_ST_NOT_CONVERGED = 4u /* an iterative solve missed its tolerance */
+};
+
+/* boundary-condition kinds per side (reference BC.Extrapolation / Wall /
+ * Periodic; tests/cases.py:115-175) */
+enum { ZB_BC_EXTRAPOLATION = 0, ZB_BC_WALL = 1, ZB_BC_PERIODIC = 2 };
+enum { ZB_RECON_CONSTANT = 0, ZB_RECON_CONSERVATIVE = 1, ZB_RECON_ETA = 2 };
+enum { ZB_RIEMANN_RUSANOV = 0, ZB_RIEMANN_RUSANOV_HR = 1, ZB_RIEMANN_HLL_HR = 2 };
+enum { ZB_LIM_MINMOD = 0, ZB_LIM_BARTH_JESPERSEN = 1, ZB_LIM_VENKATAKRISHNAN = 2,
+       ZB_LIM_NONE = 3 };
+
+/* Device control block (caller-allocated device memory, 128 bytes, 8-byte
+ * aligned).  The step kernels triple-buffer the wave-speed maximum and the
+ * time by phase = step index mod 3: step n reads slot n%3, writes slot
+ * (n+1)%3 and clears slot (n+2)%3, so K steps run without a host sync and
+ * without a race between the clearing block and the accumulating blocks. */
+typedef struct {
+  double amax[3];     /* max over faces of |lambda| (phase-indexed)         */
+  double t[3];        /* simulation time (phase-indexed)                    */
+  double dt;          /* dt taken by the last step                          */
+  double mass;        /* last zb_swe2d_mass result (sum h |cell|)           */
+  uint32_t status;    /* ZB_ST_* bits, sticky until the host clears them    */
+  uint32_t steps;     /* steps completed (incremented by the final stage)   */
+  uint32_t troubled;  /* troubled cells seen in the last step               */
+  uint32_t pad;
+  double reserved[6];
+} zb_ctrl;
+
+/* Scheme and physics of the Cartesian 2-D SWE step.  Plain C struct. */
+typedef struct {
+  int32_t nx, ny;          /* cells along x and y                         */
+  double x0, y0, dx, dy;   /* origin and spacing                          */
+  int32_t order;           /* 1: Euler + constant recon, 2: SSP-RK2 + MUSCL */
+  int32_t recon;           /* ZB_RECON_*                                   */
+  int32_t riemann;         /* ZB_RIEMANN_*                                 */
+  int32_t limiter;         /* ZB_LIM_*                                     */
+  int32_t bc[4];           /* left, right, bottom, top: ZB_BC_*            */
+  double g;                /* gravity                                      */
+  double wet_dry_eps;      /* KP hinv desingularisation                    */
+  double eps_wet;          /* eta recon dry demotion (<0: none)            */
+  double manning_n;        /* Manning coefficient (0: no friction)         */
+  int32_t implicit_source; /* 0: explicit RK1 Manning, 1: point-implicit   */
+  int32_t dim_factor;      /* d of the CFL law (2 for 2-D)                 */
+  double cfl;              /* CFL safety factor                            */
+  double dt_max;           /* dt cap (+inf: none)                          */
+  double t_end;            /* t_end clamp (+inf: none)                     */
+  int32_t degree;          /* k of the (2k+1) CFL factor                   */
+  int32_t dtype;           /* ZB_F32 / ZB_F64                              */
+} zb_swe2d_cfg;
+
+/* Library version / build info. */
+const char* zb_version(void);
+
+/* Bytes of device workspace zb_swe2d_step needs (one stage buffer of three
+ * planes plus alignment padding). */
+size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg);
+
+/* Initialise the control block for a march starting at time t0 from state Q:
+ * clears status and all slots, sets t[phase] = t0 and amax[phase] = the
+ * maximum wave speed of Q.
+ * Replaces the first dt_pass (zoomy_jax/fvm/solver2/blocks.py:36-61). */
+int zb_swe2d_init(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl,
+                  int phase, double t0, zb_stream_t stream);
+
+/* dt of the state in Q: dt_pass + reduce_dt with t_remaining = t_end - t
+ * (zoomy_jax/fvm/solver2/blocks.py:36-95).  Writes ctrl->dt. */
+int zb_swe2d_dt(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl,
+                double t, zb_stream_t stream);
+
+/* One full time step, in place on Q (the b row is read, never written):
+ * dt from ctrl->amax[phase] (CFL law, dt_max, t_end clamp), the hyperbolic
+ * sub-step (order 2: SSP-RK2 with the KP aux refreshed between stages; order
+ * 1: Euler), Manning friction, and the wave-speed maximum of the new state
+ * into ctrl->amax[(phase + 1) % 3].  phase = step index mod 3.  Replaces HyperbolicSolver.step + post_step
+ * (zoomy_jax/fvm/solver_jax.py:1095-1172) and MarchSolver.hyperbolic_step
+ * (zoomy_jax/fvm/solver2/march.py:161-175).  Graph-capturable: no host
+ * sync, no allocation. */
+int zb_swe2d_step(const zb_swe2d_cfg* cfg, void* Q, void* workspace,
+                  size_t workspace_bytes, zb_ctrl* ctrl, int phase,
+                  zb_stream_t stream);
+
+/* One launch of zb_swe2d_step: part 0 is the first stage (order 2) or the
+ * Euler stage (order 1), part 1 the second stage (order 2) or the copy-back
+ * (order 1); part -1 is the whole step.  Calling part 0 then part 1 on the
+ * same stream is exactly zb_swe2d_step; the split lets a caller bracket each
+ * kernel with events. */
+int zb_swe2d_step_part(const zb_swe2d_cfg* cfg, void* Q, void* workspace,
+                       size_t workspace_bytes, zb_ctrl* ctrl, int phase,
+                       int part, zb_stream_t stream);
+
+/* One explicit stage with a host-given dt (dt < 0: read ctrl->dt):
+ * Q_out = alpha * Q0 + (1 - alpha) * (Qk + beta * dt * (L(Qk) + S(Qk))),
+ * the Shu-Osher form of solver2's stage loop (zoomy_jax/fvm/solver2/
+ * blocks.py:241-287, march.py:126-157).  S is the Manning source with aux
+ * hinv_src (one plane; NULL: no source in the stage).  force_o1 (C bytes or
+ * NULL) demotes flagged cells to constant reconstruction, the MOOD mask of
+ * zoomy_jax/fvm/reconstruction_jax.py:1246-1251.  trouble_out (C bytes or
+ * NULL) receives the troubled predicate h < 0 | non-finite per cell
+ * (solver2/blocks.py:290-301); any troubled cell also sets ZB_ST_TROUBLED.
+ * Q_out's b row is not written.  Q_out may alias Q0 but not Qk. */
+int zb_swe2d_stage(const zb_swe2d_cfg* cfg, const void* Qk, const void* Q0,
+                   void* Q_out, double alpha, double beta, double dt,
+                   const void* hinv_src, const uint8_t* force_o1,
+                   uint8_t* trouble_out, zb_ctrl* ctrl, zb_stream_t stream);
+
+/* Source step Q += dt * S(Q, hinv0) for Manning friction, explicit RK1 or
+ * point-implicit (cfg->implicit_source), with hinv0 the aux of the step's
+ * input state (one plane of C values).  Replaces get_compute_source + ode.RK1
+ * (zoomy_jax/fvm/solver_jax.py:373-397, 1129; zoomy_jax/fvm/ode.py:14-18)
+ * and the local implicit source of the IMEX solver
+ * (zoomy_jax/fvm/solver_imex_jax.py:269-342). */
+int zb_swe2d_source(const zb_swe2d_cfg* cfg, void* Q, const void* hinv0,
+                    double dt, zb_stream_t stream);
+
+/* Sum of h * |cell| in float64 (deterministic two-pass reduction) into
+ * ctrl->mass.  partial must hold zb_swe2d_mass_partials(cfg) doubles. */
+size_t zb_swe2d_mass_partials(const zb_swe2d_cfg* cfg);
+int zb_swe2d_mass(const zb_swe2d_cfg* cfg, const void* Q, double* partial,
+                  zb_ctrl* ctrl, zb_stream_t stream);
+
+/* Post-step aux rows (zoomy_jax/fvm/solver_jax.py:284-369) into Qaux (7, C):
+ * [dqx/dx, dh/dx, dqy/dy, dh/dy, db/dx, db/dy, hinv], LSQ with
+ * extrapolation ghosts. */
+int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux,
+                 zb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZB_H */

@@ -1,0 +1,273 @@
+"""GPU parity of the Cartesian SWE path (libzb) against the float64 oracle.
+
+Tolerances (stated here, checked below):
+* float64 kernels: relative L-infinity error <= 1e-12 per step against the
+  oracle fed the same state and dt (per state row, relative to the row's
+  max-norm, with an absolute floor of 1e-14 for rows that are ~0);
+* dt: relative error <= 1e-14;
+* float32 kernels: after 200 steps of a wet dam break the depth agrees with the
+  float64 oracle to 2e-4 relative L-infinity and the momentum to 2e-3 of its
+  max-norm (float32 rounding accumulated over 400 stages);
+* mass (float64 sums) is conserved to 1e-12 relative per 10 steps in float64.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from cases import circular_dam_state, gaussian_pulse_2d
+from oracle import mesh as OM
+from oracle import swe as OS
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import zoomy_b200 as zb  # noqa: E402
+from zoomy_b200 import _lib as L  # noqa: E402
+from zoomy_b200.fvm.solver import HyperbolicSolver  # noqa: E402
+from zoomy_b200.fvm.solver2 import MarchSolver  # noqa: E402
+
+TAGS = ("left", "right", "bottom", "top")
+
+
+def make(nx, ny, domain, state, *, order=2, recon="eta", riemann="hll_hr",
+         limiter="minmod", bc="wall", manning=0.0, cfl=0.45, eps_wet=None,
+         dtype="float64", implicit=False, t_end=math.inf, mood=False, oracle=True):
+    bcs = {t: bc for t in TAGS} if isinstance(bc, str) else dict(zip(TAGS, bc))
+    model = zb.ShallowWater2D(manning_n=manning, boundary_conditions=bcs,
+                              initial_conditions=state)
+    nsm = zb.NumericalSystemModel.from_system_model(
+        model, zb.ReconstructionSpec(order, limiter), riemann)
+    mesh = zb.create_2d(domain, nx, ny)
+    solver = HyperbolicSolver(
+        time_end=t_end, compute_dt=zb.timestepping.adaptive(cfl, 2),
+        reconstruction_variables="eta" if recon == "eta" else "conservative",
+        free_surface_h_index=1 if recon == "eta" else None, eps_wet=eps_wet,
+        dtype=dtype, implicit_source=implicit, mood=mood)
+    Q, Qaux = solver.setup_simulation(mesh, nsm)
+    om = OM.create_2d(domain[0], domain[1], domain[2], domain[3], nx, ny) if oracle else None
+    scheme = OS.Scheme(order=order, limiter=limiter,
+                       recon="constant" if order == 1 else recon, riemann=riemann,
+                       eps_wet=eps_wet, cfl=cfl, bc=bcs, mood=mood,
+                       source="implicit" if implicit else "explicit")
+    params = OS.Params(manning_n=manning)
+    return solver, Q, Qaux, om, scheme, params
+
+
+def rel_err(a, b):
+    out = []
+    for v in range(a.shape[0]):
+        scale = max(np.abs(b[v]).max(), 1e-14)
+        out.append(np.abs(a[v] - b[v]).max() / scale)
+    return np.array(out)
+
+
+def moving_dam(nx, ny, domain, seed=3):
+    """Circular dam break over seeded bumps (dry islands) with a swirl so
+    every flux term is non-zero from the first step."""
+    m = zb.create_2d(domain, nx, ny)
+    xc = m.cell_centers()
+    Q = circular_dam_state(xc, seed=seed, center=(0.5 * (domain[0] + domain[1]),
+                                                 0.5 * (domain[2] + domain[3])))
+    wet = Q[1] > 0
+    Q[2] = np.where(wet, 0.1 * Q[1] * np.sin(3 * xc[1]), 0.0)
+    Q[3] = np.where(wet, -0.1 * Q[1] * np.cos(2 * xc[0]), 0.0)
+    return Q
+
+
+CONFIGS = [
+    dict(order=1, recon="constant", riemann="rusanov", bc="extrapolation"),
+    dict(order=1, recon="constant", riemann="rusanov", bc="wall"),
+    dict(order=1, recon="constant", riemann="hll_hr", bc="periodic"),
+    dict(order=2, recon="conservative", riemann="rusanov", bc="extrapolation"),
+    dict(order=2, recon="conservative", riemann="hll_hr", bc="wall"),
+    dict(order=2, recon="eta", riemann="hll_hr", bc="wall"),
+    dict(order=2, recon="eta", riemann="hll_hr", bc="periodic"),
+    dict(order=2, recon="eta", riemann="hll_hr", bc=("wall", "extrapolation",
+                                                    "extrapolation", "wall")),
+    dict(order=2, recon="eta", riemann="rusanov_hr", bc="extrapolation"),
+    dict(order=2, recon="eta", riemann="hll_hr", bc="wall", eps_wet=1e-6),
+    dict(order=2, recon="eta", riemann="hll_hr", bc="wall", limiter="venkatakrishnan"),
+    dict(order=2, recon="eta", riemann="hll_hr", bc="wall", manning=0.03),
+    dict(order=2, recon="eta", riemann="hll_hr", bc="wall", manning=0.03, implicit=True),
+]
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=lambda c: "-".join(str(v) for v in c.values()))
+def test_fused_step_matches_oracle_per_step(cfg):
+    domain = (0.0, 1.0, 0.0, 1.5)
+    nx, ny = 40, 48
+    Q0 = moving_dam(nx, ny, domain)
+    solver, Q, Qaux, om, scheme, params = make(nx, ny, domain, Q0, **cfg)
+    solver.init_march(Q)
+    for it in range(4):
+        q_before = Q.double().cpu().numpy().copy()
+        dt_ref = OS.compute_dt(om, q_before, params, scheme)
+        solver.launch_steps(Q, 1)
+        c = solver.read_ctrl()
+        assert c.status == 0, f"status {c.status} at step {it}"
+        assert c.dt == pytest.approx(dt_ref, rel=1e-14, abs=0)
+        ref = OS.step(om, q_before, c.dt, params, scheme)
+        got = Q.double().cpu().numpy()
+        err = rel_err(got, ref)
+        assert err.max() <= 1e-12, f"step {it}: rel err per row {err}"
+        assert np.array_equal(got[0], q_before[0]), "the b row must not change"
+
+
+@pytest.mark.parametrize("cfg", CONFIGS[3:7], ids=lambda c: "-".join(str(v) for v in c.values()))
+def test_host_dt_step_matches_oracle(cfg):
+    """``step(dt, t, Q, Qaux)`` with a host dt (the reference's call shape)."""
+    domain = (0.0, 1.0, 0.0, 1.5)
+    Q0 = moving_dam(40, 48, domain, seed=5)
+    solver, Q, Qaux, om, scheme, params = make(40, 48, domain, Q0, **cfg)
+    dt = solver.compute_timestep(Q, Qaux)
+    q0 = Q.double().cpu().numpy()
+    assert dt == pytest.approx(OS.compute_dt(om, q0, params, scheme), rel=1e-14)
+    Qn = solver.step(dt, 0.0, Q, Qaux)
+    err = rel_err(Qn.double().cpu().numpy(), OS.step(om, q0, dt, params, scheme))
+    assert err.max() <= 1e-12, err
+
+
+def test_aux_rows_match_oracle():
+    domain = (0.0, 1.0, 0.0, 1.5)
+    Q0 = moving_dam(40, 48, domain)
+    solver, Q, Qaux, om, scheme, params = make(40, 48, domain, Q0)
+    ref = OS.derivative_aux(om, Q.cpu().numpy(), params)
+    np.testing.assert_allclose(Qaux.cpu().numpy(), ref, rtol=1e-13, atol=1e-13)
+
+
+def test_gpu_reproduces_reference_golden_swe_2d(goldens):
+    """The reference's own 2-D golden (32x32 Gaussian pulse, first order,
+    extrapolation, CFL 0.9, t_end 0.1) through ``HyperbolicSolver.solve``."""
+    model = zb.ShallowWater2D(boundary_conditions={t: "extrapolation" for t in TAGS},
+                              initial_conditions=gaussian_pulse_2d)
+    nsm = zb.NumericalSystemModel.from_system_model(
+        model, zb.ReconstructionSpec(1, "minmod"))
+    mesh = zb.create_2d((-1.0, 1.0, -1.0, 1.0), 32, 32)
+    solver = HyperbolicSolver(time_end=0.1, compute_dt=zb.timestepping.adaptive(0.9, 2))
+    Q, Qaux = solver.solve(mesh, nsm)
+    assert solver.steps_taken == 9
+    np.testing.assert_allclose(Q.cpu().numpy(), goldens["swe_2d__Q"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(Qaux.cpu().numpy(), goldens["swe_2d__Qaux"], rtol=0, atol=1e-13)
+
+
+def test_fp32_drift_after_200_steps():
+    domain = (0.0, 1.0, 0.0, 1.0)
+    m = zb.create_2d(domain, 64, 64)
+    Q0 = circular_dam_state(m.cell_centers(), seed=7, bathymetry=False)
+    solver, Q, Qaux, om, scheme, params = make(64, 64, domain, Q0, dtype="float32",
+                                               cfl=0.45)
+    solver.init_march(Q)
+    solver.launch_steps(Q, 200)
+    c = solver.read_ctrl()
+    assert c.status == 0
+    t_gpu = c.t[200 % 3]
+    Qr = Q0.copy()
+    kind = OS.bc_kinds(om, scheme)
+    t = 0.0
+    for _ in range(200):
+        dt = OS.compute_dt(om, Qr, params, scheme)
+        Qr = OS.step(om, Qr, dt, params, scheme, kind)
+        t += dt
+    assert t_gpu == pytest.approx(t, rel=1e-4)
+    got = Q.double().cpu().numpy()
+    err = rel_err(got, Qr)
+    assert err[1] <= 2e-4, err
+    assert max(err[2], err[3]) <= 2e-3, err
+
+
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-12), ("float32", 1e-5)])
+def test_full_size_mass_and_lake_at_rest(dtype, tol):
+    """2048^2 with dry islands: a lake at rest stays at rest and a dam break
+    conserves mass (float64 sums on the device)."""
+    n = 2048
+    domain = (0.0, 1.0, 0.0, 1.0)
+    m = zb.create_2d(domain, n, n)
+    xc = m.cell_centers()
+    from cases import bumps
+    b = bumps(xc, seed=0)
+    lake = np.stack([b, np.maximum(1.0 - b, 0.0), 0 * b, 0 * b])
+    solver, Q, Qaux, *_ = make(n, n, domain, lake, dtype=dtype, eps_wet=1e-6, oracle=False)
+    solver.init_march(Q)
+    solver.launch_steps(Q, 10)
+    assert solver.read_ctrl().status == 0
+    q = Q.double().cpu().numpy()
+    wet = lake[1] > 0
+    assert np.abs((q[0] + q[1])[wet] - 1.0).max() <= tol * 10
+    assert np.abs(q[2:]).max() <= tol * 10
+    assert np.all(q[1][~wet] == 0.0)
+    dam = circular_dam_state(xc, seed=0)
+    solver, Q, Qaux, *_ = make(n, n, domain, dam, dtype=dtype, eps_wet=1e-6, oracle=False)
+    m0 = solver.mass(Q)
+    solver.init_march(Q)
+    solver.launch_steps(Q, 10)
+    assert solver.read_ctrl().status == 0
+    m1 = solver.mass(Q)
+    assert abs(m1 - m0) / m0 <= (1e-12 if dtype == "float64" else 1e-6)
+
+
+def test_steps_after_t_end_are_noops():
+    domain = (0.0, 1.0, 0.0, 1.0)
+    Q0 = moving_dam(32, 32, domain)
+    solver, Q, Qaux, *_ = make(32, 32, domain, Q0, t_end=0.01)
+    Q, Qaux = solver.run_simulation(Q, Qaux)
+    assert solver.time == pytest.approx(0.01, abs=1e-15)
+    before = Q.clone()
+    solver.launch_steps(Q, 5)
+    c = solver.read_ctrl()
+    assert c.status == 0 and c.dt == 0.0
+    assert torch.equal(Q, before)
+
+
+def test_host_injected_nan_is_fatal():
+    """Failure detection without a GPU fault: a NaN planted in the host state
+    before upload makes dt non-finite; the march aborts with the reference's
+    FloatingPointError and the troubled/dt status bits are set."""
+    domain = (0.0, 1.0, 0.0, 1.0)
+    Q0 = moving_dam(32, 32, domain)
+    Q0[1, 100] = np.nan
+    solver, Q, Qaux, *_ = make(32, 32, domain, Q0, t_end=1.0)
+    with pytest.raises(FloatingPointError, match="FATAL"):
+        solver.run_simulation(Q, Qaux)
+    assert solver.read_ctrl().status & L.ZB_ST_DT_INVALID
+
+
+def test_march_solver_matches_hyperbolic_solver():
+    domain = (0.0, 1.0, 0.0, 1.0)
+    Q0 = moving_dam(40, 40, domain)
+    solver, Q, Qaux, om, scheme, params = make(40, 40, domain, Q0)
+    solver.init_march(Q)
+    solver.launch_steps(Q, 3)
+    ms = MarchSolver(reconstruction_variables="eta", free_surface_h_index=1)
+    model = solver.nsm
+    S = ms.setup_march(solver.mesh, model, CFL=0.45)
+    S, stats = ms.march(S, n_steps=3)
+    assert stats["steps"] == 3
+    err = rel_err(S.Q.double().cpu().numpy(), Q.double().cpu().numpy())
+    assert err.max() <= 1e-13, err
+
+
+def test_mood_redo_matches_oracle():
+    """Per-cell MOOD (production): with a dt three times the CFL limit the
+    order-2 candidate goes negative at the dry front; the troubled cells are
+    demoted to first order and the step is re-run, as the oracle does."""
+    domain = (0.0, 1.0, 0.0, 1.0)
+    m = zb.create_2d(domain, 48, 48)
+    xc = m.cell_centers()
+    Q0 = np.zeros((4, m.n_cells))
+    Q0[1] = np.where(xc[0] < 0.5, 1.0, 0.0)
+    solver, Q, Qaux, om, scheme, params = make(48, 48, domain, Q0, mood=True)
+    q0 = Q.double().cpu().numpy()
+    dt = 3.0 * OS.compute_dt(om, q0, params, scheme)
+    ref_plain, trouble = OS.step(om, q0, dt, params,
+                                 OS.Scheme(**{**scheme.__dict__, "mood": False}),
+                                 return_troubled=True)
+    if not trouble.any():
+        pytest.skip("no troubled cell at this dt")
+    got = solver.step(dt, 0.0, Q, Qaux).double().cpu().numpy()
+    ref = OS.step(om, q0, dt, params, scheme)
+    assert rel_err(got, ref).max() <= 1e-12
+    assert not np.allclose(got, ref_plain)

@@ -1,0 +1,1121 @@
+// Cartesian 2-D shallow-water finite-volume step for sm_100a.
+//
+// One kernel launch = one explicit stage of zoomy_jax's flux operator fused
+// with the Shu-Osher update (zoomy_jax/fvm/solver_jax.py:722-895 and
+// 990-1074; zoomy_jax/fvm/solver2/blocks.py:129-287, march.py:126-157):
+//
+//   halo load -> W = (b, eta, u, v) or (b, h, qx, qy) -> LSQ gradient (3x3
+//   least-squares stencil, boundary ghosts) -> neighbour bounds -> limiter ->
+//   tied / demoted slopes -> face traces with the Audusse clip -> Rusanov or
+//   hydrostatic-reconstruction HLL face flux, each face once per tile ->
+//   divergence + cell-edge bed source -> Q_out = a Q0 + (1 - a)(Qk + b dt L).
+//
+// Data layout: SoA planes (the reference's (n_state, n_cells) layout), cell
+// (i, j) at i*ny + j.  A CTA owns a TX x 32 tile (32 cells along the
+// contiguous y axis = one warp-wide coalesced row) and stages the tile plus a
+// 2-cell halo in shared memory; every face of the tile is evaluated exactly
+// once.  The final stage also folds in Manning friction, the troubled-cell
+// flag and the float64 maximum wave speed that sets the next dt, so a step is
+// two launches (SSP-RK2) with no host synchronisation.
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace zb {
+
+constexpr int TY = 32;        // tile cells along y (contiguous)
+constexpr int NT = 256;       // threads per CTA
+
+template <typename T>
+struct LsqTable {
+  // [class 0..8][direction][slot]; slot 0..7 = the 3x3 neighbours (a, b) in
+  // row-major order without (0, 0), 8 = x-boundary ghost, 9 = y-boundary ghost
+  T w[9][2][10];
+};
+
+template <typename T>
+struct SweParams {
+  int nx, ny;
+  T half_dx, half_dy;       // |face centre - cell centre|
+  T kx, ky;                 // |face| / |cell| for x- and y-faces
+  T g, eps_kp, eps_wet, manning_n;
+  T vk_eps2;                // Venkatakrishnan eps^2
+  int bc[4];                // left, right, bottom, top
+  int limiter;
+  int implicit_source;
+  double cfl2r;             // cfl * 2 * r_in
+  double den_fac;           // d * (2k + 1)
+  double dt_max, t_end;
+  double alpha, beta;       // Shu-Osher coefficients (generic stage)
+  double dt_stage;          // generic stage: dt (< 0: read ctrl->dt)
+  LsqTable<T> lsq;
+};
+
+enum { MODE_STEP1 = 0, MODE_STEP2 = 1, MODE_EULER = 2, MODE_STAGE = 3 };
+
+template <typename T, int TX>
+struct Smem {
+  static constexpr int R2X = TX + 4, R2Y = TY + 4, N2 = R2X * R2Y;
+  static constexpr int R1X = TX + 2, R1Y = TY + 2, N1 = R1X * R1Y;
+  static constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);
+  T b[N2], h[N2], w1[N2], w2[N2], w3[N2], aux[N2];
+  T sx[4][N1], sy[4][N1];
+  T fxh[NFX], fxt[NFX], fxl[NFX], fxr[NFX];
+  T fyh[NFY], fyt[NFY], fyl[NFY], fyr[NFY];
+};
+
+// ── dt from the phase slot (solver2/blocks.py:64-95) ────────────────────────
+__device__ __forceinline__ double dt_from_amax(double amax, double t,
+                                               double cfl2r, double den_fac,
+                                               double dt_max, double t_end) {
+  double dt = cfl2r / (den_fac * amax);   // amax = 0 -> +inf, drops out
+  dt = nmin(dt, dt_max);
+  dt = nmin(dt, t_end - t);
+  return dt;
+}
+
+// ── limiter candidates (reconstruction_jax.py:603-691) ──────────────────────
+// Minmod / Barth-Jespersen on a Cartesian cell: the four faces carry the
+// increments +a, -a (x) and +c, -c (y); with dpos = umax - u >= 0 and
+// dneg = umin - u <= 0 the two x-faces give clip(dpos/a) and clip(dneg/-a)
+// (a > eps), whose minimum is clip(min(dpos, -dneg)/|a|): IEEE division is
+// monotone, so this is the per-face min exactly.
+template <typename T>
+__device__ __forceinline__ T phi_pair_clipmin(T a, T dpos, T dneg) {
+  const T eps = T(1e-30);
+  if (a > eps) {
+    T r1 = clip01(dpos / a);
+    T r2 = clip01(dneg / (-a));
+    return zmin(r1, r2);
+  } else if (a < -eps) {
+    T r1 = clip01(dneg / a);
+    T r2 = clip01(dpos / (-a));
+    return zmin(r1, r2);
+  }
+  return T(1);
+}
+
+template <typename T>
+__device__ __forceinline__ T vk_cand(T delta, T dpos, T dneg, T ev2) {
+  const T eps = T(1e-30);
+  if (delta > eps) {
+    T num = dpos * dpos + ev2 + T(2) * delta * dpos;
+    T den = dpos * dpos + T(2) * delta * delta + delta * dpos + ev2;
+    return clip01(num / zmax(den, eps));
+  } else if (delta < -eps) {
+    T num = dneg * dneg + ev2 + T(2) * delta * dneg;
+    T den = dneg * dneg + T(2) * delta * delta + delta * dneg + ev2;
+    return clip01(-num / zmin(den, -eps));
+  }
+  return T(1);
+}
+
+template <typename T>
+__device__ __forceinline__ T limiter_phi(int lim, T gx, T gy, T hdx, T hdy,
+                                         T dpos, T dneg, T ev2) {
+  if (lim == ZB_LIM_NONE) return T(1);
+  T a = gx * hdx, c = gy * hdy;
+  if (lim == ZB_LIM_VENKATAKRISHNAN) {
+    T p = vk_cand(a, dpos, dneg, ev2);
+    p = zmin(p, vk_cand(-a, dpos, dneg, ev2));
+    p = zmin(p, vk_cand(c, dpos, dneg, ev2));
+    p = zmin(p, vk_cand(-c, dpos, dneg, ev2));
+    return clip01(p);
+  }
+  return clip01(zmin(phi_pair_clipmin(a, dpos, dneg),
+                     phi_pair_clipmin(c, dpos, dneg)));
+}
+
+// ── face state and Riemann solvers ──────────────────────────────────────────
+template <typename T>
+struct Side {
+  T b, h, qx, qy, ux, uy;
+};
+
+// Numerical flux across a face with unit normal (nx, ny) in {(+-1,0),(0,+-1)}.
+// Outputs Fh, Fqx, Fqy and the normal-direction fluctuations DmN (owner / L)
+// and DpN (neighbour / R).  Restates numerical_flux of the oracle:
+// Rusanov (zoomy_jax/fvm/flux.py:72-82) and hydrostatic-reconstruction
+// Rusanov / HLL (Audusse et al. 2004; Harten-Lax-van Leer 1983, Davis speeds).
+template <typename T, int RIEMANN>
+__device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R,
+                                        T nx, T ny, T g, T& Fh, T& Fqx,
+                                        T& Fqy, T& Dm, T& Dp) {
+  const T half = T(0.5);
+  T unL = L.ux * nx + L.uy * ny;
+  T unR = R.ux * nx + R.uy * ny;
+  if (RIEMANN == ZB_RIEMANN_RUSANOV) {
+    T cL = sqrt(g * L.h), cR = sqrt(g * R.h);
+    T s = nmax(fabs(unL) + cL, fabs(unR) + cR);
+    T qnL = L.qx * nx + L.qy * ny;
+    T qnR = R.qx * nx + R.qy * ny;
+    T pL = half * g * (L.h * L.h), pR = half * g * (R.h * R.h);
+    T FLx = L.qx * unL + pL * nx, FLy = L.qy * unL + pL * ny;
+    T FRx = R.qx * unR + pR * nx, FRy = R.qy * unR + pR * ny;
+    T hs = half * s;
+    Fh = half * (qnL + qnR) - hs * (R.h - L.h);
+    Fqx = half * (FLx + FRx) - hs * (R.qx - L.qx);
+    Fqy = half * (FLy + FRy) - hs * (R.qy - L.qy);
+    Dm = T(0);
+    Dp = T(0);
+    return;
+  }
+  T bs = nmax(L.b, R.b);
+  T hLs = nmax(T(0), L.h + L.b - bs);
+  T hRs = nmax(T(0), R.h + R.b - bs);
+  T cL = sqrt(g * hLs), cR = sqrt(g * hRs);
+  T qLx = hLs * L.ux, qLy = hLs * L.uy;
+  T qRx = hRs * R.ux, qRy = hRs * R.uy;
+  T FLh = hLs * unL, FRh = hRs * unR;
+  T pL = half * g * (hLs * hLs), pR = half * g * (hRs * hRs);
+  T FLx = qLx * unL + pL * nx, FLy = qLy * unL + pL * ny;
+  T FRx = qRx * unR + pR * nx, FRy = qRy * unR + pR * ny;
+  if (RIEMANN == ZB_RIEMANN_RUSANOV_HR) {
+    T s = nmax(fabs(unL) + cL, fabs(unR) + cR);
+    T hs = half * s;
+    Fh = half * (FLh + FRh) - hs * (hRs - hLs);
+    Fqx = half * (FLx + FRx) - hs * (qRx - qLx);
+    Fqy = half * (FLy + FRy) - hs * (qRy - qLy);
+  } else {
+    T SL = nmin(unL - cL, unR - cR);
+    T SR = nmax(unL + cL, unR + cR);
+    T sl = nmin(SL, T(0)), sr = nmax(SR, T(0));
+    T den = sr - sl;
+    T inv = den > T(0) ? T(1) / den : T(0);
+    T slsr = sl * sr;
+    Fh = (sr * FLh - sl * FRh + slsr * (hRs - hLs)) * inv;
+    Fqx = (sr * FLx - sl * FRx + slsr * (qRx - qLx)) * inv;
+    Fqy = (sr * FLy - sl * FRy + slsr * (qRy - qLy)) * inv;
+  }
+  Dm = half * g * (L.h * L.h - hLs * hLs);
+  Dp = -(half * g * (R.h * R.h - hRs * hRs));
+}
+
+// ── the fused stage kernel ──────────────────────────────────────────────────
+template <typename T, int TX, int ORDER, int RECON, int RIEMANN, int MODE>
+__global__ void __launch_bounds__(NT)
+swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
+                   const T* __restrict__ qxP, const T* __restrict__ qyP,
+                   const T* h0P, const T* qx0P, const T* qy0P,
+                   T* hO, T* qxO, T* qyO, zb_ctrl* ctrl, int phase,
+                   const T* __restrict__ hinv_src,
+                   const unsigned char* __restrict__ force_o1,
+                   unsigned char* __restrict__ trouble_out,
+                   const SweParams<T> p) {
+  using S = Smem<T, TX>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+  __shared__ double red[NT / 32];
+
+  const int tid = threadIdx.x;
+  const int nx = p.nx, ny = p.ny;
+  const int i0 = blockIdx.y * TX, j0 = blockIdx.x * TY;
+  const bool per_x = p.bc[0] == ZB_BC_PERIODIC;
+  const bool per_y = p.bc[2] == ZB_BC_PERIODIC;
+
+  // dt of this step
+  double dtd;
+  if (MODE == MODE_STAGE) {
+    dtd = p.dt_stage >= 0.0 ? p.dt_stage : ctrl->dt;
+  } else {
+    const int ph = phase;
+    const int nph = (ph + 1) % 3, nnph = (ph + 2) % 3;
+    const double t = ctrl->t[ph];
+    dtd = dt_from_amax(ctrl->amax[ph], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
+    const bool ok = isfinite(dtd) && dtd > 0.0;
+    const bool lead = blockIdx.x == 0 && blockIdx.y == 0 && tid == 0;
+    if ((MODE == MODE_STEP1 || MODE == MODE_EULER) && lead) {
+      if (!ok && t < p.t_end) atomicOr(&ctrl->status, (unsigned)ZB_ST_DT_INVALID);
+      ctrl->dt = ok ? dtd : 0.0;
+      ctrl->t[nph] = ok ? t + dtd : t;
+      ctrl->amax[nnph] = 0.0;
+      ctrl->troubled = 0u;
+    }
+    if (!ok) {
+      // no-op step (t_end reached or dt invalid): the state is unchanged, so
+      // the next slot carries this slot's wave-speed maximum forward
+      if ((MODE == MODE_STEP2 || MODE == MODE_EULER) && lead) ctrl->amax[nph] = ctrl->amax[ph];
+      if (MODE == MODE_EULER) {
+        // the Euler path writes the workspace that is copied back: keep it equal
+        const int nx_ = p.nx, ny_ = p.ny;
+        for (int e = tid; e < TX * TY; e += NT) {
+          const int gi = i0 + e / TY, gj = j0 + e % TY;
+          if (gi < nx_ && gj < ny_) {
+            const size_t k = (size_t)gi * ny_ + gj;
+            hO[k] = hP[k]; qxO[k] = qxP[k]; qyO[k] = qyP[k];
+          }
+        }
+      }
+      return;
+    }
+  }
+  const T dt = T(dtd);
+
+  // ── phase A: halo-2 load, W transform ──
+  for (int e = tid; e < S::N2; e += NT) {
+    const int r = e / S::R2Y, c = e - r * S::R2Y;
+    int gi = i0 - 2 + r, gj = j0 - 2 + c;
+    bool ix = gi >= 0 && gi < nx, iy = gj >= 0 && gj < ny;
+    if (!ix && per_x && iy) { gi = (gi + nx) % nx; ix = true; }
+    if (!iy && per_y && ix) { gj = (gj + ny) % ny; iy = true; }
+    T vb = T(0), vh = T(0), vqx = T(0), vqy = T(0);
+    if (ix && iy) {
+      const size_t k = (size_t)gi * ny + gj;
+      vb = bP[k]; vh = hP[k]; vqx = qxP[k]; vqy = qyP[k];
+    }
+    const T hinv = kp_hinv(vh, p.eps_kp);
+    s.b[e] = vb;
+    s.h[e] = vh;
+    s.aux[e] = hinv;
+    if (RECON == ZB_RECON_ETA) {
+      s.w1[e] = vb + vh;
+      s.w2[e] = vqx * hinv;
+      s.w3[e] = vqy * hinv;
+    } else {
+      s.w1[e] = vh;
+      s.w2[e] = vqx;
+      s.w3[e] = vqy;
+    }
+  }
+  __syncthreads();
+
+  // ── phase B: gradients, bounds, limiter (halo-1 region) ──
+  if (ORDER >= 2) {
+    for (int e = tid; e < S::N1; e += NT) {
+      const int r = e / S::R1Y, c = e - r * S::R1Y;
+      const int gi = i0 - 1 + r, gj = j0 - 1 + c;
+      if (gi < 0 || gi >= nx || gj < 0 || gj >= ny) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) { s.sx[v][e] = T(0); s.sy[v][e] = T(0); }
+        continue;
+      }
+      const int e2 = (r + 1) * S::R2Y + (c + 1);
+      const bool bxl = gi == 0, bxh = gi == nx - 1, byl = gj == 0, byh = gj == ny - 1;
+      const bool interior = !(bxl || bxh || byl || byh);
+      const int cls = (bxl ? 0 : (bxh ? 2 : 1)) * 3 + (byl ? 0 : (byh ? 2 : 1));
+      const T* wv[4] = {s.b, s.w1, s.w2, s.w3};
+      T phi[4], gxa[4], gya[4];
+      const T ev2 = p.vk_eps2;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const T* W = wv[v];
+        const T u = W[e2];
+        T gx = T(0), gy = T(0), umax = u, umin = u;
+        if (interior) {
+          // slots (a, b): (-1,-1) (-1,0) (-1,1) (0,-1) (0,1) (1,-1) (1,0) (1,1)
+          const T d0 = W[e2 - S::R2Y - 1] - u, d1 = W[e2 - S::R2Y] - u;
+          const T d2 = W[e2 - S::R2Y + 1] - u, d3 = W[e2 - 1] - u;
+          const T d4 = W[e2 + 1] - u, d5 = W[e2 + S::R2Y - 1] - u;
+          const T d6 = W[e2 + S::R2Y] - u, d7 = W[e2 + S::R2Y + 1] - u;
+          const T* wx = p.lsq.w[4][0];
+          const T* wy = p.lsq.w[4][1];
+          gx = wx[0] * d0 + wx[1] * d1 + wx[2] * d2 + wx[3] * d3 + wx[4] * d4 +
+               wx[5] * d5 + wx[6] * d6 + wx[7] * d7;
+          gy = wy[0] * d0 + wy[1] * d1 + wy[2] * d2 + wy[3] * d3 + wy[4] * d4 +
+               wy[5] * d5 + wy[6] * d6 + wy[7] * d7;
+          umax = nmax(umax, W[e2 + S::R2Y]); umin = nmin(umin, W[e2 + S::R2Y]);
+          umax = nmax(umax, W[e2 - S::R2Y]); umin = nmin(umin, W[e2 - S::R2Y]);
+          umax = nmax(umax, W[e2 + 1]);      umin = nmin(umin, W[e2 + 1]);
+          umax = nmax(umax, W[e2 - 1]);      umin = nmin(umin, W[e2 - 1]);
+        } else {
+          // ghost values of this cell's boundary faces (BC at the cell state;
+          // a wall negates the normal momentum / velocity; periodic = image)
+          T gxv = u, gyv = u;
+          if (bxl || bxh) {
+            const int side = bxl ? 0 : 1;
+            if (p.bc[side] == ZB_BC_PERIODIC) gxv = W[e2 + (bxl ? -S::R2Y : S::R2Y)];
+            else if (p.bc[side] == ZB_BC_WALL && v == 2) gxv = -u;
+          }
+          if (byl || byh) {
+            const int side = byl ? 2 : 3;
+            if (p.bc[side] == ZB_BC_PERIODIC) gyv = W[e2 + (byl ? -1 : 1)];
+            else if (p.bc[side] == ZB_BC_WALL && v == 3) gyv = -u;
+          }
+          const T* wx = p.lsq.w[cls][0];
+          const T* wy = p.lsq.w[cls][1];
+          int k = 0;
+#pragma unroll
+          for (int a = -1; a <= 1; ++a) {
+#pragma unroll
+            for (int bb = -1; bb <= 1; ++bb) {
+              if (a == 0 && bb == 0) continue;
+              const bool ok = gi + a >= 0 && gi + a < nx && gj + bb >= 0 && gj + bb < ny;
+              const T d = ok ? W[e2 + a * S::R2Y + bb] - u : T(0);
+              gx += wx[k] * d;
+              gy += wy[k] * d;
+              ++k;
+            }
+          }
+          if (bxl || bxh) { const T d = gxv - u; gx += wx[8] * d; gy += wy[8] * d; }
+          if (byl || byh) { const T d = gyv - u; gx += wx[9] * d; gy += wy[9] * d; }
+          // bounds: inside face neighbours + ghost 2 u_bf - u
+          if (!bxh) { umax = nmax(umax, W[e2 + S::R2Y]); umin = nmin(umin, W[e2 + S::R2Y]); }
+          if (!bxl) { umax = nmax(umax, W[e2 - S::R2Y]); umin = nmin(umin, W[e2 - S::R2Y]); }
+          if (!byh) { umax = nmax(umax, W[e2 + 1]); umin = nmin(umin, W[e2 + 1]); }
+          if (!byl) { umax = nmax(umax, W[e2 - 1]); umin = nmin(umin, W[e2 - 1]); }
+          if (bxl || bxh) { const T gg = T(2) * gxv - u; umax = nmax(umax, gg); umin = nmin(umin, gg); }
+          if (byl || byh) { const T gg = T(2) * gyv - u; umax = nmax(umax, gg); umin = nmin(umin, gg); }
+        }
+        gxa[v] = gx;
+        gya[v] = gy;
+        phi[v] = limiter_phi(p.limiter, gx, gy, p.half_dx, p.half_dy,
+                             umax - u, umin - u, ev2);
+      }
+      if (RECON == ZB_RECON_ETA) {
+        if (p.eps_wet >= T(0) && s.h[e2] < p.eps_wet) {
+          phi[0] = phi[1] = phi[2] = phi[3] = T(0);
+        }
+        phi[0] = zmin(phi[0], phi[1]);
+        phi[2] = zmin(phi[2], phi[1]);
+        phi[3] = zmin(phi[3], phi[1]);
+      }
+      if (force_o1 != nullptr && force_o1[(size_t)gi * ny + gj]) {
+        phi[0] = phi[1] = phi[2] = phi[3] = T(0);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        s.sx[v][e] = phi[v] * gxa[v];
+        s.sy[v][e] = phi[v] * gya[v];
+      }
+    }
+    __syncthreads();
+  }
+
+  // ── phase C: faces ──
+  // side trace of the cell at R2 index e2 / R1 index e1 at offset (ox, oy)
+  auto trace = [&](int e2, int e1, T ox, T oy, Side<T>& sd) {
+    T vb = s.b[e2], w1 = s.w1[e2], w2 = s.w2[e2], w3 = s.w3[e2];
+    if (ORDER >= 2) {
+      vb = vb + (s.sx[0][e1] * ox + s.sy[0][e1] * oy);
+      w1 = w1 + (s.sx[1][e1] * ox + s.sy[1][e1] * oy);
+      w2 = w2 + (s.sx[2][e1] * ox + s.sy[2][e1] * oy);
+      w3 = w3 + (s.sx[3][e1] * ox + s.sy[3][e1] * oy);
+    }
+    sd.b = vb;
+    if (RECON == ZB_RECON_ETA) {
+      const T eta = nmax(w1, vb);
+      const T hf = eta - vb;
+      sd.h = hf;
+      sd.ux = w2;
+      sd.uy = w3;
+      sd.qx = w2 * hf;
+      sd.qy = w3 * hf;
+    } else {
+      const T hinv = s.aux[e2];
+      sd.h = w1;
+      sd.qx = w2;
+      sd.qy = w3;
+      sd.ux = w2 * hinv;
+      sd.uy = w3 * hinv;
+    }
+  };
+  // periodic seam: Q_R is the partner cell's (unreconstructed) state; its
+  // velocity is the partner's own W row on the eta path and q times the
+  // OWNER's hinv on the conservative path (the flux pass hands the inner
+  // cell's aux to both sides of a boundary face, solver_jax.py:827-866)
+  auto partner = [&](int e2img, T hinv_owner, Side<T>& sd) {
+    sd.b = s.b[e2img];
+    sd.h = s.h[e2img];
+    if (RECON == ZB_RECON_ETA) {
+      sd.ux = s.w2[e2img];
+      sd.uy = s.w3[e2img];
+      sd.qx = sd.ux * sd.h;   // not read by the hydrostatic-reconstruction fluxes
+      sd.qy = sd.uy * sd.h;
+    } else {
+      sd.qx = s.w2[e2img];
+      sd.qy = s.w3[e2img];
+      sd.ux = sd.qx * hinv_owner;
+      sd.uy = sd.qy * hinv_owner;
+    }
+  };
+  const T g = p.g;
+  const T half = T(0.5);
+  // x-faces
+  for (int e = tid; e < S::NFX; e += NT) {
+    const int fi = e / TY, fj = e - fi * TY;
+    const int gi = i0 + fi, gj = j0 + fj;
+    if (gj >= ny || gi > nx) continue;
+    const int e2L = (fi + 1) * S::R2Y + (fj + 2), e2R = e2L + S::R2Y;
+    const int e1L = fi * S::R1Y + (fj + 1), e1R = e1L + S::R1Y;
+    Side<T> A, B;
+    T Fh, Fx, Fy, Dm, Dp;
+    if (gi == 0 || gi == nx) {
+      const bool lo = gi == 0;
+      const int e2o = lo ? e2R : e2L, e1o = lo ? e1R : e1L;
+      const T sg = lo ? T(-1) : T(1);
+      trace(e2o, e1o, sg * p.half_dx, T(0), A);
+      const int kind = p.bc[lo ? 0 : 1];
+      if (kind == ZB_BC_PERIODIC) {
+        partner(lo ? e2L : e2R, s.aux[e2o], B);
+      } else {
+        B = A;
+        if (kind == ZB_BC_WALL) {
+          // q - 2 (q.n) n with n = (sg, 0)
+          const T qn = A.qx * sg + A.qy * T(0);
+          B.qx = A.qx - T(2) * qn * sg;
+          B.qy = A.qy - T(2) * qn * T(0);
+          const T un = A.ux * sg + A.uy * T(0);
+          B.ux = A.ux - T(2) * un * sg;
+          B.uy = A.uy - T(2) * un * T(0);
+        }
+      }
+      riemann<T, RIEMANN>(A, B, sg, T(0), g, Fh, Fx, Fy, Dm, Dp);
+      T ces = T(0);
+      if (ORDER >= 2) ces = half * g * (s.h[e2o] + A.h) * (A.b - s.b[e2o]);
+      const T own_n = Fx + Dm * sg + ces * sg;
+      if (lo) {
+        s.fxh[e] = -Fh; s.fxt[e] = -Fy; s.fxr[e] = own_n; s.fxl[e] = T(0);
+      } else {
+        s.fxh[e] = Fh; s.fxt[e] = Fy; s.fxl[e] = own_n; s.fxr[e] = T(0);
+      }
+    } else {
+      trace(e2L, e1L, p.half_dx, T(0), A);
+      trace(e2R, e1R, -p.half_dx, T(0), B);
+      riemann<T, RIEMANN>(A, B, T(1), T(0), g, Fh, Fx, Fy, Dm, Dp);
+      T cesA = T(0), cesB = T(0);
+      if (ORDER >= 2) {
+        cesA = half * g * (s.h[e2L] + A.h) * (A.b - s.b[e2L]);
+        cesB = -(half * g * (s.h[e2R] + B.h) * (B.b - s.b[e2R]));
+      }
+      s.fxh[e] = Fh;
+      s.fxt[e] = Fy;
+      s.fxl[e] = Fx + Dm + cesA;
+      s.fxr[e] = -Fx + Dp + cesB;
+    }
+  }
+  // y-faces
+  for (int e = tid; e < S::NFY; e += NT) {
+    const int fi = e / (TY + 1), fj = e - fi * (TY + 1);
+    const int gi = i0 + fi, gj = j0 + fj;
+    if (gi >= nx || gj > ny) continue;
+    const int e2L = (fi + 2) * S::R2Y + (fj + 1), e2R = e2L + 1;
+    const int e1L = (fi + 1) * S::R1Y + fj, e1R = e1L + 1;
+    Side<T> A, B;
+    T Fh, Fx, Fy, Dm, Dp;
+    if (gj == 0 || gj == ny) {
+      const bool lo = gj == 0;
+      const int e2o = lo ? e2R : e2L, e1o = lo ? e1R : e1L;
+      const T sg = lo ? T(-1) : T(1);
+      trace(e2o, e1o, T(0), sg * p.half_dy, A);
+      const int kind = p.bc[lo ? 2 : 3];
+      if (kind == ZB_BC_PERIODIC) {
+        partner(lo ? e2L : e2R, s.aux[e2o], B);
+      } else {
+        B = A;
+        if (kind == ZB_BC_WALL) {
+          const T qn = A.qx * T(0) + A.qy * sg;
+          B.qx = A.qx - T(2) * qn * T(0);
+          B.qy = A.qy - T(2) * qn * sg;
+          const T un = A.ux * T(0) + A.uy * sg;
+          B.ux = A.ux - T(2) * un * T(0);
+          B.uy = A.uy - T(2) * un * sg;
+        }
+      }
+      riemann<T, RIEMANN>(A, B, T(0), sg, g, Fh, Fx, Fy, Dm, Dp);
+      T ces = T(0);
+      if (ORDER >= 2) ces = half * g * (s.h[e2o] + A.h) * (A.b - s.b[e2o]);
+      const T own_n = Fy + Dm * sg + ces * sg;
+      if (lo) {
+        s.fyh[e] = -Fh; s.fyt[e] = -Fx; s.fyr[e] = own_n; s.fyl[e] = T(0);
+      } else {
+        s.fyh[e] = Fh; s.fyt[e] = Fx; s.fyl[e] = own_n; s.fyr[e] = T(0);
+      }
+    } else {
+      trace(e2L, e1L, T(0), p.half_dy, A);
+      trace(e2R, e1R, T(0), -p.half_dy, B);
+      riemann<T, RIEMANN>(A, B, T(0), T(1), g, Fh, Fx, Fy, Dm, Dp);
+      T cesA = T(0), cesB = T(0);
+      if (ORDER >= 2) {
+        cesA = half * g * (s.h[e2L] + A.h) * (A.b - s.b[e2L]);
+        cesB = -(half * g * (s.h[e2R] + B.h) * (B.b - s.b[e2R]));
+      }
+      s.fyh[e] = Fh;
+      s.fyt[e] = Fx;
+      s.fyl[e] = Fy + Dm + cesA;
+      s.fyr[e] = -Fy + Dp + cesB;
+    }
+  }
+  __syncthreads();
+
+  // ── phase D: divergence, stage update, epilogue ──
+  double amax_loc = 0.0;
+  bool bad = false;
+  for (int e = tid; e < TX * TY; e += NT) {
+    const int ti = e / TY, tj = e - ti * TY;
+    const int gi = i0 + ti, gj = j0 + tj;
+    if (gi >= nx || gj >= ny) continue;
+    const int fl = ti * TY + tj, fr = fl + TY;
+    const int fb = ti * (TY + 1) + tj, ft = fb + 1;
+    const T kx = p.kx, ky = p.ky;
+    const T dh = -(kx * (s.fxh[fr] - s.fxh[fl]) + ky * (s.fyh[ft] - s.fyh[fb]));
+    const T dqx = -(kx * (s.fxl[fr] + s.fxr[fl]) + ky * (s.fyt[ft] - s.fyt[fb]));
+    const T dqy = -(kx * (s.fxt[fr] - s.fxt[fl]) + ky * (s.fyl[ft] + s.fyr[fb]));
+    const int e2 = (ti + 2) * S::R2Y + (tj + 2);
+    const T hk = s.h[e2];
+    T qxk, qyk;
+    if (RECON == ZB_RECON_ETA) {
+      const size_t k = (size_t)gi * ny + gj;
+      qxk = qxP[k];
+      qyk = qyP[k];
+    } else {
+      qxk = s.w2[e2];
+      qyk = s.w3[e2];
+    }
+    T hn, qxn, qyn;
+    const size_t k = (size_t)gi * ny + gj;
+    if (MODE == MODE_STEP1) {
+      hn = hk + dt * dh;
+      qxn = qxk + dt * dqx;
+      qyn = qyk + dt * dqy;
+    } else if (MODE == MODE_STEP2) {
+      const T h2 = hk + dt * dh, qx2 = qxk + dt * dqx, qy2 = qyk + dt * dqy;
+      const T h0 = h0P[k], qx0 = qx0P[k], qy0 = qy0P[k];
+      hn = half * (h0 + h2);
+      qxn = half * (qx0 + qx2);
+      qyn = half * (qy0 + qy2);
+    } else if (MODE == MODE_EULER) {
+      hn = hk + dt * dh;
+      qxn = qxk + dt * dqx;
+      qyn = qyk + dt * dqy;
+    } else {
+      const T a = T(p.alpha), bt = T(p.beta);
+      T sqx = dqx, sqy = dqy;
+      if (hinv_src != nullptr && p.manning_n != T(0)) {
+        // solver2 adds the source to the stage residual at Qk with the step's
+        // aux (solver2/blocks.py:241-287, march.py:120-124)
+        const T hi = hinv_src[k];
+        const T qn = sqrt(qxk * qxk + qyk * qyk);
+        const T kf = (-p.g) * (p.manning_n * p.manning_n) * qn * (hi * hi) * cbrt(hi);
+        sqx = dqx + qxk * kf;
+        sqy = dqy + qyk * kf;
+      }
+      const T h2 = hk + bt * dt * dh, qx2 = qxk + bt * dt * sqx, qy2 = qyk + bt * dt * sqy;
+      if (p.alpha != 0.0) {
+        const T h0 = h0P[k], qx0 = qx0P[k], qy0 = qy0P[k];
+        hn = a * h0 + (T(1) - a) * h2;
+        qxn = a * qx0 + (T(1) - a) * qx2;
+        qyn = a * qy0 + (T(1) - a) * qy2;
+      } else {
+        hn = h2; qxn = qx2; qyn = qy2;
+      }
+    }
+    if ((MODE == MODE_STEP2 || MODE == MODE_EULER) && p.manning_n != T(0)) {
+      // source as RK1 after the hyperbolic step with the step's input aux
+      // (zoomy_jax/fvm/solver_jax.py:1129; ode.py:14-18)
+      const T h0 = (MODE == MODE_STEP2) ? h0P[k] : hk;
+      const T hi0 = kp_hinv(h0, p.eps_kp);
+      const T qn = sqrt(qxn * qxn + qyn * qyn);
+      const T kf = (-p.g) * (p.manning_n * p.manning_n) * qn * (hi0 * hi0) * cbrt(hi0);
+      if (p.implicit_source) {
+        const T den = T(1) + dt * (-kf);
+        qxn = qxn / den;
+        qyn = qyn / den;
+      } else {
+        qxn = qxn + dt * (qxn * kf);
+        qyn = qyn + dt * (qyn * kf);
+      }
+    }
+    hO[k] = hn;
+    qxO[k] = qxn;
+    qyO[k] = qyn;
+    const bool tr = (hn < T(0)) || !isfinite(hn) || !isfinite(qxn) || !isfinite(qyn) ||
+                    !isfinite(s.b[e2]);
+    bad = bad || tr;
+    if (trouble_out != nullptr) trouble_out[k] = tr ? 1 : 0;
+    if (MODE == MODE_STEP2 || MODE == MODE_EULER) {
+      const T hi = kp_hinv(hn, p.eps_kp);
+      const T c = sqrt(g * nmax(hn, T(0)));
+      const T lx = fabs(qxn * hi) + c, ly = fabs(qyn * hi) + c;
+      amax_loc = nmax(amax_loc, (double)nmax(lx, ly));
+    }
+  }
+  const unsigned anybad = __syncthreads_or(bad ? 1 : 0);
+  if (anybad && tid == 0) atomicOr(&ctrl->status, (unsigned)ZB_ST_TROUBLED);
+  if (MODE == MODE_STEP2 || MODE == MODE_EULER) {
+    const double m = block_max_double(amax_loc, red);
+    if (tid == 0) {
+      atomic_max_pos_double(&ctrl->amax[(phase + 1) % 3], m);
+      if (blockIdx.x == 0 && blockIdx.y == 0) atomicAdd(&ctrl->steps, 1u);
+    }
+  }
+}
+
+// ── wave-speed max / aux / mass kernels ─────────────────────────────────────
+template <typename T>
+__global__ void __launch_bounds__(NT)
+swe2d_amax_kernel(const T* __restrict__ hP, const T* __restrict__ qxP,
+                  const T* __restrict__ qyP, size_t C, T g, T eps_kp,
+                  double* out) {
+  __shared__ double red[NT / 32];
+  double m = 0.0;
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < C;
+       k += (size_t)gridDim.x * NT) {
+    const T h = hP[k];
+    const T hi = kp_hinv(h, eps_kp);
+    const T c = sqrt(g * nmax(h, T(0)));
+    const T lx = fabs(qxP[k] * hi) + c, ly = fabs(qyP[k] * hi) + c;
+    m = nmax(m, (double)nmax(lx, ly));
+  }
+  m = block_max_double(m, red);
+  if (threadIdx.x == 0) atomic_max_pos_double(out, m);
+}
+
+__global__ void swe2d_ctrl_init_kernel(zb_ctrl* ctrl, int phase, double t0) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3; ++i) { ctrl->amax[i] = 0.0; ctrl->t[i] = 0.0; }
+    ctrl->t[phase] = t0;
+    ctrl->dt = 0.0;
+    ctrl->status = 0u;
+    ctrl->steps = 0u;
+    ctrl->troubled = 0u;
+  }
+}
+
+__global__ void swe2d_dt_finalize_kernel(zb_ctrl* ctrl, double t, double cfl2r,
+                                         double den_fac, double dt_max,
+                                         double t_end) {
+  if (threadIdx.x == 0) {
+    const double dt = dt_from_amax(ctrl->reserved[0], t, cfl2r, den_fac, dt_max, t_end);
+    ctrl->dt = dt;
+    if (!(isfinite(dt) && dt > 0.0) && t < t_end)
+      atomicOr(&ctrl->status, (unsigned)ZB_ST_DT_INVALID);
+  }
+}
+
+__global__ void zero_double_kernel(double* p) { *p = 0.0; }
+
+// LSQ derivative aux rows with extrapolation ghosts (delta 0)
+template <typename T>
+__global__ void __launch_bounds__(NT)
+swe2d_aux_kernel(const T* __restrict__ Q, T* __restrict__ A, int nx, int ny,
+                 T eps_kp, const LsqTable<T> lsq) {
+  const size_t C = (size_t)nx * ny;
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < C;
+       k += (size_t)gridDim.x * NT) {
+    const int gi = (int)(k / ny), gj = (int)(k - (size_t)gi * ny);
+    const bool bxl = gi == 0, bxh = gi == nx - 1, byl = gj == 0, byh = gj == ny - 1;
+    const int cls = (bxl ? 0 : (bxh ? 2 : 1)) * 3 + (byl ? 0 : (byh ? 2 : 1));
+    const T* wx = lsq.w[cls][0];
+    const T* wy = lsq.w[cls][1];
+    T g[4][2];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const T* U = Q + (size_t)v * C;
+      const T u = U[k];
+      T gx = T(0), gy = T(0);
+      int s = 0;
+      for (int a = -1; a <= 1; ++a)
+        for (int bb = -1; bb <= 1; ++bb) {
+          if (a == 0 && bb == 0) continue;
+          const bool ok = gi + a >= 0 && gi + a < nx && gj + bb >= 0 && gj + bb < ny;
+          const T d = ok ? U[k + (long long)a * ny + bb] - u : T(0);
+          gx += wx[s] * d;
+          gy += wy[s] * d;
+          ++s;
+        }
+      g[v][0] = gx;
+      g[v][1] = gy;
+    }
+    A[0 * C + k] = g[2][0];
+    A[1 * C + k] = g[1][0];
+    A[2 * C + k] = g[3][1];
+    A[3 * C + k] = g[1][1];
+    A[4 * C + k] = g[0][0];
+    A[5 * C + k] = g[0][1];
+    A[6 * C + k] = kp_hinv(Q[C + k], eps_kp);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT)
+mass_partial_kernel(const T* __restrict__ h, size_t C, double vol, double* partial) {
+  __shared__ double red[NT];
+  double acc = 0.0;
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < C;
+       k += (size_t)gridDim.x * NT)
+    acc += (double)h[k] * vol;
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = NT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void mass_final_kernel(const double* partial, int n, zb_ctrl* ctrl) {
+  __shared__ double red[NT];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += NT) acc += partial[i];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = NT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ctrl->mass = red[0];
+}
+
+// Manning friction as RK1 with a given aux hinv0 (ode.py:14-18,
+// solver_jax.py:373-397, 1129); implicit = point-implicit closed form
+template <typename T>
+__global__ void __launch_bounds__(NT)
+swe2d_source_kernel(T* __restrict__ qx, T* __restrict__ qy, const T* __restrict__ hinv0,
+                    size_t C, T g, T n, T dt, int implicit) {
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < C;
+       k += (size_t)gridDim.x * NT) {
+    const T hi0 = hinv0[k];
+    T a = qx[k], b = qy[k];
+    const T qn = sqrt(a * a + b * b);
+    const T kf = (-g) * (n * n) * qn * (hi0 * hi0) * cbrt(hi0);
+    if (implicit) {
+      const T den = T(1) + dt * (-kf);
+      a = a / den;
+      b = b / den;
+    } else {
+      a = a + dt * (a * kf);
+      b = b + dt * (b * kf);
+    }
+    qx[k] = a;
+    qy[k] = b;
+  }
+}
+
+// ── host side ───────────────────────────────────────────────────────────────
+constexpr int MASS_BLOCKS = 1184;   // 148 SMs x 8
+
+static bool valid_cfg(const zb_swe2d_cfg* c) {
+  if (!c) return false;
+  if (c->nx < 3 || c->ny < 3) return false;
+  if ((long long)c->nx * c->ny > (1LL << 31)) return false;
+  if (!(c->dx > 0 && c->dy > 0)) return false;
+  if (c->order != 1 && c->order != 2) return false;
+  if (c->recon < 0 || c->recon > 2 || c->riemann < 0 || c->riemann > 2) return false;
+  if (c->limiter < 0 || c->limiter > 3) return false;
+  for (int i = 0; i < 4; ++i)
+    if (c->bc[i] < 0 || c->bc[i] > 2) return false;
+  if ((c->bc[0] == ZB_BC_PERIODIC) != (c->bc[1] == ZB_BC_PERIODIC)) return false;
+  if ((c->bc[2] == ZB_BC_PERIODIC) != (c->bc[3] == ZB_BC_PERIODIC)) return false;
+  if (c->dtype != ZB_F32 && c->dtype != ZB_F64) return false;
+  if (c->order == 1 && c->recon != ZB_RECON_CONSTANT) return false;
+  if (c->order == 2 && c->recon == ZB_RECON_CONSTANT) return false;
+  if (c->dim_factor < 1 || c->degree < 0) return false;
+  return true;
+}
+
+// Least-squares weights of the 9 Cartesian cell classes: pseudo-inverse of the
+// offsets of the in-domain 3x3 neighbours plus, per derivative direction, the
+// ghost of the boundary face normal to that direction (oracle/mesh.py,
+// _lsq_weights; pinned against the reference's derivative aux rows).
+template <typename T>
+static LsqTable<T> make_lsq(double dx, double dy) {
+  LsqTable<T> tab;
+  std::memset(&tab, 0, sizeof(tab));
+  for (int ci = 0; ci < 3; ++ci)
+    for (int cj = 0; cj < 3; ++cj) {
+      const int cls = ci * 3 + cj;
+      for (int d = 0; d < 2; ++d) {
+        double px[10], py[10];
+        int slot[10], n = 0, k = 0;
+        for (int a = -1; a <= 1; ++a)
+          for (int b = -1; b <= 1; ++b) {
+            if (a == 0 && b == 0) continue;
+            const bool okx = !(ci == 0 && a < 0) && !(ci == 2 && a > 0);
+            const bool oky = !(cj == 0 && b < 0) && !(cj == 2 && b > 0);
+            if (okx && oky) { px[n] = a * dx; py[n] = b * dy; slot[n] = k; ++n; }
+            ++k;
+          }
+        if (d == 0 && ci != 1) { px[n] = (ci == 0 ? -1.0 : 1.0) * dx; py[n] = 0.0; slot[n] = 8; ++n; }
+        if (d == 1 && cj != 1) { px[n] = 0.0; py[n] = (cj == 0 ? -1.0 : 1.0) * dy; slot[n] = 9; ++n; }
+        double sxx = 0, sxy = 0, syy = 0;
+        for (int m = 0; m < n; ++m) { sxx += px[m] * px[m]; sxy += px[m] * py[m]; syy += py[m] * py[m]; }
+        const double det = sxx * syy - sxy * sxy;
+        const double i00 = syy / det, i01 = -sxy / det, i11 = sxx / det;
+        for (int m = 0; m < n; ++m) {
+          const double wxm = i00 * px[m] + i01 * py[m];
+          const double wym = i01 * px[m] + i11 * py[m];
+          tab.w[cls][d][slot[m]] = (T)(d == 0 ? wxm : wym);
+        }
+      }
+    }
+  return tab;
+}
+
+template <typename T>
+static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta,
+                                double dt_stage = -1.0) {
+  SweParams<T> p;
+  std::memset(&p, 0, sizeof(p));
+  p.nx = c->nx;
+  p.ny = c->ny;
+  p.half_dx = (T)(0.5 * c->dx);
+  p.half_dy = (T)(0.5 * c->dy);
+  const double vol = c->dx * c->dy;
+  p.kx = (T)(c->dy / vol);
+  p.ky = (T)(c->dx / vol);
+  p.g = (T)c->g;
+  p.eps_kp = (T)c->wet_dry_eps;
+  p.eps_wet = (T)(c->eps_wet < 0 ? -1.0 : c->eps_wet);
+  p.manning_n = (T)c->manning_n;
+  const double hv = std::pow(vol, 0.5);
+  p.vk_eps2 = (T)(hv * hv);
+  for (int i = 0; i < 4; ++i) p.bc[i] = c->bc[i];
+  p.limiter = c->limiter;
+  p.implicit_source = c->implicit_source;
+  const double r_in = c->dx * c->dy / (c->dx + c->dy);
+  p.cfl2r = c->cfl * 2.0 * r_in;
+  p.den_fac = (double)c->dim_factor * (double)(2 * c->degree + 1);
+  p.dt_max = c->dt_max;
+  p.t_end = c->t_end;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.dt_stage = dt_stage;
+  p.lsq = make_lsq<T>(c->dx, c->dy);
+  return p;
+}
+
+template <typename T>
+constexpr int tile_x() { return sizeof(T) == 4 ? 16 : 8; }
+
+template <typename T, int ORDER, int RECON, int RIEMANN, int MODE>
+static int launch_stage(const zb_swe2d_cfg* c, const T* b, const T* h, const T* qx,
+                        const T* qy, const T* h0, const T* qx0, const T* qy0,
+                        T* ho, T* qxo, T* qyo, zb_ctrl* ctrl, int phase,
+                        const SweParams<T>& p, cudaStream_t st,
+                        const T* hinv_src = nullptr,
+                        const unsigned char* force_o1 = nullptr,
+                        unsigned char* trouble_out = nullptr) {
+  constexpr int TX = tile_x<T>();
+  auto kern = swe2d_stage_kernel<T, TX, ORDER, RECON, RIEMANN, MODE>;
+  const size_t sm = sizeof(Smem<T, TX>);
+  static unsigned attr_mask = 0u;   // per instantiation, one bit per device
+  int dev = 0;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 32) return ZB_E_UNSUPPORTED;
+  if (!(attr_mask & (1u << dev))) {
+    ZB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr_mask |= 1u << dev;
+  }
+  dim3 grid((c->ny + TY - 1) / TY, (c->nx + TX - 1) / TX);
+  kern<<<grid, NT, sm, st>>>(b, h, qx, qy, h0, qx0, qy0, ho, qxo, qyo, ctrl, phase,
+                             hinv_src, force_o1, trouble_out, p);
+  return zb_launch_check();
+}
+
+// part: -1 = the whole step, 0 = first launch only, 1 = second launch only
+template <typename T, int ORDER, int RECON, int RIEMANN>
+static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase,
+                    int part, cudaStream_t st) {
+  const size_t C = (size_t)c->nx * c->ny;
+  T *b = Q, *h = Q + C, *qx = Q + 2 * C, *qy = Q + 3 * C;
+  const SweParams<T> p = make_params<T>(c, 0.0, 1.0);
+  T *h1 = ws, *qx1 = ws + C, *qy1 = ws + 2 * C;
+  if (ORDER == 1) {
+    // Euler reads the stencil of Q and cannot write Q in place: write the
+    // workspace (launch 0), then copy the three evolving planes back (part 1)
+    if (part != 1) {
+      int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_EULER>(
+          c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, p, st);
+      if (rc) return rc;
+    }
+    if (part != 0)
+      ZB_CUDA_TRY(cudaMemcpyAsync(h, h1, 3 * C * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    return ZB_OK;
+  }
+  if (part != 1) {
+    int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP1>(
+        c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, p, st);
+    if (rc) return rc;
+  }
+  if (part == 0) return ZB_OK;
+  return launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP2>(
+      c, b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, p, st);
+}
+
+template <typename T, int ORDER, int RECON, int RIEMANN>
+static int run_generic_stage(const zb_swe2d_cfg* c, const T* Qk, const T* Q0, T* Qo,
+                             double alpha, double beta, double dt, zb_ctrl* ctrl,
+                             const T* hinv_src, const unsigned char* force_o1,
+                             unsigned char* trouble_out, cudaStream_t st) {
+  const size_t C = (size_t)c->nx * c->ny;
+  const SweParams<T> p = make_params<T>(c, alpha, beta, dt);
+  const T* b0 = Q0 ? Q0 : Qk;
+  return launch_stage<T, ORDER, RECON, RIEMANN, MODE_STAGE>(
+      c, b0, Qk + C, Qk + 2 * C, Qk + 3 * C, Q0 ? Q0 + C : nullptr,
+      Q0 ? Q0 + 2 * C : nullptr, Q0 ? Q0 + 3 * C : nullptr, Qo + C, Qo + 2 * C,
+      Qo + 3 * C, ctrl, 0, p, st, hinv_src, force_o1, trouble_out);
+}
+
+// dispatch over (order, recon, riemann)
+template <typename T, typename F>
+static int dispatch(const zb_swe2d_cfg* c, F&& f) {
+#define ZB_CASE(O, R, M)                                                       \
+  if (c->order == O && c->recon == R && c->riemann == M)                       \
+    return f(std::integral_constant<int, O>(), std::integral_constant<int, R>(), \
+             std::integral_constant<int, M>());
+  ZB_CASE(1, ZB_RECON_CONSTANT, ZB_RIEMANN_RUSANOV)
+  ZB_CASE(1, ZB_RECON_CONSTANT, ZB_RIEMANN_RUSANOV_HR)
+  ZB_CASE(1, ZB_RECON_CONSTANT, ZB_RIEMANN_HLL_HR)
+  ZB_CASE(2, ZB_RECON_CONSERVATIVE, ZB_RIEMANN_RUSANOV)
+  ZB_CASE(2, ZB_RECON_CONSERVATIVE, ZB_RIEMANN_RUSANOV_HR)
+  ZB_CASE(2, ZB_RECON_CONSERVATIVE, ZB_RIEMANN_HLL_HR)
+  ZB_CASE(2, ZB_RECON_ETA, ZB_RIEMANN_RUSANOV_HR)
+  ZB_CASE(2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR)
+#undef ZB_CASE
+  return ZB_E_UNSUPPORTED;
+}
+
+template <typename T>
+static int amax_into(const zb_swe2d_cfg* c, const T* Q, double* dst, cudaStream_t st) {
+  const size_t C = (size_t)c->nx * c->ny;
+  zero_double_kernel<<<1, 1, 0, st>>>(dst);
+  const int blocks = (int)std::min<size_t>((C + NT - 1) / NT, 148 * 16);
+  swe2d_amax_kernel<T><<<blocks, NT, 0, st>>>(Q + C, Q + 2 * C, Q + 3 * C, C, (T)c->g,
+                                              (T)c->wet_dry_eps, dst);
+  return zb_launch_check();
+}
+
+}  // namespace zb
+
+using namespace zb;
+
+extern "C" {
+
+const char* zb_version(void) { return "libzb 0.1 (sm_100a)"; }
+
+size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg) {
+  if (!valid_cfg(cfg)) return 0;
+  const size_t es = cfg->dtype == ZB_F64 ? 8 : 4;
+  return 3 * (size_t)cfg->nx * cfg->ny * es + 256;
+}
+
+int zb_swe2d_init(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl, int phase,
+                  double t0, zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !ctrl || phase < 0 || phase > 2) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  swe2d_ctrl_init_kernel<<<1, 32, 0, st>>>(ctrl, phase, t0);
+  if (cfg->dtype == ZB_F32) return amax_into<float>(cfg, (const float*)Q, &ctrl->amax[phase], st);
+  return amax_into<double>(cfg, (const double*)Q, &ctrl->amax[phase], st);
+}
+
+int zb_swe2d_dt(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl, double t,
+                zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !ctrl) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = cfg->dtype == ZB_F32
+               ? amax_into<float>(cfg, (const float*)Q, &ctrl->reserved[0], st)
+               : amax_into<double>(cfg, (const double*)Q, &ctrl->reserved[0], st);
+  if (rc) return rc;
+  const double r_in = cfg->dx * cfg->dy / (cfg->dx + cfg->dy);
+  swe2d_dt_finalize_kernel<<<1, 32, 0, st>>>(
+      ctrl, t, cfg->cfl * 2.0 * r_in,
+      (double)cfg->dim_factor * (double)(2 * cfg->degree + 1), cfg->dt_max, cfg->t_end);
+  return zb_launch_check();
+}
+
+int zb_swe2d_step_part(const zb_swe2d_cfg* cfg, void* Q, void* workspace,
+                       size_t workspace_bytes, zb_ctrl* ctrl, int phase, int part,
+                       zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !ctrl || phase < 0 || phase > 2) return ZB_E_ARG;
+  if (part < -1 || part > 1) return ZB_E_ARG;
+  if (!workspace || workspace_bytes < zb_swe2d_workspace_bytes(cfg)) return ZB_E_ARG;
+  if (cfg->recon == ZB_RECON_ETA && cfg->riemann == ZB_RIEMANN_RUSANOV) return ZB_E_UNSUPPORTED;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cfg->dtype == ZB_F32) {
+    return dispatch<float>(cfg, [&](auto O, auto R, auto M) {
+      return run_step<float, decltype(O)::value, decltype(R)::value, decltype(M)::value>(
+          cfg, (float*)Q, (float*)workspace, ctrl, phase, part, st);
+    });
+  }
+  return dispatch<double>(cfg, [&](auto O, auto R, auto M) {
+    return run_step<double, decltype(O)::value, decltype(R)::value, decltype(M)::value>(
+        cfg, (double*)Q, (double*)workspace, ctrl, phase, part, st);
+  });
+}
+
+int zb_swe2d_step(const zb_swe2d_cfg* cfg, void* Q, void* workspace, size_t workspace_bytes,
+                  zb_ctrl* ctrl, int phase, zb_stream_t stream) {
+  return zb_swe2d_step_part(cfg, Q, workspace, workspace_bytes, ctrl, phase, -1, stream);
+}
+
+int zb_swe2d_stage(const zb_swe2d_cfg* cfg, const void* Qk, const void* Q0, void* Q_out,
+                   double alpha, double beta, double dt, const void* hinv_src,
+                   const uint8_t* force_o1, uint8_t* trouble_out, zb_ctrl* ctrl,
+                   zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Qk || !Q_out || !ctrl) return ZB_E_ARG;
+  if (Q_out == Qk) return ZB_E_ARG;
+  if (!(dt >= 0.0) && !(dt < 0.0)) return ZB_E_ARG;
+  if (alpha != 0.0 && !Q0) return ZB_E_ARG;
+  if (cfg->recon == ZB_RECON_ETA && cfg->riemann == ZB_RIEMANN_RUSANOV) return ZB_E_UNSUPPORTED;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cfg->dtype == ZB_F32) {
+    return dispatch<float>(cfg, [&](auto O, auto R, auto M) {
+      return run_generic_stage<float, decltype(O)::value, decltype(R)::value, decltype(M)::value>(
+          cfg, (const float*)Qk, (const float*)Q0, (float*)Q_out, alpha, beta, dt, ctrl,
+          (const float*)hinv_src, force_o1, trouble_out, st);
+    });
+  }
+  return dispatch<double>(cfg, [&](auto O, auto R, auto M) {
+    return run_generic_stage<double, decltype(O)::value, decltype(R)::value, decltype(M)::value>(
+        cfg, (const double*)Qk, (const double*)Q0, (double*)Q_out, alpha, beta, dt, ctrl,
+        (const double*)hinv_src, force_o1, trouble_out, st);
+  });
+}
+
+int zb_swe2d_source(const zb_swe2d_cfg* cfg, void* Q, const void* hinv0, double dt,
+                    zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !hinv0 || !(dt >= 0.0)) return ZB_E_ARG;
+  if (cfg->manning_n == 0.0) return ZB_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t C = (size_t)cfg->nx * cfg->ny;
+  const int blocks = (int)std::min<size_t>((C + NT - 1) / NT, 148 * 16);
+  if (cfg->dtype == ZB_F32)
+    swe2d_source_kernel<float><<<blocks, NT, 0, st>>>(
+        (float*)Q + 2 * C, (float*)Q + 3 * C, (const float*)hinv0, C, (float)cfg->g,
+        (float)cfg->manning_n, (float)dt, cfg->implicit_source);
+  else
+    swe2d_source_kernel<double><<<blocks, NT, 0, st>>>(
+        (double*)Q + 2 * C, (double*)Q + 3 * C, (const double*)hinv0, C, cfg->g,
+        cfg->manning_n, dt, cfg->implicit_source);
+  return zb_launch_check();
+}
+
+size_t zb_swe2d_mass_partials(const zb_swe2d_cfg* cfg) {
+  (void)cfg;
+  return MASS_BLOCKS;
+}
+
+int zb_swe2d_mass(const zb_swe2d_cfg* cfg, const void* Q, double* partial, zb_ctrl* ctrl,
+                  zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !partial || !ctrl) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t C = (size_t)cfg->nx * cfg->ny;
+  const double vol = cfg->dx * cfg->dy;
+  if (cfg->dtype == ZB_F32)
+    mass_partial_kernel<float><<<MASS_BLOCKS, NT, 0, st>>>((const float*)Q + C, C, vol, partial);
+  else
+    mass_partial_kernel<double><<<MASS_BLOCKS, NT, 0, st>>>((const double*)Q + C, C, vol, partial);
+  mass_final_kernel<<<1, NT, 0, st>>>(partial, MASS_BLOCKS, ctrl);
+  return zb_launch_check();
+}
+
+int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux, zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !Qaux) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t C = (size_t)cfg->nx * cfg->ny;
+  const int blocks = (int)std::min<size_t>((C + NT - 1) / NT, 148 * 16);
+  if (cfg->dtype == ZB_F32)
+    swe2d_aux_kernel<float><<<blocks, NT, 0, st>>>((const float*)Q, (float*)Qaux, cfg->nx,
+                                                   cfg->ny, (float)cfg->wet_dry_eps,
+                                                   make_lsq<float>(cfg->dx, cfg->dy));
+  else
+    swe2d_aux_kernel<double><<<blocks, NT, 0, st>>>((const double*)Q, (double*)Qaux, cfg->nx,
+                                                    cfg->ny, cfg->wet_dry_eps,
+                                                    make_lsq<double>(cfg->dx, cfg->dy));
+  return zb_launch_check();
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+"""ctypes binding of libzb (the C ABI declared in include/zb.h).
+
+The host package never computes on the CPU: every public solver call goes
+through this library on a CUDA device, and importing a solver without the
+built library or without a GPU raises instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import pathlib
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent.parent / "lib" / "libzb.so"
+
+ZB_F32, ZB_F64 = 0, 1
+ZB_OK, ZB_E_ARG, ZB_E_CUDA, ZB_E_UNSUPPORTED = 0, -1, -2, -3
+ZB_ST_DT_INVALID, ZB_ST_TROUBLED, ZB_ST_NOT_CONVERGED = 1, 2, 4
+BC = {"extrapolation": 0, "wall": 1, "periodic": 2}
+RECON = {"constant": 0, "conservative": 1, "eta": 2}
+RIEMANN = {"rusanov": 0, "rusanov_hr": 1, "hll_hr": 2}
+LIMITER = {"minmod": 0, "barth_jespersen": 1, "venkatakrishnan": 2, "none": 3}
+
+
+class ZbCtrl(C.Structure):
+    _fields_ = [("amax", C.c_double * 3), ("t", C.c_double * 3),
+                ("dt", C.c_double), ("mass", C.c_double),
+                ("status", C.c_uint32), ("steps", C.c_uint32),
+                ("troubled", C.c_uint32), ("pad", C.c_uint32),
+                ("reserved", C.c_double * 6)]
+
+
+CTRL_BYTES = C.sizeof(ZbCtrl)
+
+
+class ZbSwe2dCfg(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32),
+                ("x0", C.c_double), ("y0", C.c_double),
+                ("dx", C.c_double), ("dy", C.c_double),
+                ("order", C.c_int32), ("recon", C.c_int32),
+                ("riemann", C.c_int32), ("limiter", C.c_int32),
+                ("bc", C.c_int32 * 4),
+                ("g", C.c_double), ("wet_dry_eps", C.c_double),
+                ("eps_wet", C.c_double), ("manning_n", C.c_double),
+                ("implicit_source", C.c_int32), ("dim_factor", C.c_int32),
+                ("cfl", C.c_double), ("dt_max", C.c_double),
+                ("t_end", C.c_double), ("degree", C.c_int32),
+                ("dtype", C.c_int32)]
+
+
+# (name, restype, argtypes) of every symbol include/zb.h declares
+_P = C.c_void_p
+_CFG = C.POINTER(ZbSwe2dCfg)
+SIGNATURES = [
+    ("zb_version", C.c_char_p, []),
+    ("zb_swe2d_workspace_bytes", C.c_size_t, [_CFG]),
+    ("zb_swe2d_init", C.c_int, [_CFG, _P, _P, C.c_int, C.c_double, _P]),
+    ("zb_swe2d_dt", C.c_int, [_CFG, _P, _P, C.c_double, _P]),
+    ("zb_swe2d_step", C.c_int, [_CFG, _P, _P, C.c_size_t, _P, C.c_int, _P]),
+    ("zb_swe2d_step_part", C.c_int, [_CFG, _P, _P, C.c_size_t, _P, C.c_int, C.c_int, _P]),
+    ("zb_swe2d_stage", C.c_int, [_CFG, _P, _P, _P, C.c_double, C.c_double,
+                                 C.c_double, _P, _P, _P, _P, _P]),
+    ("zb_swe2d_source", C.c_int, [_CFG, _P, _P, C.c_double, _P]),
+    ("zb_swe2d_mass_partials", C.c_size_t, [_CFG]),
+    ("zb_swe2d_mass", C.c_int, [_CFG, _P, _P, _P, _P]),
+    ("zb_swe2d_aux", C.c_int, [_CFG, _P, _P, _P]),
+]
+
+_lib = None
+
+
+def load():
+    """Load libzb.so (build it with ``python zoomy-jax_b200/build.py``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"libzb.so not found at {LIB_PATH}; build it with "
+            f"`python zoomy-jax_b200/build.py` (nvcc, sm_100a). There is no "
+            f"CPU fallback.")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class ZbError(RuntimeError):
+    pass
+
+
+def check(rc, what):
+    if rc != ZB_OK:
+        names = {ZB_E_ARG: "invalid argument", ZB_E_CUDA: "CUDA error",
+                 ZB_E_UNSUPPORTED: "unsupported configuration"}
+        raise ZbError(f"{what} failed: {names.get(rc, rc)}")
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "zoomy_b200 runs on a CUDA device (sm_100a) only; no GPU is "
+            "visible and there is no CPU fallback.")
+    load()
+
+
+def ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def inf_or(x):
+    return math.inf if x is None else float(x)

@@ -1,0 +1,298 @@
+"""``HyperbolicSolver`` -- the reference's explicit FV solver API on libzb.
+
+Same methods and knobs as ``zoomy_jax.fvm.solver_jax.HyperbolicSolver``
+(``setup_simulation`` :901-988, ``compute_timestep`` :1222-1236, ``step``
+:1095-1131, ``post_step`` :1133-1172, ``run_simulation`` :1238-1352,
+``solve`` :1356-1368).  ``Q`` and ``Qaux`` are CUDA tensors in the reference
+layout ``(n_state, n_cells)``; every operator is a libzb call on the current
+torch stream.  The time loop of ``run_simulation`` is device-resident: dt,
+time and the CFL wave-speed maximum live in a device control block and the
+host only polls it between batches of steps.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from .. import _lib as L
+from ..mesh import CartesianMesh
+from ..model import NumericalSystemModel
+from ..timestepping import Adaptive, Constant, adaptive
+
+
+class EllipticSolveError(RuntimeError):
+    pass
+
+
+class HyperbolicSolver:
+    """Explicit SSP-RK2 / Euler finite-volume solver for 2-D shallow water.
+
+    Parameters follow the reference (``solver_jax.py:183-226``):
+    ``time_end``, ``compute_dt``, ``free_surface_h_index``,
+    ``free_surface_b_index``, ``reconstruction_variables`` (``conservative`` |
+    ``eta``), ``positivity_method``, ``front_theta_tol``, ``mood``; plus
+    ``dtype`` (``float64`` default, as the reference enables x64, or
+    ``float32``) and ``eps_wet`` (the emitted dry-cell demotion threshold of
+    the eta reconstruction, ``None`` = off).
+    """
+
+    def __init__(self, time_end=1.0, compute_dt=None, free_surface_h_index=None,
+                 free_surface_b_index=0, free_surface_momentum_indices=None,
+                 reconstruction_variables="conservative", positivity_method="",
+                 front_theta_tol=None, mood=False, dtype="float64", eps_wet=None,
+                 implicit_source=False, device=None):
+        self.time_end = float(time_end)
+        self.compute_dt = compute_dt if compute_dt is not None else adaptive(0.45, 2)
+        self.free_surface_h_index = free_surface_h_index
+        self.free_surface_b_index = free_surface_b_index
+        self.free_surface_momentum_indices = free_surface_momentum_indices
+        if reconstruction_variables not in ("conservative", "eta", "xz"):
+            raise ValueError(reconstruction_variables)
+        self.reconstruction_variables = reconstruction_variables
+        self.positivity_method = positivity_method
+        self.front_theta_tol = front_theta_tol
+        self.mood = bool(mood)
+        if dtype not in ("float32", "float64"):
+            raise ValueError("dtype must be float32 or float64")
+        self.dtype = dtype
+        self.eps_wet = eps_wet
+        self.implicit_source = bool(implicit_source)
+        self.device = device
+
+    # ── configuration ─────────────────────────────────────────────────────
+    def _torch_dtype(self):
+        import torch
+        return torch.float64 if self.dtype == "float64" else torch.float32
+
+    def _make_cfg(self, mesh: CartesianMesh, nsm: NumericalSystemModel):
+        m = nsm.model
+        order = nsm.reconstruction.order
+        recon = "constant" if order == 1 else (
+            "eta" if self.reconstruction_variables == "eta" else "conservative")
+        if order >= 2 and self.reconstruction_variables == "eta" \
+                and self.free_surface_h_index is None:
+            raise AssertionError("reconstruction_variables='eta' requires "
+                                 "free_surface_h_index to be set")
+        if order >= 2 and self.reconstruction_variables == "xz":
+            raise NotImplementedError("reconstruction_variables='xz' (Xing-Zhang "
+                                      "scaling) is not on the GPU path")
+        if self.positivity_method or self.front_theta_tol is not None:
+            raise NotImplementedError("positivity_method / front_theta_tol are "
+                                      "not on the GPU path")
+        if self.mood and recon != "eta":
+            raise NotImplementedError(
+                "mood=True needs a reconstruction that supports per-cell "
+                "1st-order demotion (reconstruction_variables='eta')")
+        if recon == "eta" and nsm.riemann == "rusanov":
+            raise NotImplementedError("the eta reconstruction needs a "
+                                      "hydrostatic-reconstruction flux "
+                                      "(rusanov_hr or hll_hr)")
+        cd = self.compute_dt
+        if isinstance(cd, Adaptive):
+            cd = cd.with_dt_max(nsm.dt_max)
+        cfg = L.ZbSwe2dCfg()
+        cfg.nx, cfg.ny = mesh.nx, mesh.ny
+        cfg.x0, cfg.y0, cfg.dx, cfg.dy = mesh.x0, mesh.y0, mesh.dx, mesh.dy
+        cfg.order = order
+        cfg.recon = L.RECON[recon]
+        cfg.riemann = L.RIEMANN[nsm.riemann]
+        cfg.limiter = L.LIMITER[nsm.reconstruction.limiter]
+        for i, k in enumerate(m.bc_kinds()):
+            cfg.bc[i] = L.BC[k]
+        cfg.g = m.g
+        cfg.wet_dry_eps = m.wet_dry_eps
+        cfg.eps_wet = -1.0 if self.eps_wet is None else float(self.eps_wet)
+        cfg.manning_n = m.manning_n
+        cfg.implicit_source = int(self.implicit_source)
+        if isinstance(cd, Adaptive):
+            cfg.dim_factor = cd.dimension
+            cfg.cfl = cd.CFL
+            cfg.dt_max = cd.dt_max
+            cfg.degree = cd.degree
+        else:
+            cfg.dim_factor, cfg.cfl, cfg.dt_max, cfg.degree = 2, 1.0, math.inf, 0
+        cfg.t_end = self.time_end
+        cfg.dtype = L.ZB_F64 if self.dtype == "float64" else L.ZB_F32
+        return cfg
+
+    # ── setup ─────────────────────────────────────────────────────────────
+    def setup_simulation(self, mesh, model):
+        """Build the device state and operators (``solver_jax.py:901-988``).
+        ``model`` is a :class:`NumericalSystemModel`.  Returns ``(Q, Qaux)``
+        on the device."""
+        import torch
+        L.require_cuda()
+        self.lib = L.load()
+        nsm = model
+        self.nsm = nsm
+        self.mesh = mesh
+        self.cfg = self._make_cfg(mesh, nsm)
+        dev = torch.device(self.device or "cuda")
+        td = self._torch_dtype()
+        Q = torch.as_tensor(nsm.model.initial_state(mesh), dtype=td, device=dev).contiguous()
+        self._ws_bytes = int(self.lib.zb_swe2d_workspace_bytes(C.byref(self.cfg)))
+        self._ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=dev)
+        self._ctrl = torch.zeros(L.CTRL_BYTES, dtype=torch.uint8, device=dev)
+        self._mass_part = torch.zeros(
+            int(self.lib.zb_swe2d_mass_partials(C.byref(self.cfg))),
+            dtype=torch.float64, device=dev)
+        Qaux = self.update_qaux(Q)
+        return Q, Qaux
+
+    # ── operators ─────────────────────────────────────────────────────────
+    def _s(self):
+        return L.stream_ptr()
+
+    def update_qaux(self, Q):
+        """KP ``hinv`` plus the LSQ derivative rows (``solver_jax.py:284-369``)."""
+        import torch
+        Qaux = torch.empty((7, Q.shape[1]), dtype=Q.dtype, device=Q.device)
+        L.check(self.lib.zb_swe2d_aux(C.byref(self.cfg), L.ptr(Q), L.ptr(Qaux),
+                                      self._s()), "zb_swe2d_aux")
+        return Qaux
+
+    def read_ctrl(self):
+        """Copy the device control block to the host (synchronises)."""
+        raw = self._ctrl.cpu().numpy().tobytes()
+        return L.ZbCtrl.from_buffer_copy(raw)
+
+    def compute_timestep(self, Q, Qaux=None, parameters=None, time=0.0):
+        """dt of the state (``solver_jax.py:1222-1236``): the adaptive CFL law
+        over faces, capped by ``dt_max`` and by ``time_end - time``."""
+        if isinstance(self.compute_dt, Constant):
+            return min(self.compute_dt.dt, self.time_end - time)
+        L.check(self.lib.zb_swe2d_dt(C.byref(self.cfg), L.ptr(Q), L.ptr(self._ctrl),
+                                     float(time), self._s()), "zb_swe2d_dt")
+        return float(self.read_ctrl().dt)
+
+    def _advance(self, Q, dt, force_o1=None, trouble=None):
+        """Hyperbolic sub-step with a host dt: SSP-RK2 in Shu-Osher form
+        (alpha = 0.5 is exact: scaling by 1/2 commutes with rounding, so it is
+        bit-identical to 0.5 (Q0 + Q2)) or Euler.  Optional per-cell MOOD mask
+        and troubled-mask output (C bytes)."""
+        import torch
+        cfg = C.byref(self.cfg)
+        fo = L.ptr(force_o1) if force_o1 is not None else None
+        tr = L.ptr(trouble) if trouble is not None else None
+        Qn = Q.clone()
+        if self.cfg.order >= 2:
+            Q1 = torch.empty_like(Q)
+            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Q), None, L.ptr(Q1), 0.0, 1.0, dt,
+                                            None, fo, None, L.ptr(self._ctrl), self._s()),
+                    "stage 1")
+            Q1[0].copy_(Q[0])
+            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Q1), L.ptr(Q), L.ptr(Qn), 0.5, 1.0,
+                                            dt, None, fo, tr, L.ptr(self._ctrl),
+                                            self._s()), "stage 2")
+        else:
+            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Q), None, L.ptr(Qn), 0.0, 1.0, dt,
+                                            None, fo, tr, L.ptr(self._ctrl), self._s()),
+                    "stage")
+        return Qn
+
+    def step(self, dt, time, Q, Qaux, parameters=None):
+        """One explicit step with a host dt (``solver_jax.py:1095-1131``):
+        SSP-RK2 (order 2) or Euler (order 1); with ``mood`` the candidate's
+        troubled cells (h < 0 or non-finite) are demoted to first order and
+        the step is re-run (``solver_jax.py:1055-1071``); then the source as
+        RK1 with the step's input aux.  Returns a new state tensor."""
+        import torch
+        dt = float(dt)
+        if self.mood:
+            mask = torch.zeros(Q.shape[1], dtype=torch.uint8, device=Q.device)
+            Qn = self._advance(Q, dt, trouble=mask)
+            if bool(mask.any()):
+                Qn = self._advance(Q, dt, force_o1=mask)
+        else:
+            Qn = self._advance(Q, dt)
+        if self.cfg.manning_n != 0.0:
+            hinv0 = Qaux[6].contiguous()
+            L.check(self.lib.zb_swe2d_source(C.byref(self.cfg), L.ptr(Qn), L.ptr(hinv0),
+                                             dt, self._s()), "source")
+        return Qn
+
+    def post_step(self, time, dt, Q, Qold, Qaux, parameters=None):
+        """``update_q`` (identity: the SWE declares no ``update_variables``)
+        and ``update_qaux`` (``solver_jax.py:1133-1172``)."""
+        return Q, self.update_qaux(Q)
+
+    def mass(self, Q):
+        """``sum h |cell|`` in float64 on the device."""
+        L.check(self.lib.zb_swe2d_mass(C.byref(self.cfg), L.ptr(Q), L.ptr(self._mass_part),
+                                       L.ptr(self._ctrl), self._s()), "zb_swe2d_mass")
+        return float(self.read_ctrl().mass)
+
+    # ── device-resident march ─────────────────────────────────────────────
+    def init_march(self, Q, t0=0.0):
+        """Reset the control block and seed the wave-speed maximum."""
+        L.check(self.lib.zb_swe2d_init(C.byref(self.cfg), L.ptr(Q), L.ptr(self._ctrl),
+                                       0, float(t0), self._s()), "zb_swe2d_init")
+        self._n = 0
+
+    def launch_steps(self, Q, n):
+        """Queue ``n`` fused steps (no host sync).  The step index modulo 3
+        selects the control-block slots."""
+        cfg = C.byref(self.cfg)
+        ws, wsb = L.ptr(self._ws), C.c_size_t(self._ws_bytes)
+        ctrl, st = L.ptr(self._ctrl), self._s()
+        qp = L.ptr(Q)
+        for _ in range(n):
+            rc = self.lib.zb_swe2d_step(cfg, qp, ws, wsb, ctrl, self._n % 3, st)
+            if rc != L.ZB_OK:
+                L.check(rc, "zb_swe2d_step")
+            self._n += 1
+
+    def _raise_dt(self, Q, t):
+        from ..diagnostics import worst_face
+        raise FloatingPointError(
+            f"dt became non-finite or non-positive at t = {t} (iteration "
+            f"{self._n}) -- FATAL. {worst_face(self, Q)}")
+
+    def run_simulation(self, Q, Qaux, write_output=False, parameters=None,
+                       max_steps=10 ** 7):
+        """March to ``time_end`` (``solver_jax.py:1238-1352``).
+
+        Without MOOD the loop is device-resident: fused steps are queued in
+        growing batches and the host only polls the control block; after
+        ``time_end`` a queued step takes dt = 0 and leaves the state unchanged.
+        With MOOD the host drives ``compute_timestep`` / ``step`` /
+        ``post_step`` per step (the redo decision needs the troubled mask).
+        The state is returned with its aux."""
+        if self.mood:
+            t, n = 0.0, 0
+            while t < self.time_end:
+                dt = self.compute_timestep(Q, Qaux, time=t)
+                if not (math.isfinite(dt) and dt > 0.0):
+                    self._n = n
+                    self._raise_dt(Q, t)
+                Qn = self.step(dt, t, Q, Qaux)
+                Q, Qaux = self.post_step(t + dt, dt, Qn, Q, Qaux)
+                t += dt
+                n += 1
+                if n >= max_steps:
+                    raise FloatingPointError(f"march exceeded max_steps = {max_steps}")
+            self.time, self.steps_taken = t, n
+            return Q, Qaux
+        self.init_march(Q, 0.0)
+        batch = 1
+        while True:
+            self.launch_steps(Q, batch)
+            c = self.read_ctrl()
+            t = c.t[self._n % 3]
+            if c.status & L.ZB_ST_DT_INVALID:
+                self._raise_dt(Q, t)
+            if t >= self.time_end:
+                break
+            if self._n >= max_steps:
+                raise FloatingPointError(f"march exceeded max_steps = {max_steps}")
+            batch = min(batch * 2, 64)
+        self.time = t
+        self.steps_taken = int(c.steps)
+        return Q, self.update_qaux(Q)
+
+    def solve(self, mesh, model, write_output=False):
+        """``setup_simulation`` then ``run_simulation`` (``solver_jax.py:1356-1368``)."""
+        Q, Qaux = self.setup_simulation(mesh, model)
+        return self.run_simulation(Q, Qaux, write_output=write_output)

@@ -1,0 +1,51 @@
+"""Seeded synthetic workloads of the benchmark configurations (host NumPy).
+
+The reference measures on test cases rather than datasets; these seeded
+generators stand in for them with the configured shapes and distributions.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def bumps(xc, seed=0, n=16, amp=(0.0, 0.8), width=(0.02, 0.1), domain=(0, 1, 0, 1)):
+    """Sum of ``n`` seeded Gaussian bumps with amplitude U[amp], width
+    U[width] and centre U[domain]; ``xc`` is ``(2, C)``."""
+    rng = np.random.default_rng(seed)
+    b = np.zeros(xc.shape[1])
+    x0, x1, y0, y1 = domain
+    for _ in range(n):
+        A = rng.uniform(*amp)
+        w = rng.uniform(*width)
+        cx = rng.uniform(x0, x1)
+        cy = rng.uniform(y0, y1)
+        b += A * np.exp(-((xc[0] - cx) ** 2 + (xc[1] - cy) ** 2) / (2 * w * w))
+    return b
+
+
+def circular_dam_state(xc, seed=0, r0=0.2, h_in=2.0, h_out=1.0, noise=1e-3,
+                       center=(0.5, 0.5), bathymetry=True):
+    """Circular dam break over the seeded bumps: level ``h_in`` inside radius
+    ``r0`` else ``h_out`` plus ``noise * N(0, 1)``; ``h = max(level - b, 0)``
+    (dry where a bump tops the level); ``u = v = 0``.  Returns ``(4, C)``
+    float64 ``[b, h, q_x, q_y]``."""
+    b = bumps(xc, seed) if bathymetry else np.zeros(xc.shape[1])
+    rng = np.random.default_rng(seed + 1)
+    r = np.sqrt((xc[0] - center[0]) ** 2 + (xc[1] - center[1]) ** 2)
+    level = np.where(r < r0, h_in, h_out) + noise * rng.standard_normal(xc.shape[1])
+    h = np.maximum(level - b, 0.0)
+    return np.stack([b, h, np.zeros_like(b), np.zeros_like(b)])
+
+
+def cartesian_centers(n, domain=(0.0, 1.0, 0.0, 1.0)):
+    """``(2, n*n)`` cell centres of the ``n x n`` grid in cell order."""
+    x0, x1, y0, y1 = domain
+    dx = (x1 - x0) / n
+    dy = (y1 - y0) / n
+    i, j = np.divmod(np.arange(n * n), n)
+    return np.stack([x0 + (i + 0.5) * dx, y0 + (j + 0.5) * dy])
+
+
+def dam_break_2048(n=2048, seed=0):
+    """The 2048^2 configuration's initial state on the unit square."""
+    return circular_dam_state(cartesian_centers(n), seed=seed)
