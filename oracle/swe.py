@@ -71,11 +71,21 @@ def velocities(Q, hinv):
 # ── boundary conditions ─────────────────────────────────────────────────────
 
 def bc_kinds(mesh, scheme):
+    """Per-boundary-face BC kind (0 extrapolation, 1 wall, 2 periodic).  A
+    periodic side is paired with its opposite side (``resolve_periodic_bcs``,
+    ``zoomy_jax/fvm/solver_jax.py:931-941``) the first time it is seen."""
     kinds = []
     for t in mesh.tag_names:
         kinds.append(scheme.bc.get(t, "extrapolation"))
-    return np.array([{"extrapolation": 0, "wall": 1, "periodic": 2}[k]
-                     for k in kinds])[mesh.bf_tag]
+    out = np.array([{"extrapolation": 0, "wall": 1, "periodic": 2}[k]
+                    for k in kinds])[mesh.bf_tag]
+    per = out == 2
+    if per.any() and (mesh.bf_partner is None or (mesh.bf_partner[per] < 0).any()):
+        opposite = {"left": "right", "right": "left", "bottom": "top", "top": "bottom"}
+        pairs = [(t, opposite[t]) for t, k in zip(mesh.tag_names, kinds)
+                 if k == "periodic"]
+        mesh.set_periodic(pairs)
+    return out
 
 
 def apply_bc(mesh, kind, q, normals):
@@ -184,7 +194,7 @@ def limiter_phi(mesh, limiter, u, grad, umin, umax):
         return np.ones(C)
     it, rA, rB, rbnd = _face_offsets(mesh)
     fc = mesh.face_cells
-    ev2 = mesh.cell_volumes ** (2.0 / mesh.dim)       # (vol^{1/d})^2
+    ev2 = (mesh.cell_volumes ** (1.0 / mesh.dim)) ** 2   # reconstruction_jax.py:396-399
     phi = np.ones(C)
     for cells, r in ((fc[0, it], rA), (fc[1, it], rB), (mesh.bf_cell, rbnd)):
         delta = (grad[:, cells] * r).sum(axis=0)
