@@ -23,7 +23,11 @@ LIB = HERE / "lib" / "libzb.so"
 INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -prec-div/-prec-sqrt/-ftz affect single precision only: the float kernels
+# use fast division and square root (stated tolerance), the double kernels stay
+# IEEE (float64 parity with the oracle to 1e-12)
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+         "-prec-div=false", "-prec-sqrt=false", "-ftz=true",
          "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]
 
 

@@ -25,16 +25,29 @@ __device__ __forceinline__ float nmax(float a, float b) { return (a != a || a > 
 __device__ __forceinline__ double nmax(double a, double b) { return (a != a || a > b) ? a : b; }
 __device__ __forceinline__ float nmin(float a, float b) { return (a != a || a < b) ? a : b; }
 __device__ __forceinline__ double nmin(double a, double b) { return (a != a || a < b) ? a : b; }
-template <typename T> __device__ __forceinline__ T clip01(T x) {
-  return x < T(0) ? T(0) : (x > T(1) ? T(1) : x);
-}
+// Hot-path min / max: one FMNMX / DMNMX instruction.  NaN-dropping, unlike
+// NumPy's np.maximum; a non-finite state is still detected through the
+// owning cell's own update and the NaN-propagating dt reduction (nmax).
+__device__ __forceinline__ float fmx(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmx(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float fmn(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double fmn(double a, double b) { return fmin(a, b); }
+
+__device__ __forceinline__ float clip01(float x) { return __saturatef(x); }
+__device__ __forceinline__ double clip01(double x) { return fmin(fmax(x, 0.0), 1.0); }
 
 // KP-desingularised inverse depth: sqrt(2) h / sqrt(h^4 + max(h, eps)^4)
-// (zoomy_jax/fvm/solver_jax.py:291-292).
-template <typename T> __device__ __forceinline__ T kp_hinv(T h, T eps) {
-  T m = h > eps ? h : eps;
-  T h2 = h * h, m2 = m * m;
-  return (T(1.4142135623730951) * h) / sqrt(h2 * h2 + m2 * m2);
+// (zoomy_jax/fvm/solver_jax.py:291-292).  float: one reciprocal square root;
+// double: IEEE division and square root (float64 parity with the oracle).
+__device__ __forceinline__ float kp_hinv(float h, float eps) {
+  const float m = fmaxf(h, eps);
+  const float h2 = h * h, m2 = m * m;
+  return (1.41421356237309515f * h) * rsqrtf(h2 * h2 + m2 * m2);
+}
+__device__ __forceinline__ double kp_hinv(double h, double eps) {
+  const double m = h > eps ? h : eps;
+  const double h2 = h * h, m2 = m * m;
+  return (1.4142135623730951 * h) / sqrt(h2 * h2 + m2 * m2);
 }
 
 // Non-negative doubles order like their bit patterns: atomicMax on the bits.

@@ -78,24 +78,20 @@ __device__ __forceinline__ double dt_from_amax(double amax, double t,
 }
 
 // ── limiter candidates (reconstruction_jax.py:603-691) ──────────────────────
-// Minmod / Barth-Jespersen on a Cartesian cell: the four faces carry the
-// increments +a, -a (x) and +c, -c (y); with dpos = umax - u >= 0 and
-// dneg = umin - u <= 0 the two x-faces give clip(dpos/a) and clip(dneg/-a)
-// (a > eps), whose minimum is clip(min(dpos, -dneg)/|a|): IEEE division is
-// monotone, so this is the per-face min exactly.
+// Minmod / Barth-Jespersen on a Cartesian cell.  The four faces carry the
+// increments +a, -a (x) and +c, -c (y).  With dpos = umax - u >= 0 and
+// dneg = umin - u <= 0 a face with increment d > eps gives clip(dpos / d) and
+// one with d < -eps gives clip(dneg / d) = clip(-dneg / |d|).  IEEE division
+// is monotone in both operands, so the minimum over the four faces is exactly
+// clip(min(dpos, -dneg) / max(|a|, |c|)) whenever max(|a|, |c|) > eps (a pair
+// with |d| <= eps contributes 1 and never the minimum), and 1 otherwise: one
+// division per variable instead of four, bit-identical to the per-face form.
 template <typename T>
-__device__ __forceinline__ T phi_pair_clipmin(T a, T dpos, T dneg) {
-  const T eps = T(1e-30);
-  if (a > eps) {
-    T r1 = clip01(dpos / a);
-    T r2 = clip01(dneg / (-a));
-    return zmin(r1, r2);
-  } else if (a < -eps) {
-    T r1 = clip01(dneg / a);
-    T r2 = clip01(dpos / (-a));
-    return zmin(r1, r2);
-  }
-  return T(1);
+__device__ __forceinline__ T phi_clipmin(T a, T c, T dpos, T dneg) {
+  const T m = fmx(fabs(a), fabs(c));
+  const T dm = fmn(dpos, -dneg);
+  const T r = clip01(dm / m);
+  return m > T(1e-30) ? r : T(1);
 }
 
 template <typename T>
@@ -125,8 +121,7 @@ __device__ __forceinline__ T limiter_phi(int lim, T gx, T gy, T hdx, T hdy,
     p = zmin(p, vk_cand(-c, dpos, dneg, ev2));
     return clip01(p);
   }
-  return clip01(zmin(phi_pair_clipmin(a, dpos, dneg),
-                     phi_pair_clipmin(c, dpos, dneg)));
+  return phi_clipmin(a, c, dpos, dneg);
 }
 
 // ── face state and Riemann solvers ──────────────────────────────────────────
@@ -149,7 +144,7 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R,
   T unR = R.ux * nx + R.uy * ny;
   if (RIEMANN == ZB_RIEMANN_RUSANOV) {
     T cL = sqrt(g * L.h), cR = sqrt(g * R.h);
-    T s = nmax(fabs(unL) + cL, fabs(unR) + cR);
+    T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
     T qnL = L.qx * nx + L.qy * ny;
     T qnR = R.qx * nx + R.qy * ny;
     T pL = half * g * (L.h * L.h), pR = half * g * (R.h * R.h);
@@ -163,9 +158,9 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R,
     Dp = T(0);
     return;
   }
-  T bs = nmax(L.b, R.b);
-  T hLs = nmax(T(0), L.h + L.b - bs);
-  T hRs = nmax(T(0), R.h + R.b - bs);
+  T bs = fmx(L.b, R.b);
+  T hLs = fmx(T(0), L.h + L.b - bs);
+  T hRs = fmx(T(0), R.h + R.b - bs);
   T cL = sqrt(g * hLs), cR = sqrt(g * hRs);
   T qLx = hLs * L.ux, qLy = hLs * L.uy;
   T qRx = hRs * R.ux, qRy = hRs * R.uy;
@@ -174,15 +169,15 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R,
   T FLx = qLx * unL + pL * nx, FLy = qLy * unL + pL * ny;
   T FRx = qRx * unR + pR * nx, FRy = qRy * unR + pR * ny;
   if (RIEMANN == ZB_RIEMANN_RUSANOV_HR) {
-    T s = nmax(fabs(unL) + cL, fabs(unR) + cR);
+    T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
     T hs = half * s;
     Fh = half * (FLh + FRh) - hs * (hRs - hLs);
     Fqx = half * (FLx + FRx) - hs * (qRx - qLx);
     Fqy = half * (FLy + FRy) - hs * (qRy - qLy);
   } else {
-    T SL = nmin(unL - cL, unR - cR);
-    T SR = nmax(unL + cL, unR + cR);
-    T sl = nmin(SL, T(0)), sr = nmax(SR, T(0));
+    T SL = fmn(unL - cL, unR - cR);
+    T SR = fmx(unL + cL, unR + cR);
+    T sl = fmn(SL, T(0)), sr = fmx(SR, T(0));
     T den = sr - sl;
     T inv = den > T(0) ? T(1) / den : T(0);
     T slsr = sl * sr;
@@ -316,10 +311,10 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
                wx[5] * d5 + wx[6] * d6 + wx[7] * d7;
           gy = wy[0] * d0 + wy[1] * d1 + wy[2] * d2 + wy[3] * d3 + wy[4] * d4 +
                wy[5] * d5 + wy[6] * d6 + wy[7] * d7;
-          umax = nmax(umax, W[e2 + S::R2Y]); umin = nmin(umin, W[e2 + S::R2Y]);
-          umax = nmax(umax, W[e2 - S::R2Y]); umin = nmin(umin, W[e2 - S::R2Y]);
-          umax = nmax(umax, W[e2 + 1]);      umin = nmin(umin, W[e2 + 1]);
-          umax = nmax(umax, W[e2 - 1]);      umin = nmin(umin, W[e2 - 1]);
+          umax = fmx(umax, W[e2 + S::R2Y]); umin = fmn(umin, W[e2 + S::R2Y]);
+          umax = fmx(umax, W[e2 - S::R2Y]); umin = fmn(umin, W[e2 - S::R2Y]);
+          umax = fmx(umax, W[e2 + 1]);      umin = fmn(umin, W[e2 + 1]);
+          umax = fmx(umax, W[e2 - 1]);      umin = fmn(umin, W[e2 - 1]);
         } else {
           // ghost values of this cell's boundary faces (BC at the cell state;
           // a wall negates the normal momentum / velocity; periodic = image)
@@ -352,12 +347,12 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
           if (bxl || bxh) { const T d = gxv - u; gx += wx[8] * d; gy += wy[8] * d; }
           if (byl || byh) { const T d = gyv - u; gx += wx[9] * d; gy += wy[9] * d; }
           // bounds: inside face neighbours + ghost 2 u_bf - u
-          if (!bxh) { umax = nmax(umax, W[e2 + S::R2Y]); umin = nmin(umin, W[e2 + S::R2Y]); }
-          if (!bxl) { umax = nmax(umax, W[e2 - S::R2Y]); umin = nmin(umin, W[e2 - S::R2Y]); }
-          if (!byh) { umax = nmax(umax, W[e2 + 1]); umin = nmin(umin, W[e2 + 1]); }
-          if (!byl) { umax = nmax(umax, W[e2 - 1]); umin = nmin(umin, W[e2 - 1]); }
-          if (bxl || bxh) { const T gg = T(2) * gxv - u; umax = nmax(umax, gg); umin = nmin(umin, gg); }
-          if (byl || byh) { const T gg = T(2) * gyv - u; umax = nmax(umax, gg); umin = nmin(umin, gg); }
+          if (!bxh) { umax = fmx(umax, W[e2 + S::R2Y]); umin = fmn(umin, W[e2 + S::R2Y]); }
+          if (!bxl) { umax = fmx(umax, W[e2 - S::R2Y]); umin = fmn(umin, W[e2 - S::R2Y]); }
+          if (!byh) { umax = fmx(umax, W[e2 + 1]); umin = fmn(umin, W[e2 + 1]); }
+          if (!byl) { umax = fmx(umax, W[e2 - 1]); umin = fmn(umin, W[e2 - 1]); }
+          if (bxl || bxh) { const T gg = T(2) * gxv - u; umax = fmx(umax, gg); umin = fmn(umin, gg); }
+          if (byl || byh) { const T gg = T(2) * gyv - u; umax = fmx(umax, gg); umin = fmn(umin, gg); }
         }
         gxa[v] = gx;
         gya[v] = gy;
@@ -396,7 +391,7 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
     }
     sd.b = vb;
     if (RECON == ZB_RECON_ETA) {
-      const T eta = nmax(w1, vb);
+      const T eta = fmx(w1, vb);
       const T hf = eta - vb;
       sd.h = hf;
       sd.ux = w2;
@@ -627,7 +622,7 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
     if (trouble_out != nullptr) trouble_out[k] = tr ? 1 : 0;
     if (MODE == MODE_STEP2 || MODE == MODE_EULER) {
       const T hi = kp_hinv(hn, p.eps_kp);
-      const T c = sqrt(g * nmax(hn, T(0)));
+      const T c = sqrt(g * fmx(hn, T(0)));
       const T lx = fabs(qxn * hi) + c, ly = fabs(qyn * hi) + c;
       amax_loc = nmax(amax_loc, (double)nmax(lx, ly));
     }
