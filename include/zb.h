@@ -43,7 +43,8 @@ enum {
   ZB_OK = 0,
   ZB_E_ARG = -1,      /* invalid argument (size, enum, null pointer) */
   ZB_E_CUDA = -2,     /* CUDA launch / runtime error */
-  ZB_E_UNSUPPORTED = -3
+  ZB_E_UNSUPPORTED = -3,
+  ZB_E_TOO_LARGE = -4 /* grid exceeds the fixed scratch of zb_swe2d_step_noalloc */
 };
 
 /* status bits written by the kernels into zb_ctrl.status */
@@ -130,6 +131,29 @@ int zb_swe2d_dt(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl,
 int zb_swe2d_step(const zb_swe2d_cfg* cfg, void* Q, void* workspace,
                   size_t workspace_bytes, zb_ctrl* ctrl, int phase,
                   zb_stream_t stream);
+
+/* Largest grid (nx * ny) zb_swe2d_step_noalloc accepts. */
+#define ZB_NOALLOC_MAX_CELLS (1u << 20)
+
+/* zb_swe2d_step for callers that cannot allocate device memory.  No
+ * counterpart in the reference.  Such callers are plugins inside a framework
+ * that owns every device byte (an XLA / JAX FFI custom call declared without
+ * a scratch operand, an inference-engine plugin at enqueue time) and code
+ * running while a stream is captured into a CUDA graph, where a synchronous
+ * cudaMalloc is not allowed.  The caller passes Q and ctrl as for
+ * zb_swe2d_step; the stage-1 scratch is a file-scope device array inside
+ * libzb sized for ZB_NOALLOC_MAX_CELLS cells (24 MiB, held on every GPU that
+ * loads the library until the process exits).  Larger grids return
+ * ZB_E_TOO_LARGE without launching.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current, so
+ * make that first call before any stream capture.  Nothing is allocated and
+ * no library routine that allocates is called.  Every call shares the one
+ * array and it keeps the last call's contents (the step overwrites every
+ * scratch cell it reads, so nothing needs clearing); calls that overlap on
+ * the GPU -- concurrent streams, or several host threads on one device --
+ * race on it and must be serialised by the caller. */
+int zb_swe2d_step_noalloc(const zb_swe2d_cfg* cfg, void* Q, zb_ctrl* ctrl,
+                          int phase, zb_stream_t stream);
 
 /* One launch of zb_swe2d_step: part 0 is the first stage (order 2) or the
  * Euler stage (order 1), part 1 the second stage (order 2) or the copy-back

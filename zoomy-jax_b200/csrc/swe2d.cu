@@ -21,6 +21,7 @@
 #include <cstring>
 #include <cmath>
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -1111,6 +1112,48 @@ int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux, zb_stream_t
                                                     cfg->ny, cfg->wet_dry_eps,
                                                     make_lsq<double>(cfg->dx, cfg->dy));
   return zb_launch_check();
+}
+
+// ── allocation-free step ────────────────────────────────────────────────────
+// Some callers cannot call cudaMalloc: a framework that owns every device
+// byte and hands a plugin only its operands (an XLA / JAX FFI custom call
+// declared without a scratch buffer, an inference-engine plugin at enqueue
+// time), or code running while a stream is being captured into a CUDA graph,
+// where a synchronous cudaMalloc is not permitted.  For them the stage-1
+// state of the fused step lives in this file-scope device array instead of a
+// caller workspace: three planes of up to ZB_NOALLOC_MAX_CELLS cells in
+// float64 (float32 uses the first half), 24 MiB plus 256 bytes of padding.
+// Every GPU that loads libzb holds the array until the process exits.
+static __device__ __align__(256) double g_noalloc_scratch[3 * ZB_NOALLOC_MAX_CELLS + 32];
+
+// The array's name in host code is only a host-side stand-in; the kernels
+// need its device address, fetched once per device with that device current.
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[64] = {};
+
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return ZB_E_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) return ZB_E_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return ZB_OK;
+}
+
+int zb_swe2d_step_noalloc(const zb_swe2d_cfg* cfg, void* Q, zb_ctrl* ctrl, int phase,
+                          zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !Q || !ctrl || phase < 0 || phase > 2) return ZB_E_ARG;
+  if ((size_t)cfg->nx * (size_t)cfg->ny > (size_t)ZB_NOALLOC_MAX_CELLS) return ZB_E_TOO_LARGE;
+  void* ws = nullptr;
+  const int rc = noalloc_scratch(&ws);
+  if (rc != ZB_OK) return rc;
+  return zb_swe2d_step(cfg, Q, ws, sizeof(g_noalloc_scratch), ctrl, phase, stream);
 }
 
 }  // extern "C"

@@ -13,7 +13,8 @@ import pathlib
 LIB_PATH = pathlib.Path(__file__).resolve().parent.parent / "lib" / "libzb.so"
 
 ZB_F32, ZB_F64 = 0, 1
-ZB_OK, ZB_E_ARG, ZB_E_CUDA, ZB_E_UNSUPPORTED = 0, -1, -2, -3
+ZB_OK, ZB_E_ARG, ZB_E_CUDA, ZB_E_UNSUPPORTED, ZB_E_TOO_LARGE = 0, -1, -2, -3, -4
+ZB_NOALLOC_MAX_CELLS = 1 << 20
 ZB_ST_DT_INVALID, ZB_ST_TROUBLED, ZB_ST_NOT_CONVERGED = 1, 2, 4
 BC = {"extrapolation": 0, "wall": 1, "periodic": 2}
 RECON = {"constant": 0, "conservative": 1, "eta": 2}
@@ -57,6 +58,7 @@ SIGNATURES = [
     ("zb_swe2d_dt", C.c_int, [_CFG, _P, _P, C.c_double, _P]),
     ("zb_swe2d_step", C.c_int, [_CFG, _P, _P, C.c_size_t, _P, C.c_int, _P]),
     ("zb_swe2d_step_part", C.c_int, [_CFG, _P, _P, C.c_size_t, _P, C.c_int, C.c_int, _P]),
+    ("zb_swe2d_step_noalloc", C.c_int, [_CFG, _P, _P, C.c_int, _P]),
     ("zb_swe2d_stage", C.c_int, [_CFG, _P, _P, _P, C.c_double, C.c_double,
                                  C.c_double, _P, _P, _P, _P, _P]),
     ("zb_swe2d_source", C.c_int, [_CFG, _P, _P, C.c_double, _P]),
