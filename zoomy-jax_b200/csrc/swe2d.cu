@@ -22,6 +22,7 @@
 #include <cmath>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -131,27 +132,28 @@ struct Side {
   T b, h, qx, qy, ux, uy;
 };
 
-// Numerical flux across a face with unit normal (nx, ny) in {(+-1,0),(0,+-1)}.
-// Outputs Fh, Fqx, Fqy and the normal-direction fluctuations DmN (owner / L)
-// and DpN (neighbour / R).  Restates numerical_flux of the oracle:
+// Numerical flux across a face with unit normal n = sg * e_AXIS (sg = +-1).
+// Outputs Fh, Fqx, Fqy and the scalar fluctuations Dm (owner / L side) and Dp
+// (neighbour / R side) that multiply n.  Restates numerical_flux of the oracle:
 // Rusanov (zoomy_jax/fvm/flux.py:72-82) and hydrostatic-reconstruction
 // Rusanov / HLL (Audusse et al. 2004; Harten-Lax-van Leer 1983, Davis speeds).
-template <typename T, int RIEMANN>
-__device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R,
-                                        T nx, T ny, T g, T& Fh, T& Fqx,
-                                        T& Fqy, T& Dm, T& Dp) {
+// With an axis normal u.n = sg * u_AXIS and p n = sg * p e_AXIS exactly, so the
+// terms the general form multiplies by a zero normal component are dropped.
+template <typename T, int RIEMANN, int AXIS>
+__device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R, T sg, T g,
+                                        T& Fh, T& Fqx, T& Fqy, T& Dm, T& Dp) {
   const T half = T(0.5);
-  T unL = L.ux * nx + L.uy * ny;
-  T unR = R.ux * nx + R.uy * ny;
+  const T unL = sg * (AXIS == 0 ? L.ux : L.uy);
+  const T unR = sg * (AXIS == 0 ? R.ux : R.uy);
   if (RIEMANN == ZB_RIEMANN_RUSANOV) {
-    T cL = sqrt(g * L.h), cR = sqrt(g * R.h);
-    T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
-    T qnL = L.qx * nx + L.qy * ny;
-    T qnR = R.qx * nx + R.qy * ny;
-    T pL = half * g * (L.h * L.h), pR = half * g * (R.h * R.h);
-    T FLx = L.qx * unL + pL * nx, FLy = L.qy * unL + pL * ny;
-    T FRx = R.qx * unR + pR * nx, FRy = R.qy * unR + pR * ny;
-    T hs = half * s;
+    const T cL = sqrt(g * L.h), cR = sqrt(g * R.h);
+    const T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
+    const T qnL = sg * (AXIS == 0 ? L.qx : L.qy);
+    const T qnR = sg * (AXIS == 0 ? R.qx : R.qy);
+    const T pL = sg * (half * g * (L.h * L.h)), pR = sg * (half * g * (R.h * R.h));
+    T FLx = L.qx * unL, FLy = L.qy * unL, FRx = R.qx * unR, FRy = R.qy * unR;
+    if (AXIS == 0) { FLx += pL; FRx += pR; } else { FLy += pL; FRy += pR; }
+    const T hs = half * s;
     Fh = half * (qnL + qnR) - hs * (R.h - L.h);
     Fqx = half * (FLx + FRx) - hs * (R.qx - L.qx);
     Fqy = half * (FLy + FRy) - hs * (R.qy - L.qy);
@@ -159,29 +161,29 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R,
     Dp = T(0);
     return;
   }
-  T bs = fmx(L.b, R.b);
-  T hLs = fmx(T(0), L.h + L.b - bs);
-  T hRs = fmx(T(0), R.h + R.b - bs);
-  T cL = sqrt(g * hLs), cR = sqrt(g * hRs);
-  T qLx = hLs * L.ux, qLy = hLs * L.uy;
-  T qRx = hRs * R.ux, qRy = hRs * R.uy;
-  T FLh = hLs * unL, FRh = hRs * unR;
-  T pL = half * g * (hLs * hLs), pR = half * g * (hRs * hRs);
-  T FLx = qLx * unL + pL * nx, FLy = qLy * unL + pL * ny;
-  T FRx = qRx * unR + pR * nx, FRy = qRy * unR + pR * ny;
+  const T bs = fmx(L.b, R.b);
+  const T hLs = fmx(T(0), L.h + L.b - bs);
+  const T hRs = fmx(T(0), R.h + R.b - bs);
+  const T cL = sqrt(g * hLs), cR = sqrt(g * hRs);
+  const T qLx = hLs * L.ux, qLy = hLs * L.uy;
+  const T qRx = hRs * R.ux, qRy = hRs * R.uy;
+  const T FLh = hLs * unL, FRh = hRs * unR;
+  const T pL = sg * (half * g * (hLs * hLs)), pR = sg * (half * g * (hRs * hRs));
+  T FLx = qLx * unL, FLy = qLy * unL, FRx = qRx * unR, FRy = qRy * unR;
+  if (AXIS == 0) { FLx += pL; FRx += pR; } else { FLy += pL; FRy += pR; }
   if (RIEMANN == ZB_RIEMANN_RUSANOV_HR) {
-    T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
-    T hs = half * s;
+    const T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
+    const T hs = half * s;
     Fh = half * (FLh + FRh) - hs * (hRs - hLs);
     Fqx = half * (FLx + FRx) - hs * (qRx - qLx);
     Fqy = half * (FLy + FRy) - hs * (qRy - qLy);
   } else {
-    T SL = fmn(unL - cL, unR - cR);
-    T SR = fmx(unL + cL, unR + cR);
-    T sl = fmn(SL, T(0)), sr = fmx(SR, T(0));
-    T den = sr - sl;
-    T inv = den > T(0) ? T(1) / den : T(0);
-    T slsr = sl * sr;
+    const T SL = fmn(unL - cL, unR - cR);
+    const T SR = fmx(unL + cL, unR + cR);
+    const T sl = fmn(SL, T(0)), sr = fmx(SR, T(0));
+    const T den = sr - sl;
+    const T inv = den > T(0) ? T(1) / den : T(0);
+    const T slsr = sl * sr;
     Fh = (sr * FLh - sl * FRh + slsr * (hRs - hLs)) * inv;
     Fqx = (sr * FLx - sl * FRx + slsr * (qRx - qLx)) * inv;
     Fqy = (sr * FLy - sl * FRy + slsr * (qRy - qLy)) * inv;
@@ -381,14 +383,19 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
   }
 
   // ── phase C: faces ──
-  // side trace of the cell at R2 index e2 / R1 index e1 at offset (ox, oy)
-  auto trace = [&](int e2, int e1, T ox, T oy, Side<T>& sd) {
+  // side trace of the cell at R2 index e2 / R1 index e1 at offset o along the
+  // face axis (the other offset component is zero: its term is dropped)
+  auto trace = [&](auto axis_tag, int e2, int e1, T o, Side<T>& sd) {
+    constexpr int AX = decltype(axis_tag)::value;
     T vb = s.b[e2], w1 = s.w1[e2], w2 = s.w2[e2], w3 = s.w3[e2];
     if (ORDER >= 2) {
-      vb = vb + (s.sx[0][e1] * ox + s.sy[0][e1] * oy);
-      w1 = w1 + (s.sx[1][e1] * ox + s.sy[1][e1] * oy);
-      w2 = w2 + (s.sx[2][e1] * ox + s.sy[2][e1] * oy);
-      w3 = w3 + (s.sx[3][e1] * ox + s.sy[3][e1] * oy);
+      if (AX == 0) {
+        vb = vb + s.sx[0][e1] * o; w1 = w1 + s.sx[1][e1] * o;
+        w2 = w2 + s.sx[2][e1] * o; w3 = w3 + s.sx[3][e1] * o;
+      } else {
+        vb = vb + s.sy[0][e1] * o; w1 = w1 + s.sy[1][e1] * o;
+        w2 = w2 + s.sy[2][e1] * o; w3 = w3 + s.sy[3][e1] * o;
+      }
     }
     sd.b = vb;
     if (RECON == ZB_RECON_ETA) {
@@ -408,6 +415,8 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
       sd.uy = w3 * hinv;
     }
   };
+  using AxX = std::integral_constant<int, 0>;
+  using AxY = std::integral_constant<int, 1>;
   // periodic seam: Q_R is the partner cell's (unreconstructed) state; its
   // velocity is the partner's own W row on the eta path and q times the
   // OWNER's hinv on the conservative path (the flux pass hands the inner
@@ -442,23 +451,18 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
       const bool lo = gi == 0;
       const int e2o = lo ? e2R : e2L, e1o = lo ? e1R : e1L;
       const T sg = lo ? T(-1) : T(1);
-      trace(e2o, e1o, sg * p.half_dx, T(0), A);
+      trace(AxX(), e2o, e1o, sg * p.half_dx, A);
       const int kind = p.bc[lo ? 0 : 1];
       if (kind == ZB_BC_PERIODIC) {
         partner(lo ? e2L : e2R, s.aux[e2o], B);
       } else {
         B = A;
-        if (kind == ZB_BC_WALL) {
-          // q - 2 (q.n) n with n = (sg, 0)
-          const T qn = A.qx * sg + A.qy * T(0);
-          B.qx = A.qx - T(2) * qn * sg;
-          B.qy = A.qy - T(2) * qn * T(0);
-          const T un = A.ux * sg + A.uy * T(0);
-          B.ux = A.ux - T(2) * un * sg;
-          B.uy = A.uy - T(2) * un * T(0);
+        if (kind == ZB_BC_WALL) {   // q - 2 (q.n) n with n = (sg, 0): q_x -> -q_x
+          B.qx = -A.qx;
+          B.ux = -A.ux;
         }
       }
-      riemann<T, RIEMANN>(A, B, sg, T(0), g, Fh, Fx, Fy, Dm, Dp);
+      riemann<T, RIEMANN, 0>(A, B, sg, g, Fh, Fx, Fy, Dm, Dp);
       T ces = T(0);
       if (ORDER >= 2) ces = half * g * (s.h[e2o] + A.h) * (A.b - s.b[e2o]);
       const T own_n = Fx + Dm * sg + ces * sg;
@@ -468,9 +472,9 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
         s.fxh[e] = Fh; s.fxt[e] = Fy; s.fxl[e] = own_n; s.fxr[e] = T(0);
       }
     } else {
-      trace(e2L, e1L, p.half_dx, T(0), A);
-      trace(e2R, e1R, -p.half_dx, T(0), B);
-      riemann<T, RIEMANN>(A, B, T(1), T(0), g, Fh, Fx, Fy, Dm, Dp);
+      trace(AxX(), e2L, e1L, p.half_dx, A);
+      trace(AxX(), e2R, e1R, -p.half_dx, B);
+      riemann<T, RIEMANN, 0>(A, B, T(1), g, Fh, Fx, Fy, Dm, Dp);
       T cesA = T(0), cesB = T(0);
       if (ORDER >= 2) {
         cesA = half * g * (s.h[e2L] + A.h) * (A.b - s.b[e2L]);
@@ -495,22 +499,18 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
       const bool lo = gj == 0;
       const int e2o = lo ? e2R : e2L, e1o = lo ? e1R : e1L;
       const T sg = lo ? T(-1) : T(1);
-      trace(e2o, e1o, T(0), sg * p.half_dy, A);
+      trace(AxY(), e2o, e1o, sg * p.half_dy, A);
       const int kind = p.bc[lo ? 2 : 3];
       if (kind == ZB_BC_PERIODIC) {
         partner(lo ? e2L : e2R, s.aux[e2o], B);
       } else {
         B = A;
-        if (kind == ZB_BC_WALL) {
-          const T qn = A.qx * T(0) + A.qy * sg;
-          B.qx = A.qx - T(2) * qn * T(0);
-          B.qy = A.qy - T(2) * qn * sg;
-          const T un = A.ux * T(0) + A.uy * sg;
-          B.ux = A.ux - T(2) * un * T(0);
-          B.uy = A.uy - T(2) * un * sg;
+        if (kind == ZB_BC_WALL) {   // n = (0, sg): q_y -> -q_y
+          B.qy = -A.qy;
+          B.uy = -A.uy;
         }
       }
-      riemann<T, RIEMANN>(A, B, T(0), sg, g, Fh, Fx, Fy, Dm, Dp);
+      riemann<T, RIEMANN, 1>(A, B, sg, g, Fh, Fx, Fy, Dm, Dp);
       T ces = T(0);
       if (ORDER >= 2) ces = half * g * (s.h[e2o] + A.h) * (A.b - s.b[e2o]);
       const T own_n = Fy + Dm * sg + ces * sg;
@@ -520,9 +520,9 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
         s.fyh[e] = Fh; s.fyt[e] = Fx; s.fyl[e] = own_n; s.fyr[e] = T(0);
       }
     } else {
-      trace(e2L, e1L, T(0), p.half_dy, A);
-      trace(e2R, e1R, T(0), -p.half_dy, B);
-      riemann<T, RIEMANN>(A, B, T(0), T(1), g, Fh, Fx, Fy, Dm, Dp);
+      trace(AxY(), e2L, e1L, p.half_dy, A);
+      trace(AxY(), e2R, e1R, -p.half_dy, B);
+      riemann<T, RIEMANN, 1>(A, B, T(1), g, Fh, Fx, Fy, Dm, Dp);
       T cesA = T(0), cesB = T(0);
       if (ORDER >= 2) {
         cesA = half * g * (s.h[e2L] + A.h) * (A.b - s.b[e2L]);
