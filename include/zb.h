@@ -200,6 +200,92 @@ int zb_swe2d_mass(const zb_swe2d_cfg* cfg, const void* Q, double* partial,
 int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux,
                  zb_stream_t stream);
 
+/* ── unstructured triangles ─────────────────────────────────────────────── */
+
+/* Scheme of the triangle path (the Cartesian fields it shares keep their
+ * meaning; limiter: minmod / Barth-Jespersen / none). */
+typedef struct {
+  int32_t order, recon, riemann, limiter;
+  double g, wet_dry_eps, eps_wet, manning_n;
+  int32_t implicit_source, dim_factor;
+  double cfl, dt_max, t_end;
+  int32_t degree, dtype;
+} zb_tri_cfg;
+
+/* Device arrays of a triangle mesh (caller-owned; SoA, int32 connectivity,
+ * geometry in the state precision except face_inr which is float64).
+ * [3][C] arrays hold the cell's three slots plane by plane.  Built by the
+ * host from MeshJAX-equivalent data (zoomy_jax/mesh/mesh.py:123-264,
+ * solver2/context.py:99-163). */
+typedef struct {
+  int32_t n_cells, n_faces, n_bf;
+  const int32_t* lsq_idx;     /* [3][C] neighbour cell or -1 - boundary face  */
+  const void* lsq_wx;         /* [3][C] least-squares weights, x-derivative   */
+  const void* lsq_wy;         /* [3][C] least-squares weights, y-derivative   */
+  const void* cf_rx;          /* [3][C] face centre - cell centre, x          */
+  const void* cf_ry;          /* [3][C] face centre - cell centre, y          */
+  const int32_t* cell_face;   /* [3][C] 2 f + side (0 owner, 1 neighbour)     */
+  const void* cell_inv_area;  /* [C]                                          */
+  const int32_t* face_a;      /* [F] owner cell                               */
+  const int32_t* face_b;      /* [F] neighbour cell, or -1 - boundary face    */
+  const void* face_nx;        /* [F] unit normal out of the owner             */
+  const void* face_ny;
+  const void* face_len;       /* [F] face length                              */
+  const void* face_rax;       /* [F] face centre - owner centre               */
+  const void* face_ray;
+  const void* face_rbx;       /* [F] face centre - neighbour centre           */
+  const void* face_rby;
+  const double* face_inr;     /* [F] min inradius of the two cells (CFL)     */
+  const int32_t* bf_kind;     /* [n_bf] ZB_BC_EXTRAPOLATION / ZB_BC_WALL      */
+  const void* bf_nx;          /* [n_bf] boundary normals                      */
+  const void* bf_ny;
+} zb_tri_mesh;
+
+/* Workspace of zb_tri_step / zb_tri_stage / zb_tri_dt. */
+size_t zb_tri_workspace_bytes(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh);
+
+/* Control-block set-up for a triangle march from time t0 (the dt slots hold a
+ * running minimum of the per-face CFL limit here). */
+int zb_tri_init(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, zb_ctrl* ctrl,
+                int phase, double t0, zb_stream_t stream);
+
+/* One full step in place on Q (4, C): the face pass of the first stage
+ * reduces the CFL dt over faces (zoomy_jax/fvm/solver2/blocks.py:36-95),
+ * SSP-RK2 with gradient / face / gather-update launches per stage
+ * (solver_jax.py:722-1131), Manning friction after the step.  Every face is
+ * evaluated once and each cell gathers its faces in a fixed order, so the
+ * update is deterministic and exactly conservative. */
+int zb_tri_step(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, void* Q,
+                void* workspace, size_t workspace_bytes, zb_ctrl* ctrl,
+                int phase, zb_stream_t stream);
+
+/* One Shu-Osher stage with a host dt (dt < 0: ctrl->dt), as zb_swe2d_stage. */
+int zb_tri_stage(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh,
+                 const void* Qk, const void* Q0, void* Q_out, double alpha,
+                 double beta, double dt, const void* hinv_src,
+                 const uint8_t* force_o1, uint8_t* trouble_out, void* workspace,
+                 size_t workspace_bytes, zb_ctrl* ctrl, zb_stream_t stream);
+
+/* dt of the state (CFL law over faces, dt_max, t_end - t) into ctrl->dt. */
+int zb_tri_dt(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, const void* Q,
+              void* workspace, size_t workspace_bytes, zb_ctrl* ctrl, double t,
+              zb_stream_t stream);
+
+/* Manning source step Q += dt S(Q, hinv0), as zb_swe2d_source. */
+int zb_tri_source(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, void* Q,
+                  const void* hinv0, double dt, zb_stream_t stream);
+
+/* Post-step aux rows into Qaux (7, C), as zb_swe2d_aux
+ * (zoomy_jax/fvm/solver_jax.py:284-369). */
+int zb_tri_aux(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, const void* Q,
+               void* Qaux, zb_stream_t stream);
+
+/* sum h |cell| in float64 into ctrl->mass; partial holds
+ * zb_tri_mass_partials() doubles. */
+size_t zb_tri_mass_partials(void);
+int zb_tri_mass(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, const void* Q,
+                double* partial, zb_ctrl* ctrl, zb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -380,10 +380,7 @@ def create_tri(n_side, jitter=0.3, seed=0, domain=(0.0, 1.0, 0.0, 1.0),
 
     ``n_side x n_side`` lattice points on the domain, interior points jittered
     by ``jitter * spacing`` (boundary points stay on the boundary), giving about
-    ``2 n_side^2`` triangles.  Cells are renumbered in Morton order.  The
-    gradient stencil is the (up to three) face neighbours plus the boundary
-    ghosts -- zoomy_core's triangle stencil is absent, so this one is defined
-    here.
+    ``2 n_side^2`` triangles, renumbered in Morton order of their centroids.
     """
     from scipy.spatial import Delaunay
     rng = np.random.default_rng(seed)
@@ -399,21 +396,27 @@ def create_tri(n_side, jitter=0.3, seed=0, domain=(0.0, 1.0, 0.0, 1.0),
     jit[onx, 0] = 0.0
     jit[ony, 1] = 0.0
     P = P + jit
-    tri = Delaunay(P)
-    T = tri.simplices.astype(np.int64)
-    # orient counter-clockwise
+    T = Delaunay(P).simplices.astype(np.int64)
+    cen = (P[T[:, 0]] + P[T[:, 1]] + P[T[:, 2]]) / 3.0
+    T = T[morton_order(cen)]
+    return tri_from_points(P, T, build_lsq=build_lsq)
+
+
+def tri_from_points(P, T, build_lsq=True):
+    """Face-based triangle mesh from vertices ``P (n, 2)`` and triangles
+    ``T (C, 3)``, keeping the given cell order.  Faces are numbered by sorted
+    vertex pair; the owner is the first triangle listing the edge, the normal
+    points out of it; the boundary tag follows the outward normal
+    (left/right/bottom/top for |n_x| > 0.5 / otherwise)."""
+    P = np.asarray(P, dtype=np.float64)
+    T = np.asarray(T, dtype=np.int64).copy()
     a, b, c = P[T[:, 0]], P[T[:, 1]], P[T[:, 2]]
     cross = (b[:, 0] - a[:, 0]) * (c[:, 1] - a[:, 1]) - (b[:, 1] - a[:, 1]) * (c[:, 0] - a[:, 0])
     neg = cross < 0
     T[neg, 1], T[neg, 2] = T[neg, 2].copy(), T[neg, 1].copy()
     area = 0.5 * np.abs(cross)
     cen = (P[T[:, 0]] + P[T[:, 1]] + P[T[:, 2]]) / 3.0
-    perm = morton_order(cen)
-    T = T[perm]
-    area = area[perm]
-    cen = cen[perm]
     C = len(T)
-    # edges
     e = np.concatenate([T[:, [0, 1]], T[:, [1, 2]], T[:, [2, 0]]], axis=0)
     owner = np.concatenate([np.arange(C)] * 3)
     key = np.sort(e, axis=1)
@@ -424,8 +427,6 @@ def create_tri(n_side, jitter=0.3, seed=0, domain=(0.0, 1.0, 0.0, 1.0),
     first[1:] = k1s[1:] != k1s[:-1]
     fid_sorted = np.cumsum(first) - 1
     F = int(fid_sorted[-1] + 1)
-    fid = np.empty_like(fid_sorted)
-    fid[order] = fid_sorted
     fcells = np.full((2, F), -1, dtype=np.int64)
     fverts = np.zeros((F, 2), dtype=np.int64)
     # first occurrence = owner (its directed ccw edge gives the outward normal)

@@ -48,9 +48,31 @@ class ZbSwe2dCfg(C.Structure):
                 ("dtype", C.c_int32)]
 
 
+class ZbTriCfg(C.Structure):
+    _fields_ = [("order", C.c_int32), ("recon", C.c_int32), ("riemann", C.c_int32),
+                ("limiter", C.c_int32), ("g", C.c_double), ("wet_dry_eps", C.c_double),
+                ("eps_wet", C.c_double), ("manning_n", C.c_double),
+                ("implicit_source", C.c_int32), ("dim_factor", C.c_int32),
+                ("cfl", C.c_double), ("dt_max", C.c_double), ("t_end", C.c_double),
+                ("degree", C.c_int32), ("dtype", C.c_int32)]
+
+
+TRI_MESH_FIELDS = ["lsq_idx", "lsq_wx", "lsq_wy", "cf_rx", "cf_ry", "cell_face",
+                   "cell_inv_area", "face_a", "face_b", "face_nx", "face_ny", "face_len",
+                   "face_rax", "face_ray", "face_rbx", "face_rby", "face_inr", "bf_kind",
+                   "bf_nx", "bf_ny"]
+
+
+class ZbTriMesh(C.Structure):
+    _fields_ = ([("n_cells", C.c_int32), ("n_faces", C.c_int32), ("n_bf", C.c_int32)]
+                + [(n, C.c_void_p) for n in TRI_MESH_FIELDS])
+
+
 # (name, restype, argtypes) of every symbol include/zb.h declares
 _P = C.c_void_p
 _CFG = C.POINTER(ZbSwe2dCfg)
+_TCFG = C.POINTER(ZbTriCfg)
+_TMESH = C.POINTER(ZbTriMesh)
 SIGNATURES = [
     ("zb_version", C.c_char_p, []),
     ("zb_swe2d_workspace_bytes", C.c_size_t, [_CFG]),
@@ -65,6 +87,16 @@ SIGNATURES = [
     ("zb_swe2d_mass_partials", C.c_size_t, [_CFG]),
     ("zb_swe2d_mass", C.c_int, [_CFG, _P, _P, _P, _P]),
     ("zb_swe2d_aux", C.c_int, [_CFG, _P, _P, _P]),
+    ("zb_tri_workspace_bytes", C.c_size_t, [_TCFG, _TMESH]),
+    ("zb_tri_init", C.c_int, [_TCFG, _TMESH, _P, C.c_int, C.c_double, _P]),
+    ("zb_tri_step", C.c_int, [_TCFG, _TMESH, _P, _P, C.c_size_t, _P, C.c_int, _P]),
+    ("zb_tri_stage", C.c_int, [_TCFG, _TMESH, _P, _P, _P, C.c_double, C.c_double,
+                               C.c_double, _P, _P, _P, _P, C.c_size_t, _P, _P]),
+    ("zb_tri_dt", C.c_int, [_TCFG, _TMESH, _P, _P, C.c_size_t, _P, C.c_double, _P]),
+    ("zb_tri_source", C.c_int, [_TCFG, _TMESH, _P, _P, C.c_double, _P]),
+    ("zb_tri_aux", C.c_int, [_TCFG, _TMESH, _P, _P, _P]),
+    ("zb_tri_mass_partials", C.c_size_t, []),
+    ("zb_tri_mass", C.c_int, [_TCFG, _TMESH, _P, _P, _P, _P]),
 ]
 
 _lib = None

@@ -6,24 +6,94 @@ Same methods and knobs as ``zoomy_jax.fvm.solver_jax.HyperbolicSolver``
 ``solve`` :1356-1368).  ``Q`` and ``Qaux`` are CUDA tensors in the reference
 layout ``(n_state, n_cells)``; every operator is a libzb call on the current
 torch stream.  The time loop of ``run_simulation`` is device-resident: dt,
-time and the CFL wave-speed maximum live in a device control block and the
-host only polls it between batches of steps.
+time and the CFL reduction live in a device control block and the host only
+polls it between batches of steps.
+
+Two meshes are served through one backend interface: the Cartesian mesh
+(``create_2d``; fused tile kernels) and the unstructured triangle mesh
+(``trimesh.create_tri``; gradient / face / gather-update kernels).
 """
 from __future__ import annotations
 
 import ctypes as C
 import math
 
-import numpy as np
-
 from .. import _lib as L
 from ..mesh import CartesianMesh
-from ..model import NumericalSystemModel
 from ..timestepping import Adaptive, Constant, adaptive
+from ..trimesh import TriangleMesh
 
 
-class EllipticSolveError(RuntimeError):
-    pass
+class _CartBackend:
+    """libzb calls of the Cartesian path (``zb_swe2d_*``)."""
+
+    def __init__(self, lib, cfg):
+        self.lib, self.cfg = lib, cfg
+        self.ref = C.byref(cfg)
+
+    def workspace_bytes(self):
+        return int(self.lib.zb_swe2d_workspace_bytes(self.ref))
+
+    def mass_partials(self):
+        return int(self.lib.zb_swe2d_mass_partials(self.ref))
+
+    def init(self, Q, ctrl, t0, st):
+        return self.lib.zb_swe2d_init(self.ref, Q, ctrl, 0, t0, st)
+
+    def step(self, Q, ws, wsb, ctrl, phase, st):
+        return self.lib.zb_swe2d_step(self.ref, Q, ws, wsb, ctrl, phase, st)
+
+    def stage(self, cfgref, Qk, Q0, Qo, a, b, dt, hinv, fo, tr, ws, wsb, ctrl, st):
+        return self.lib.zb_swe2d_stage(cfgref, Qk, Q0, Qo, a, b, dt, hinv, fo, tr, ctrl, st)
+
+    def dt(self, cfgref, Q, ws, wsb, ctrl, t, st):
+        return self.lib.zb_swe2d_dt(cfgref, Q, ctrl, t, st)
+
+    def source(self, Q, hinv, dt, st):
+        return self.lib.zb_swe2d_source(self.ref, Q, hinv, dt, st)
+
+    def mass(self, Q, part, ctrl, st):
+        return self.lib.zb_swe2d_mass(self.ref, Q, part, ctrl, st)
+
+    def aux(self, Q, A, st):
+        return self.lib.zb_swe2d_aux(self.ref, Q, A, st)
+
+
+class _TriBackend:
+    """libzb calls of the triangle path (``zb_tri_*``)."""
+
+    def __init__(self, lib, cfg, mesh_struct):
+        self.lib, self.cfg, self.mesh = lib, cfg, mesh_struct
+        self.ref = C.byref(cfg)
+        self.mref = C.byref(mesh_struct)
+
+    def workspace_bytes(self):
+        return int(self.lib.zb_tri_workspace_bytes(self.ref, self.mref))
+
+    def mass_partials(self):
+        return int(self.lib.zb_tri_mass_partials())
+
+    def init(self, Q, ctrl, t0, st):
+        return self.lib.zb_tri_init(self.ref, self.mref, ctrl, 0, t0, st)
+
+    def step(self, Q, ws, wsb, ctrl, phase, st):
+        return self.lib.zb_tri_step(self.ref, self.mref, Q, ws, wsb, ctrl, phase, st)
+
+    def stage(self, cfgref, Qk, Q0, Qo, a, b, dt, hinv, fo, tr, ws, wsb, ctrl, st):
+        return self.lib.zb_tri_stage(cfgref, self.mref, Qk, Q0, Qo, a, b, dt, hinv, fo, tr,
+                                     ws, wsb, ctrl, st)
+
+    def dt(self, cfgref, Q, ws, wsb, ctrl, t, st):
+        return self.lib.zb_tri_dt(cfgref, self.mref, Q, ws, wsb, ctrl, t, st)
+
+    def source(self, Q, hinv, dt, st):
+        return self.lib.zb_tri_source(self.ref, self.mref, Q, hinv, dt, st)
+
+    def mass(self, Q, part, ctrl, st):
+        return self.lib.zb_tri_mass(self.ref, self.mref, Q, part, ctrl, st)
+
+    def aux(self, Q, A, st):
+        return self.lib.zb_tri_aux(self.ref, self.mref, Q, A, st)
 
 
 class HyperbolicSolver:
@@ -34,8 +104,9 @@ class HyperbolicSolver:
     ``free_surface_b_index``, ``reconstruction_variables`` (``conservative`` |
     ``eta``), ``positivity_method``, ``front_theta_tol``, ``mood``; plus
     ``dtype`` (``float64`` default, as the reference enables x64, or
-    ``float32``) and ``eps_wet`` (the emitted dry-cell demotion threshold of
-    the eta reconstruction, ``None`` = off).
+    ``float32``), ``eps_wet`` (the emitted dry-cell demotion threshold of the
+    eta reconstruction, ``None`` = off) and ``implicit_source`` (point-implicit
+    Manning, the IMEX local solve).
     """
 
     def __init__(self, time_end=1.0, compute_dt=None, free_surface_h_index=None,
@@ -66,8 +137,7 @@ class HyperbolicSolver:
         import torch
         return torch.float64 if self.dtype == "float64" else torch.float32
 
-    def _make_cfg(self, mesh: CartesianMesh, nsm: NumericalSystemModel):
-        m = nsm.model
+    def _scheme(self, nsm):
         order = nsm.reconstruction.order
         recon = "constant" if order == 1 else (
             "eta" if self.reconstruction_variables == "eta" else "conservative")
@@ -92,36 +162,51 @@ class HyperbolicSolver:
         cd = self.compute_dt
         if isinstance(cd, Adaptive):
             cd = cd.with_dt_max(nsm.dt_max)
-        cfg = L.ZbSwe2dCfg()
-        cfg.nx, cfg.ny = mesh.nx, mesh.ny
-        cfg.x0, cfg.y0, cfg.dx, cfg.dy = mesh.x0, mesh.y0, mesh.dx, mesh.dy
+        return order, recon, cd
+
+    def _fill_common(self, cfg, nsm, order, recon, cd):
+        m = nsm.model
         cfg.order = order
         cfg.recon = L.RECON[recon]
         cfg.riemann = L.RIEMANN[nsm.riemann]
         cfg.limiter = L.LIMITER[nsm.reconstruction.limiter]
-        for i, k in enumerate(m.bc_kinds()):
-            cfg.bc[i] = L.BC[k]
         cfg.g = m.g
         cfg.wet_dry_eps = m.wet_dry_eps
         cfg.eps_wet = -1.0 if self.eps_wet is None else float(self.eps_wet)
         cfg.manning_n = m.manning_n
         cfg.implicit_source = int(self.implicit_source)
         if isinstance(cd, Adaptive):
-            cfg.dim_factor = cd.dimension
-            cfg.cfl = cd.CFL
-            cfg.dt_max = cd.dt_max
-            cfg.degree = cd.degree
+            cfg.dim_factor, cfg.cfl, cfg.dt_max, cfg.degree = (
+                cd.dimension, cd.CFL, cd.dt_max, cd.degree)
         else:
             cfg.dim_factor, cfg.cfl, cfg.dt_max, cfg.degree = 2, 1.0, math.inf, 0
         cfg.t_end = self.time_end
         cfg.dtype = L.ZB_F64 if self.dtype == "float64" else L.ZB_F32
         return cfg
 
+    def _make_cfg(self, mesh, nsm):
+        """The libzb config struct for ``mesh`` (Cartesian or triangle)."""
+        order, recon, cd = self._scheme(nsm)
+        if isinstance(mesh, TriangleMesh):
+            kinds = nsm.model.bc_kinds()
+            if "periodic" in kinds:
+                raise NotImplementedError("periodic boundaries on the triangle mesh")
+            if nsm.reconstruction.limiter == "venkatakrishnan":
+                raise NotImplementedError("Venkatakrishnan on the triangle mesh")
+            return self._fill_common(L.ZbTriCfg(), nsm, order, recon, cd)
+        cfg = self._fill_common(L.ZbSwe2dCfg(), nsm, order, recon, cd)
+        cfg.nx, cfg.ny = mesh.nx, mesh.ny
+        cfg.x0, cfg.y0, cfg.dx, cfg.dy = mesh.x0, mesh.y0, mesh.dx, mesh.dy
+        for i, k in enumerate(nsm.model.bc_kinds()):
+            cfg.bc[i] = L.BC[k]
+        return cfg
+
     # ── setup ─────────────────────────────────────────────────────────────
     def setup_simulation(self, mesh, model):
         """Build the device state and operators (``solver_jax.py:901-988``).
-        ``model`` is a :class:`NumericalSystemModel`.  Returns ``(Q, Qaux)``
-        on the device."""
+        ``model`` is a :class:`NumericalSystemModel`; ``mesh`` a
+        :class:`CartesianMesh` or a :class:`TriangleMesh`.  Returns
+        ``(Q, Qaux)`` on the device."""
         import torch
         L.require_cuda()
         self.lib = L.load()
@@ -131,13 +216,23 @@ class HyperbolicSolver:
         self.cfg = self._make_cfg(mesh, nsm)
         dev = torch.device(self.device or "cuda")
         td = self._torch_dtype()
+        if isinstance(mesh, TriangleMesh):
+            self._mesh_arrays = mesh.device_arrays(
+                td, dev, [L.BC[k] for k in nsm.model.bc_kinds()])
+            ms = L.ZbTriMesh()
+            ms.n_cells, ms.n_faces, ms.n_bf = mesh.n_cells, mesh.n_faces, len(mesh.bf)
+            for name in L.TRI_MESH_FIELDS:
+                setattr(ms, name, self._mesh_arrays[name].data_ptr())
+            self._mesh_struct = ms
+            self.be = _TriBackend(self.lib, self.cfg, ms)
+        else:
+            self.be = _CartBackend(self.lib, self.cfg)
         Q = torch.as_tensor(nsm.model.initial_state(mesh), dtype=td, device=dev).contiguous()
-        self._ws_bytes = int(self.lib.zb_swe2d_workspace_bytes(C.byref(self.cfg)))
+        self._ws_bytes = self.be.workspace_bytes()
         self._ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=dev)
         self._ctrl = torch.zeros(L.CTRL_BYTES, dtype=torch.uint8, device=dev)
-        self._mass_part = torch.zeros(
-            int(self.lib.zb_swe2d_mass_partials(C.byref(self.cfg))),
-            dtype=torch.float64, device=dev)
+        self._mass_part = torch.zeros(self.be.mass_partials(), dtype=torch.float64, device=dev)
+        self._n = 0
         Qaux = self.update_qaux(Q)
         return Q, Qaux
 
@@ -149,8 +244,7 @@ class HyperbolicSolver:
         """KP ``hinv`` plus the LSQ derivative rows (``solver_jax.py:284-369``)."""
         import torch
         Qaux = torch.empty((7, Q.shape[1]), dtype=Q.dtype, device=Q.device)
-        L.check(self.lib.zb_swe2d_aux(C.byref(self.cfg), L.ptr(Q), L.ptr(Qaux),
-                                      self._s()), "zb_swe2d_aux")
+        L.check(self.be.aux(L.ptr(Q), L.ptr(Qaux), self._s()), "aux")
         return Qaux
 
     def read_ctrl(self):
@@ -163,9 +257,19 @@ class HyperbolicSolver:
         over faces, capped by ``dt_max`` and by ``time_end - time``."""
         if isinstance(self.compute_dt, Constant):
             return min(self.compute_dt.dt, self.time_end - time)
-        L.check(self.lib.zb_swe2d_dt(C.byref(self.cfg), L.ptr(Q), L.ptr(self._ctrl),
-                                     float(time), self._s()), "zb_swe2d_dt")
+        L.check(self.be.dt(C.byref(self.cfg), L.ptr(Q), L.ptr(self._ws),
+                           C.c_size_t(self._ws_bytes), L.ptr(self._ctrl), float(time),
+                           self._s()), "dt")
         return float(self.read_ctrl().dt)
+
+    def _stage(self, cfg, Qk, Q0, Qo, alpha, beta, dt, hinv=None, fo=None, tr=None):
+        L.check(self.be.stage(
+            C.byref(cfg), L.ptr(Qk), L.ptr(Q0) if Q0 is not None else None, L.ptr(Qo),
+            float(alpha), float(beta), float(dt),
+            L.ptr(hinv) if hinv is not None else None,
+            L.ptr(fo) if fo is not None else None, L.ptr(tr) if tr is not None else None,
+            L.ptr(self._ws), C.c_size_t(self._ws_bytes), L.ptr(self._ctrl), self._s()),
+            "stage")
 
     def _advance(self, Q, dt, force_o1=None, trouble=None):
         """Hyperbolic sub-step with a host dt: SSP-RK2 in Shu-Osher form
@@ -173,23 +277,14 @@ class HyperbolicSolver:
         bit-identical to 0.5 (Q0 + Q2)) or Euler.  Optional per-cell MOOD mask
         and troubled-mask output (C bytes)."""
         import torch
-        cfg = C.byref(self.cfg)
-        fo = L.ptr(force_o1) if force_o1 is not None else None
-        tr = L.ptr(trouble) if trouble is not None else None
         Qn = Q.clone()
         if self.cfg.order >= 2:
             Q1 = torch.empty_like(Q)
-            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Q), None, L.ptr(Q1), 0.0, 1.0, dt,
-                                            None, fo, None, L.ptr(self._ctrl), self._s()),
-                    "stage 1")
             Q1[0].copy_(Q[0])
-            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Q1), L.ptr(Q), L.ptr(Qn), 0.5, 1.0,
-                                            dt, None, fo, tr, L.ptr(self._ctrl),
-                                            self._s()), "stage 2")
+            self._stage(self.cfg, Q, None, Q1, 0.0, 1.0, dt, fo=force_o1)
+            self._stage(self.cfg, Q1, Q, Qn, 0.5, 1.0, dt, fo=force_o1, tr=trouble)
         else:
-            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Q), None, L.ptr(Qn), 0.0, 1.0, dt,
-                                            None, fo, tr, L.ptr(self._ctrl), self._s()),
-                    "stage")
+            self._stage(self.cfg, Q, None, Qn, 0.0, 1.0, dt, fo=force_o1, tr=trouble)
         return Qn
 
     def step(self, dt, time, Q, Qaux, parameters=None):
@@ -209,8 +304,7 @@ class HyperbolicSolver:
             Qn = self._advance(Q, dt)
         if self.cfg.manning_n != 0.0:
             hinv0 = Qaux[6].contiguous()
-            L.check(self.lib.zb_swe2d_source(C.byref(self.cfg), L.ptr(Qn), L.ptr(hinv0),
-                                             dt, self._s()), "source")
+            L.check(self.be.source(L.ptr(Qn), L.ptr(hinv0), dt, self._s()), "source")
         return Qn
 
     def post_step(self, time, dt, Q, Qold, Qaux, parameters=None):
@@ -220,35 +314,36 @@ class HyperbolicSolver:
 
     def mass(self, Q):
         """``sum h |cell|`` in float64 on the device."""
-        L.check(self.lib.zb_swe2d_mass(C.byref(self.cfg), L.ptr(Q), L.ptr(self._mass_part),
-                                       L.ptr(self._ctrl), self._s()), "zb_swe2d_mass")
+        L.check(self.be.mass(L.ptr(Q), L.ptr(self._mass_part), L.ptr(self._ctrl),
+                             self._s()), "mass")
         return float(self.read_ctrl().mass)
 
     # ── device-resident march ─────────────────────────────────────────────
     def init_march(self, Q, t0=0.0):
-        """Reset the control block and seed the wave-speed maximum."""
-        L.check(self.lib.zb_swe2d_init(C.byref(self.cfg), L.ptr(Q), L.ptr(self._ctrl),
-                                       0, float(t0), self._s()), "zb_swe2d_init")
+        """Reset the control block for a march from ``t0``."""
+        L.check(self.be.init(L.ptr(Q), L.ptr(self._ctrl), float(t0), self._s()), "init")
         self._n = 0
 
     def launch_steps(self, Q, n):
         """Queue ``n`` fused steps (no host sync).  The step index modulo 3
         selects the control-block slots."""
-        cfg = C.byref(self.cfg)
         ws, wsb = L.ptr(self._ws), C.c_size_t(self._ws_bytes)
-        ctrl, st = L.ptr(self._ctrl), self._s()
-        qp = L.ptr(Q)
+        ctrl, st, qp = L.ptr(self._ctrl), self._s(), L.ptr(Q)
         for _ in range(n):
-            rc = self.lib.zb_swe2d_step(cfg, qp, ws, wsb, ctrl, self._n % 3, st)
+            rc = self.be.step(qp, ws, wsb, ctrl, self._n % 3, st)
             if rc != L.ZB_OK:
-                L.check(rc, "zb_swe2d_step")
+                L.check(rc, "step")
             self._n += 1
 
     def _raise_dt(self, Q, t):
-        from ..diagnostics import worst_face
+        if isinstance(self.mesh, CartesianMesh):
+            from ..diagnostics import worst_face
+            where = worst_face(self, Q)
+        else:
+            where = ""
         raise FloatingPointError(
             f"dt became non-finite or non-positive at t = {t} (iteration "
-            f"{self._n}) -- FATAL. {worst_face(self, Q)}")
+            f"{self._n}) -- FATAL. {where}")
 
     def run_simulation(self, Q, Qaux, write_output=False, parameters=None,
                        max_steps=10 ** 7):

@@ -84,7 +84,7 @@ class MarchSolver(HyperbolicSolver):
         self.tableau = TABLEAU_SSPRK2 if self.cfg.order >= 2 else TABLEAU_EULER
         # the order-1 configuration used by the MOOD redo (constant recon,
         # same Riemann solver, no cell-interior term)
-        o1 = L.ZbSwe2dCfg.from_buffer_copy(bytes(self.cfg))
+        o1 = type(self.cfg).from_buffer_copy(bytes(self.cfg))
         o1.order, o1.recon = 1, L.RECON["constant"]
         self._cfg_o1 = o1
         return MarchState(0.0, 0, 0, Q, Qaux)
@@ -95,8 +95,9 @@ class MarchSolver(HyperbolicSolver):
         saved = cfg.t_end
         cfg.t_end = math.inf if clamp is None else float(S.time) + float(clamp)
         try:
-            L.check(self.lib.zb_swe2d_dt(C.byref(cfg), L.ptr(S.Q), L.ptr(self._ctrl),
-                                         float(S.time), self._s()), "zb_swe2d_dt")
+            L.check(self.be.dt(C.byref(cfg), L.ptr(S.Q), L.ptr(self._ws),
+                               C.c_size_t(self._ws_bytes), L.ptr(self._ctrl),
+                               float(S.time), self._s()), "dt")
         finally:
             cfg.t_end = saved
         dt = float(self.read_ctrl().dt)
@@ -105,18 +106,14 @@ class MarchSolver(HyperbolicSolver):
     def stage_loop(self, Q0, Qaux, dt, o1=False):
         """Shu-Osher stages; returns ``(Q, troubled_any)``."""
         import torch
-        cfg = C.byref(self._cfg_o1 if o1 else self.cfg)
+        cfg = self._cfg_o1 if o1 else self.cfg
         hinv = Qaux[6].contiguous() if self.cfg.manning_n != 0.0 else None
-        hp = L.ptr(hinv) if hinv is not None else None
         mask = torch.zeros(Q0.shape[1], dtype=torch.uint8, device=Q0.device)
         Qk = Q0
         for alpha, beta in self.tableau:
             out = torch.empty_like(Q0)
             out[0].copy_(Q0[0])
-            L.check(self.lib.zb_swe2d_stage(cfg, L.ptr(Qk), L.ptr(Q0), L.ptr(out),
-                                            float(alpha), float(beta), float(dt), hp,
-                                            None, L.ptr(mask), L.ptr(self._ctrl),
-                                            self._s()), "zb_swe2d_stage")
+            self._stage(cfg, Qk, Q0, out, alpha, beta, dt, hinv=hinv, tr=mask)
             Qk = out
         return Qk, bool(mask.any())
 
