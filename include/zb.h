@@ -200,6 +200,50 @@ int zb_swe2d_mass(const zb_swe2d_cfg* cfg, const void* Q, double* partial,
 int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux,
                  zb_stream_t stream);
 
+/* ── batched ensemble of Cartesian instances ─────────────────────────────── */
+
+/* One independent instance of the ensemble (host description).  Its state
+ * is (4, nx*ny) at element offset q_offset of the batch state array and its
+ * stage buffer (3, nx*ny) at element offset ws_offset of the batch
+ * workspace.  Every other scheme field comes from the common config. */
+typedef struct {
+  int32_t nx, ny;
+  double dx, dy;
+  int64_t q_offset;
+  int64_t ws_offset;
+  double manning_n;
+  double t_end;
+} zb_ens_instance;
+
+/* Device bytes of the instance table + work list for a tile height of
+ * tile_x (8 or 16) cells; 0 if the configuration is not supported (the
+ * ensemble runs the order-2 eta reconstruction with HR-HLL, wall or
+ * extrapolation boundaries). */
+size_t zb_ens_table_bytes(const zb_swe2d_cfg* common,
+                          const zb_ens_instance* inst, int n_inst, int tile_x);
+
+/* Build the per-instance parameter blocks (spacing, least-squares weights,
+ * Manning, t_end) and the (instance, tile) work list, and copy them to the
+ * device table (synchronous host-to-device copies: call at set-up, outside
+ * stream capture).  *n_items_out receives the work-list length. */
+int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
+                   int n_inst, int tile_x, void* table, size_t table_bytes,
+                   int* n_items_out);
+
+/* Reset the n_inst control blocks ctrls[0..n_inst) and seed each instance's
+ * wave-speed maximum from its state (zb_swe2d_init per instance). */
+int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst,
+                const void* Q, zb_ctrl* ctrls, int phase, double t0,
+                zb_stream_t stream);
+
+/* One SSP-RK2 step of every instance: part 0 = the first-stage launch, 1 =
+ * the second, -1 = both.  Each launch is one persistent kernel whose CTAs
+ * walk the work list; grid <= 0 picks SMs x occupancy.  Each instance takes
+ * its own CFL dt (zb_swe2d_step semantics per instance). */
+int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst,
+                     int n_items, int tile_x, int grid, void* Q, void* W,
+                     zb_ctrl* ctrls, int phase, int part, zb_stream_t stream);
+
 /* ── unstructured triangles ─────────────────────────────────────────────── */
 
 /* Scheme of the triangle path (the Cartesian fields it shares keep their

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <mutex>
 #include <type_traits>
+#include <vector>
 
 #include "common.cuh"
 
@@ -192,64 +193,24 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R, T sg
   Dp = -(half * g * (R.h * R.h - hRs * hRs));
 }
 
-// ── the fused stage kernel ──────────────────────────────────────────────────
+// ── one tile of one stage ───────────────────────────────────────────────────
+// The body of a stage for the TX x 32 tile at (i0, j0), with the stage dt
+// already decided.  Shared by the single-grid kernel (one tile per CTA) and
+// the ensemble kernel (a persistent CTA walks (instance, tile) work items).
+// p may live in kernel-parameter space or in global memory.
 template <typename T, int TX, int ORDER, int RECON, int RIEMANN, int MODE>
-__global__ void __launch_bounds__(NT)
-swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
-                   const T* __restrict__ qxP, const T* __restrict__ qyP,
-                   const T* h0P, const T* qx0P, const T* qy0P,
-                   T* hO, T* qxO, T* qyO, zb_ctrl* ctrl, int phase,
-                   const T* __restrict__ hinv_src,
-                   const unsigned char* __restrict__ force_o1,
-                   unsigned char* __restrict__ trouble_out,
-                   const SweParams<T> p) {
+__device__ __forceinline__ void stage_tile(
+    Smem<T, TX>& s, double* red, const int i0, const int j0,
+    const T* __restrict__ bP, const T* __restrict__ hP, const T* __restrict__ qxP,
+    const T* __restrict__ qyP, const T* h0P, const T* qx0P, const T* qy0P, T* hO, T* qxO,
+    T* qyO, zb_ctrl* ctrl, const int phase, const T* __restrict__ hinv_src,
+    const unsigned char* __restrict__ force_o1, unsigned char* __restrict__ trouble_out,
+    const SweParams<T>& p, const double dtd, const bool lead_block) {
   using S = Smem<T, TX>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S& s = *reinterpret_cast<S*>(smem_raw);
-  __shared__ double red[NT / 32];
-
   const int tid = threadIdx.x;
   const int nx = p.nx, ny = p.ny;
-  const int i0 = blockIdx.y * TX, j0 = blockIdx.x * TY;
   const bool per_x = p.bc[0] == ZB_BC_PERIODIC;
   const bool per_y = p.bc[2] == ZB_BC_PERIODIC;
-
-  // dt of this step
-  double dtd;
-  if (MODE == MODE_STAGE) {
-    dtd = p.dt_stage >= 0.0 ? p.dt_stage : ctrl->dt;
-  } else {
-    const int ph = phase;
-    const int nph = (ph + 1) % 3, nnph = (ph + 2) % 3;
-    const double t = ctrl->t[ph];
-    dtd = dt_from_amax(ctrl->amax[ph], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
-    const bool ok = isfinite(dtd) && dtd > 0.0;
-    const bool lead = blockIdx.x == 0 && blockIdx.y == 0 && tid == 0;
-    if ((MODE == MODE_STEP1 || MODE == MODE_EULER) && lead) {
-      if (!ok && t < p.t_end) atomicOr(&ctrl->status, (unsigned)ZB_ST_DT_INVALID);
-      ctrl->dt = ok ? dtd : 0.0;
-      ctrl->t[nph] = ok ? t + dtd : t;
-      ctrl->amax[nnph] = 0.0;
-      ctrl->troubled = 0u;
-    }
-    if (!ok) {
-      // no-op step (t_end reached or dt invalid): the state is unchanged, so
-      // the next slot carries this slot's wave-speed maximum forward
-      if ((MODE == MODE_STEP2 || MODE == MODE_EULER) && lead) ctrl->amax[nph] = ctrl->amax[ph];
-      if (MODE == MODE_EULER) {
-        // the Euler path writes the workspace that is copied back: keep it equal
-        const int nx_ = p.nx, ny_ = p.ny;
-        for (int e = tid; e < TX * TY; e += NT) {
-          const int gi = i0 + e / TY, gj = j0 + e % TY;
-          if (gi < nx_ && gj < ny_) {
-            const size_t k = (size_t)gi * ny_ + gj;
-            hO[k] = hP[k]; qxO[k] = qxP[k]; qyO[k] = qyP[k];
-          }
-        }
-      }
-      return;
-    }
-  }
   const T dt = T(dtd);
 
   // ── phase A: halo-2 load, W transform ──
@@ -634,7 +595,158 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
     const double m = block_max_double(amax_loc, red);
     if (tid == 0) {
       atomic_max_pos_double(&ctrl->amax[(phase + 1) % 3], m);
-      if (blockIdx.x == 0 && blockIdx.y == 0) atomicAdd(&ctrl->steps, 1u);
+      if (lead_block) atomicAdd(&ctrl->steps, 1u);
+    }
+  }
+}
+
+// ── the fused stage kernel (one tile per CTA) ───────────────────────────────
+template <typename T, int TX, int ORDER, int RECON, int RIEMANN, int MODE>
+__global__ void __launch_bounds__(NT)
+swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
+                   const T* __restrict__ qxP, const T* __restrict__ qyP,
+                   const T* h0P, const T* qx0P, const T* qy0P,
+                   T* hO, T* qxO, T* qyO, zb_ctrl* ctrl, int phase,
+                   const T* __restrict__ hinv_src,
+                   const unsigned char* __restrict__ force_o1,
+                   unsigned char* __restrict__ trouble_out,
+                   const SweParams<T> p) {
+  using S = Smem<T, TX>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+  __shared__ double red[NT / 32];
+
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.y * TX, j0 = blockIdx.x * TY;
+
+  // dt of this step
+  double dtd;
+  if (MODE == MODE_STAGE) {
+    dtd = p.dt_stage >= 0.0 ? p.dt_stage : ctrl->dt;
+  } else {
+    const int ph = phase;
+    const int nph = (ph + 1) % 3, nnph = (ph + 2) % 3;
+    const double t = ctrl->t[ph];
+    dtd = dt_from_amax(ctrl->amax[ph], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
+    const bool ok = isfinite(dtd) && dtd > 0.0;
+    const bool lead = blockIdx.x == 0 && blockIdx.y == 0 && tid == 0;
+    if ((MODE == MODE_STEP1 || MODE == MODE_EULER) && lead) {
+      if (!ok && t < p.t_end) atomicOr(&ctrl->status, (unsigned)ZB_ST_DT_INVALID);
+      ctrl->dt = ok ? dtd : 0.0;
+      ctrl->t[nph] = ok ? t + dtd : t;
+      ctrl->amax[nnph] = 0.0;
+      ctrl->troubled = 0u;
+    }
+    if (!ok) {
+      // no-op step (t_end reached or dt invalid): the state is unchanged, so
+      // the next slot carries this slot's wave-speed maximum forward
+      if ((MODE == MODE_STEP2 || MODE == MODE_EULER) && lead) ctrl->amax[nph] = ctrl->amax[ph];
+      if (MODE == MODE_EULER) {
+        // the Euler path writes the workspace that is copied back: keep it equal
+        const int nx_ = p.nx, ny_ = p.ny;
+        for (int e = tid; e < TX * TY; e += NT) {
+          const int gi = i0 + e / TY, gj = j0 + e % TY;
+          if (gi < nx_ && gj < ny_) {
+            const size_t k = (size_t)gi * ny_ + gj;
+            hO[k] = hP[k]; qxO[k] = qxP[k]; qyO[k] = qyP[k];
+          }
+        }
+      }
+      return;
+    }
+  }
+  stage_tile<T, TX, ORDER, RECON, RIEMANN, MODE>(
+      s, red, i0, j0, bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO, ctrl, phase, hinv_src,
+      force_o1, trouble_out, p, dtd, blockIdx.x == 0 && blockIdx.y == 0);
+}
+
+
+// ── batched ensemble: one persistent launch per stage over all instances ────
+// Each instance is an independent Cartesian grid with its own size, spacing,
+// Manning coefficient, dt and control block.  The work list holds one item
+// per (instance, tile): {instance, i0, j0, first-tile flag}.  A persistent CTA
+// walks items with a grid stride; every item is one stage_tile() call with its
+// instance's own dt (read from the instance's control slots), so the whole
+// ensemble advances one stage per launch.
+template <typename T>
+struct EnsDesc {
+  SweParams<T> p;
+  long long q_off;   // element offset of the instance's (4, C) state
+  long long ws_off;  // element offset of its (3, C) stage buffer
+};
+
+template <typename T, int TX, int ORDER, int RECON, int RIEMANN, int MODE>
+__global__ void __launch_bounds__(NT)
+ens_stage_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ items,
+                 int n_items, T* Q, T* W, zb_ctrl* ctrls, int phase) {
+  using S = Smem<T, TX>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+  __shared__ double red[NT / 32];
+  const int tid = threadIdx.x;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int4 w = items[it];
+    const EnsDesc<T>* d = desc + w.x;
+    const SweParams<T>& p = d->p;
+    zb_ctrl* ctrl = ctrls + w.x;
+    const size_t C = (size_t)p.nx * p.ny;
+    T* q = Q + d->q_off;
+    T* ws = W + d->ws_off;
+    const int ph = phase, nph = (ph + 1) % 3, nnph = (ph + 2) % 3;
+    const double t = ctrl->t[ph];
+    double dtd = dt_from_amax(ctrl->amax[ph], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
+    const bool ok = isfinite(dtd) && dtd > 0.0;
+    const bool lead = w.w != 0 && tid == 0;
+    __syncthreads();   // the previous item is done with shared memory
+    if (MODE == MODE_STEP1 && lead) {
+      if (!ok && t < p.t_end) atomicOr(&ctrl->status, (unsigned)ZB_ST_DT_INVALID);
+      ctrl->dt = ok ? dtd : 0.0;
+      ctrl->t[nph] = ok ? t + dtd : t;
+      ctrl->amax[nnph] = 0.0;
+    }
+    if (!ok) {
+      if (MODE == MODE_STEP2 && lead) ctrl->amax[nph] = ctrl->amax[ph];
+      continue;   // block-uniform: every thread of the CTA skips this item
+    }
+    if (MODE == MODE_STEP1) {
+      stage_tile<T, TX, ORDER, RECON, RIEMANN, MODE_STEP1>(
+          s, red, w.y, w.z, q, q + C, q + 2 * C, q + 3 * C, nullptr, nullptr, nullptr, ws,
+          ws + C, ws + 2 * C, ctrl, ph, nullptr, nullptr, nullptr, p, dtd, w.w != 0);
+    } else {
+      stage_tile<T, TX, ORDER, RECON, RIEMANN, MODE_STEP2>(
+          s, red, w.y, w.z, q, ws, ws + C, ws + 2 * C, q + C, q + 2 * C, q + 3 * C, q + C,
+          q + 2 * C, q + 3 * C, ctrl, ph, nullptr, nullptr, nullptr, p, dtd, w.w != 0);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT)
+ens_amax_kernel(const EnsDesc<T>* __restrict__ desc, const T* __restrict__ Q, zb_ctrl* ctrls,
+                int n_inst, int phase, double t0, T g, T eps) {
+  __shared__ double red[NT / 32];
+  for (int i = blockIdx.x; i < n_inst; i += gridDim.x) {
+    const EnsDesc<T>* d = desc + i;
+    const size_t C = (size_t)d->p.nx * d->p.ny;
+    const T* q = Q + d->q_off;
+    double m = 0.0;
+    for (size_t k = threadIdx.x; k < C; k += NT) {
+      const T h = q[C + k];
+      const T hi = kp_hinv(h, eps);
+      const T c = sqrt(g * nmax(h, T(0)));
+      m = nmax(m, (double)nmax(fabs(q[2 * C + k] * hi) + c, fabs(q[3 * C + k] * hi) + c));
+    }
+    __syncthreads();
+    m = block_max_double(m, red);
+    if (threadIdx.x == 0) {
+      zb_ctrl* ctrl = ctrls + i;
+      for (int j = 0; j < 3; ++j) { ctrl->amax[j] = 0.0; ctrl->t[j] = 0.0; }
+      ctrl->amax[phase] = m;
+      ctrl->t[phase] = t0;
+      ctrl->dt = 0.0;
+      ctrl->status = 0u;
+      ctrl->steps = 0u;
+      ctrl->troubled = 0u;
     }
   }
 }
@@ -974,6 +1086,62 @@ static int amax_into(const zb_swe2d_cfg* c, const T* Q, double* dst, cudaStream_
   return zb_launch_check();
 }
 
+
+// ── ensemble host side ──────────────────────────────────────────────────────
+template <typename T>
+static size_t ens_desc_bytes(int n_inst) {
+  return ((size_t)n_inst * sizeof(EnsDesc<T>) + 255) / 256 * 256;
+}
+
+static int ens_tiles(const zb_ens_instance& in, int tile_x) {
+  return ((in.nx + tile_x - 1) / tile_x) * ((in.ny + TY - 1) / TY);
+}
+
+static bool ens_valid(const zb_swe2d_cfg* c, const zb_ens_instance* inst, int n, int tile_x) {
+  if (!c || !inst || n < 1 || (tile_x != 8 && tile_x != 16)) return false;
+  if (c->order != 2 || c->recon != ZB_RECON_ETA || c->riemann != ZB_RIEMANN_HLL_HR) return false;
+  if (c->dtype != ZB_F32 && c->dtype != ZB_F64) return false;
+  for (int i = 0; i < 4; ++i)
+    if (c->bc[i] != ZB_BC_WALL && c->bc[i] != ZB_BC_EXTRAPOLATION) return false;
+  for (int i = 0; i < n; ++i)
+    if (inst[i].nx < 3 || inst[i].ny < 3 || !(inst[i].dx > 0) || !(inst[i].dy > 0) ||
+        inst[i].q_offset < 0 || inst[i].ws_offset < 0)
+      return false;
+  return true;
+}
+
+template <typename T, int TX>
+static int ens_launch(int part, const void* table, int n_inst, int n_items, int grid, void* Q,
+                      void* W, zb_ctrl* ctrls, int phase, cudaStream_t st) {
+  const EnsDesc<T>* desc = (const EnsDesc<T>*)table;
+  const int4* items = (const int4*)((const char*)table + ens_desc_bytes<T>(n_inst));
+  const size_t sm = sizeof(Smem<T, TX>);
+  int dev = 0;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 32) return ZB_E_UNSUPPORTED;
+  static unsigned mask1 = 0u, mask2 = 0u;
+  auto k1 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>;
+  auto k2 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>;
+  if (!(mask1 & (1u << dev))) {
+    ZB_CUDA_TRY(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    ZB_CUDA_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    mask1 |= 1u << dev;
+  }
+  (void)mask2;
+  if (grid <= 0) {
+    int per_sm = 0, sms = 0;
+    ZB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1, NT, sm));
+    ZB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    grid = std::max(1, per_sm) * sms;
+  }
+  grid = std::min(grid, n_items);
+  if (part == 0)
+    k1<<<grid, NT, sm, st>>>(desc, items, n_items, (T*)Q, (T*)W, ctrls, phase);
+  else
+    k2<<<grid, NT, sm, st>>>(desc, items, n_items, (T*)Q, (T*)W, ctrls, phase);
+  return zb_launch_check();
+}
+
 }  // namespace zb
 
 using namespace zb;
@@ -1154,6 +1322,92 @@ int zb_swe2d_step_noalloc(const zb_swe2d_cfg* cfg, void* Q, zb_ctrl* ctrl, int p
   const int rc = noalloc_scratch(&ws);
   if (rc != ZB_OK) return rc;
   return zb_swe2d_step(cfg, Q, ws, sizeof(g_noalloc_scratch), ctrl, phase, stream);
+}
+
+
+// ── ensemble C ABI ──────────────────────────────────────────────────────────
+size_t zb_ens_table_bytes(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
+                          int tile_x) {
+  if (!ens_valid(common, inst, n_inst, tile_x)) return 0;
+  size_t items = 0;
+  for (int i = 0; i < n_inst; ++i) items += (size_t)ens_tiles(inst[i], tile_x);
+  const size_t d = common->dtype == ZB_F64 ? ens_desc_bytes<double>(n_inst)
+                                           : ens_desc_bytes<float>(n_inst);
+  return d + items * sizeof(int4);
+}
+
+int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
+                   int tile_x, void* table, size_t table_bytes, int* n_items_out) {
+  if (!ens_valid(common, inst, n_inst, tile_x) || !table || !n_items_out) return ZB_E_ARG;
+  if (table_bytes < zb_ens_table_bytes(common, inst, n_inst, tile_x)) return ZB_E_ARG;
+  auto build = [&](auto tag) -> int {
+    using T = decltype(tag);
+    std::vector<EnsDesc<T>> desc(n_inst);
+    std::vector<int4> items;
+    for (int i = 0; i < n_inst; ++i) {
+      zb_swe2d_cfg c = *common;
+      c.nx = inst[i].nx;
+      c.ny = inst[i].ny;
+      c.dx = inst[i].dx;
+      c.dy = inst[i].dy;
+      c.manning_n = inst[i].manning_n;
+      c.t_end = inst[i].t_end;
+      std::memset(&desc[i], 0, sizeof(EnsDesc<T>));
+      desc[i].p = make_params<T>(&c, 0.0, 1.0);
+      desc[i].q_off = inst[i].q_offset;
+      desc[i].ws_off = inst[i].ws_offset;
+      int first = 1;
+      for (int i0 = 0; i0 < c.nx; i0 += tile_x)
+        for (int j0 = 0; j0 < c.ny; j0 += TY) {
+          items.push_back(make_int4(i, i0, j0, first));
+          first = 0;
+        }
+    }
+    const size_t db = ens_desc_bytes<T>(n_inst);
+    ZB_CUDA_TRY(cudaMemcpy(table, desc.data(), desc.size() * sizeof(EnsDesc<T>),
+                           cudaMemcpyHostToDevice));
+    ZB_CUDA_TRY(cudaMemcpy((char*)table + db, items.data(), items.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice));
+    *n_items_out = (int)items.size();
+    return ZB_OK;
+  };
+  return common->dtype == ZB_F64 ? build(double()) : build(float());
+}
+
+int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst, const void* Q,
+                zb_ctrl* ctrls, int phase, double t0, zb_stream_t stream) {
+  if (!common || !table || !Q || !ctrls || n_inst < 1 || phase < 0 || phase > 2) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int grid = std::min(n_inst, 148 * 8);
+  if (common->dtype == ZB_F64)
+    ens_amax_kernel<double><<<grid, NT, 0, st>>>((const EnsDesc<double>*)table, (const double*)Q,
+                                                 ctrls, n_inst, phase, t0, common->g,
+                                                 common->wet_dry_eps);
+  else
+    ens_amax_kernel<float><<<grid, NT, 0, st>>>((const EnsDesc<float>*)table, (const float*)Q,
+                                                ctrls, n_inst, phase, t0, (float)common->g,
+                                                (float)common->wet_dry_eps);
+  return zb_launch_check();
+}
+
+int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst, int n_items,
+                     int tile_x, int grid, void* Q, void* W, zb_ctrl* ctrls, int phase,
+                     int part, zb_stream_t stream) {
+  if (!common || !table || !Q || !W || !ctrls || n_inst < 1 || n_items < 1) return ZB_E_ARG;
+  if (phase < 0 || phase > 2 || part < -1 || part > 1) return ZB_E_ARG;
+  if (tile_x != 8 && tile_x != 16) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int pt = (part == 1 ? 1 : 0); pt <= (part == 0 ? 0 : 1); ++pt) {
+    int rc;
+    if (common->dtype == ZB_F64)
+      rc = tile_x == 8 ? ens_launch<double, 8>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st)
+                       : ens_launch<double, 16>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st);
+    else
+      rc = tile_x == 8 ? ens_launch<float, 8>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st)
+                       : ens_launch<float, 16>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st);
+    if (rc) return rc;
+  }
+  return ZB_OK;
 }
 
 }  // extern "C"

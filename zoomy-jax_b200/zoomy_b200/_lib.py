@@ -57,6 +57,12 @@ class ZbTriCfg(C.Structure):
                 ("degree", C.c_int32), ("dtype", C.c_int32)]
 
 
+class ZbEnsInstance(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("dx", C.c_double), ("dy", C.c_double),
+                ("q_offset", C.c_int64), ("ws_offset", C.c_int64),
+                ("manning_n", C.c_double), ("t_end", C.c_double)]
+
+
 TRI_MESH_FIELDS = ["lsq_idx", "lsq_wx", "lsq_wy", "cf_rx", "cf_ry", "cell_face",
                    "cell_inv_area", "face_a", "face_b", "face_nx", "face_ny", "face_len",
                    "face_rax", "face_ray", "face_rbx", "face_rby", "face_inr", "bf_kind",
@@ -87,6 +93,12 @@ SIGNATURES = [
     ("zb_swe2d_mass_partials", C.c_size_t, [_CFG]),
     ("zb_swe2d_mass", C.c_int, [_CFG, _P, _P, _P, _P]),
     ("zb_swe2d_aux", C.c_int, [_CFG, _P, _P, _P]),
+    ("zb_ens_table_bytes", C.c_size_t, [_CFG, _P, C.c_int, C.c_int]),
+    ("zb_ens_prepare", C.c_int, [_CFG, _P, C.c_int, C.c_int, _P, C.c_size_t,
+                                 C.POINTER(C.c_int)]),
+    ("zb_ens_init", C.c_int, [_CFG, _P, C.c_int, _P, _P, C.c_int, C.c_double, _P]),
+    ("zb_ens_step_part", C.c_int, [_CFG, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P,
+                                   _P, C.c_int, C.c_int, _P]),
     ("zb_tri_workspace_bytes", C.c_size_t, [_TCFG, _TMESH]),
     ("zb_tri_init", C.c_int, [_TCFG, _TMESH, _P, C.c_int, C.c_double, _P]),
     ("zb_tri_step", C.c_int, [_TCFG, _TMESH, _P, _P, C.c_size_t, _P, C.c_int, _P]),

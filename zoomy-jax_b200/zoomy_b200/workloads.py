@@ -49,3 +49,27 @@ def cartesian_centers(n, domain=(0.0, 1.0, 0.0, 1.0)):
 def dam_break_2048(n=2048, seed=0):
     """The 2048^2 configuration's initial state on the unit square."""
     return circular_dam_state(cartesian_centers(n), seed=seed)
+
+
+def ensemble_512(n_inst=512, seed=0, side=(64, 512)):
+    """Seeded ensemble of the batched configuration: sides log-uniform in
+    ``side`` (``round(64 * 8**U)``), dam height U[1.1, 3] inside radius 0.2
+    (depth 1 outside), Manning n U[0.01, 0.05], flat bed, fluid at rest.
+    Returns ``(sides, heights, manning)`` arrays."""
+    rng = np.random.default_rng(seed)
+    lo, hi = side
+    u = rng.uniform(0.0, 1.0, n_inst)
+    sides = np.rint(lo * (hi / lo) ** u).astype(np.int64)
+    heights = rng.uniform(1.1, 3.0, n_inst)
+    manning = rng.uniform(0.01, 0.05, n_inst)
+    return sides, heights, manning
+
+
+def ensemble_state(n, height):
+    """``(4, n*n)`` flat-bed circular dam of the given height on the unit
+    square (the ensemble instance's initial state)."""
+    xc = cartesian_centers(n)
+    r = np.sqrt((xc[0] - 0.5) ** 2 + (xc[1] - 0.5) ** 2)
+    h = np.where(r < 0.2, height, 1.0)
+    z = np.zeros_like(h)
+    return np.stack([z, h, z, z])
