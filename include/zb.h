@@ -244,6 +244,143 @@ int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst,
                      int n_items, int tile_x, int grid, void* Q, void* W,
                      zb_ctrl* ctrls, int phase, int part, zb_stream_t stream);
 
+/* ── Chorin pressure solve ─────────────────────────────────────────────────
+ * Variable-coefficient Poisson -div(c grad p) = f on an nx x ny Cartesian grid
+ * (c = clip(h, cmin, cmax), harmonic face means, Dirichlet p = 0), float64
+ * flexible CG preconditioned by a float32 geometric-multigrid V-cycle.
+ * Replaces the pressure solve of the reference's Chorin projection
+ * (zoomy_jax/fvm/solver_chorin_vam_jax.py:673-883: unpreconditioned GMRES on
+ * VAM's operator) and its corrector (:885-907). */
+typedef struct {
+  int32_t nx, ny;
+  double dx;
+  double cmin, cmax;
+  int32_t nu;            /* pre- and post-smoothing red-black sweeps          */
+  int32_t coarse_sweeps; /* symmetric sweep pairs on the coarsest level       */
+  int32_t coarsest;      /* stop coarsening at this side                      */
+} zb_poisson_cfg;
+
+/* The learned smoother: a two-level convolutional U-Net (c1 channels at full
+ * resolution, c2 at half resolution; (c1, c2) one of (8, 16), (16, 16),
+ * (16, 32), (24, 48) -- the last has 52.6k parameters -- tanh) with bf16
+ * weights and float32 accumulation.  Given a residual r it returns the
+ * correction s dx^2 / c * U([r / s, c / cmax]) (s = RMS of r, c the cell
+ * coefficient): a learned local smoother in place of the red-black
+ * sweeps of the level-0 multigrid smoothing.  Counterpart of the learned
+ * V-cycle smoother of the reference (zoomy_jax/gnn_blueprint/
+ * vcycle_structured_gnn.py:74-122, graph_mp_multibranch.py:9-16).  Weights are
+ * [Cout][Cin][3][3] per layer, layers e1 (2->c1), e2 (c1->c1), m1 (c1->c2),
+ * m2 (c2->c2), o1 (c2+c1->c1), out (c1->1), concatenated. */
+typedef struct zb_smoother {
+  int32_t c1, c2;
+  const void* w;          /* bf16 weights, device                            */
+  const float* b;         /* float32 biases, device                          */
+  float cmax;             /* coefficient normalisation                       */
+  void* act;              /* activation workspace, device                    */
+  size_t act_bytes;       /* >= zb_smoother_workspace_bytes(c1, c2, nx, ny)  */
+  int32_t max_nx, max_ny;
+} zb_smoother;
+
+/* Parameters of a (c1, c2) U-Net: returns weights + biases. */
+size_t zb_unet_param_count(int c1, int c2, size_t* n_weights, size_t* n_biases);
+size_t zb_smoother_workspace_bytes(int c1, int c2, int nx, int ny);
+
+/* x_out = x_in + S(f - A x_in) on one nx x ny grid (x_in may be NULL for a
+ * zero start; x_out may alias x_in); cx, cy are the float32 face
+ * coefficients, r_scratch holds nx*ny floats. */
+int zb_smoother_apply(const zb_smoother* smoother, const float* f,
+                      const float* x_in, float* x_out, const float* cx,
+                      const float* cy, float* r_scratch, int nx, int ny,
+                      double dx, int pre, zb_stream_t stream);
+
+/* Training state (device pointers).  Patches: batch images of n x n cells
+ * with their own face coefficients cx (batch, n+1, n) and cy (batch, n, n+1)
+ * and Dirichlet boundaries.  Loss = mean over the batch of
+ * |r - A S(r)|^2 / |r|^2, the residual left after one smoother application. */
+typedef struct {
+  int32_t c1, c2, batch, n;
+  float cmax;
+  float* w_master;        /* float32 master weights                          */
+  float* b_master;        /* float32 biases                                  */
+  float *m_w, *v_w, *m_b, *v_b;   /* Adam moments                            */
+  float *g_w, *g_b;       /* gradients                                       */
+  void* w_bf16;           /* bf16 weights used by the forward                */
+  void* b_shadow;         /* bf16 scratch for the bias update (>= n_biases)  */
+  void* act;              /* >= zb_unet_train_workspace_bytes(c1, c2, batch, n) */
+} zb_unet_trainer;
+
+size_t zb_unet_train_workspace_bytes(int c1, int c2, int batch, int n);
+
+/* y = S(r) for the batch (forward only, activations kept for backward). */
+int zb_unet_forward(const zb_unet_trainer* t, const float* r, const float* cx,
+                    const float* cy, double dx, float* y, zb_stream_t stream);
+
+/* Loss (into *loss_out, device float64, may be NULL) and its gradient with
+ * respect to the bf16 weights and the biases into g_w, g_b. */
+int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* cx,
+                     const float* cy, double dx, double* loss_out,
+                     zb_stream_t stream);
+
+/* One Adam step (lr, beta1 0.9, beta2 0.999, eps 1e-8; step counts from 1);
+ * refreshes the bf16 weights from the float32 master. */
+int zb_unet_adam(const zb_unet_trainer* t, float lr, int step, zb_stream_t stream);
+
+enum { ZB_PRECOND_NONE = 0, ZB_PRECOND_MG = 1, ZB_PRECOND_LEARNED = 2 };
+
+size_t zb_poisson_workspace_bytes(const zb_poisson_cfg* cfg);
+
+/* Byte offsets inside the workspace: [0] r, [1] z, [2] p, [3] q (float64
+ * Krylov vectors), [4] scalars (float64: b.b, r.r, p.q, p.r, z.q, alpha,
+ * beta, relative residual at index 7, iteration count at 8), [5] level-0
+ * float32 x, [6] level-0 float32 f, [7] number of levels, [8] first one-CTA level, [9] level-0
+ * float32 x-face coefficients, [10] y-face coefficients.  out holds 11. */
+int zb_poisson_layout(const zb_poisson_cfg* cfg, int64_t* out);
+
+/* Face coefficients of every level from the depth h (C values, dtype). */
+int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype,
+                     void* ws, size_t ws_bytes, zb_stream_t stream);
+
+/* q = A p (float64). */
+int zb_poisson_apply(const zb_poisson_cfg* cfg, void* ws, const double* p,
+                     double* q, zb_stream_t stream);
+
+/* z = M r: one V-cycle from zero (float32); precond ZB_PRECOND_*. */
+int zb_poisson_vcycle(const zb_poisson_cfg* cfg, void* ws, const float* r,
+                      float* z, int precond, const zb_smoother* smoother,
+                      zb_stream_t stream);
+
+/* b = -div(q*) / dt from the state Q (4, C) (face-averaged fluxes, walls). */
+int zb_poisson_rhs(const zb_poisson_cfg* cfg, const void* Q, int dtype,
+                   double dt, double* b, zb_stream_t stream);
+
+/* q -= dt * cell-averaged c_f grad p on the momentum rows of Q. */
+int zb_poisson_correct(const zb_poisson_cfg* cfg, void* ws, void* Q, int dtype,
+                       const double* p, double dt, zb_stream_t stream);
+
+/* Flexible CG (one-term, Notay): start computes r = b - A x, |b|, the first
+ * preconditioned direction; each iterate performs one iteration and leaves
+ * the relative residual |r| / |b| at scalar index 7.  Both are
+ * graph-capturable (no host sync, no allocation). */
+int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b,
+                 double* x, int precond, const zb_smoother* smoother,
+                 zb_stream_t stream);
+int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
+                   const zb_smoother* smoother, zb_stream_t stream);
+
+/* The whole solve as one CUDA graph (start + a conditional WHILE node over
+ * iterate): each launch runs from the current x until |r|/|b| <= tol or maxit
+ * iterations, without a host round trip; the iteration count is left at
+ * scalar index 8.  b, x, ws and the smoother are bound at creation.  Replaces
+ * the host GMRES loop of the reference's pressure step
+ * (zoomy_jax/fvm/solver_chorin_vam_jax.py:800-823). */
+typedef struct zb_fcg_graph zb_fcg_graph;
+int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b,
+                        double* x, int precond, const zb_smoother* smoother,
+                        double tol, int maxit, zb_fcg_graph** out,
+                        zb_stream_t stream);
+int zb_fcg_graph_launch(zb_fcg_graph* graph, zb_stream_t stream);
+void zb_fcg_graph_destroy(zb_fcg_graph* graph);
+
 /* ── unstructured triangles ─────────────────────────────────────────────── */
 
 /* Scheme of the triangle path (the Cartesian fields it shares keep their

@@ -1,0 +1,350 @@
+"""GPU parity of the Chorin pressure solve and the learned smoother (libzb)
+against the float64 oracle.
+
+Tolerances (stated here, checked below):
+* operator, right-hand side and corrector (float64): relative L-infinity
+  <= 1e-13 against the oracle;
+* V-cycle (float32 multigrid): relative L2 <= 2e-5 against the float64 oracle
+  V-cycle on the same residual;
+* FCG to 1e-8: the true float64 residual |b - A x| / |b| <= 1.05e-8, the
+  iteration count within 1 of the oracle's FCG, and the pressure within 1e-6
+  (relative L2) of the sparse direct solve;
+* U-Net forward (bf16 weights, float32 accumulation) relative L2 <= 1e-4,
+  gradients relative L2 <= 2e-3 per layer, against the float64 restatement
+  fed the same bf16-rounded weights.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from cases import circular_dam_state
+from oracle import mesh as OM
+from oracle import poisson as OP
+from oracle import swe as OS
+from oracle import unet as OU
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import zoomy_b200 as zb  # noqa: E402
+from zoomy_b200.fvm.chorin import (ChorinSolver, EllipticSolveError,  # noqa: E402
+                                   PoissonSolver)
+from zoomy_b200.learned import LearnedSmoother, PatchSet, SmootherTrainer  # noqa: E402
+from zoomy_b200.workloads import cartesian_centers  # noqa: E402
+
+DEV = torch.device("cuda")
+
+
+def depth(n, seed=0):
+    """Depth of the seeded dam break over bumps on an n x n grid."""
+    return circular_dam_state(cartesian_centers(n), seed=seed)[1].reshape(n, n)
+
+
+def rel_inf(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def gpu(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a).reshape(-1), dtype=dtype, device=DEV)
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 96), (96, 128)])
+def test_apply_matches_oracle(nx, ny):
+    rng = np.random.default_rng(1)
+    h = rng.uniform(0.0, 2.5, (nx, ny))
+    P = PoissonSolver(nx, ny, 1.0 / nx)
+    P.setup(gpu(h))
+    cx, cy = OP.face_coefficients(h)
+    p = rng.standard_normal((nx, ny))
+    q = P.apply(gpu(p)).cpu().numpy().reshape(nx, ny)
+    assert rel_inf(q, OP.apply(cx, cy, p, 1.0 / nx)) <= 1e-13
+    # level-0 float32 coefficients are the rounded float64 ones
+    assert np.array_equal(P.cx32.cpu().numpy().reshape(nx + 1, ny), cx.astype(np.float32))
+    assert np.array_equal(P.cy32.cpu().numpy().reshape(nx, ny + 1), cy.astype(np.float32))
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 128), (128, 96), (256, 256)])
+def test_vcycle_matches_oracle(nx, ny):
+    rng = np.random.default_rng(2)
+    h = depth(max(nx, ny))[:nx, :ny]
+    dx = 1.0 / nx
+    P = PoissonSolver(nx, ny, dx, coarse_sweeps=8, coarsest=4)
+    P.setup(gpu(h))
+    cx, cy = OP.face_coefficients(h)
+    H = OP.Hierarchy(cx, cy, dx, coarsest=4)
+    assert len(H.levels) == P.n_levels
+    r = rng.standard_normal((nx, ny))
+    z = P.vcycle(gpu(r, torch.float32)).cpu().numpy().astype(np.float64).reshape(nx, ny)
+    zo = OP.vcycle(H, r, nu=2, coarse_sweeps=8)
+    assert rel_l2(z, zo) <= 2e-5
+
+
+@pytest.mark.parametrize("precond", ["mg", "none"])
+def test_fcg_converges_to_direct_solve(precond):
+    n = 128 if precond == "mg" else 64
+    rng = np.random.default_rng(3)
+    h = depth(n, seed=4)
+    dx = 1.0 / n
+    cx, cy = OP.face_coefficients(h)
+    b = rng.standard_normal((n, n))
+    P = PoissonSolver(n, n, dx, coarse_sweeps=8, coarsest=4)
+    P.setup(gpu(h))
+    x, it, rel = P.solve(gpu(b), tol=1e-8, maxit=3000, precond=precond)
+    x = x.cpu().numpy().reshape(n, n)
+    true_rel = np.linalg.norm(b - OP.apply(cx, cy, x, dx)) / np.linalg.norm(b)
+    assert rel <= 1e-8 and true_rel <= 1.05e-8
+    assert abs(true_rel - rel) <= 1e-3 * rel + 1e-15
+    H = OP.Hierarchy(cx, cy, dx, coarsest=4)
+    if precond == "mg":
+        _, it_o, _ = OP.fcg(H, b, tol=1e-8, maxit=200, precond="mg")
+        assert abs(it - it_o) <= 1, (it, it_o)
+        assert it <= 20
+    xd = OP.direct_solve(cx, cy, b, dx)
+    assert rel_l2(x, xd) <= 1e-6
+
+
+def test_graph_and_stepwise_solves_agree():
+    n = 128
+    rng = np.random.default_rng(5)
+    h = depth(n, seed=6)
+    P = PoissonSolver(n, n, 1.0 / n)
+    P.setup(gpu(h))
+    b = gpu(rng.standard_normal(n * n))
+    x1, it1, rel1 = P.solve(b, tol=1e-10, maxit=100)
+    x1 = x1.clone()
+    x2, it2, rel2 = P.solve_stepwise(b, tol=1e-10, maxit=100)
+    assert it1 == it2 and rel1 == rel2
+    assert torch.equal(x1, x2)
+    # a second launch of the same graph repeats the solve exactly
+    x3, it3, _ = P.solve(b, tol=1e-10, maxit=100)
+    assert it3 == it1 and torch.equal(x3, x1)
+
+
+def test_maxit_stops_the_graph_loop():
+    n = 64
+    P = PoissonSolver(n, n, 1.0 / n)
+    P.setup(gpu(depth(n)))
+    b = gpu(np.random.default_rng(7).standard_normal(n * n))
+    _, it, rel = P.solve(b, tol=1e-14, maxit=3, precond="none")
+    assert it == 3 and rel > 1e-14
+
+
+def test_rhs_and_corrector_match_oracle():
+    n = 96
+    rng = np.random.default_rng(8)
+    h = depth(n)
+    dx = 1.0 / n
+    P = PoissonSolver(n, n, dx)
+    P.setup(gpu(h))
+    Q = np.stack([np.zeros(n * n), h.reshape(-1), rng.standard_normal(n * n),
+                  rng.standard_normal(n * n)])
+    Qg = gpu(Q).reshape(4, -1).contiguous()
+    dt = 1.7e-3
+    b = P.rhs(Qg, dt).cpu().numpy().reshape(n, n)
+    bo = OP.divergence_rhs(Q[2].reshape(n, n), Q[3].reshape(n, n), dt, dx)
+    assert rel_inf(b, bo) <= 1e-13
+    p = rng.standard_normal((n, n))
+    P.correct(Qg, gpu(p), dt)
+    cx, cy = OP.face_coefficients(h)
+    qx, qy = OP.corrector(Q[2].reshape(n, n), Q[3].reshape(n, n), p, cx, cy, dt, dx)
+    out = Qg.cpu().numpy()
+    assert rel_inf(out[2].reshape(n, n), qx) <= 1e-13
+    assert rel_inf(out[3].reshape(n, n), qy) <= 1e-13
+
+
+# ── U-Net kernels against the float64 restatement ─────────────────────────
+
+def _batch(B, n, seed):
+    rng = np.random.default_rng(seed)
+    r = rng.standard_normal((B, n, n)).astype(np.float32)
+    cx = rng.uniform(0.1, 2.0, (B, n + 1, n)).astype(np.float32)
+    cy = rng.uniform(0.1, 2.0, (B, n, n + 1)).astype(np.float32)
+    return r, cx, cy
+
+
+def _oracle_weights(sm):
+    w = OU.bf16_round(sm.w.cpu().numpy())
+    return OU.split(w, sm.b.cpu().numpy().astype(np.float64), sm.c1, sm.c2)
+
+
+@pytest.mark.parametrize("c1,c2", [(8, 16), (24, 48)])
+def test_unet_forward_and_gradients_match_oracle(c1, c2):
+    B, n = 3, 16
+    sm = LearnedSmoother(c1, c2, seed=11)
+    # give every layer non-trivial weights (the default output layer is small)
+    sm.w.mul_(4.0)
+    sm.b.normal_(0.0, 0.1, generator=torch.Generator(device=DEV).manual_seed(1))
+    sm.refresh()
+    tr = SmootherTrainer(sm, batch=B, n=n)
+    r, cx, cy = _batch(B, n, 12)
+    dx = 1.0 / 64
+    rg, cxg, cyg = (torch.as_tensor(a, device=DEV) for a in (r, cx, cy))
+    y = tr.forward(rg, cxg, cyg, dx).cpu().numpy().astype(np.float64)
+    Ws, bs = _oracle_weights(sm)
+    r64, cx64, cy64 = r.astype(np.float64), cx.astype(np.float64), cy.astype(np.float64)
+    yo, _ = OU.forward(Ws, bs, r64, cx64, cy64, dx, sm.cmax)
+    assert rel_l2(y, yo) <= 1e-4
+    loss = float(tr.loss_and_grad(rg, cxg, cyg, dx).item())
+    lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r64, cx64, cy64, dx, sm.cmax)
+    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    gw = tr.g_w.cpu().numpy().astype(np.float64)
+    gb = tr.g_b.cpu().numpy().astype(np.float64)
+    gWs, gbs = OU.split(gw, gb, c1, c2)
+    for k in range(6):
+        assert rel_l2(gWs[k], dWs[k]) <= 2e-3, (k, rel_l2(gWs[k], dWs[k]))
+        assert rel_l2(gbs[k], dbs[k]) <= 2e-3, (k, rel_l2(gbs[k], dbs[k]))
+
+
+def test_smoother_apply_matches_oracle():
+    nx, ny = 64, 48
+    sm = LearnedSmoother(16, 16, seed=3)
+    sm.w.mul_(3.0)
+    sm.refresh()
+    rng = np.random.default_rng(13)
+    h = rng.uniform(0.05, 2.5, (nx, ny))
+    cx, cy = OP.face_coefficients(h)
+    f = rng.standard_normal((nx, ny))
+    x = rng.standard_normal((nx, ny)) * 1e-3
+    dx = 1.0 / nx
+    g32 = lambda a: gpu(a, torch.float32)  # noqa: E731
+    out = sm.apply(nx, ny, g32(f), g32(cx), g32(cy), dx, x=g32(x)).cpu().numpy()
+    Ws, bs = _oracle_weights(sm)
+    cx32, cy32 = cx.astype(np.float32).astype(np.float64), cy.astype(np.float32).astype(np.float64)
+    f32, x32 = f.astype(np.float32).astype(np.float64), x.astype(np.float32).astype(np.float64)
+    ref = OU.smoother_apply(Ws, bs, f32, x32, cx32, cy32, dx, sm.cmax)
+    assert rel_l2(out.reshape(nx, ny).astype(np.float64), ref) <= 1e-4
+
+
+def test_adam_step_matches_formula():
+    sm = LearnedSmoother(8, 16, seed=5)
+    tr = SmootherTrainer(sm, batch=2, n=8, lr=1e-2)
+    r, cx, cy = (torch.as_tensor(a, device=DEV) for a in _batch(2, 8, 14))
+    w0 = sm.w.clone()
+    tr.step(r, cx, cy, 1.0 / 32)
+    g = tr.g_w
+    m = 0.1 * g
+    v = 0.001 * g * g
+    expect = w0 - 1e-2 * (m / 0.1) / (torch.sqrt(v / 0.001) + 1e-8)
+    assert torch.allclose(sm.w, expect, rtol=1e-5, atol=1e-7)
+    assert torch.equal(sm.w_bf16, sm.w.to(torch.bfloat16))
+
+
+# ── training and the learned preconditioner ───────────────────────────────
+
+def _patches(n_grid=128, patch=16, count=2048, seed=0):
+    rng = np.random.default_rng(seed)
+    h = depth(n_grid, seed=seed)
+    P = PoissonSolver(n_grid, n_grid, 1.0 / n_grid)
+    P.setup(gpu(h))
+    rec = []
+    P.solve_stepwise(gpu(rng.standard_normal(n_grid * n_grid)), tol=1e-8, maxit=50, record=rec)
+    fields = torch.stack(rec)
+    g = torch.Generator(device=DEV).manual_seed(seed)
+    r, cx, cy = PatchSet.cut(fields, P.cx32, P.cy32, n_grid, n_grid, patch, count, g)
+    return PatchSet(r, cx, cy, 1.0 / n_grid)
+
+
+def test_training_reduces_the_loss():
+    sm = LearnedSmoother(8, 16, seed=0)
+    tr = SmootherTrainer(sm, batch=32, n=16, lr=3e-3)
+    data = _patches()
+    hist = tr.fit(data, steps=300, log_every=50)
+    first, last = hist[0][1], hist[-1][1]
+    assert math.isfinite(last) and last < 0.7 * first, hist
+
+
+def test_learned_preconditioner_solves_to_tolerance():
+    n = 128
+    sm = LearnedSmoother(8, 16, seed=0)
+    SmootherTrainer(sm, batch=32, n=16).fit(_patches(), steps=300)
+    h = depth(n, seed=9)
+    dx = 1.0 / n
+    cx, cy = OP.face_coefficients(h)
+    b = np.random.default_rng(10).standard_normal((n, n))
+    P = PoissonSolver(n, n, dx)
+    P.setup(gpu(h))
+    x, it, rel = P.solve(gpu(b), tol=1e-8, maxit=200, precond="learned", smoother=sm)
+    x = x.cpu().numpy().reshape(n, n)
+    true_rel = np.linalg.norm(b - OP.apply(cx, cy, x, dx)) / np.linalg.norm(b)
+    assert rel <= 1e-8 and true_rel <= 1.05e-8
+    assert rel_l2(x, OP.direct_solve(cx, cy, b, dx)) <= 1e-6
+
+
+# ── the Chorin march ──────────────────────────────────────────────────────
+
+TAGS = ("left", "right", "bottom", "top")
+
+
+def _chorin(n, precond="mg", smoother=None, time_order=1, maxit=200, dtype="float64"):
+    state = circular_dam_state(cartesian_centers(n), seed=0)
+    model = zb.ShallowWater2D(boundary_conditions={t: "wall" for t in TAGS},
+                              initial_conditions=state)
+    nsm = zb.NumericalSystemModel.from_system_model(model, zb.ReconstructionSpec(2, "minmod"),
+                                                    "hll_hr")
+    mesh = zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n)
+    solver = ChorinSolver(pressure_tol=1e-8, pressure_maxit=maxit, time_order=time_order,
+                          precond=precond, smoother=smoother,
+                          compute_dt=zb.timestepping.adaptive(0.45, 2),
+                          reconstruction_variables="eta", free_surface_h_index=1,
+                          eps_wet=1e-6, dtype=dtype)
+    Q, Qaux = solver.setup_simulation(mesh, nsm)
+    return solver, Q, state
+
+
+def _oracle_stage(n, Q, dt):
+    om = OM.create_2d(0.0, 1.0, 0.0, 1.0, n, n)
+    bcs = {t: "wall" for t in TAGS}
+    scheme = OS.Scheme(order=2, limiter="minmod", recon="eta", riemann="hll_hr", eps_wet=1e-6,
+                       cfl=0.45, bc=bcs)
+    params = OS.Params()
+    kind = OS.bc_kinds(om, scheme)
+    Qs = Q + dt * OS.flux_operator(om, Q, scheme, params, kind)
+    h = Qs[1].reshape(n, n)
+    cx, cy = OP.face_coefficients(h)
+    dx = 1.0 / n
+    b = OP.divergence_rhs(Qs[2].reshape(n, n), Qs[3].reshape(n, n), dt, dx)
+    p = OP.direct_solve(cx, cy, b, dx)
+    qx, qy = OP.corrector(Qs[2].reshape(n, n), Qs[3].reshape(n, n), p, cx, cy, dt, dx)
+    out = Qs.copy()
+    out[2], out[3] = qx.reshape(-1), qy.reshape(-1)
+    return out, p
+
+
+def test_chorin_stage_matches_oracle():
+    n = 64
+    solver, Q, state = _chorin(n)
+    dt = solver.compute_timestep(Q)
+    Qn = solver.step(dt, 0.0, Q)
+    ref, p = _oracle_stage(n, state, dt)
+    got = Qn.cpu().numpy()
+    assert solver.last_elliptic_rel_resid <= 1e-8
+    assert rel_l2(solver.p.cpu().numpy().reshape(n, n), p) <= 1e-6
+    assert rel_inf(got[1], ref[1]) <= 1e-12          # the depth is the predictor's
+    for k in (2, 3):
+        assert rel_l2(got[k], ref[k]) <= 1e-6
+
+
+def test_chorin_march_conserves_mass_and_orders_agree():
+    n = 64
+    solver, Q, _ = _chorin(n, time_order=2)
+    m0 = solver.mass(Q)
+    dt = solver.compute_timestep(Q)
+    Q2, t = solver.run_jit_steps(dt, 5, Q)
+    assert abs(solver.mass(Q2) - m0) <= 1e-12 * m0
+    assert solver.last_elliptic_rel_resid <= 1e-8
+    assert math.isclose(t, 5 * dt)
+
+
+def test_missed_tolerance_raises():
+    solver, Q, _ = _chorin(32, maxit=1)
+    dt = solver.compute_timestep(Q)
+    with pytest.raises(EllipticSolveError, match="did NOT converge"):
+        solver.step(dt, 0.0, Q)

@@ -1,0 +1,1008 @@
+// Chorin pressure solve on B200: variable-coefficient Poisson, geometric
+// multigrid, flexible CG.
+//
+// Reference: zoomy_jax/fvm/solver_chorin_vam_jax.py -- chorin_stage (:524-572)
+// runs hyperbolic Euler -> pressure solve (_step_pressure_pure :673-883,
+// unpreconditioned restarted GMRES on VAM's operator) -> corrector
+// (_step_corrector_pure :885-907).  Here the pressure operator is
+//   (A p)_i = sum_f c_f (p_i - p_j) / dx^2,   Dirichlet ghost p_j = -p_i,
+// c_f the harmonic face mean of c = clip(h, cmin, cmax), the right-hand side
+// f = -div(q*) / dt, and the corrector q -= dt * cell-averaged c_f grad p.
+//
+// Precision: the Krylov vectors, the operator and the residual are float64;
+// the multigrid preconditioner runs in float32 (iterative refinement inside
+// flexible CG).  Multigrid: cell-centred factor-2 coarsening, coarse face
+// coefficient = mean of the two fine faces it covers, bilinear prolongation P
+// with odd reflection at the Dirichlet boundary, restriction R = P^T / 4,
+// red-black Gauss-Seidel (pre red/black, post black/red), a symmetric V-cycle.
+// Levels whose side is <= 64 run in ONE CTA with every array in shared memory
+// (their launches would otherwise be pure latency).  Layout: cell (i, j) at
+// i*ny + j; x-faces (nx+1, ny) at i*ny + j; y-faces (nx, ny+1) at i*(ny+1)+j.
+#include <cstring>
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace zb {
+namespace pois {
+
+constexpr int NT = 256;
+constexpr int MAXL = 16;
+constexpr int SMALL = 64;        // levels with nx, ny <= SMALL go to the one-CTA kernel
+constexpr int RED_BLOCKS = 592;  // 148 SMs x 4
+
+struct Level {
+  int nx, ny;
+  float dx;
+  long long cx, cy, dg, x, f, r;   // float offsets into the workspace
+};
+
+struct Plan {
+  int nlev, small0;          // number of levels, first one-CTA level
+  Level L[MAXL];
+  long long cx64, cy64, dg64;  // double offsets (level-0 operator)
+  long long vr, vz, vp, vq;    // double offsets (Krylov vectors)
+  long long part;              // double offset of the reduction partials
+  long long scal;              // double offset of the scalars
+  long long fbase;             // byte offset of the float region
+  long long bytes;
+  int nu, coarse_sweeps;
+  double dx;
+};
+
+// scalars (doubles) at plan.scal
+enum { S_BB = 0, S_RR, S_PQ, S_PR, S_ZQ, S_ALPHA, S_BETA, S_REL, S_ITER, S_COUNT = 16 };
+
+static Plan make_plan(const zb_poisson_cfg* c) {
+  Plan P;
+  std::memset(&P, 0, sizeof(P));
+  P.nu = c->nu;
+  P.coarse_sweeps = c->coarse_sweeps;
+  P.dx = c->dx;
+  int nx = c->nx, ny = c->ny;
+  float dx = (float)c->dx;
+  long long f = 0;
+  int l = 0;
+  P.small0 = -1;
+  while (l < MAXL) {
+    Level& L = P.L[l];
+    L.nx = nx;
+    L.ny = ny;
+    L.dx = dx;
+    L.cx = f; f += (long long)(nx + 1) * ny;
+    L.cy = f; f += (long long)nx * (ny + 1);
+    L.dg = f; f += (long long)nx * ny;
+    L.x = f; f += (long long)nx * ny;
+    L.f = f; f += (long long)nx * ny;
+    L.r = f; f += (long long)nx * ny;
+    if (P.small0 < 0 && nx <= SMALL && ny <= SMALL) P.small0 = l;
+    ++l;
+    if (nx <= c->coarsest || ny <= c->coarsest || (nx & 1) || (ny & 1)) break;
+    nx /= 2;
+    ny /= 2;
+    dx *= 2.0f;
+  }
+  P.nlev = l;
+  if (P.small0 < 0) P.small0 = l;   // no level small enough: no one-CTA part
+  const long long C = (long long)c->nx * c->ny;
+  long long d = 0;
+  P.cx64 = d; d += (long long)(c->nx + 1) * c->ny;
+  P.cy64 = d; d += (long long)c->nx * (c->ny + 1);
+  P.dg64 = d; d += C;
+  P.vr = d; d += C;
+  P.vz = d; d += C;
+  P.vp = d; d += C;
+  P.vq = d; d += C;
+  P.part = d; d += 4 * RED_BLOCKS;
+  P.scal = d; d += S_COUNT;
+  P.fbase = ((d * 8 + 255) / 256) * 256;
+  P.bytes = P.fbase + f * 4 + 256;
+  return P;
+}
+
+__device__ __forceinline__ double* D(void* ws, long long off) { return (double*)ws + off; }
+__device__ __forceinline__ float* F(void* ws, const Plan& P, long long off) {
+  return (float*)((char*)ws + P.fbase) + off;
+}
+
+// ── set-up kernels ──────────────────────────────────────────────────────────
+template <typename T>
+__global__ void coef_from_h(const T* __restrict__ h, int nx, int ny, double cmin, double cmax,
+                            double* cx64, double* cy64, float* cx32, float* cy32) {
+  const long long nfx = (long long)(nx + 1) * ny, nfy = (long long)nx * (ny + 1);
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < nfx + nfy;
+       k += (long long)gridDim.x * NT) {
+    double v;
+    if (k < nfx) {
+      const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+      const double a = i > 0 ? fmin(fmax((double)h[(long long)(i - 1) * ny + j], cmin), cmax) : -1.0;
+      const double b = i < nx ? fmin(fmax((double)h[(long long)i * ny + j], cmin), cmax) : -1.0;
+      v = (a < 0) ? b : (b < 0 ? a : 2.0 * a * b / (a + b));
+      cx64[k] = v;
+      cx32[k] = (float)v;
+    } else {
+      const long long kk = k - nfx;
+      const int i = (int)(kk / (ny + 1)), j = (int)(kk - (long long)i * (ny + 1));
+      const double a = j > 0 ? fmin(fmax((double)h[(long long)i * ny + j - 1], cmin), cmax) : -1.0;
+      const double b = j < ny ? fmin(fmax((double)h[(long long)i * ny + j], cmin), cmax) : -1.0;
+      v = (a < 0) ? b : (b < 0 ? a : 2.0 * a * b / (a + b));
+      cy64[kk] = v;
+      cy32[kk] = (float)v;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T diag_at(const T* cx, const T* cy, int nx, int ny, int i, int j, T idx2) {
+  const T a = cx[(long long)i * ny + j], b = cx[(long long)(i + 1) * ny + j];
+  const T c = cy[(long long)i * (ny + 1) + j], d = cy[(long long)i * (ny + 1) + j + 1];
+  T s = (a + b) + (c + d);
+  if (i == 0) s += a;
+  if (i == nx - 1) s += b;
+  if (j == 0) s += c;
+  if (j == ny - 1) s += d;
+  return s * idx2;
+}
+
+__global__ void diag_kernel64(const double* cx, const double* cy, int nx, int ny, double idx2,
+                              double* dg) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    dg[k] = diag_at<double>(cx, cy, nx, ny, i, j, idx2);
+  }
+}
+
+__global__ void diag_kernel32(const float* cx, const float* cy, int nx, int ny, float idx2,
+                              float* dg) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    dg[k] = diag_at<float>(cx, cy, nx, ny, i, j, idx2);
+  }
+}
+
+__global__ void coarsen_kernel(const float* cxf, const float* cyf, int nxc, int nyc, float* cxc,
+                               float* cyc) {
+  const int nyf = 2 * nyc;
+  const long long nfx = (long long)(nxc + 1) * nyc, nfy = (long long)nxc * (nyc + 1);
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < nfx + nfy;
+       k += (long long)gridDim.x * NT) {
+    if (k < nfx) {
+      const int I = (int)(k / nyc), J = (int)(k - (long long)I * nyc);
+      const long long f0 = (long long)(2 * I) * nyf + 2 * J;
+      cxc[k] = 0.5f * (cxf[f0] + cxf[f0 + 1]);
+    } else {
+      const long long kk = k - nfx;
+      const int I = (int)(kk / (nyc + 1)), J = (int)(kk - (long long)I * (nyc + 1));
+      const long long f0 = (long long)(2 * I) * (nyf + 1) + 2 * J;
+      cyc[kk] = 0.5f * (cyf[f0] + cyf[f0 + (nyf + 1)]);
+    }
+  }
+}
+
+// ── float64 Krylov kernels ──────────────────────────────────────────────────
+__device__ __forceinline__ double ghost_or(const double* p, int nx, int ny, int i, int j,
+                                           double self) {
+  return (i < 0 || i >= nx || j < 0 || j >= ny) ? -self : p[(long long)i * ny + j];
+}
+
+__device__ __forceinline__ void block_sum(double v, double* red, double* out) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double w = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    if (threadIdx.x == 0) *out = w;
+  }
+}
+
+// q = A p; partial[b] = sum p.q ; partial2[b] = sum p.r
+__global__ void __launch_bounds__(NT)
+apply_dot_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
+                 const double* __restrict__ p, const double* __restrict__ r,
+                 double* __restrict__ q, int nx, int ny, double idx2, double* part_pq,
+                 double* part_pr) {
+  __shared__ double red[NT / 32];
+  double spq = 0.0, spr = 0.0;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    const double pc = p[k];
+    const double v = (cx[(long long)(i + 1) * ny + j] * (pc - ghost_or(p, nx, ny, i + 1, j, pc)) +
+                      cx[(long long)i * ny + j] * (pc - ghost_or(p, nx, ny, i - 1, j, pc)) +
+                      cy[(long long)i * (ny + 1) + j + 1] * (pc - ghost_or(p, nx, ny, i, j + 1, pc)) +
+                      cy[(long long)i * (ny + 1) + j] * (pc - ghost_or(p, nx, ny, i, j - 1, pc))) *
+                     idx2;
+    if (q) q[k] = v;
+    spq += pc * v;
+    if (r) spr += pc * r[k];
+  }
+  block_sum(spq, red, &part_pq[blockIdx.x]);
+  __syncthreads();
+  if (part_pr) block_sum(spr, red, &part_pr[blockIdx.x]);
+}
+
+// generic dots: part_a[b] = sum a.b, part_c[b] = sum c.d (either may be null)
+__global__ void __launch_bounds__(NT)
+dot2_kernel(const double* __restrict__ a, const double* __restrict__ b,
+            const double* __restrict__ c, const double* __restrict__ d, long long n,
+            double* part_ab, double* part_cd) {
+  __shared__ double red[NT / 32];
+  double s1 = 0.0, s2 = 0.0;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
+    s1 += a[k] * b[k];
+    if (c) s2 += c[k] * d[k];
+  }
+  block_sum(s1, red, &part_ab[blockIdx.x]);
+  __syncthreads();
+  if (part_cd) block_sum(s2, red, &part_cd[blockIdx.x]);
+}
+
+// scal[dst] = sum of partials (fixed order: deterministic)
+__global__ void sum_partials_kernel(const double* part, int n, double* scal, int dst) {
+  __shared__ double red[NT / 32];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < n; k += NT) s += part[k];
+  block_sum(s, red, &scal[dst]);
+}
+
+// scalars of the FCG iteration
+__global__ void fcg_scalar_kernel(double* scal, int what) {
+  if (threadIdx.x != 0) return;
+  if (what == 0) {                       // alpha = p.r / p.q
+    const double pq = scal[S_PQ];
+    scal[S_ALPHA] = pq != 0.0 ? scal[S_PR] / pq : 0.0;
+  } else if (what == 1) {                // rel = sqrt(r.r / b.b)
+    scal[S_REL] = sqrt(scal[S_RR] / scal[S_BB]);
+  } else {                               // beta = z.q / p.q
+    const double pq = scal[S_PQ];
+    scal[S_BETA] = pq != 0.0 ? scal[S_ZQ] / pq : 0.0;
+  }
+}
+
+// x += alpha p ; r -= alpha q ; partial r.r ; r32 = (float) r
+__global__ void __launch_bounds__(NT)
+update_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                 const double* __restrict__ q, const double* scal, long long n,
+                 double* part_rr, float* __restrict__ r32) {
+  __shared__ double red[NT / 32];
+  const double a = scal[S_ALPHA];
+  double s = 0.0;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
+    x[k] += a * p[k];
+    const double rk = r[k] - a * q[k];
+    r[k] = rk;
+    s += rk * rk;
+    if (r32) r32[k] = (float)rk;
+  }
+  block_sum(s, red, &part_rr[blockIdx.x]);
+}
+
+// z = (double) z32 ; partial z.q
+__global__ void __launch_bounds__(NT)
+z_from32_kernel(const float* __restrict__ z32, double* __restrict__ z,
+                const double* __restrict__ q, long long n, double* part_zq) {
+  __shared__ double red[NT / 32];
+  double s = 0.0;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
+    const double v = (double)z32[k];
+    z[k] = v;
+    if (q) s += v * q[k];
+  }
+  if (part_zq) block_sum(s, red, &part_zq[blockIdx.x]);
+}
+
+// p = z - beta p
+__global__ void p_update_kernel(double* __restrict__ p, const double* __restrict__ z,
+                                const double* scal, long long n, int first) {
+  const double b = first ? 0.0 : scal[S_BETA];
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
+    p[k] = first ? z[k] : z[k] - b * p[k];
+}
+
+// r = b - A x ; partial r.r and b.b ; r32
+__global__ void __launch_bounds__(NT)
+residual64_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
+                  const double* __restrict__ x, const double* __restrict__ b,
+                  double* __restrict__ r, int nx, int ny, double idx2, double* part_rr,
+                  double* part_bb, float* __restrict__ r32) {
+  __shared__ double red[NT / 32];
+  double srr = 0.0, sbb = 0.0;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    const double pc = x[k];
+    const double ax = (cx[(long long)(i + 1) * ny + j] * (pc - ghost_or(x, nx, ny, i + 1, j, pc)) +
+                       cx[(long long)i * ny + j] * (pc - ghost_or(x, nx, ny, i - 1, j, pc)) +
+                       cy[(long long)i * (ny + 1) + j + 1] * (pc - ghost_or(x, nx, ny, i, j + 1, pc)) +
+                       cy[(long long)i * (ny + 1) + j] * (pc - ghost_or(x, nx, ny, i, j - 1, pc))) *
+                      idx2;
+    const double rk = b[k] - ax;
+    r[k] = rk;
+    srr += rk * rk;
+    sbb += b[k] * b[k];
+    if (r32) r32[k] = (float)rk;
+  }
+  block_sum(srr, red, &part_rr[blockIdx.x]);
+  __syncthreads();
+  block_sum(sbb, red, &part_bb[blockIdx.x]);
+}
+
+// ── float32 multigrid kernels ───────────────────────────────────────────────
+__device__ __forceinline__ float gx(const float* x, int nx, int ny, int i, int j, float self) {
+  return (i < 0 || i >= nx || j < 0 || j >= ny) ? -self : x[i * ny + j];
+}
+
+__device__ __forceinline__ float apply_at(const float* x, const float* cx, const float* cy,
+                                          int nx, int ny, int i, int j, float idx2,
+                                          float& offdiag_sum) {
+  const float xc = x[i * ny + j];
+  const float a = cx[(i + 1) * ny + j], b = cx[i * ny + j];
+  const float c = cy[i * (ny + 1) + j + 1], d = cy[i * (ny + 1) + j];
+  const float xe = gx(x, nx, ny, i + 1, j, xc), xw = gx(x, nx, ny, i - 1, j, xc);
+  const float xn = gx(x, nx, ny, i, j + 1, xc), xs = gx(x, nx, ny, i, j - 1, xc);
+  offdiag_sum = (a * xe + b * xw + c * xn + d * xs) * idx2;
+  return (a * (xc - xe) + b * (xc - xw) + c * (xc - xn) + d * (xc - xs)) * idx2;
+}
+
+// one red-black half sweep: x_i += (f_i - (A x)_i) / d_i on cells of `color`
+__global__ void __launch_bounds__(NT)
+rbgs_kernel(float* __restrict__ x, const float* __restrict__ f, const float* __restrict__ cx,
+            const float* __restrict__ cy, const float* __restrict__ dg, int nx, int ny,
+            float idx2, int color) {
+  const int half = (ny + 1) / 2;
+  for (long long t = blockIdx.x * (long long)NT + threadIdx.x; t < (long long)nx * half;
+       t += (long long)gridDim.x * NT) {
+    const int i = (int)(t / half), m = (int)(t - (long long)i * half);
+    const int j = 2 * m + ((i + color) & 1);
+    if (j >= ny) continue;
+    float od;
+    const float ax = apply_at(x, cx, cy, nx, ny, i, j, idx2, od);
+    x[i * ny + j] += (f[i * ny + j] - ax) / dg[i * ny + j];
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+residual32_kernel(const float* __restrict__ x, const float* __restrict__ f,
+                  const float* __restrict__ cx, const float* __restrict__ cy,
+                  float* __restrict__ r, int nx, int ny, float idx2) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    float od;
+    r[k] = f[k] - apply_at(x, cx, cy, nx, ny, i, j, idx2, od);
+  }
+}
+
+// Weight with which fine cell (fi, fj) interpolates from coarse cell (I, J)
+// under bilinear prolongation with odd reflection (see the oracle); R = P^T/4
+__device__ __forceinline__ float pweight(int fi, int fj, int I, int J, int nxc, int nyc) {
+  const int ci = fi >> 1, cj = fj >> 1;
+  const int sx = (fi & 1) ? 1 : -1, sy = (fj & 1) ? 1 : -1;
+  float w = 0.0f;
+  // the four coarse sources of the fine cell: (ci, cj) 9/16, (ci+sx, cj) 3/16,
+  // (ci, cj+sy) 3/16, (ci+sx, cj+sy) 1/16; an out-of-range source maps to the
+  // clipped in-range index with a minus sign per clipped axis
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    int ii = ci + ((s & 1) ? sx : 0), jj = cj + ((s & 2) ? sy : 0);
+    float ww = (s == 0) ? 9.0f / 16.0f : ((s == 3) ? 1.0f / 16.0f : 3.0f / 16.0f);
+    if (ii < 0 || ii >= nxc) { ii = ci; ww = -ww; }
+    if (jj < 0 || jj >= nyc) { jj = cj; ww = -ww; }
+    if (ii == I && jj == J) w += ww;
+  }
+  return w;
+}
+
+__global__ void __launch_bounds__(NT)
+restrict_kernel(const float* __restrict__ rf, float* __restrict__ fc, int nxc, int nyc) {
+  const int nyf = 2 * nyc;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nxc * nyc;
+       k += (long long)gridDim.x * NT) {
+    const int I = (int)(k / nyc), J = (int)(k - (long long)I * nyc);
+    float s = 0.0f;
+    for (int fi = 2 * I - 1; fi <= 2 * I + 2; ++fi) {
+      if (fi < 0 || fi >= 2 * nxc) continue;
+      for (int fj = 2 * J - 1; fj <= 2 * J + 2; ++fj) {
+        if (fj < 0 || fj >= nyf) continue;
+        const float w = pweight(fi, fj, I, J, nxc, nyc);
+        if (w != 0.0f) s += w * rf[fi * nyf + fj];
+      }
+    }
+    fc[k] = 0.25f * s;
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+prolong_add_kernel(const float* __restrict__ ec, float* __restrict__ xf, int nxc, int nyc) {
+  const int nxf = 2 * nxc, nyf = 2 * nyc;
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nxf * nyf;
+       k += (long long)gridDim.x * NT) {
+    const int fi = (int)(k / nyf), fj = (int)(k - (long long)fi * nyf);
+    const int ci = fi >> 1, cj = fj >> 1;
+    const int sx = (fi & 1) ? 1 : -1, sy = (fj & 1) ? 1 : -1;
+    float v = 0.0f;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      int ii = ci + ((s & 1) ? sx : 0), jj = cj + ((s & 2) ? sy : 0);
+      float ww = (s == 0) ? 9.0f / 16.0f : ((s == 3) ? 1.0f / 16.0f : 3.0f / 16.0f);
+      if (ii < 0 || ii >= nxc) { ii = ci; ww = -ww; }
+      if (jj < 0 || jj >= nyc) { jj = cj; ww = -ww; }
+      v += ww * ec[ii * nyc + jj];
+    }
+    xf[k] += v;
+  }
+}
+
+__global__ void zero32_kernel(float* x, long long n) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
+    x[k] = 0.0f;
+}
+
+__global__ void copy32_kernel(const float* a, float* b, long long n) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
+    b[k] = a[k];
+}
+
+// ── the one-CTA coarse V-cycle (levels small0 .. nlev-1 in shared memory) ───
+constexpr int CT = 1024;
+
+__device__ void cta_rbgs(float* x, const float* f, const float* cx, const float* cy,
+                         const float* dg, int nx, int ny, float idx2, int color) {
+  const int half = (ny + 1) / 2;
+  for (int t = threadIdx.x; t < nx * half; t += CT) {
+    const int i = t / half, m = t - i * half;
+    const int j = 2 * m + ((i + color) & 1);
+    if (j >= ny) continue;
+    float od;
+    const float ax = apply_at(x, cx, cy, nx, ny, i, j, idx2, od);
+    x[i * ny + j] += (f[i * ny + j] - ax) / dg[i * ny + j];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(CT)
+coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
+  extern __shared__ float sm[];
+  // shared copies of x, f, r, cx, cy, dg for every small level
+  float* sx[MAXL]; float* sf[MAXL]; float* sr[MAXL];
+  float* scx[MAXL]; float* scy[MAXL]; float* sdg[MAXL];
+  long long o = 0;
+  for (int l = P.small0; l < P.nlev; ++l) {
+    const Level& L = P.L[l];
+    const int n = L.nx * L.ny;
+    sx[l] = sm + o; o += n;
+    sf[l] = sm + o; o += n;
+    sr[l] = sm + o; o += n;
+    scx[l] = sm + o; o += (L.nx + 1) * L.ny;
+    scy[l] = sm + o; o += L.nx * (L.ny + 1);
+    sdg[l] = sm + o; o += n;
+  }
+  for (int l = P.small0; l < P.nlev; ++l) {
+    const Level& L = P.L[l];
+    const int n = L.nx * L.ny;
+    for (int k = threadIdx.x; k < (L.nx + 1) * L.ny; k += CT) scx[l][k] = ws_f[L.cx + k];
+    for (int k = threadIdx.x; k < L.nx * (L.ny + 1); k += CT) scy[l][k] = ws_f[L.cy + k];
+    for (int k = threadIdx.x; k < n; k += CT) {
+      sdg[l][k] = ws_f[L.dg + k];
+      sx[l][k] = 0.0f;
+      if (l == P.small0) sf[l][k] = ws_f[L.f + k];
+    }
+  }
+  __syncthreads();
+  // descend
+  for (int l = P.small0; l < P.nlev; ++l) {
+    const Level& L = P.L[l];
+    const float idx2 = 1.0f / (L.dx * L.dx);
+    if (l == P.nlev - 1) {
+      for (int s = 0; s < coarse_sweeps; ++s) {
+        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
+        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
+      }
+      for (int s = 0; s < coarse_sweeps; ++s) {
+        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
+        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
+      }
+      break;
+    }
+    for (int s = 0; s < nu; ++s) {
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
+    }
+    for (int k = threadIdx.x; k < L.nx * L.ny; k += CT) {
+      const int i = k / L.ny, j = k - i * L.ny;
+      float od;
+      sr[l][k] = sf[l][k] - apply_at(sx[l], scx[l], scy[l], L.nx, L.ny, i, j, idx2, od);
+    }
+    __syncthreads();
+    const Level& Lc = P.L[l + 1];
+    for (int k = threadIdx.x; k < Lc.nx * Lc.ny; k += CT) {
+      const int I = k / Lc.ny, J = k - I * Lc.ny;
+      float s = 0.0f;
+      for (int fi = 2 * I - 1; fi <= 2 * I + 2; ++fi) {
+        if (fi < 0 || fi >= L.nx) continue;
+        for (int fj = 2 * J - 1; fj <= 2 * J + 2; ++fj) {
+          if (fj < 0 || fj >= L.ny) continue;
+          const float w = pweight(fi, fj, I, J, Lc.nx, Lc.ny);
+          if (w != 0.0f) s += w * sr[l][fi * L.ny + fj];
+        }
+      }
+      sf[l + 1][k] = 0.25f * s;
+    }
+    __syncthreads();
+  }
+  // ascend
+  for (int l = P.nlev - 2; l >= P.small0; --l) {
+    const Level& L = P.L[l];
+    const Level& Lc = P.L[l + 1];
+    const float idx2 = 1.0f / (L.dx * L.dx);
+    for (int k = threadIdx.x; k < L.nx * L.ny; k += CT) {
+      const int fi = k / L.ny, fj = k - fi * L.ny;
+      const int ci = fi >> 1, cj = fj >> 1;
+      const int sxg = (fi & 1) ? 1 : -1, syg = (fj & 1) ? 1 : -1;
+      float v = 0.0f;
+      for (int s = 0; s < 4; ++s) {
+        int ii = ci + ((s & 1) ? sxg : 0), jj = cj + ((s & 2) ? syg : 0);
+        float ww = (s == 0) ? 9.0f / 16.0f : ((s == 3) ? 1.0f / 16.0f : 3.0f / 16.0f);
+        if (ii < 0 || ii >= Lc.nx) { ii = ci; ww = -ww; }
+        if (jj < 0 || jj >= Lc.ny) { jj = cj; ww = -ww; }
+        v += ww * sx[l + 1][ii * Lc.ny + jj];
+      }
+      sx[l][k] += v;
+    }
+    __syncthreads();
+    for (int s = 0; s < nu; ++s) {
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
+    }
+  }
+  const Level& L0 = P.L[P.small0];
+  for (int k = threadIdx.x; k < L0.nx * L0.ny; k += CT) ws_f[L0.x + k] = sx[P.small0][k];
+}
+
+static size_t coarse_smem(const Plan& P) {
+  size_t o = 0;
+  for (int l = P.small0; l < P.nlev; ++l) {
+    const Level& L = P.L[l];
+    const size_t n = (size_t)L.nx * L.ny;
+    o += 4 * n + (size_t)(L.nx + 1) * L.ny + (size_t)L.nx * (L.ny + 1);
+  }
+  return o * sizeof(float);
+}
+
+// opt the one-CTA kernel into the full 227 KB of shared memory (once per
+// device; called from set-up, never inside a stream capture)
+static int enable_coarse_smem() {
+  static unsigned set_mask = 0u;
+  int dev = 0;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 32 && !(set_mask & (1u << dev))) {
+    ZB_CUDA_TRY(cudaFuncSetAttribute(coarse_vcycle_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    set_mask |= 1u << dev;
+  }
+  return ZB_OK;
+}
+
+// loop control of the graph solve: counts the iteration and keeps the WHILE
+// node running while the relative residual is above tol (NaN stops it)
+__global__ void fcg_cond_kernel(double* scal, cudaGraphConditionalHandle h, double tol, int maxit,
+                                int first) {
+  if (threadIdx.x != 0) return;
+  const double it = first ? 0.0 : scal[S_ITER] + 1.0;
+  scal[S_ITER] = it;
+  const double rel = scal[S_REL];
+  const bool go = rel > tol && it < (double)maxit;   // false for NaN
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+static int grid_for(long long n) {
+  return (int)std::max<long long>(1, std::min<long long>((n + NT - 1) / NT, 148 * 8));
+}
+
+}  // namespace pois
+}  // namespace zb
+
+// ── coupling to the SWE state: right-hand side and corrector ────────────────
+namespace zb {
+namespace pois {
+
+template <typename T>
+__global__ void rhs_kernel(const T* __restrict__ qx, const T* __restrict__ qy, int nx, int ny,
+                           double inv_dt_dx, double* __restrict__ b) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    const double qc = (double)qx[k], pc = (double)qy[k];
+    const double fe = i + 1 < nx ? 0.5 * (qc + (double)qx[k + ny]) : 0.0;
+    const double fw = i > 0 ? 0.5 * ((double)qx[k - ny] + qc) : 0.0;
+    const double fn = j + 1 < ny ? 0.5 * (pc + (double)qy[k + 1]) : 0.0;
+    const double fs = j > 0 ? 0.5 * ((double)qy[k - 1] + pc) : 0.0;
+    b[k] = -((fe - fw) + (fn - fs)) * inv_dt_dx;
+  }
+}
+
+template <typename T>
+__global__ void correct_kernel(T* __restrict__ qx, T* __restrict__ qy,
+                               const double* __restrict__ cx, const double* __restrict__ cy,
+                               const double* __restrict__ p, int nx, int ny, double dt,
+                               double inv_dx) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
+       k += (long long)gridDim.x * NT) {
+    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
+    const double pc = p[k];
+    const double gw = cx[(long long)i * ny + j] * (pc - ghost_or(p, nx, ny, i - 1, j, pc)) * inv_dx;
+    const double ge = cx[(long long)(i + 1) * ny + j] * (ghost_or(p, nx, ny, i + 1, j, pc) - pc) * inv_dx;
+    const double gs = cy[(long long)i * (ny + 1) + j] * (pc - ghost_or(p, nx, ny, i, j - 1, pc)) * inv_dx;
+    const double gn = cy[(long long)i * (ny + 1) + j + 1] * (ghost_or(p, nx, ny, i, j + 1, pc) - pc) * inv_dx;
+    qx[k] = (T)((double)qx[k] - dt * 0.5 * (gw + ge));
+    qy[k] = (T)((double)qy[k] - dt * 0.5 * (gs + gn));
+  }
+}
+
+static bool valid(const zb_poisson_cfg* c) {
+  return c && c->nx >= 2 && c->ny >= 2 && c->dx > 0 && c->cmin > 0 && c->cmax >= c->cmin &&
+         c->nu >= 0 && c->coarse_sweeps >= 1 && c->coarsest >= 2 &&
+         (long long)c->nx * c->ny < (1LL << 31);
+}
+
+// z32 = M r32 on level 0 (f0 already holds r); precond: 0 none, 1 MG, 2 MG with
+// the level-0 smoothing replaced by the learned smoother
+static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, cudaStream_t st) {
+  float* fw = (float*)((char*)ws + P.fbase);
+  const Level& L0 = P.L[0];
+  const long long n0 = (long long)L0.nx * L0.ny;
+  if (precond == 0) {
+    copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + L0.f, fw + L0.x, n0);
+    return zb_launch_check();
+  }
+  for (int l = 0; l < P.small0 && l < P.nlev - 1; ++l) {
+    const Level& L = P.L[l];
+    const long long n = (long long)L.nx * L.ny;
+    const float idx2 = 1.0f / (L.dx * L.dx);
+    zero32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, n);
+    if (l == 0 && precond == 2) {
+      int rc = zb_smoother_apply(smo, fw + L.f, nullptr, fw + L.x, fw + L.cx, fw + L.cy,
+                                 fw + L.r, L.nx, L.ny, (double)L.dx, 1, (void*)st);
+      if (rc) return rc;
+    } else {
+      for (int s = 0; s < P.nu; ++s) {
+        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                        fw + L.dg, L.nx, L.ny, idx2, 0);
+        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                        fw + L.dg, L.nx, L.ny, idx2, 1);
+      }
+    }
+    residual32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                  fw + L.r, L.nx, L.ny, idx2);
+    const Level& Lc = P.L[l + 1];
+    restrict_kernel<<<grid_for((long long)Lc.nx * Lc.ny), NT, 0, st>>>(fw + L.r, fw + Lc.f, Lc.nx,
+                                                                        Lc.ny);
+  }
+  if (P.small0 < P.nlev) {
+    const size_t smem = coarse_smem(P);
+    coarse_vcycle_kernel<<<1, CT, smem, st>>>(P, fw, P.nu, P.coarse_sweeps);
+  } else {
+    // no level fits the one-CTA kernel: smooth the coarsest level in place
+    const Level& L = P.L[P.nlev - 1];
+    const long long n = (long long)L.nx * L.ny;
+    const float idx2 = 1.0f / (L.dx * L.dx);
+    zero32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, n);
+    for (int s = 0; s < 2 * P.coarse_sweeps; ++s) {
+      const int c0 = s < P.coarse_sweeps ? 0 : 1;
+      rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                      fw + L.dg, L.nx, L.ny, idx2, c0);
+      rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                      fw + L.dg, L.nx, L.ny, idx2, 1 - c0);
+    }
+  }
+  for (int l = std::min(P.small0, P.nlev - 1) - 1; l >= 0; --l) {
+    const Level& L = P.L[l];
+    const Level& Lc = P.L[l + 1];
+    const long long n = (long long)L.nx * L.ny;
+    const float idx2 = 1.0f / (L.dx * L.dx);
+    prolong_add_kernel<<<grid_for(n), NT, 0, st>>>(fw + Lc.x, fw + L.x, Lc.nx, Lc.ny);
+    if (l == 0 && precond == 2) {
+      int rc = zb_smoother_apply(smo, fw + L.f, fw + L.x, fw + L.x, fw + L.cx, fw + L.cy,
+                                 fw + L.r, L.nx, L.ny, (double)L.dx, 0, (void*)st);
+      if (rc) return rc;
+    } else {
+      for (int s = 0; s < P.nu; ++s) {
+        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                        fw + L.dg, L.nx, L.ny, idx2, 1);
+        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                        fw + L.dg, L.nx, L.ny, idx2, 0);
+      }
+    }
+  }
+  return zb_launch_check();
+}
+
+}  // namespace pois
+}  // namespace zb
+
+using namespace zb;
+using namespace zb::pois;
+
+extern "C" {
+
+size_t zb_poisson_workspace_bytes(const zb_poisson_cfg* cfg) {
+  if (!valid(cfg)) return 0;
+  return (size_t)make_plan(cfg).bytes;
+}
+
+int zb_poisson_layout(const zb_poisson_cfg* cfg, int64_t* out) {
+  if (!valid(cfg) || !out) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  // byte offsets: r, z, p, q (float64 Krylov vectors), scalars, level-0 float
+  // arrays x and f, number of levels, first one-CTA level
+  out[0] = P.vr * 8;
+  out[1] = P.vz * 8;
+  out[2] = P.vp * 8;
+  out[3] = P.vq * 8;
+  out[4] = P.scal * 8;
+  out[5] = P.fbase + P.L[0].x * 4;
+  out[6] = P.fbase + P.L[0].f * 4;
+  out[7] = P.nlev;
+  out[8] = P.small0;
+  out[9] = P.fbase + P.L[0].cx * 4;
+  out[10] = P.fbase + P.L[0].cy * 4;
+  return ZB_OK;
+}
+
+int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* ws,
+                     size_t wsb, zb_stream_t stream) {
+  if (!valid(cfg) || !h || !ws || (dtype != ZB_F32 && dtype != ZB_F64)) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  if (wsb < (size_t)P.bytes) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* fw = (float*)((char*)ws + P.fbase);
+  double* dw = (double*)ws;
+  const Level& L0 = P.L[0];
+  const long long nf = (long long)(L0.nx + 1) * L0.ny + (long long)L0.nx * (L0.ny + 1);
+  if (dtype == ZB_F64)
+    coef_from_h<double><<<grid_for(nf), NT, 0, st>>>((const double*)h, L0.nx, L0.ny, cfg->cmin,
+                                                     cfg->cmax, dw + P.cx64, dw + P.cy64,
+                                                     fw + L0.cx, fw + L0.cy);
+  else
+    coef_from_h<float><<<grid_for(nf), NT, 0, st>>>((const float*)h, L0.nx, L0.ny, cfg->cmin,
+                                                    cfg->cmax, dw + P.cx64, dw + P.cy64,
+                                                    fw + L0.cx, fw + L0.cy);
+  if (P.small0 < P.nlev) {
+    if (coarse_smem(P) > 227 * 1024) return ZB_E_TOO_LARGE;
+    if (const int e = enable_coarse_smem()) return e;
+  }
+  const long long n0 = (long long)L0.nx * L0.ny;
+  diag_kernel64<<<grid_for(n0), NT, 0, st>>>(dw + P.cx64, dw + P.cy64, L0.nx, L0.ny,
+                                             1.0 / (cfg->dx * cfg->dx), dw + P.dg64);
+  for (int l = 0; l < P.nlev; ++l) {
+    const Level& L = P.L[l];
+    if (l > 0) {
+      const Level& Lf = P.L[l - 1];
+      const long long nfc = (long long)(L.nx + 1) * L.ny + (long long)L.nx * (L.ny + 1);
+      coarsen_kernel<<<grid_for(nfc), NT, 0, st>>>(fw + Lf.cx, fw + Lf.cy, L.nx, L.ny, fw + L.cx,
+                                                   fw + L.cy);
+    }
+    diag_kernel32<<<grid_for((long long)L.nx * L.ny), NT, 0, st>>>(
+        fw + L.cx, fw + L.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.dg);
+  }
+  return zb_launch_check();
+}
+
+int zb_poisson_apply(const zb_poisson_cfg* cfg, void* ws, const double* p, double* q,
+                     zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !p || !q) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  cudaStream_t st = (cudaStream_t)stream;
+  double* dw = (double*)ws;
+  apply_dot_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, p, nullptr, q, cfg->nx,
+                                              cfg->ny, 1.0 / (cfg->dx * cfg->dx), dw + P.part,
+                                              nullptr);
+  return zb_launch_check();
+}
+
+int zb_poisson_vcycle(const zb_poisson_cfg* cfg, void* ws, const float* r, float* z, int precond,
+                      const zb_smoother* smo, zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !r || !z || precond < 0 || precond > 2) return ZB_E_ARG;
+  if (precond == 2 && !smo) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  cudaStream_t st = (cudaStream_t)stream;
+  float* fw = (float*)((char*)ws + P.fbase);
+  const long long n0 = (long long)cfg->nx * cfg->ny;
+  copy32_kernel<<<grid_for(n0), NT, 0, st>>>(r, fw + P.L[0].f, n0);
+  int rc = vcycle(P, ws, precond, smo, st);
+  if (rc) return rc;
+  copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + P.L[0].x, z, n0);
+  return zb_launch_check();
+}
+
+int zb_poisson_rhs(const zb_poisson_cfg* cfg, const void* Q, int dtype, double dt, double* b,
+                   zb_stream_t stream) {
+  if (!valid(cfg) || !Q || !b || !(dt > 0.0)) return ZB_E_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)cfg->nx * cfg->ny;
+  const double s = 1.0 / (dt * cfg->dx);
+  if (dtype == ZB_F64)
+    rhs_kernel<double><<<grid_for(n), NT, 0, st>>>((const double*)Q + 2 * n,
+                                                   (const double*)Q + 3 * n, cfg->nx, cfg->ny, s, b);
+  else if (dtype == ZB_F32)
+    rhs_kernel<float><<<grid_for(n), NT, 0, st>>>((const float*)Q + 2 * n, (const float*)Q + 3 * n,
+                                                  cfg->nx, cfg->ny, s, b);
+  else
+    return ZB_E_ARG;
+  return zb_launch_check();
+}
+
+int zb_poisson_correct(const zb_poisson_cfg* cfg, void* ws, void* Q, int dtype, const double* p,
+                       double dt, zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !Q || !p || !(dt >= 0.0)) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  cudaStream_t st = (cudaStream_t)stream;
+  double* dw = (double*)ws;
+  const long long n = (long long)cfg->nx * cfg->ny;
+  if (dtype == ZB_F64)
+    correct_kernel<double><<<grid_for(n), NT, 0, st>>>((double*)Q + 2 * n, (double*)Q + 3 * n,
+                                                       dw + P.cx64, dw + P.cy64, p, cfg->nx,
+                                                       cfg->ny, dt, 1.0 / cfg->dx);
+  else if (dtype == ZB_F32)
+    correct_kernel<float><<<grid_for(n), NT, 0, st>>>((float*)Q + 2 * n, (float*)Q + 3 * n,
+                                                      dw + P.cx64, dw + P.cy64, p, cfg->nx,
+                                                      cfg->ny, dt, 1.0 / cfg->dx);
+  else
+    return ZB_E_ARG;
+  return zb_launch_check();
+}
+
+int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x, int precond,
+                 const zb_smoother* smo, zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !b || !x || precond < 0 || precond > 2) return ZB_E_ARG;
+  if (precond == 2 && !smo) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  cudaStream_t st = (cudaStream_t)stream;
+  double* dw = (double*)ws;
+  float* fw = (float*)((char*)ws + P.fbase);
+  const long long n = (long long)cfg->nx * cfg->ny;
+  double* part = dw + P.part;
+  double* scal = dw + P.scal;
+  residual64_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, x, b, dw + P.vr, cfg->nx,
+                                               cfg->ny, 1.0 / (cfg->dx * cfg->dx), part,
+                                               part + RED_BLOCKS, fw + P.L[0].f);
+  sum_partials_kernel<<<1, NT, 0, st>>>(part, RED_BLOCKS, scal, S_RR);
+  sum_partials_kernel<<<1, NT, 0, st>>>(part + RED_BLOCKS, RED_BLOCKS, scal, S_BB);
+  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 1);
+  int rc = vcycle(P, ws, precond, smo, st);
+  if (rc) return rc;
+  z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, nullptr, n, nullptr);
+  p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1);
+  return zb_launch_check();
+}
+
+int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
+                   const zb_smoother* smo, zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !x || precond < 0 || precond > 2) return ZB_E_ARG;
+  if (precond == 2 && !smo) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  cudaStream_t st = (cudaStream_t)stream;
+  double* dw = (double*)ws;
+  float* fw = (float*)((char*)ws + P.fbase);
+  const long long n = (long long)cfg->nx * cfg->ny;
+  double* part = dw + P.part;
+  double* scal = dw + P.scal;
+  apply_dot_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, dw + P.vp, dw + P.vr,
+                                              dw + P.vq, cfg->nx, cfg->ny,
+                                              1.0 / (cfg->dx * cfg->dx), part, part + RED_BLOCKS);
+  sum_partials_kernel<<<1, NT, 0, st>>>(part, RED_BLOCKS, scal, S_PQ);
+  sum_partials_kernel<<<1, NT, 0, st>>>(part + RED_BLOCKS, RED_BLOCKS, scal, S_PR);
+  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 0);
+  update_xr_kernel<<<RED_BLOCKS, NT, 0, st>>>(x, dw + P.vr, dw + P.vp, dw + P.vq, scal, n,
+                                              part + 2 * RED_BLOCKS, fw + P.L[0].f);
+  sum_partials_kernel<<<1, NT, 0, st>>>(part + 2 * RED_BLOCKS, RED_BLOCKS, scal, S_RR);
+  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 1);
+  int rc = vcycle(P, ws, precond, smo, st);
+  if (rc) return rc;
+  z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, dw + P.vq, n,
+                                             part + 3 * RED_BLOCKS);
+  sum_partials_kernel<<<1, NT, 0, st>>>(part + 3 * RED_BLOCKS, RED_BLOCKS, scal, S_ZQ);
+  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 2);
+  p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0);
+  return zb_launch_check();
+}
+
+
+// A whole FCG solve as one CUDA graph: the start, then a conditional WHILE
+// node whose body is one iteration plus the loop-control kernel.  One launch
+// runs to convergence (or maxit) with no host round trip; the iteration count
+// lands at scalar index 8 and the relative residual at index 7.
+struct zb_fcg_graph {
+  cudaGraphExec_t exec;
+  cudaGraph_t graph;
+};
+
+int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x,
+                        int precond, const zb_smoother* smo, double tol, int maxit,
+                        zb_fcg_graph** out, zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !b || !x || !out || precond < 0 || precond > 2 || maxit < 1 ||
+      !(tol >= 0.0))
+    return ZB_E_ARG;
+  if (precond == 2 && !smo) return ZB_E_ARG;
+  *out = nullptr;
+  (void)stream;   // capture runs on private streams; nothing executes here
+  const Plan P = make_plan(cfg);
+  double* scal = (double*)ws + P.scal;
+  cudaStream_t st = nullptr, body = nullptr;
+  ZB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  if (cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaStreamDestroy(st);
+    return ZB_E_CUDA;
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  int rc = ZB_OK;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) { cudaStreamDestroy(body); cudaStreamDestroy(st); return ZB_E_CUDA; }
+  do {
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr) != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault) != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    if ((rc = zb_fcg_start(cfg, ws, b, x, precond, smo, (void*)st))) break;
+    fcg_cond_kernel<<<1, 32, 0, st>>>(scal, h, tol, maxit, 1);
+    if (cudaGetLastError() != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, deps, ndeps, &np) != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    cudaGraph_t bg = np.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(body, bg, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    int rb = zb_fcg_iterate(cfg, ws, x, precond, smo, (void*)body);
+    fcg_cond_kernel<<<1, 32, 0, body>>>(scal, h, tol, maxit, 0);
+    cudaGraph_t bg2 = nullptr;
+    const cudaError_t eb = cudaStreamEndCapture(body, &bg2);
+    if (rb) { rc = rb; break; }
+    if (eb != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) { rc = ZB_E_CUDA; break; }
+  } while (0);
+  cudaGraph_t gout = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(st, &gout);
+  cudaStreamDestroy(body);
+  cudaStreamDestroy(st);
+  if (rc == ZB_OK && ee != cudaSuccess) rc = ZB_E_CUDA;
+  if (rc != ZB_OK) {
+    if (gout) cudaGraphDestroy(gout);
+    cudaGetLastError();
+    return rc;
+  }
+  if (cudaGraphInstantiate(&ex, gout, 0) != cudaSuccess) {
+    cudaGraphDestroy(gout);
+    cudaGetLastError();
+    return ZB_E_CUDA;
+  }
+  zb_fcg_graph* G = new zb_fcg_graph;
+  G->exec = ex;
+  G->graph = gout;
+  *out = G;
+  return ZB_OK;
+}
+
+int zb_fcg_graph_launch(zb_fcg_graph* G, zb_stream_t stream) {
+  if (!G) return ZB_E_ARG;
+  ZB_CUDA_TRY(cudaGraphLaunch(G->exec, (cudaStream_t)stream));
+  return ZB_OK;
+}
+
+void zb_fcg_graph_destroy(zb_fcg_graph* G) {
+  if (!G) return;
+  cudaGraphExecDestroy(G->exec);
+  cudaGraphDestroy(G->graph);
+  delete G;
+}
+
+}  // extern "C"

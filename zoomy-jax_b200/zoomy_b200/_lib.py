@@ -63,6 +63,31 @@ class ZbEnsInstance(C.Structure):
                 ("manning_n", C.c_double), ("t_end", C.c_double)]
 
 
+class ZbPoissonCfg(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("dx", C.c_double),
+                ("cmin", C.c_double), ("cmax", C.c_double), ("nu", C.c_int32),
+                ("coarse_sweeps", C.c_int32), ("coarsest", C.c_int32)]
+
+
+class ZbSmoother(C.Structure):
+    _fields_ = [("c1", C.c_int32), ("c2", C.c_int32), ("w", C.c_void_p),
+                ("b", C.c_void_p), ("cmax", C.c_float), ("act", C.c_void_p),
+                ("act_bytes", C.c_size_t), ("max_nx", C.c_int32), ("max_ny", C.c_int32)]
+
+
+class ZbUnetTrainer(C.Structure):
+    _fields_ = [("c1", C.c_int32), ("c2", C.c_int32), ("batch", C.c_int32), ("n", C.c_int32),
+                ("cmax", C.c_float),
+                ("w_master", C.c_void_p), ("b_master", C.c_void_p),
+                ("m_w", C.c_void_p), ("v_w", C.c_void_p), ("m_b", C.c_void_p),
+                ("v_b", C.c_void_p), ("g_w", C.c_void_p), ("g_b", C.c_void_p),
+                ("w_bf16", C.c_void_p), ("b_shadow", C.c_void_p), ("act", C.c_void_p)]
+
+
+PRECOND = {"none": 0, "mg": 1, "learned": 2}
+# scalar slots of the Poisson workspace (float64)
+S_REL, S_ITER = 7, 8
+
 TRI_MESH_FIELDS = ["lsq_idx", "lsq_wx", "lsq_wy", "cf_rx", "cf_ry", "cell_face",
                    "cell_inv_area", "face_a", "face_b", "face_nx", "face_ny", "face_len",
                    "face_rax", "face_ray", "face_rbx", "face_rby", "face_inr", "bf_kind",
@@ -79,6 +104,9 @@ _P = C.c_void_p
 _CFG = C.POINTER(ZbSwe2dCfg)
 _TCFG = C.POINTER(ZbTriCfg)
 _TMESH = C.POINTER(ZbTriMesh)
+_PCFG = C.POINTER(ZbPoissonCfg)
+_SMO = C.POINTER(ZbSmoother)
+_TRN = C.POINTER(ZbUnetTrainer)
 SIGNATURES = [
     ("zb_version", C.c_char_p, []),
     ("zb_swe2d_workspace_bytes", C.c_size_t, [_CFG]),
@@ -109,6 +137,28 @@ SIGNATURES = [
     ("zb_tri_aux", C.c_int, [_TCFG, _TMESH, _P, _P, _P]),
     ("zb_tri_mass_partials", C.c_size_t, []),
     ("zb_tri_mass", C.c_int, [_TCFG, _TMESH, _P, _P, _P, _P]),
+    ("zb_unet_param_count", C.c_size_t, [C.c_int, C.c_int, C.POINTER(C.c_size_t),
+                                         C.POINTER(C.c_size_t)]),
+    ("zb_smoother_workspace_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("zb_smoother_apply", C.c_int, [_SMO, _P, _P, _P, _P, _P, _P, C.c_int, C.c_int,
+                                    C.c_double, C.c_int, _P]),
+    ("zb_unet_train_workspace_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("zb_unet_forward", C.c_int, [_TRN, _P, _P, _P, C.c_double, _P, _P]),
+    ("zb_unet_backward", C.c_int, [_TRN, _P, _P, _P, C.c_double, _P, _P]),
+    ("zb_unet_adam", C.c_int, [_TRN, C.c_float, C.c_int, _P]),
+    ("zb_poisson_workspace_bytes", C.c_size_t, [_PCFG]),
+    ("zb_poisson_layout", C.c_int, [_PCFG, C.POINTER(C.c_int64)]),
+    ("zb_poisson_setup", C.c_int, [_PCFG, _P, C.c_int, _P, C.c_size_t, _P]),
+    ("zb_poisson_apply", C.c_int, [_PCFG, _P, _P, _P, _P]),
+    ("zb_poisson_vcycle", C.c_int, [_PCFG, _P, _P, _P, C.c_int, _SMO, _P]),
+    ("zb_poisson_rhs", C.c_int, [_PCFG, _P, C.c_int, C.c_double, _P, _P]),
+    ("zb_poisson_correct", C.c_int, [_PCFG, _P, _P, C.c_int, _P, C.c_double, _P]),
+    ("zb_fcg_start", C.c_int, [_PCFG, _P, _P, _P, C.c_int, _SMO, _P]),
+    ("zb_fcg_iterate", C.c_int, [_PCFG, _P, _P, C.c_int, _SMO, _P]),
+    ("zb_fcg_graph_create", C.c_int, [_PCFG, _P, _P, _P, C.c_int, _SMO, C.c_double, C.c_int,
+                                      C.POINTER(C.c_void_p), _P]),
+    ("zb_fcg_graph_launch", C.c_int, [_P, _P]),
+    ("zb_fcg_graph_destroy", None, [_P]),
 ]
 
 _lib = None
