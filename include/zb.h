@@ -281,6 +281,16 @@ typedef struct zb_smoother {
   int32_t max_nx, max_ny;
 } zb_smoother;
 
+/* Convolution engine of the U-Net's forward and data-gradient passes:
+ * 1 = tcgen05 implicit GEMM (bf16 operands, float32 accumulation; default),
+ * 0 = CUDA-core direct convolution (float32 operands).  Returns the previous
+ * setting (process-wide; any other value only queries). */
+int zb_unet_conv_impl(int impl);
+
+/* Error word of the tensor-core kernels: non-zero when a bounded wait timed
+ * out (the tile's outputs were not written).  Synchronous; clear != 0 resets. */
+int zb_unet_status(int clear);
+
 /* Parameters of a (c1, c2) U-Net: returns weights + biases. */
 size_t zb_unet_param_count(int c1, int c2, size_t* n_weights, size_t* n_biases);
 size_t zb_smoother_workspace_bytes(int c1, int c2, int nx, int ny);
@@ -295,8 +305,10 @@ int zb_smoother_apply(const zb_smoother* smoother, const float* f,
 
 /* Training state (device pointers).  Patches: batch images of n x n cells
  * with their own face coefficients cx (batch, n+1, n) and cy (batch, n, n+1)
- * and Dirichlet boundaries.  Loss = mean over the batch of
- * |r - A S(r)|^2 / |r|^2, the residual left after one smoother application. */
+ * and Dirichlet boundaries.  Residual loss = mean over the batch of
+ * |r - A S(r)|^2 / |r|^2, the residual left after one smoother application;
+ * see zb_unet_backward for the energy-norm loss.  Adam skips non-finite
+ * gradient entries. */
 typedef struct {
   int32_t c1, c2, batch, n;
   float cmax;
@@ -316,16 +328,25 @@ int zb_unet_forward(const zb_unet_trainer* t, const float* r, const float* cx,
                     const float* cy, double dx, float* y, zb_stream_t stream);
 
 /* Loss (into *loss_out, device float64, may be NULL) and its gradient with
- * respect to the bf16 weights and the biases into g_w, g_b. */
-int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* cx,
-                     const float* cy, double dx, double* loss_out,
-                     zb_stream_t stream);
+ * respect to the bf16 weights and the biases into g_w, g_b.  target NULL:
+ * the residual loss above; target = the exact errors e (A e = r, same shape as
+ * r): the energy-norm loss mean_b (d . A d) / (e . A e), d = e - S(r), the
+ * error left after the correction measured as conjugate gradients measure it.
+ * Images without signal (denominator <= 1e-30) are left out. */
+int zb_unet_backward(const zb_unet_trainer* t, const float* r,
+                     const float* target, const float* cx, const float* cy,
+                     double dx, double* loss_out, zb_stream_t stream);
 
 /* One Adam step (lr, beta1 0.9, beta2 0.999, eps 1e-8; step counts from 1);
  * refreshes the bf16 weights from the float32 master. */
 int zb_unet_adam(const zb_unet_trainer* t, float lr, int step, zb_stream_t stream);
 
-enum { ZB_PRECOND_NONE = 0, ZB_PRECOND_MG = 1, ZB_PRECOND_LEARNED = 2 };
+/* Preconditioners of the flexible CG: none (plain CG), the multigrid
+ * V-cycle, the V-cycle followed by one learned smoothing step on the finest
+ * level (x += S(r - A x), the learned post-smoother), or the V-cycle with the
+ * finest level's red-black sweeps replaced by the learned smoother. */
+enum { ZB_PRECOND_NONE = 0, ZB_PRECOND_MG = 1, ZB_PRECOND_LEARNED = 2,
+       ZB_PRECOND_LEARNED_REPLACE = 3 };
 
 size_t zb_poisson_workspace_bytes(const zb_poisson_cfg* cfg);
 

@@ -27,6 +27,12 @@ arithmetic float64 here):
 ``conv`` is a 3x3 cross-correlation with zero padding; weights are
 ``[Cout][Cin][3][3]``.  Loss over a batch of patches with Dirichlet walls:
 ``mean_b |r_b - A_b y_b|^2 / |r_b|^2``.
+
+``bf16_inputs=True`` mirrors the tensor-core engine: the input of every
+convolution of the forward pass and of every data-gradient convolution of the
+backward pass is rounded to bf16 (the MMA operands), while the weight
+gradients are formed from the unrounded float32 values (the CUDA-core
+weight-gradient kernel reads those).
 """
 from __future__ import annotations
 
@@ -78,16 +84,18 @@ def conv(x, W, b=None):
     return out
 
 
-def conv_back(x, W, g):
-    """Gradients of conv(x, W, b) for the output gradient g: (dx, dW, db)."""
+def conv_back(x, W, g, bf16_inputs=False):
+    """Gradients of conv(x, W, b) for the output gradient g: (dx, dW, db).
+    With ``bf16_inputs`` the data gradient is formed from g rounded to bf16."""
     cin, B, H, Wd = x.shape
     xp = np.pad(x, ((0, 0), (0, 0), (1, 1), (1, 1)))
+    gd = bf16_round(g) if bf16_inputs else g
     dW = np.zeros_like(W)
     dxp = np.zeros_like(xp)
     for dy in range(3):
         for dx in range(3):
             dW[:, :, dy, dx] = np.einsum("obhw,ibhw->oi", g, xp[:, :, dy:dy + H, dx:dx + Wd])
-            dxp[:, :, dy:dy + H, dx:dx + Wd] += np.einsum("oi,obhw->ibhw", W[:, :, dy, dx], g)
+            dxp[:, :, dy:dy + H, dx:dx + Wd] += np.einsum("oi,obhw->ibhw", W[:, :, dy, dx], gd)
     return dxp[:, :, 1:-1, 1:-1], dW, g.sum(axis=(1, 2, 3))
 
 
@@ -117,22 +125,23 @@ def apply_batch(cx, cy, x, dx):
             + cy[:, :, 1:] * (xc - xp[:, 1:-1, 2:]) + cy[:, :, :-1] * (xc - xp[:, 1:-1, :-2])) / dx ** 2
 
 
-def forward(Ws, bs, r, cx, cy, dx, cmax):
+def forward(Ws, bs, r, cx, cy, dx, cmax, bf16_inputs=False):
     """r (B, H, W) -> (y (B, H, W), cache).  Ws must already be bf16-rounded."""
+    rnd = bf16_round if bf16_inputs else (lambda a: a)
     B = r.shape[0]
     s = np.sqrt(np.mean(r.reshape(B, -1) ** 2, axis=1))
     s = np.maximum(s, 1e-30)
     c = cell_coefficient(cx, cy)
     x_in = np.stack([r / s[:, None, None], c / cmax])
-    e1 = np.tanh(conv(x_in, Ws[0], bs[0]))
-    e2 = np.tanh(conv(e1, Ws[1], bs[1]))
+    e1 = np.tanh(conv(rnd(x_in), Ws[0], bs[0]))
+    e2 = np.tanh(conv(rnd(e1), Ws[1], bs[1]))
     p = pool(e2)
-    m1 = np.tanh(conv(p, Ws[2], bs[2]))
-    m2 = np.tanh(conv(m1, Ws[3], bs[3]))
+    m1 = np.tanh(conv(rnd(p), Ws[2], bs[2]))
+    m2 = np.tanh(conv(rnd(m1), Ws[3], bs[3]))
     u = up(m2)
     cat = np.concatenate([u, e2])
-    o1 = np.tanh(conv(cat, Ws[4], bs[4]))
-    out = conv(o1, Ws[5], bs[5])[0]
+    o1 = np.tanh(conv(rnd(cat), Ws[4], bs[4]))
+    out = conv(rnd(o1), Ws[5], bs[5])[0]
     scale = s[:, None, None] * dx ** 2 / c
     y = scale * out
     cache = dict(x_in=x_in, e1=e1, e2=e2, p=p, m1=m1, m2=m2, u=u, cat=cat, o1=o1,
@@ -140,40 +149,54 @@ def forward(Ws, bs, r, cx, cy, dx, cmax):
     return y, cache
 
 
-def loss_and_grads(Ws, bs, r, cx, cy, dx, cmax):
-    """Loss ``mean_b |r - A y|^2 / |r|^2`` and its gradients (dWs, dbs)."""
+def loss_and_grads(Ws, bs, r, cx, cy, dx, cmax, bf16_inputs=False, target=None):
+    """Loss and its gradients (dWs, dbs).  Without ``target``: the residual
+    loss ``mean_b |r - A y|^2 / |r|^2``; with the exact errors ``target``
+    (``A e = r``): the energy-norm loss ``mean_b (d . A d) / (e . A e)``,
+    ``d = e - y``.  Images with a denominator <= 1e-30 are left out."""
     B = r.shape[0]
-    y, k = forward(Ws, bs, r, cx, cy, dx, cmax)
-    res = r - apply_batch(cx, cy, y, dx)
-    den = np.maximum(np.sum(r.reshape(B, -1) ** 2, axis=1), 1e-30)
-    loss = float(np.mean(np.sum(res.reshape(B, -1) ** 2, axis=1) / den))
-    dy = -2.0 * apply_batch(cx, cy, res, dx) / (B * den[:, None, None])
+    q = bf16_inputs
+    y, k = forward(Ws, bs, r, cx, cy, dx, cmax, bf16_inputs=q)
+    if target is None:
+        res = r - apply_batch(cx, cy, y, dx)
+        Ares = apply_batch(cx, cy, res, dx)
+        num = np.sum(res.reshape(B, -1) ** 2, axis=1)
+        den = np.sum(r.reshape(B, -1) ** 2, axis=1)
+    else:
+        res = target - y
+        Ares = apply_batch(cx, cy, res, dx)
+        num = np.sum((res * Ares).reshape(B, -1), axis=1)
+        den = np.sum((target * apply_batch(cx, cy, target, dx)).reshape(B, -1), axis=1)
+    ok = den > 1e-30
+    dsafe = np.where(ok, den, 1.0)
+    loss = float(np.sum(np.where(ok, num / dsafe, 0.0)) / B)
+    dy = np.where(ok[:, None, None], -2.0 * Ares / (B * dsafe[:, None, None]), 0.0)
     d_out = (dy * k["scale"])[None]
     dWs = [None] * 6
     dbs = [None] * 6
-    d_o1, dWs[5], dbs[5] = conv_back(k["o1"], Ws[5], d_out)
+    d_o1, dWs[5], dbs[5] = conv_back(k["o1"], Ws[5], d_out, q)
     d_o1 = d_o1 * (1.0 - k["o1"] ** 2)
-    d_cat, dWs[4], dbs[4] = conv_back(k["cat"], Ws[4], d_o1)
+    d_cat, dWs[4], dbs[4] = conv_back(k["cat"], Ws[4], d_o1, q)
     c2 = Ws[3].shape[0]
     d_u, d_e2_skip = d_cat[:c2], d_cat[c2:]
     C, Bb, H, W = d_u.shape
     d_m2 = d_u.reshape(C, Bb, H // 2, 2, W // 2, 2).sum(axis=(3, 5))
     d_m2 = d_m2 * (1.0 - k["m2"] ** 2)
-    d_m1, dWs[3], dbs[3] = conv_back(k["m1"], Ws[3], d_m2)
+    d_m1, dWs[3], dbs[3] = conv_back(k["m1"], Ws[3], d_m2, q)
     d_m1 = d_m1 * (1.0 - k["m1"] ** 2)
-    d_p, dWs[2], dbs[2] = conv_back(k["p"], Ws[2], d_m1)
+    d_p, dWs[2], dbs[2] = conv_back(k["p"], Ws[2], d_m1, q)
     d_e2 = up(d_p) / 4.0 + d_e2_skip
     d_e2 = d_e2 * (1.0 - k["e2"] ** 2)
-    d_e1, dWs[1], dbs[1] = conv_back(k["e1"], Ws[1], d_e2)
+    d_e1, dWs[1], dbs[1] = conv_back(k["e1"], Ws[1], d_e2, q)
     d_e1 = d_e1 * (1.0 - k["e1"] ** 2)
     _, dWs[0], dbs[0] = conv_back(k["x_in"], Ws[0], d_e1)
     return loss, dWs, dbs
 
 
-def smoother_apply(Ws, bs, f, x, cx, cy, dx, cmax):
+def smoother_apply(Ws, bs, f, x, cx, cy, dx, cmax, bf16_inputs=False):
     """One learned smoothing on a single grid: x + S(f - A x).
     cx (H+1, W), cy (H, W+1); x may be None (zero start)."""
     x0 = np.zeros_like(f) if x is None else x
     r = f - apply_batch(cx[None], cy[None], x0[None], dx)[0]
-    y, _ = forward(Ws, bs, r[None], cx[None], cy[None], dx, cmax)
+    y, _ = forward(Ws, bs, r[None], cx[None], cy[None], dx, cmax, bf16_inputs=bf16_inputs)
     return x0 + y[0]

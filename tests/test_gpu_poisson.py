@@ -9,9 +9,10 @@ Tolerances (stated here, checked below):
 * FCG to 1e-8: the true float64 residual |b - A x| / |b| <= 1.05e-8, the
   iteration count within 1 of the oracle's FCG, and the pressure within 1e-6
   (relative L2) of the sparse direct solve;
-* U-Net forward (bf16 weights, float32 accumulation) relative L2 <= 1e-4,
-  gradients relative L2 <= 2e-3 per layer, against the float64 restatement
-  fed the same bf16-rounded weights.
+* U-Net forward (bf16 weights, float32 accumulation) relative L2 <= 1e-4 on
+  the CUDA-core engine and <= 1e-3 on the tensor-core engine (bf16 operands,
+  mirrored by the oracle), gradients relative L2 <= 2e-3 / 5e-3 per layer,
+  against the float64 restatement fed the same bf16-rounded weights.
 """
 import math
 
@@ -31,6 +32,7 @@ if not torch.cuda.is_available():
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
 import zoomy_b200 as zb  # noqa: E402
+from zoomy_b200 import _lib as L  # noqa: E402
 from zoomy_b200.fvm.chorin import (ChorinSolver, EllipticSolveError,  # noqa: E402
                                    PoissonSolver)
 from zoomy_b200.learned import LearnedSmoother, PatchSet, SmootherTrainer  # noqa: E402
@@ -170,13 +172,26 @@ def _batch(B, n, seed):
     return r, cx, cy
 
 
+@pytest.fixture(params=[1, 0], ids=["tcgen05", "cuda_core"])
+def conv_impl(request):
+    """Run a U-Net test on the tensor-core engine (bf16 operands) and on the
+    CUDA-core engine (float32 operands); the oracle mirrors the rounding."""
+    lib = L.load()
+    prev = lib.zb_unet_conv_impl(request.param)
+    lib.zb_unet_status(1)
+    yield request.param
+    torch.cuda.synchronize()
+    assert lib.zb_unet_status(1) == 0, "a tensor-core wait timed out"
+    lib.zb_unet_conv_impl(prev)
+
+
 def _oracle_weights(sm):
     w = OU.bf16_round(sm.w.cpu().numpy())
     return OU.split(w, sm.b.cpu().numpy().astype(np.float64), sm.c1, sm.c2)
 
 
-@pytest.mark.parametrize("c1,c2", [(8, 16), (24, 48)])
-def test_unet_forward_and_gradients_match_oracle(c1, c2):
+@pytest.mark.parametrize("c1,c2", [(8, 16), (16, 32), (24, 48)])
+def test_unet_forward_and_gradients_match_oracle(c1, c2, conv_impl):
     B, n = 3, 16
     sm = LearnedSmoother(c1, c2, seed=11)
     # give every layer non-trivial weights (the default output layer is small)
@@ -190,20 +205,48 @@ def test_unet_forward_and_gradients_match_oracle(c1, c2):
     y = tr.forward(rg, cxg, cyg, dx).cpu().numpy().astype(np.float64)
     Ws, bs = _oracle_weights(sm)
     r64, cx64, cy64 = r.astype(np.float64), cx.astype(np.float64), cy.astype(np.float64)
-    yo, _ = OU.forward(Ws, bs, r64, cx64, cy64, dx, sm.cmax)
-    assert rel_l2(y, yo) <= 1e-4
+    q = conv_impl == 1
+    yo, _ = OU.forward(Ws, bs, r64, cx64, cy64, dx, sm.cmax, bf16_inputs=q)
+    assert rel_l2(y, yo) <= (1e-3 if q else 1e-4)
     loss = float(tr.loss_and_grad(rg, cxg, cyg, dx).item())
-    lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r64, cx64, cy64, dx, sm.cmax)
-    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r64, cx64, cy64, dx, sm.cmax, bf16_inputs=q)
+    assert abs(loss - lo) <= (1e-3 if q else 1e-4) * abs(lo)
     gw = tr.g_w.cpu().numpy().astype(np.float64)
     gb = tr.g_b.cpu().numpy().astype(np.float64)
     gWs, gbs = OU.split(gw, gb, c1, c2)
+    tol = 5e-3 if q else 2e-3
     for k in range(6):
-        assert rel_l2(gWs[k], dWs[k]) <= 2e-3, (k, rel_l2(gWs[k], dWs[k]))
-        assert rel_l2(gbs[k], dbs[k]) <= 2e-3, (k, rel_l2(gbs[k], dbs[k]))
+        assert rel_l2(gWs[k], dWs[k]) <= tol, (k, rel_l2(gWs[k], dWs[k]))
+        assert rel_l2(gbs[k], dbs[k]) <= tol, (k, rel_l2(gbs[k], dbs[k]))
 
 
-def test_smoother_apply_matches_oracle():
+def test_unet_energy_loss_gradients_match_oracle(conv_impl):
+    c1, c2, B, n = 8, 16, 4, 16
+    sm = LearnedSmoother(c1, c2, seed=21)
+    sm.w.mul_(4.0)
+    sm.refresh()
+    tr = SmootherTrainer(sm, batch=B, n=n)
+    r, cx, cy = _batch(B, n, 22)
+    dx = 1.0 / 64
+    e = (np.random.default_rng(23).standard_normal((B, n, n)) * dx ** 2).astype(np.float32)
+    e[1] = 0.0      # an image without signal drops out of the loss
+    rg, cxg, cyg, eg = (torch.as_tensor(a, device=DEV) for a in (r, cx, cy, e))
+    loss = float(tr.loss_and_grad(rg, cxg, cyg, dx, target=eg).item())
+    Ws, bs = _oracle_weights(sm)
+    q = conv_impl == 1
+    lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r.astype(np.float64), cx.astype(np.float64),
+                                     cy.astype(np.float64), dx, sm.cmax, bf16_inputs=q,
+                                     target=e.astype(np.float64))
+    assert math.isfinite(loss) and abs(loss - lo) <= (1e-3 if q else 1e-4) * abs(lo)
+    gWs, gbs = OU.split(tr.g_w.cpu().numpy().astype(np.float64),
+                        tr.g_b.cpu().numpy().astype(np.float64), c1, c2)
+    tol = 5e-3 if q else 2e-3
+    for k in range(6):
+        assert rel_l2(gWs[k], dWs[k]) <= tol, (k, rel_l2(gWs[k], dWs[k]))
+        assert rel_l2(gbs[k], dbs[k]) <= tol, (k, rel_l2(gbs[k], dbs[k]))
+
+
+def test_smoother_apply_matches_oracle(conv_impl):
     nx, ny = 64, 48
     sm = LearnedSmoother(16, 16, seed=3)
     sm.w.mul_(3.0)
@@ -219,8 +262,9 @@ def test_smoother_apply_matches_oracle():
     Ws, bs = _oracle_weights(sm)
     cx32, cy32 = cx.astype(np.float32).astype(np.float64), cy.astype(np.float32).astype(np.float64)
     f32, x32 = f.astype(np.float32).astype(np.float64), x.astype(np.float32).astype(np.float64)
-    ref = OU.smoother_apply(Ws, bs, f32, x32, cx32, cy32, dx, sm.cmax)
-    assert rel_l2(out.reshape(nx, ny).astype(np.float64), ref) <= 1e-4
+    ref = OU.smoother_apply(Ws, bs, f32, x32, cx32, cy32, dx, sm.cmax,
+                            bf16_inputs=conv_impl == 1)
+    assert rel_l2(out.reshape(nx, ny).astype(np.float64), ref) <= (1e-3 if conv_impl else 1e-4)
 
 
 def test_adam_step_matches_formula():

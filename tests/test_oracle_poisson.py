@@ -83,7 +83,8 @@ def test_bf16_rounding_matches_torch():
     assert np.array_equal(ours, theirs)
 
 
-def test_unet_backward_matches_finite_differences():
+@pytest.mark.parametrize("energy", [False, True], ids=["residual_loss", "energy_loss"])
+def test_unet_backward_matches_finite_differences(energy):
     c1, c2 = 8, 16
     rng = np.random.default_rng(8)
     nw, nb = OU.param_counts(c1, c2)
@@ -93,7 +94,9 @@ def test_unet_backward_matches_finite_differences():
     cx = rng.uniform(0.1, 2, (B, n + 1, n))
     cy = rng.uniform(0.1, 2, (B, n, n + 1))
     dx = 1.0 / n
-    _, dWs, dbs = OU.loss_and_grads(Ws, bs, r, cx, cy, dx, 2.0)
+    tgt = rng.standard_normal((B, n, n)) * dx ** 2 if energy else None
+    lg = lambda W_, b_: OU.loss_and_grads(W_, b_, r, cx, cy, dx, 2.0, target=tgt)  # noqa: E731
+    _, dWs, dbs = lg(Ws, bs)
     eps = 1e-6
     for layer in range(6):
         idx = tuple(int(rng.integers(0, s)) for s in Ws[layer].shape)
@@ -101,16 +104,14 @@ def test_unet_backward_matches_finite_differences():
         Wm = [W.copy() for W in Ws]
         Wp[layer][idx] += eps
         Wm[layer][idx] -= eps
-        fd = (OU.loss_and_grads(Wp, bs, r, cx, cy, dx, 2.0)[0]
-              - OU.loss_and_grads(Wm, bs, r, cx, cy, dx, 2.0)[0]) / (2 * eps)
+        fd = (lg(Wp, bs)[0] - lg(Wm, bs)[0]) / (2 * eps)
         assert abs(fd - dWs[layer][idx]) <= 1e-6 * max(1.0, abs(fd))
         j = int(rng.integers(0, bs[layer].shape[0]))
         bp = [b.copy() for b in bs]
         bm = [b.copy() for b in bs]
         bp[layer][j] += eps
         bm[layer][j] -= eps
-        fd = (OU.loss_and_grads(Ws, bp, r, cx, cy, dx, 2.0)[0]
-              - OU.loss_and_grads(Ws, bm, r, cx, cy, dx, 2.0)[0]) / (2 * eps)
+        fd = (lg(Ws, bp)[0] - lg(Ws, bm)[0]) / (2 * eps)
         assert abs(fd - dbs[layer][j]) <= 1e-6 * max(1.0, abs(fd))
 
 

@@ -1,0 +1,257 @@
+// 3x3 convolution as an implicit GEMM on the 5th-generation tensor cores
+// (tcgen05.mma, kind::f16 with bf16 operands, float32 accumulation in TMEM).
+//
+// GEMM view of one output tile: M = 128 pixels (an 8-wide by 16-tall block;
+// GEMM row m is pixel (x0 + m % 8, y0 + m / 8)), N = output channels rounded
+// up to 16, K = 9 taps x input channels rounded up to 16.  No im2col copy is
+// made: the input tile with its one-pixel halo (10 x 18 pixels) is staged once
+// in shared memory in the canonical no-swizzle K-major layout,
+//   byte(chunk, q) = chunk * (180 * 16) + q * 16,   q = halo pixel (y * 10 + x),
+// 8 consecutive channels (one 16-byte core-matrix row) per (chunk, q), so the
+// A operand of tap (dy, dx) is the same buffer with its descriptor start moved
+// by (dy * 10 + dx) * 16 bytes: rows of one 8-pixel line are 16 bytes apart
+// (the core matrix), successive lines 160 bytes apart (stride byte offset),
+// the two 8-channel halves of a K=16 step 2880 bytes apart (leading byte
+// offset).  The weights sit next to it as [tap][chunk][n][8 channels].  One
+// thread issues the 9 * Cin/16 MMAs of a tile and commits them to an
+// mbarrier; the four warps then read the accumulator rows they own out of TMEM
+// (tcgen05.ld 32x32b), add the bias, apply tanh and store float32 planes.
+// CTAs are persistent over the tiles; the weights are staged once per CTA.
+//
+// Every wait is bounded: on a timeout the kernel raises a flag in the error
+// word, skips the tile's stores, and still releases its TMEM columns.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace zb {
+namespace unet {
+
+constexpr int TCX = 8, TCY = 16;            // output tile (M = 128)
+constexpr int THX = TCX + 2, THY = TCY + 2; // halo tile
+constexpr int THP = THX * THY;              // 180 halo pixels
+constexpr int TC_THREADS = 128;
+constexpr unsigned TC_SPIN_LIMIT = 1u << 24;
+
+__host__ __device__ constexpr int pad16(int c) { return (c + 15) & ~15; }
+
+__host__ __device__ inline size_t tc_smem_bytes(int cinp, int coutp) {
+  return (size_t)cinp * THP * 2 + (size_t)9 * cinp * coutp * 2 + 64;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// canonical K-major, no-swizzle shared-memory matrix descriptor (sm_100)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;   // descriptor version for sm_100
+  // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+  return d;
+}
+
+// instruction descriptor: D f32, A and B bf16, both K-major, M = 128, N
+__device__ __forceinline__ uint32_t tc_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t"
+      "}\n"
+      :
+      : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :
+               : "r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t"
+      "}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// out[co][b][y][x] = act(bias[co] + sum_ci sum_tap w[co][ci][tap] in[ci][b][y+dy-1][x+dx-1])
+// with the input channels [0, cin_a) from inA and [cin_a, cin) from inB, the
+// input rounded to bf16, zero padding at the image border.  err (may be null)
+// receives 1 when an mbarrier wait timed out.
+__global__ void __launch_bounds__(TC_THREADS)
+conv3x3_tc(const float* __restrict__ inA, int cin_a, const float* __restrict__ inB, int cin,
+           const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
+           float* __restrict__ out, int cout, int B, int H, int W, int act, int tmem_cols,
+           unsigned* err) {
+  extern __shared__ __align__(128) unsigned char tc_sm[];
+  const int cinp = pad16(cin), coutp = pad16(cout);
+  const int nch = cinp / 8;
+  unsigned char* sA = tc_sm;
+  unsigned char* sB = tc_sm + (size_t)cinp * THP * 2;
+  unsigned long long* mbar = (unsigned long long*)(sB + (size_t)9 * cinp * coutp * 2);
+  uint32_t* tmem_slot = (uint32_t*)(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // weights: [tap][chunk][n][8] bf16, zero outside (cout, cin)
+  for (int e = tid; e < 9 * nch * coutp; e += TC_THREADS) {
+    const int n = e % coutp;
+    const int rest = e / coutp;
+    const int ch = rest % nch, tap = rest / nch;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ci = ch * 8 + k;
+      v[k] = (n < cout && ci < cin) ? w[((size_t)n * cin + ci) * 9 + tap] : __float2bfloat16(0.0f);
+    }
+    *(uint4*)(sB + ((size_t)(tap * nch + ch) * coutp + n) * 16) = *(const uint4*)v;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :
+                 : "r"(smem_u32(tmem_slot)), "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t mbar_a = smem_u32(mbar);
+  const uint32_t sA_a = smem_u32(sA), sB_a = smem_u32(sB);
+  const uint32_t idesc = tc_idesc(coutp);
+  const size_t plane = (size_t)B * H * W;
+  const int tiles_x = (W + TCX - 1) / TCX, tiles_y = (H + TCY - 1) / TCY;
+  const int ntiles = tiles_x * tiles_y * B;
+  uint32_t parity = 0;
+  bool failed = false;
+
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int b = t / (tiles_x * tiles_y);
+    const int r = t - b * tiles_x * tiles_y;
+    const int x0 = (r % tiles_x) * TCX, y0 = (r / tiles_x) * TCY;
+    const size_t img = (size_t)b * H * W;
+    // halo tile: one thread per (chunk, halo pixel), 8 channels -> 16 bytes
+    for (int e = tid; e < nch * THP; e += TC_THREADS) {
+      const int q = e % THP, ch = e / THP;
+      const int yy = y0 - 1 + q / THX, xx = x0 - 1 + q % THX;
+      __align__(16) __nv_bfloat16 v[8];
+      const bool inside = yy >= 0 && yy < H && xx >= 0 && xx < W;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int ci = ch * 8 + k;
+        float f = 0.0f;
+        if (inside && ci < cin) {
+          const float* src = ci < cin_a ? inA + (size_t)ci * plane
+                                        : inB + (size_t)(ci - cin_a) * plane;
+          f = src[img + (size_t)yy * W + xx];
+        }
+        v[k] = __float2bfloat16_rn(f);
+      }
+      *(uint4*)(sA + ((size_t)ch * THP + q) * 16) = *(const uint4*)v;
+    }
+    // make the generic-proxy stores visible to the tensor core's async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      uint32_t acc = 0;
+      for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap % 3;
+        for (int g = 0; g < cinp / 16; ++g) {
+          const uint32_t a = sA_a + (uint32_t)(2 * g) * (THP * 16) + (uint32_t)(dy * THX + dx) * 16;
+          const uint32_t bb = sB_a + (uint32_t)((tap * nch + 2 * g) * coutp) * 16;
+          tc_mma(tmem, tc_desc(a, THP * 16, THX * 16), tc_desc(bb, coutp * 16, 128), idesc, acc);
+          acc = 1;
+        }
+      }
+      tc_commit(mbar_a);
+    }
+    // wait for the tile's MMAs (bounded); the CTA agrees on the outcome so
+    // every warp takes the same path through the collective TMEM loads
+    bool done = false;
+    for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it) {
+      if (mbar_try_wait(mbar_a, parity)) { done = true; break; }
+    }
+    parity ^= 1u;
+    if (__syncthreads_or(done ? 0 : 1)) {
+      failed = true;
+      if (err && tid == 0) atomicExch(err, 1u);
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: warp w owns accumulator rows (pixels) 32w .. 32w+31
+    const int m = warp * 32 + lane;
+    const int x = x0 + (m % TCX), y = y0 + (m / TCX);
+    const bool store = x < W && y < H;
+    for (int c0 = 0; c0 < coutp; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int co = c0 + i;
+        if (store && co < cout) {
+          float s = v[i] + (bias ? bias[co] : 0.0f);
+          if (act) s = tanhf(s);
+          out[(size_t)co * plane + img + (size_t)y * W + x] = s;
+        }
+      }
+    }
+    // TMEM reads and smem reads of this tile complete before the next tile
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (failed) {
+    // give an in-flight MMA a bounded chance to land before releasing TMEM
+    for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it)
+      if (mbar_try_wait(mbar_a, parity ^ 1u)) break;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(tmem_cols)
+                 : "memory");
+  }
+}
+
+}  // namespace unet
+}  // namespace zb

@@ -648,8 +648,9 @@ static bool valid(const zb_poisson_cfg* c) {
          (long long)c->nx * c->ny < (1LL << 31);
 }
 
-// z32 = M r32 on level 0 (f0 already holds r); precond: 0 none, 1 MG, 2 MG with
-// the level-0 smoothing replaced by the learned smoother
+// z32 = M r32 on level 0 (f0 already holds r); precond: 0 none, 1 MG, 2 MG
+// followed by one learned smoothing step on level 0 (x += S(f - A x)), 3 MG
+// with the level-0 red-black smoothing replaced by the learned smoother
 static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, cudaStream_t st) {
   float* fw = (float*)((char*)ws + P.fbase);
   const Level& L0 = P.L[0];
@@ -663,7 +664,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     const long long n = (long long)L.nx * L.ny;
     const float idx2 = 1.0f / (L.dx * L.dx);
     zero32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, n);
-    if (l == 0 && precond == 2) {
+    if (l == 0 && precond == 3) {
       int rc = zb_smoother_apply(smo, fw + L.f, nullptr, fw + L.x, fw + L.cx, fw + L.cy,
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 1, (void*)st);
       if (rc) return rc;
@@ -704,7 +705,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     const long long n = (long long)L.nx * L.ny;
     const float idx2 = 1.0f / (L.dx * L.dx);
     prolong_add_kernel<<<grid_for(n), NT, 0, st>>>(fw + Lc.x, fw + L.x, Lc.nx, Lc.ny);
-    if (l == 0 && precond == 2) {
+    if (l == 0 && precond == 3) {
       int rc = zb_smoother_apply(smo, fw + L.f, fw + L.x, fw + L.x, fw + L.cx, fw + L.cy,
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 0, (void*)st);
       if (rc) return rc;
@@ -716,6 +717,11 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
                                                         fw + L.dg, L.nx, L.ny, idx2, 0);
       }
     }
+  }
+  if (precond == 2) {
+    int rc = zb_smoother_apply(smo, fw + L0.f, fw + L0.x, fw + L0.x, fw + L0.cx, fw + L0.cy,
+                               fw + L0.r, L0.nx, L0.ny, (double)L0.dx, 0, (void*)st);
+    if (rc) return rc;
   }
   return zb_launch_check();
 }
@@ -805,8 +811,8 @@ int zb_poisson_apply(const zb_poisson_cfg* cfg, void* ws, const double* p, doubl
 
 int zb_poisson_vcycle(const zb_poisson_cfg* cfg, void* ws, const float* r, float* z, int precond,
                       const zb_smoother* smo, zb_stream_t stream) {
-  if (!valid(cfg) || !ws || !r || !z || precond < 0 || precond > 2) return ZB_E_ARG;
-  if (precond == 2 && !smo) return ZB_E_ARG;
+  if (!valid(cfg) || !ws || !r || !z || precond < 0 || precond > 3) return ZB_E_ARG;
+  if (precond >= 2 && !smo) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
   cudaStream_t st = (cudaStream_t)stream;
   float* fw = (float*)((char*)ws + P.fbase);
@@ -857,8 +863,8 @@ int zb_poisson_correct(const zb_poisson_cfg* cfg, void* ws, void* Q, int dtype, 
 
 int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x, int precond,
                  const zb_smoother* smo, zb_stream_t stream) {
-  if (!valid(cfg) || !ws || !b || !x || precond < 0 || precond > 2) return ZB_E_ARG;
-  if (precond == 2 && !smo) return ZB_E_ARG;
+  if (!valid(cfg) || !ws || !b || !x || precond < 0 || precond > 3) return ZB_E_ARG;
+  if (precond >= 2 && !smo) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
   cudaStream_t st = (cudaStream_t)stream;
   double* dw = (double*)ws;
@@ -881,8 +887,8 @@ int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x
 
 int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
                    const zb_smoother* smo, zb_stream_t stream) {
-  if (!valid(cfg) || !ws || !x || precond < 0 || precond > 2) return ZB_E_ARG;
-  if (precond == 2 && !smo) return ZB_E_ARG;
+  if (!valid(cfg) || !ws || !x || precond < 0 || precond > 3) return ZB_E_ARG;
+  if (precond >= 2 && !smo) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
   cudaStream_t st = (cudaStream_t)stream;
   double* dw = (double*)ws;
@@ -923,10 +929,10 @@ struct zb_fcg_graph {
 int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x,
                         int precond, const zb_smoother* smo, double tol, int maxit,
                         zb_fcg_graph** out, zb_stream_t stream) {
-  if (!valid(cfg) || !ws || !b || !x || !out || precond < 0 || precond > 2 || maxit < 1 ||
+  if (!valid(cfg) || !ws || !b || !x || !out || precond < 0 || precond > 3 || maxit < 1 ||
       !(tol >= 0.0))
     return ZB_E_ARG;
-  if (precond == 2 && !smo) return ZB_E_ARG;
+  if (precond >= 2 && !smo) return ZB_E_ARG;
   *out = nullptr;
   (void)stream;   // capture runs on private streams; nothing executes here
   const Plan P = make_plan(cfg);

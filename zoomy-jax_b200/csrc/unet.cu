@@ -30,6 +30,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "conv_tc.cuh"
 
 namespace zb {
 namespace unet {
@@ -236,7 +237,8 @@ __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float*
                             const float* __restrict__ g, __nv_bfloat16* __restrict__ wb, int n,
                             float lr, float b1, float b2, float eps, float c1, float c2) {
   for (int k = blockIdx.x * NT + threadIdx.x; k < n; k += gridDim.x * NT) {
-    const float gk = g[k];
+    const float g0 = g[k];
+    const float gk = isfinite(g0) ? g0 : 0.0f;   // a non-finite entry is skipped
     const float mk = b1 * m[k] + (1.0f - b1) * gk;
     const float vk = b2 * v[k] + (1.0f - b2) * gk * gk;
     m[k] = mk;
@@ -338,16 +340,20 @@ __global__ void patch_residual(const float* __restrict__ f, const float* __restr
   }
 }
 
-// loss terms per image: lnum[b] = |res_b|^2, lden[b] = |r_b|^2
-__global__ void loss_kernel(const float* __restrict__ res, const float* __restrict__ r, int B,
+// loss terms per image: lnum[b] = a_b . b_b, lden[b] = c_b . d_b (residual
+// loss: a = b = res, c = d = r; energy loss: a = res, b = A res, c = e,
+// d = A e).  An image whose denominator is not a positive finite number above
+// 1e-30 (a patch without signal) is left out of the loss and its gradient.
+__global__ void loss_kernel(const float* __restrict__ a_, const float* __restrict__ b_,
+                            const float* __restrict__ c_, const float* __restrict__ d_, int B,
                             size_t npix, float* __restrict__ lnum, float* __restrict__ lden) {
   __shared__ float red[2][NT / 32];
   const int b = blockIdx.x;
   float a = 0.0f, c = 0.0f;
   for (size_t k = threadIdx.x; k < npix; k += NT) {
-    const float u = res[(size_t)b * npix + k], v = r[(size_t)b * npix + k];
-    a += u * u;
-    c += v * v;
+    const size_t q = (size_t)b * npix + k;
+    a += a_[q] * b_[q];
+    c += c_[q] * d_[q];
   }
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -359,38 +365,75 @@ __global__ void loss_kernel(const float* __restrict__ res, const float* __restri
     float ta = 0.0f, tc = 0.0f;
     for (int i = 0; i < NT / 32; ++i) { ta += red[0][i]; tc += red[1][i]; }
     lnum[b] = ta;
-    lden[b] = fmaxf(tc, 1e-30f);
+    lden[b] = tc;
   }
 }
+
+__device__ __forceinline__ bool loss_counts(float den) { return den > 1e-30f && den < 3e38f; }
 
 __global__ void loss_total(const float* lnum, const float* lden, int B, double* out) {
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int b = 0; b < B; ++b) t += (double)lnum[b] / (double)lden[b];
+    for (int b = 0; b < B; ++b)
+      if (loss_counts(lden[b])) t += (double)lnum[b] / (double)lden[b];
     *out = t / B;
   }
 }
 
-// dL/dout = -2 (A res)_b / (B |r_b|^2) * s_b dx^2 / c   (A symmetric)
-__global__ void loss_grad_kernel(const float* __restrict__ res, const float* __restrict__ cx,
-                                 const float* __restrict__ cy, const float* __restrict__ lden,
-                                 const float* __restrict__ s, int B, int H, int W, float idx2,
-                                 float dx2, float* __restrict__ dout) {
+// A x per image (Dirichlet ghost -x)
+__global__ void patch_apply(const float* __restrict__ x, const float* __restrict__ cx,
+                            const float* __restrict__ cy, int B, int H, int W, float idx2,
+                            float* __restrict__ out) {
   const size_t npix = (size_t)H * W, n = (size_t)B * npix;
   for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < n; k += (size_t)gridDim.x * NT) {
     const int b = (int)(k / npix);
     const size_t p = k - (size_t)b * npix;
     const int i = (int)(p / W), j = (int)(p - (size_t)i * W);
-    const float* rb = res + (size_t)b * npix;
+    const float* xb = x + (size_t)b * npix;
     const float* ax_ = cx + (size_t)b * (H + 1) * W;
     const float* ay_ = cy + (size_t)b * H * (W + 1);
-    const float rc = rb[p];
-    const float ar = (ax_[(size_t)(i + 1) * W + j] * (rc - xg(rb, H, W, i + 1, j, rc)) +
-                      ax_[(size_t)i * W + j] * (rc - xg(rb, H, W, i - 1, j, rc)) +
-                      ay_[(size_t)i * (W + 1) + j + 1] * (rc - xg(rb, H, W, i, j + 1, rc)) +
-                      ay_[(size_t)i * (W + 1) + j] * (rc - xg(rb, H, W, i, j - 1, rc))) * idx2;
+    const float xc = xb[p];
+    out[k] = (ax_[(size_t)(i + 1) * W + j] * (xc - xg(xb, H, W, i + 1, j, xc)) +
+              ax_[(size_t)i * W + j] * (xc - xg(xb, H, W, i - 1, j, xc)) +
+              ay_[(size_t)i * (W + 1) + j + 1] * (xc - xg(xb, H, W, i, j + 1, xc)) +
+              ay_[(size_t)i * (W + 1) + j] * (xc - xg(xb, H, W, i, j - 1, xc))) * idx2;
+  }
+}
+
+__global__ void sub_kernel(const float* __restrict__ a, const float* __restrict__ b, size_t n,
+                           float* __restrict__ out) {
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < n; k += (size_t)gridDim.x * NT)
+    out[k] = a[k] - b[k];
+}
+
+// dL/dout = -2 (A res)_b / (B den_b) * s_b dx^2 / c   (A symmetric); ar holds
+// A res (energy loss) or is null, in which case A res is formed here from res
+__global__ void loss_grad_kernel(const float* __restrict__ res, const float* __restrict__ ar_in,
+                                 const float* __restrict__ cx, const float* __restrict__ cy,
+                                 const float* __restrict__ lden, const float* __restrict__ s,
+                                 int B, int H, int W, float idx2, float dx2,
+                                 float* __restrict__ dout) {
+  const size_t npix = (size_t)H * W, n = (size_t)B * npix;
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < n; k += (size_t)gridDim.x * NT) {
+    const int b = (int)(k / npix);
+    const size_t p = k - (size_t)b * npix;
+    const int i = (int)(p / W), j = (int)(p - (size_t)i * W);
+    float ar;
+    if (ar_in) {
+      ar = ar_in[k];
+    } else {
+      const float* rb = res + (size_t)b * npix;
+      const float* ax_ = cx + (size_t)b * (H + 1) * W;
+      const float* ay_ = cy + (size_t)b * H * (W + 1);
+      const float rc = rb[p];
+      ar = (ax_[(size_t)(i + 1) * W + j] * (rc - xg(rb, H, W, i + 1, j, rc)) +
+            ax_[(size_t)i * W + j] * (rc - xg(rb, H, W, i - 1, j, rc)) +
+            ay_[(size_t)i * (W + 1) + j + 1] * (rc - xg(rb, H, W, i, j + 1, rc)) +
+            ay_[(size_t)i * (W + 1) + j] * (rc - xg(rb, H, W, i, j - 1, rc))) * idx2;
+    }
+    const float den = lden[b];
     const float c = cell_c(cx, cy, b, H, W, i, j);
-    dout[k] = -2.0f * ar / ((float)B * lden[b]) * s[b] * dx2 / c;
+    dout[k] = loss_counts(den) ? -2.0f * ar / ((float)B * den) * s[b] * dx2 / c : 0.0f;
   }
 }
 
@@ -429,9 +472,66 @@ static bool valid_channels(int c1, int c2) {
          (c1 == 24 && c2 == 48);
 }
 
+// which convolution runs the forward and data-gradient passes: the tcgen05
+// implicit GEMM (bf16 operands, the default) or the CUDA-core direct
+// convolution (float32 operands, kept as the exactness reference)
+static int g_conv_impl = 1;
+static __device__ unsigned g_unet_err;
+
+static unsigned* unet_err_word() {
+  static unsigned* ptrs[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_unet_err) != cudaSuccess) return nullptr;
+    ptrs[dev] = (unsigned*)p;
+  }
+  return ptrs[dev];
+}
+
+static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin,
+                          const __nv_bfloat16* w, const float* bias, float* out, int cout, int B,
+                          int H, int W, int act, cudaStream_t st) {
+  const int cinp = pad16(cin), coutp = pad16(cout);
+  if (coutp > 256 || cinp > 256) return ZB_E_UNSUPPORTED;
+  int cols = 32;
+  while (cols < coutp) cols *= 2;
+  static int sms[64] = {0};
+  static bool attr[64] = {false};
+  int dev = 0;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return ZB_E_CUDA;
+  if (!sms[dev]) ZB_CUDA_TRY(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+  if (!attr[dev]) {
+    ZB_CUDA_TRY(cudaFuncSetAttribute(conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024));
+    attr[dev] = true;
+  }
+  // resident CTAs of one SM must never ask for more than its 512 TMEM
+  // columns: pad the shared memory so that at most 512 / cols fit
+  const int smem_sm = 228 * 1024, per_cta_reserved = 1024;
+  const int by_tmem = 512 / cols, by_threads = 2048 / TC_THREADS;
+  size_t smem = tc_smem_bytes(cinp, coutp);
+  if (by_tmem < by_threads) {
+    const size_t floor_bytes = (size_t)(smem_sm / (by_tmem + 1) - per_cta_reserved + 16);
+    smem = std::max(smem, floor_bytes);
+  }
+  if (smem > 227 * 1024) return ZB_E_UNSUPPORTED;
+  const int fit = std::min(by_threads, (int)(smem_sm / (smem + per_cta_reserved)));
+  const long long ntiles =
+      (long long)((W + TCX - 1) / TCX) * ((H + TCY - 1) / TCY) * B;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(ntiles, (long long)sms[dev] * std::max(1, fit)));
+  conv3x3_tc<<<grid, TC_THREADS, smem, st>>>(inA, cin_a, inB, cin, w, bias, out, cout, B, H, W,
+                                             act, cols, unet_err_word());
+  return zb_launch_check();
+}
+
 static int conv(const float* inA, int cin_a, const float* inB, int cin,
                 const __nv_bfloat16* w, const float* bias, float* out, int cout, int B, int H,
                 int W, int act, cudaStream_t st) {
+  if (g_conv_impl == 1)
+    return conv_tc_launch(inA, cin_a, inB, cin, w, bias, out, cout, B, H, W, act, st);
   dim3 grid((W + TS - 1) / TS, (H + TS - 1) / TS, B);
   switch (cout) {
 #define ZB_CONV(N) case N: conv3x3_fwd<N><<<grid, NTT, 0, st>>>(inA, cin_a, inB, cin, w, bias, out, B, H, W, act); break;
@@ -535,6 +635,24 @@ using namespace zb::unet;
 
 extern "C" {
 
+int zb_unet_conv_impl(int impl) {
+  const int prev = g_conv_impl;
+  if (impl == 0 || impl == 1) g_conv_impl = impl;
+  return prev;
+}
+
+int zb_unet_status(int clear) {
+  unsigned* p = unet_err_word();
+  if (!p) return ZB_E_CUDA;
+  unsigned v = 0;
+  ZB_CUDA_TRY(cudaMemcpy(&v, p, sizeof(v), cudaMemcpyDeviceToHost));
+  if (clear && v) {
+    const unsigned z = 0;
+    ZB_CUDA_TRY(cudaMemcpy(p, &z, sizeof(z), cudaMemcpyHostToDevice));
+  }
+  return (int)v;
+}
+
 size_t zb_unet_param_count(int c1, int c2, size_t* n_weights, size_t* n_biases) {
   if (!valid_channels(c1, c2)) return 0;
   const Net n = net_layout(c1, c2);
@@ -595,8 +713,9 @@ int zb_unet_forward(const zb_unet_trainer* t, const float* r, const float* cx, c
   return zb_launch_check();
 }
 
-int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* cx, const float* cy,
-                     double dx, double* loss_out, zb_stream_t stream) {
+int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* target,
+                     const float* cx, const float* cy, double dx, double* loss_out,
+                     zb_stream_t stream) {
   if (!t || !r || !cx || !cy || !valid_channels(t->c1, t->c2)) return ZB_E_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   const Net n = net_layout(t->c1, t->c2);
@@ -608,10 +727,23 @@ int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* cx, 
   int rc;
   // forward (keeps activations), y into a.tmp
   if ((rc = zb_unet_forward(t, r, cx, cy, dx, a.tmp, stream))) return rc;
-  patch_residual<<<gridn(N0), NT, 0, st>>>(r, a.tmp, cx, cy, B, H, W, idx2, a.res);
-  loss_kernel<<<B, NT, 0, st>>>(a.res, r, B, (size_t)H * W, a.lnum, a.lden);
-  if (loss_out) loss_total<<<1, 32, 0, st>>>(a.lnum, a.lden, B, loss_out);
-  loss_grad_kernel<<<gridn(N0), NT, 0, st>>>(a.res, cx, cy, a.lden, a.s, B, H, W, idx2, dx2, a.d_out);
+  if (target) {
+    // energy loss: res = e - y, (res . A res) / (e . A e); A res -> d_out,
+    // A e -> tmp (y is no longer needed once res is formed)
+    sub_kernel<<<gridn(N0), NT, 0, st>>>(target, a.tmp, N0, a.res);
+    patch_apply<<<gridn(N0), NT, 0, st>>>(a.res, cx, cy, B, H, W, idx2, a.d_out);
+    patch_apply<<<gridn(N0), NT, 0, st>>>(target, cx, cy, B, H, W, idx2, a.tmp);
+    loss_kernel<<<B, NT, 0, st>>>(a.res, a.d_out, target, a.tmp, B, (size_t)H * W, a.lnum, a.lden);
+    if (loss_out) loss_total<<<1, 32, 0, st>>>(a.lnum, a.lden, B, loss_out);
+    loss_grad_kernel<<<gridn(N0), NT, 0, st>>>(a.res, a.d_out, cx, cy, a.lden, a.s, B, H, W, idx2,
+                                               dx2, a.d_out);
+  } else {
+    patch_residual<<<gridn(N0), NT, 0, st>>>(r, a.tmp, cx, cy, B, H, W, idx2, a.res);
+    loss_kernel<<<B, NT, 0, st>>>(a.res, a.res, r, r, B, (size_t)H * W, a.lnum, a.lden);
+    if (loss_out) loss_total<<<1, 32, 0, st>>>(a.lnum, a.lden, B, loss_out);
+    loss_grad_kernel<<<gridn(N0), NT, 0, st>>>(a.res, nullptr, cx, cy, a.lden, a.s, B, H, W, idx2,
+                                               dx2, a.d_out);
+  }
   cudaMemsetAsync(t->g_w, 0, n.nw * sizeof(float), st);
   cudaMemsetAsync(t->g_b, 0, n.nb * sizeof(float), st);
   float* gw = t->g_w;

@@ -84,7 +84,7 @@ class ZbUnetTrainer(C.Structure):
                 ("w_bf16", C.c_void_p), ("b_shadow", C.c_void_p), ("act", C.c_void_p)]
 
 
-PRECOND = {"none": 0, "mg": 1, "learned": 2}
+PRECOND = {"none": 0, "mg": 1, "learned": 2, "learned_replace": 3}
 # scalar slots of the Poisson workspace (float64)
 S_REL, S_ITER = 7, 8
 
@@ -137,6 +137,8 @@ SIGNATURES = [
     ("zb_tri_aux", C.c_int, [_TCFG, _TMESH, _P, _P, _P]),
     ("zb_tri_mass_partials", C.c_size_t, []),
     ("zb_tri_mass", C.c_int, [_TCFG, _TMESH, _P, _P, _P, _P]),
+    ("zb_unet_conv_impl", C.c_int, [C.c_int]),
+    ("zb_unet_status", C.c_int, [C.c_int]),
     ("zb_unet_param_count", C.c_size_t, [C.c_int, C.c_int, C.POINTER(C.c_size_t),
                                          C.POINTER(C.c_size_t)]),
     ("zb_smoother_workspace_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -144,7 +146,7 @@ SIGNATURES = [
                                     C.c_double, C.c_int, _P]),
     ("zb_unet_train_workspace_bytes", C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
     ("zb_unet_forward", C.c_int, [_TRN, _P, _P, _P, C.c_double, _P, _P]),
-    ("zb_unet_backward", C.c_int, [_TRN, _P, _P, _P, C.c_double, _P, _P]),
+    ("zb_unet_backward", C.c_int, [_TRN, _P, _P, _P, _P, C.c_double, _P, _P]),
     ("zb_unet_adam", C.c_int, [_TRN, C.c_float, C.c_int, _P]),
     ("zb_poisson_workspace_bytes", C.c_size_t, [_PCFG]),
     ("zb_poisson_layout", C.c_int, [_PCFG, C.POINTER(C.c_int64)]),

@@ -39,8 +39,10 @@ def elliptic_accept(tol):
 class PoissonSolver:
     """``-div(c grad p) = f`` on an ``nx x ny`` grid (spacing ``dx``, p = 0
     on the walls), ``c`` from a depth field: float64 FCG with a float32
-    V-cycle preconditioner; ``precond`` is ``'none'`` (plain CG), ``'mg'``
-    or ``'learned'`` (V-cycle with the U-Net as level-0 smoother)."""
+    V-cycle preconditioner; ``precond`` is ``'none'`` (plain CG), ``'mg'``,
+    ``'learned'`` (the V-cycle followed by one learned smoothing step on the
+    finest level) or ``'learned_replace'`` (the U-Net in place of the finest
+    level's red-black sweeps)."""
 
     def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
                  device=None):
@@ -85,7 +87,7 @@ class PoissonSolver:
         return L.stream_ptr()
 
     def _smo(self, precond, smoother):
-        if precond == "learned":
+        if precond.startswith("learned"):
             if smoother is None:
                 raise ValueError("precond='learned' needs a LearnedSmoother")
             return C.byref(smoother.struct(self.nx, self.ny))
@@ -164,11 +166,22 @@ class PoissonSolver:
         s = self.scal[7:9].cpu()
         return self.x, int(s[1].item()), float(s[0].item())
 
+    def post_vcycle_residual(self):
+        """``r - A z`` (float32) for the residual ``r`` and the V-cycle output
+        ``z = M r`` the last FCG start/iteration left in the workspace: what
+        the preconditioner failed to remove."""
+        import torch
+        n = self.nx * self.ny
+        z = self.ws[self.layout[5]:self.layout[5] + 4 * n].view(torch.float32)
+        return (self.r - self.apply(z.double())).float()
+
     def solve_stepwise(self, b=None, x0=None, tol=1e-8, maxit=200, precond="mg",
-                       smoother=None, record=None):
+                       smoother=None, record=None, record_post=None):
         """The same solve driven from the host one iteration at a time
         (a sync per iteration); ``record`` (a list) receives a float32 copy
-        of the residual after the start and after every iteration."""
+        of the residual after the start and after every iteration,
+        ``record_post`` the residual left by each preconditioner application
+        (:meth:`post_vcycle_residual`)."""
         if b is not None and b.data_ptr() != self.b.data_ptr():
             self.b.copy_(b.reshape(-1))
         if x0 is None:
@@ -181,6 +194,8 @@ class PoissonSolver:
                                       L.ptr(self.x), pc, smo, self._s()), "fcg_start")
         if record is not None:
             record.append(self.r.float().clone())
+        if record_post is not None:
+            record_post.append(self.post_vcycle_residual())
         it = 0
         rel = float(self.scal[7].item())
         while rel > tol and it < maxit:
@@ -190,6 +205,8 @@ class PoissonSolver:
             rel = float(self.scal[7].item())
             if record is not None:
                 record.append(self.r.float().clone())
+            if record_post is not None and rel > tol:
+                record_post.append(self.post_vcycle_residual())
         return self.x, it, rel
 
 

@@ -178,18 +178,23 @@ class SmootherTrainer:
                                          float(dx), L.ptr(y), L.stream_ptr()), "unet_forward")
         return y
 
-    def loss_and_grad(self, r, cx, cy, dx):
-        """Loss (device float64 tensor) and gradients into ``g_w``, ``g_b``."""
+    def loss_and_grad(self, r, cx, cy, dx, target=None):
+        """Loss (device float64 tensor) and gradients into ``g_w``, ``g_b``:
+        the residual loss, or with ``target`` (the exact errors ``e``,
+        ``A e = r``) the energy-norm loss."""
         self._check(r, cx, cy)
-        L.check(self.lib.zb_unet_backward(C.byref(self.t), L.ptr(r), L.ptr(cx), L.ptr(cy),
-                                          float(dx), L.ptr(self.loss), L.stream_ptr()),
-                "unet_backward")
+        if target is not None and (target.shape != r.shape or not target.is_contiguous()):
+            raise ValueError("target must match r")
+        L.check(self.lib.zb_unet_backward(C.byref(self.t), L.ptr(r),
+                                          L.ptr(target) if target is not None else None,
+                                          L.ptr(cx), L.ptr(cy), float(dx), L.ptr(self.loss),
+                                          L.stream_ptr()), "unet_backward")
         return self.loss
 
-    def step(self, r, cx, cy, dx, lr=None):
+    def step(self, r, cx, cy, dx, lr=None, target=None):
         """One Adam step on a batch; returns the batch loss (device tensor,
         before the update)."""
-        loss = self.loss_and_grad(r, cx, cy, dx)
+        loss = self.loss_and_grad(r, cx, cy, dx, target)
         self.step_count += 1
         L.check(self.lib.zb_unet_adam(C.byref(self.t), float(self.lr if lr is None else lr),
                                       self.step_count, L.stream_ptr()), "unet_adam")
@@ -208,8 +213,9 @@ class SmootherTrainer:
             idx = torch.randint(0, patches.count, (self.batch,), generator=g,
                                 device=patches.r.device)
             r, cx, cy = patches.batch(idx)
+            e = patches.e[idx].contiguous() if patches.e is not None else None
             lr = lr1 + 0.5 * (lr0 - lr1) * (1.0 + math.cos(math.pi * s / max(1, steps)))
-            loss = self.step(r, cx, cy, patches.dx, lr=lr)
+            loss = self.step(r, cx, cy, patches.dx, lr=lr, target=e)
             if log_every and (s % log_every == 0 or s == steps - 1):
                 hist.append((s, float(loss.item())))
         return hist
@@ -218,19 +224,23 @@ class SmootherTrainer:
 class PatchSet:
     """Training patches on the device: residual/right-hand-side patches
     ``r (N, n, n)`` with their face coefficients ``cx (N, n+1, n)``,
-    ``cy (N, n, n+1)``, all float32, grid spacing ``dx``."""
+    ``cy (N, n, n+1)``, optionally the exact errors ``e (N, n, n)`` that solve
+    ``A e = r`` on the whole grid, all float32, grid spacing ``dx``."""
 
-    def __init__(self, r, cx, cy, dx):
-        self.r, self.cx, self.cy, self.dx = r, cx, cy, float(dx)
+    def __init__(self, r, cx, cy, dx, e=None):
+        self.r, self.cx, self.cy, self.dx, self.e = r, cx, cy, float(dx), e
         self.count = r.shape[0]
 
     def batch(self, idx):
         return (self.r[idx].contiguous(), self.cx[idx].contiguous(), self.cy[idx].contiguous())
 
     @staticmethod
-    def cut(fields, cx, cy, nx, ny, n, count, generator):
+    def cut(fields, cx, cy, nx, ny, n, count, generator, targets=None, min_rms=0.0):
         """Random ``n x n`` patches of the grid fields ``fields (K, nx*ny)``
-        with the matching windows of ``cx ((nx+1)*ny)``, ``cy (nx*(ny+1))``."""
+        (and of ``targets``, same shape) with the matching windows of
+        ``cx ((nx+1)*ny)``, ``cy (nx*(ny+1))``.  Patches whose RMS is below
+        ``min_rms`` times the RMS of their source field are dropped (patches
+        without signal teach nothing).  Returns ``(r, cx, cy, e or None)``."""
         import torch
         dev = fields.device
         K = fields.shape[0]
@@ -239,10 +249,80 @@ class PatchSet:
         j0 = torch.randint(0, ny - n + 1, (count,), generator=generator, device=dev)
         a = torch.arange(n, device=dev)
         a1 = torch.arange(n + 1, device=dev)
+        ii = i0[:, None, None] + a[None, :, None]
+        jj = j0[:, None, None] + a[None, None, :]
         F = fields.view(K, nx, ny)
-        r = F[k[:, None, None], i0[:, None, None] + a[None, :, None], j0[:, None, None] + a[None, None, :]]
+        r = F[k[:, None, None], ii, jj]
         CX = cx.view(nx + 1, ny)
         CY = cy.view(nx, ny + 1)
-        pcx = CX[i0[:, None, None] + a1[None, :, None], j0[:, None, None] + a[None, None, :]]
-        pcy = CY[i0[:, None, None] + a[None, :, None], j0[:, None, None] + a1[None, None, :]]
-        return r.float().contiguous(), pcx.float().contiguous(), pcy.float().contiguous()
+        pcx = CX[i0[:, None, None] + a1[None, :, None], jj[:, :1, :].expand(-1, n + 1, -1)]
+        pcy = CY[ii[:, :, :1].expand(-1, -1, n + 1), j0[:, None, None] + a1[None, None, :]]
+        e = targets.view(K, nx, ny)[k[:, None, None], ii, jj] if targets is not None else None
+        keep = None
+        if min_rms > 0.0:
+            src = fields.float().pow(2).mean(dim=1).sqrt()
+            rms = r.float().pow(2).mean(dim=(1, 2)).sqrt()
+            keep = rms > min_rms * src[k]
+        out = [r.float(), pcx.float(), pcy.float(), e.float() if e is not None else None]
+        if keep is not None:
+            out = [t[keep] if t is not None else None for t in out]
+        return tuple(t.contiguous() if t is not None else None for t in out)
+
+
+def solver_training_set(n_grid=256, seeds=(1, 2, 3, 4), steps=3, patch=32, count=10000,
+                        tol=1e-8, seed=0, device=None, targets=True):
+    """Training patches generated by the solver itself: short seeded Chorin
+    marches (dam break over Gaussian bumps, ``n_grid^2``, plain multigrid
+    preconditioner) whose pressure solves are re-run step by step to record
+    the residual each V-cycle leaves, ``r' = r - A M r`` -- the input of the
+    learned post-smoother -- and, with ``targets``, the exact error behind it
+    (``A e' = r'`` solved to 1e-10), the output it should produce.  Returns a
+    :class:`PatchSet` of ``count`` random ``patch x patch`` windows with
+    signal, with their face coefficients."""
+    import torch
+    import zoomy_b200 as zb
+    from .fvm.chorin import ChorinSolver
+    from .workloads import cartesian_centers, circular_dam_state
+    tags = ("left", "right", "bottom", "top")
+    snaps = []
+    for s in seeds:
+        state = circular_dam_state(cartesian_centers(n_grid), seed=int(s))
+        model = zb.ShallowWater2D(boundary_conditions={t: "wall" for t in tags},
+                                  initial_conditions=state)
+        nsm = zb.NumericalSystemModel.from_system_model(model, zb.ReconstructionSpec(2, "minmod"),
+                                                        "hll_hr")
+        sol = ChorinSolver(pressure_tol=tol, precond="mg",
+                           compute_dt=zb.timestepping.adaptive(0.45, 2),
+                           reconstruction_variables="eta", free_surface_h_index=1, eps_wet=1e-6,
+                           dtype="float32", device=device)
+        Q, _ = sol.setup_simulation(zb.create_2d((0.0, 1.0, 0.0, 1.0), n_grid, n_grid), nsm)
+        dt = sol.compute_timestep(Q)
+        for k in range(int(steps)):
+            Qs = sol._hyperbolic_stage(dt, k * dt, Q)
+            P = sol.poisson
+            P.setup(Qs[1])
+            P.rhs(Qs, dt)
+            post = []
+            P.solve_stepwise(None, tol=tol, maxit=100, precond="mg", record_post=post)
+            F = torch.stack(post)
+            E = None
+            if targets:
+                errs = []
+                for rp in post:
+                    x, _, _ = P.solve(rp.double(), tol=1e-10, maxit=100, precond="mg")
+                    errs.append(x.float().clone())
+                E = torch.stack(errs)
+            snaps.append((F, E, P.cx32.clone(), P.cy32.clone()))
+            # march on with the proper pressure of this step
+            P.setup(Qs[1])
+            P.rhs(Qs, dt)
+            P.solve(None, tol=tol, maxit=100, precond="mg")
+            Q = sol._step_corrector(Qs, dt)
+    g = torch.Generator(device=snaps[0][0].device).manual_seed(int(seed))
+    per = -(-2 * int(count) // len(snaps))
+    parts = [PatchSet.cut(F, cx, cy, n_grid, n_grid, patch, per, g, targets=E, min_rms=1e-2)
+             for F, E, cx, cy in snaps]
+    r = torch.cat([p[0] for p in parts])
+    perm = torch.randperm(r.shape[0], generator=g, device=r.device)[:int(count)]
+    cat = lambda i: torch.cat([p[i] for p in parts])[perm].contiguous()  # noqa: E731
+    return PatchSet(cat(0), cat(1), cat(2), 1.0 / n_grid, e=cat(3) if targets else None)
