@@ -20,6 +20,11 @@ and the max-over-ranks of the timing.
 cannot be installed: it needs jax and zoomy_core, absent here) on the host's
 cores: one process per core, each stepping a 256 x 256 sample of the same
 workload; rank 0 only.
+
+Rank 0 also reports, in the same JSON line, the two other configurations:
+"chorin" (1024^2 Chorin steps at a 1e-8 pressure residual, plain multigrid FCG
+against the learned U-Net smoother) and "ensemble" (512 uneven instances in one
+persistent launch per stage); --no-extra skips them.
 """
 from __future__ import annotations
 
@@ -330,6 +335,117 @@ def run_gpu(args, rank, world, local_rank):
     }
 
 
+def _ev_ms(fn, reps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_chorin(local_rank, n=1024, steps=10, warmup=3):
+    """The non-hydrostatic configuration: Chorin steps (hyperbolic Euler ->
+    pressure Poisson to 1e-8 -> corrector) on an n x n grid, plain multigrid
+    FCG against the learned U-Net post-smoother (trained here on the GPU by
+    the project's kernels on 10k solver-generated patches; training is
+    outside the timed region and reported)."""
+    import torch
+    import zoomy_b200 as zb
+    from zoomy_b200.fvm.chorin import ChorinSolver, elliptic_accept
+    from zoomy_b200.learned import LearnedSmoother, SmootherTrainer, solver_training_set
+    from zoomy_b200.workloads import cartesian_centers, circular_dam_state
+    tags = ("left", "right", "bottom", "top")
+    dev = f"cuda:{local_rank}"
+
+    def make(precond, smoother=None):
+        state = circular_dam_state(cartesian_centers(n), seed=0)
+        model = zb.ShallowWater2D(boundary_conditions={t: "wall" for t in tags},
+                                  initial_conditions=state)
+        nsm = zb.NumericalSystemModel.from_system_model(
+            model, zb.ReconstructionSpec(2, "minmod"), "hll_hr")
+        sol = ChorinSolver(pressure_tol=1e-8, pressure_maxit=200, precond=precond,
+                           smoother=smoother, compute_dt=zb.timestepping.adaptive(0.45, 2),
+                           reconstruction_variables="eta", free_surface_h_index=1,
+                           eps_wet=1e-6, dtype="float32", device=dev)
+        Q, _ = sol.setup_simulation(zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n), nsm)
+        return sol, Q
+
+    def measure(precond, smoother=None):
+        sol, Q = make(precond, smoother)
+        dt = sol.compute_timestep(Q)
+        Qw, _ = sol.run_jit_steps(dt, warmup, Q)
+        sol._max_rel.zero_()
+        sol._iters.zero_()
+        state = {"Q": Q}
+
+        def one():
+            state["Q"] = sol.chorin_cycle(dt, 0.0, state["Q"], sync=False)
+        torch.cuda.synchronize()
+        ms = _ev_ms(one, steps)
+        rel = float(sol._max_rel.item())
+        its = float(sol._iters.item()) / steps
+        return {"ms_per_step": round(ms, 4), "fcg_iterations_per_solve": its,
+                "max_rel_residual": rel, "gate_ok": rel <= elliptic_accept(1e-8)}
+
+    out = {"grid": [n, n], "tol": 1e-8, "steps": steps, "warmup": warmup,
+           "step": "hyperbolic Euler (eta-MUSCL + HR-HLL) + pressure FCG + corrector, fp32 "
+                   "state, fp64 Krylov / fp32 V-cycle(2,2), exact coarsest solve",
+           "plain_mg": measure("mg")}
+    t0 = time.perf_counter()
+    data = solver_training_set(n_grid=256, seeds=(1, 2, 3, 4), steps=3, patch=32, count=10000,
+                               targets=False, device=dev)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    for key, (c1, c2) in (("learned", (24, 48)), ("learned_small", (8, 16))):
+        sm = LearnedSmoother(c1, c2, seed=0, device=dev)
+        tr = SmootherTrainer(sm, batch=64, n=32, lr=3e-3)
+        t0 = time.perf_counter()
+        hist = tr.fit(data, steps=2000, log_every=1000)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        r = measure("learned", sm)
+        r.update({"network": f"U-Net c1={c1} c2={c2}, {sm.n_params} params, bf16 weights, "
+                             f"tcgen05 convolutions, fp32 accumulation",
+                  "train_s": round(t_train, 2), "train_steps": 2000,
+                  "train_loss": [round(v, 4) for _, v in hist],
+                  "training_set": f"{data.count} 32x32 patches from 256^2 solver runs "
+                                  f"({round(t_data, 2)} s to generate)",
+                  "speed_vs_plain": round(out["plain_mg"]["ms_per_step"] / r["ms_per_step"], 3)})
+        out[key] = r
+    return out
+
+
+def run_ensemble(local_rank, steps=2000):
+    """The batched configuration: 512 uneven SWE instances (sides log-uniform
+    in [64, 512]) advanced together by one persistent launch per stage,
+    autotuned tile height, replayed from a CUDA graph of 30 steps."""
+    import torch
+    from zoomy_b200.ensemble import Ensemble
+    from zoomy_b200.workloads import ensemble_512, ensemble_state
+    sides, heights, manning = ensemble_512(seed=0)
+    ens = Ensemble(sides, manning, dtype="float32", device=f"cuda:{local_rank}")
+    ens.setup([ensemble_state(int(k), h) for k, h in zip(sides, heights)])
+    tuned = ens.autotune(steps=6)
+    ens.init()
+    chunk = 30
+    ens.capture(chunk)
+    ens.init()
+    ens.replay(1)
+    torch.cuda.synchronize()
+    reps = max(1, steps // chunk)
+    ms = _ev_ms(lambda: ens.replay(1), reps)
+    cells = int(ens.total_cells)
+    return {"instances": int(len(sides)), "cells": cells, "steps": reps * chunk,
+            "ms_per_step": round(ms / chunk, 4),
+            "value": cells * chunk / (ms * 1e-3), "unit": "cell-updates/s",
+            "launches_per_step": 2, "autotune_ms_per_step": {f"tile{t}_grid{g}": round(v, 4)
+                                                            for (t, g), v in tuned.items()},
+            "status_ok": ens.status_any() == 0}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -340,6 +456,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the Chorin and ensemble legs")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -392,6 +510,10 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    extra = {}
+    if not args.no_extra:
+        extra["chorin"] = run_chorin(local_rank)
+        extra["ensemble"] = run_ensemble(local_rank)
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["ms_per_step"], "higher_is_better": True,
@@ -401,6 +523,7 @@ def main():
             "cpu_baseline": cpu, "e2e": res["e2e"], "clocks": res["clocks"],
             "gpu_launches": res["gpu_launches"], "status_ok": res["status_ok"],
             "sim_time": res["sim_time"]}
+    line.update(extra)
     print(json.dumps(line), flush=True)
 
 

@@ -192,13 +192,21 @@ def rbgs(x, f, cx, cy, dx, diag, color):
     return x
 
 
+DENSE_MAX_CELLS = 64
+
+
 def vcycle(H, f, level=0, nu=2, coarse_sweeps=40, smoother=None):
-    """Symmetric V-cycle for ``A x = f`` from x = 0.  ``smoother(level, x, f)``
-    replaces the level-0 pre/post smoothing when given (the learned path)."""
+    """Symmetric V-cycle for ``A x = f`` from x = 0: the coarsest level is
+    solved exactly when it has at most 64 cells, else by ``coarse_sweeps``
+    symmetric red-black sweep pairs.  ``smoother(x, f, pre)`` replaces the
+    level-0 pre/post smoothing when given (the learned path)."""
     cx, cy, dx = H.levels[level]
     d = H.diag[level]
     x = np.zeros_like(f)
     if level == len(H.levels) - 1:
+        if f.size <= DENSE_MAX_CELLS:
+            # exact coarsest solve (the device inverts this level at set-up)
+            return np.linalg.solve(matrix(cx, cy, dx).toarray(), f.reshape(-1)).reshape(f.shape)
         for _ in range(coarse_sweeps):
             x = rbgs(x, f, cx, cy, dx, d, 0)
             x = rbgs(x, f, cx, cy, dx, d, 1)

@@ -35,7 +35,8 @@ import zoomy_b200 as zb  # noqa: E402
 from zoomy_b200 import _lib as L  # noqa: E402
 from zoomy_b200.fvm.chorin import (ChorinSolver, EllipticSolveError,  # noqa: E402
                                    PoissonSolver)
-from zoomy_b200.learned import LearnedSmoother, PatchSet, SmootherTrainer  # noqa: E402
+from zoomy_b200.learned import (LearnedSmoother, PatchSet, SmootherTrainer,  # noqa: E402
+                                solver_training_set)
 from zoomy_b200.workloads import cartesian_centers  # noqa: E402
 
 DEV = torch.device("cuda")
@@ -292,7 +293,7 @@ def _patches(n_grid=128, patch=16, count=2048, seed=0):
     P.solve_stepwise(gpu(rng.standard_normal(n_grid * n_grid)), tol=1e-8, maxit=50, record=rec)
     fields = torch.stack(rec)
     g = torch.Generator(device=DEV).manual_seed(seed)
-    r, cx, cy = PatchSet.cut(fields, P.cx32, P.cy32, n_grid, n_grid, patch, count, g)
+    r, cx, cy, _ = PatchSet.cut(fields, P.cx32, P.cy32, n_grid, n_grid, patch, count, g)
     return PatchSet(r, cx, cy, 1.0 / n_grid)
 
 
@@ -305,21 +306,43 @@ def test_training_reduces_the_loss():
     assert math.isfinite(last) and last < 0.7 * first, hist
 
 
-def test_learned_preconditioner_solves_to_tolerance():
+def test_learned_post_smoother_against_plain_multigrid():
+    """The trained network inside FCG: converges to the tolerance, agrees with
+    the direct solve, and never needs more iterations than plain multigrid
+    (the measured gain is recorded; on these pressure problems multigrid FCG
+    already contracts ~10x per iteration and the learned step rarely saves
+    one)."""
     n = 128
+    data = solver_training_set(n_grid=128, seeds=(1, 2), steps=2, patch=16, count=2048,
+                               targets=False)
     sm = LearnedSmoother(8, 16, seed=0)
-    SmootherTrainer(sm, batch=32, n=16).fit(_patches(), steps=300)
+    hist = SmootherTrainer(sm, batch=32, n=16).fit(data, steps=400, log_every=399)
+    assert hist[-1][1] < 0.5 * hist[0][1]
     h = depth(n, seed=9)
     dx = 1.0 / n
     cx, cy = OP.face_coefficients(h)
     b = np.random.default_rng(10).standard_normal((n, n))
     P = PoissonSolver(n, n, dx)
     P.setup(gpu(h))
+    _, it_mg, _ = P.solve(gpu(b), tol=1e-8, maxit=200, precond="mg")
     x, it, rel = P.solve(gpu(b), tol=1e-8, maxit=200, precond="learned", smoother=sm)
     x = x.cpu().numpy().reshape(n, n)
     true_rel = np.linalg.norm(b - OP.apply(cx, cy, x, dx)) / np.linalg.norm(b)
     assert rel <= 1e-8 and true_rel <= 1.05e-8
     assert rel_l2(x, OP.direct_solve(cx, cy, b, dx)) <= 1e-6
+    assert it <= it_mg, (it, it_mg)
+    print(f"learned post-smoother: {it} FCG iterations, plain multigrid: {it_mg}")
+
+
+def test_learned_replacement_smoother_converges():
+    n = 64
+    sm = LearnedSmoother(8, 16, seed=0)
+    SmootherTrainer(sm, batch=32, n=16).fit(_patches(n_grid=64, count=512), steps=200)
+    P = PoissonSolver(n, n, 1.0 / n)
+    P.setup(gpu(depth(n, seed=2)))
+    b = gpu(np.random.default_rng(3).standard_normal(n * n))
+    _, it, rel = P.solve(b, tol=1e-8, maxit=400, precond="learned_replace", smoother=sm)
+    assert rel <= 1e-8
 
 
 # ── the Chorin march ──────────────────────────────────────────────────────

@@ -14,10 +14,15 @@
 // flexible CG).  Multigrid: cell-centred factor-2 coarsening, coarse face
 // coefficient = mean of the two fine faces it covers, bilinear prolongation P
 // with odd reflection at the Dirichlet boundary, restriction R = P^T / 4,
-// red-black Gauss-Seidel (pre red/black, post black/red), a symmetric V-cycle.
-// Levels whose side is <= 64 run in ONE CTA with every array in shared memory
-// (their launches would otherwise be pure latency).  Layout: cell (i, j) at
-// i*ny + j; x-faces (nx+1, ny) at i*ny + j; y-faces (nx, ny+1) at i*(ny+1)+j.
+// red-black Gauss-Seidel (pre red/black, post black/red), a symmetric V-cycle
+// whose coarsest level (at most 64 cells) is solved exactly with an inverse
+// built at set-up.  Each level larger than 32 x 32 costs two launches per
+// V-cycle: a fused pre-smooth + residual + restriction kernel on the way down
+// and a fused prolongation + post-smooth kernel on the way up (32 x 32 tiles
+// with a halo in shared memory).  Levels whose side is <= 32 run in ONE CTA
+// with every array in shared memory (their launches would otherwise be pure
+// latency).  Layout: cell (i, j) at i*ny + j; x-faces (nx+1, ny) at i*ny + j;
+// y-faces (nx, ny+1) at i*(ny+1) + j.
 #include <cstring>
 #include <algorithm>
 
@@ -28,8 +33,9 @@ namespace pois {
 
 constexpr int NT = 256;
 constexpr int MAXL = 16;
-constexpr int SMALL = 64;        // levels with nx, ny <= SMALL go to the one-CTA kernel
+constexpr int SMALL = 32;        // levels with nx, ny <= SMALL go to the one-CTA kernel
 constexpr int RED_BLOCKS = 592;  // 148 SMs x 4
+constexpr int DENSE_MAX_CELLS = 64;   // coarsest levels this small are solved exactly
 
 struct Level {
   int nx, ny;
@@ -44,6 +50,7 @@ struct Plan {
   long long vr, vz, vp, vq;    // double offsets (Krylov vectors)
   long long part;              // double offset of the reduction partials
   long long scal;              // double offset of the scalars
+  long long cinv;              // float offset of the coarsest inverse (-1: none)
   long long fbase;             // byte offset of the float region
   long long bytes;
   int nu, coarse_sweeps;
@@ -84,6 +91,16 @@ static Plan make_plan(const zb_poisson_cfg* c) {
   }
   P.nlev = l;
   if (P.small0 < 0) P.small0 = l;   // no level small enough: no one-CTA part
+  {
+    const Level& Lc = P.L[l - 1];
+    const long long nc = (long long)Lc.nx * Lc.ny;
+    if (nc <= DENSE_MAX_CELLS) {
+      P.cinv = f;
+      f += nc * nc;
+    } else {
+      P.cinv = -1;
+    }
+  }
   const long long C = (long long)c->nx * c->ny;
   long long d = 0;
   P.cx64 = d; d += (long long)(c->nx + 1) * c->ny;
@@ -376,24 +393,54 @@ residual32_kernel(const float* __restrict__ x, const float* __restrict__ f,
   }
 }
 
-// Weight with which fine cell (fi, fj) interpolates from coarse cell (I, J)
-// under bilinear prolongation with odd reflection (see the oracle); R = P^T/4
-__device__ __forceinline__ float pweight(int fi, int fj, int I, int J, int nxc, int nyc) {
+// One axis of the bilinear cell-centred prolongation with odd reflection at
+// the Dirichlet wall: the weight with which fine index fi (of 2 nc) takes
+// coarse index I.  A fine cell takes 3/4 of its own coarse cell and 1/4 of the
+// neighbour on its side; a neighbour beyond the wall is the reflection -e of
+// the own cell.  The 2-D weights are products of the two axes (9, 3, 3, 1)/16.
+__device__ __forceinline__ float w1d(int fi, int I, int nc) {
+  const int ci = fi >> 1, nb = ci + ((fi & 1) ? 1 : -1);
+  float w = 0.0f;
+  if (ci == I) w += 0.75f;
+  if (nb == I) w += 0.25f;
+  if ((nb < 0 || nb >= nc) && ci == I) w -= 0.25f;
+  return w;
+}
+
+// restriction R = P^T / 4 at coarse cell (I, J) of a fine residual read by
+// rf(fi, fj) (fine indices in range); the fixed loop order makes every
+// implementation below produce the same bits
+template <typename F>
+__device__ __forceinline__ float restrict_at(F rf, int I, int J, int nxc, int nyc) {
+  float s = 0.0f;
+  for (int fi = 2 * I - 1; fi <= 2 * I + 2; ++fi) {
+    if (fi < 0 || fi >= 2 * nxc) continue;
+    const float wx = w1d(fi, I, nxc);
+    float t = 0.0f;
+    for (int fj = 2 * J - 1; fj <= 2 * J + 2; ++fj) {
+      if (fj < 0 || fj >= 2 * nyc) continue;
+      t += w1d(fj, J, nyc) * rf(fi, fj);
+    }
+    s += wx * t;
+  }
+  return 0.25f * s;
+}
+
+// prolongation P e at fine cell (fi, fj) of a coarse field read by ec(I, J)
+template <typename F>
+__device__ __forceinline__ float prolong_at(F ec, int fi, int fj, int nxc, int nyc) {
   const int ci = fi >> 1, cj = fj >> 1;
   const int sx = (fi & 1) ? 1 : -1, sy = (fj & 1) ? 1 : -1;
-  float w = 0.0f;
-  // the four coarse sources of the fine cell: (ci, cj) 9/16, (ci+sx, cj) 3/16,
-  // (ci, cj+sy) 3/16, (ci+sx, cj+sy) 1/16; an out-of-range source maps to the
-  // clipped in-range index with a minus sign per clipped axis
+  float v = 0.0f;
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
     int ii = ci + ((s & 1) ? sx : 0), jj = cj + ((s & 2) ? sy : 0);
     float ww = (s == 0) ? 9.0f / 16.0f : ((s == 3) ? 1.0f / 16.0f : 3.0f / 16.0f);
     if (ii < 0 || ii >= nxc) { ii = ci; ww = -ww; }
     if (jj < 0 || jj >= nyc) { jj = cj; ww = -ww; }
-    if (ii == I && jj == J) w += ww;
+    v += ww * ec(ii, jj);
   }
-  return w;
+  return v;
 }
 
 __global__ void __launch_bounds__(NT)
@@ -402,16 +449,7 @@ restrict_kernel(const float* __restrict__ rf, float* __restrict__ fc, int nxc, i
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nxc * nyc;
        k += (long long)gridDim.x * NT) {
     const int I = (int)(k / nyc), J = (int)(k - (long long)I * nyc);
-    float s = 0.0f;
-    for (int fi = 2 * I - 1; fi <= 2 * I + 2; ++fi) {
-      if (fi < 0 || fi >= 2 * nxc) continue;
-      for (int fj = 2 * J - 1; fj <= 2 * J + 2; ++fj) {
-        if (fj < 0 || fj >= nyf) continue;
-        const float w = pweight(fi, fj, I, J, nxc, nyc);
-        if (w != 0.0f) s += w * rf[fi * nyf + fj];
-      }
-    }
-    fc[k] = 0.25f * s;
+    fc[k] = restrict_at([&](int fi, int fj) { return rf[fi * nyf + fj]; }, I, J, nxc, nyc);
   }
 }
 
@@ -421,18 +459,180 @@ prolong_add_kernel(const float* __restrict__ ec, float* __restrict__ xf, int nxc
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nxf * nyf;
        k += (long long)gridDim.x * NT) {
     const int fi = (int)(k / nyf), fj = (int)(k - (long long)fi * nyf);
-    const int ci = fi >> 1, cj = fj >> 1;
-    const int sx = (fi & 1) ? 1 : -1, sy = (fj & 1) ? 1 : -1;
-    float v = 0.0f;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      int ii = ci + ((s & 1) ? sx : 0), jj = cj + ((s & 2) ? sy : 0);
-      float ww = (s == 0) ? 9.0f / 16.0f : ((s == 3) ? 1.0f / 16.0f : 3.0f / 16.0f);
-      if (ii < 0 || ii >= nxc) { ii = ci; ww = -ww; }
-      if (jj < 0 || jj >= nyc) { jj = cj; ww = -ww; }
-      v += ww * ec[ii * nyc + jj];
+    xf[k] += prolong_at([&](int I, int J) { return ec[I * nyc + J]; }, fi, fj, nxc, nyc);
+  }
+}
+
+// ── fused fine-level kernels: one launch per level on the way down and one on
+// the way up.  A CTA owns a 32 x 32 tile and stages the tile plus a halo in
+// shared memory; each red-black half-sweep is valid one cell further inside
+// the staged region than the last, so after 2 nu half-sweeps the tile (plus
+// the ring the residual and restriction need) holds exactly the values the
+// level-wide sweeps produce.  The operator and update are the same float
+// expressions as apply_at / rbgs_kernel, so the result is bit-identical to the
+// one-kernel-per-sweep sequence.
+constexpr int FT = 32;
+constexpr int FNT = 256;          // 32 x 8 threads
+
+__host__ __device__ inline size_t fused_smem(int halo) {
+  const int R = FT + 2 * halo;
+  return (size_t)(4 * R * R + 2 * (R + 1) * R) * sizeof(float);
+}
+
+// 4-byte asynchronous global -> shared copy; src_bytes 0 writes a zero
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Shared-memory image of a level's tile plus a HALO-wide ring: x, f, r, dg
+// (R x R) and the face coefficients cx ((R+1) x R), cy (R x (R+1)).
+template <int HALO>
+struct Stage {
+  static constexpr int R = FT + 2 * HALO;
+  int i0, j0, nx, ny;
+  float *x, *f, *r, *dg, *cx, *cy;
+  __device__ bool inside(int a, int b) const {
+    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+    return gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+  }
+  __device__ float ax(int a, int b, float idx2) const {
+    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+    const float xc = x[a * R + b];
+    const float ea = cx[(a + 1) * R + b], wa = cx[a * R + b];
+    const float nb = cy[a * (R + 1) + b + 1], sb = cy[a * (R + 1) + b];
+    const float xe = gi + 1 < nx ? x[(a + 1) * R + b] : -xc;
+    const float xw = gi > 0 ? x[(a - 1) * R + b] : -xc;
+    const float xn = gj + 1 < ny ? x[a * R + b + 1] : -xc;
+    const float xs = gj > 0 ? x[a * R + b - 1] : -xc;
+    return (ea * (xc - xe) + wa * (xc - xw) + nb * (xc - xn) + sb * (xc - xs)) * idx2;
+  }
+  // one half-sweep over the cells of `color` at least m cells inside the
+  // staged region; rows over threadIdx.y, same-colour columns over threadIdx.x
+  __device__ void sweep(int color, int m, float idx2) const {
+    for (int a = m + (int)threadIdx.y; a < R - m; a += FNT / 32) {
+      const int gi = i0 - HALO + a;
+      // first column b >= m with (gi + gj) % 2 == color, gj = j0 - HALO + b
+      int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
+      for (; b < R - m; b += 64) {
+        if (!inside(a, b)) continue;
+        const float v = ax(a, b, idx2);
+        x[a * R + b] += (f[a * R + b] - v) / dg[a * R + b];
+      }
     }
-    xf[k] += v;
+    __syncthreads();
+  }
+};
+
+template <int HALO>
+__device__ Stage<HALO> stage_level(float* sm, int i0, int j0, int nx, int ny,
+                                   const float* __restrict__ f, const float* __restrict__ cx,
+                                   const float* __restrict__ cy, const float* __restrict__ dg,
+                                   const float* __restrict__ x) {
+  constexpr int R = Stage<HALO>::R;
+  Stage<HALO> S;
+  S.i0 = i0; S.j0 = j0; S.nx = nx; S.ny = ny;
+  S.x = sm; S.f = sm + R * R; S.r = sm + 2 * R * R; S.dg = sm + 3 * R * R;
+  S.cx = sm + 4 * R * R; S.cy = S.cx + (R + 1) * R;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  // every copy is issued before any is waited for
+  for (int e = tid; e < R * R; e += FNT) {
+    const int a = e / R, b = e - (e / R) * R;
+    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+    const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+    const long long k = in ? (long long)gi * ny + gj : 0;
+    cp_async4(S.f + e, f + k, in);
+    cp_async4(S.dg + e, dg + k, in);
+    if (x) cp_async4(S.x + e, x + k, in);
+    else S.x[e] = 0.0f;
+  }
+  for (int e = tid; e < (R + 1) * R; e += FNT) {
+    {
+      const int a = e / R, b = e - (e / R) * R;
+      const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+      const bool in = gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
+      cp_async4(S.cx + e, cx + (in ? (long long)gi * ny + gj : 0), in);
+    }
+    {
+      const int a = e / (R + 1), b = e - (e / (R + 1)) * (R + 1);
+      const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+      const bool in = gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
+      cp_async4(S.cy + e, cy + (in ? (long long)gi * (ny + 1) + gj : 0), in);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  return S;
+}
+
+// pre-smoothing from x = 0 (NU red/black pairs), residual, restriction:
+// writes the tile's x and the coarse right-hand side of its 16 x 16 coarse cells
+template <int NU>
+__global__ void __launch_bounds__(FNT)
+mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
+               const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
+               float* __restrict__ fc, int nx, int ny, float idx2) {
+  extern __shared__ float fsm[];
+  constexpr int HALO = 2 * NU + 2;
+  constexpr int R = Stage<HALO>::R;
+  const int i0 = blockIdx.y * FT, j0 = blockIdx.x * FT;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const Stage<HALO> S = stage_level<HALO>(fsm, i0, j0, nx, ny, f, cx, cy, dg, nullptr);
+  for (int s = 0; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
+  // residual where the sweeps are final and one ring beyond the tile
+  {
+    constexpr int m = 2 * NU + 1;
+    for (int a = m + (int)threadIdx.y; a < R - m; a += FNT / 32)
+      for (int b = m + (int)threadIdx.x; b < R - m; b += 32)
+        S.r[a * R + b] = S.inside(a, b) ? S.f[a * R + b] - S.ax(a, b, idx2) : 0.0f;
+  }
+  __syncthreads();
+  for (int e = tid; e < FT * FT; e += FNT) {
+    const int ti = e / FT, tj = e % FT;
+    const int gi = i0 + ti, gj = j0 + tj;
+    if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
+  }
+  const int nxc = nx / 2, nyc = ny / 2;
+  for (int e = tid; e < (FT / 2) * (FT / 2); e += FNT) {
+    const int I = i0 / 2 + e / (FT / 2), J = j0 / 2 + e % (FT / 2);
+    if (I >= nxc || J >= nyc) continue;
+    fc[(long long)I * nyc + J] = restrict_at(
+        [&](int fi, int fj) { return S.r[(fi - i0 + HALO) * R + (fj - j0 + HALO)]; }, I, J, nxc,
+        nyc);
+  }
+}
+
+// x += P e (coarse correction), post-smoothing (NU black/red pairs)
+template <int NU>
+__global__ void __launch_bounds__(FNT)
+mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
+             const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
+             const float* __restrict__ ec, int nx, int ny, float idx2) {
+  extern __shared__ float fsm[];
+  constexpr int HALO = 2 * NU;
+  constexpr int R = Stage<HALO>::R;
+  const int i0 = blockIdx.y * FT, j0 = blockIdx.x * FT;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const Stage<HALO> S = stage_level<HALO>(fsm, i0, j0, nx, ny, f, cx, cy, dg, x);
+  const int nxc = nx / 2, nyc = ny / 2;
+  for (int a = (int)threadIdx.y; a < R; a += FNT / 32)
+    for (int b = (int)threadIdx.x; b < R; b += 32) {
+      if (!S.inside(a, b)) continue;
+      const int fi = i0 - HALO + a, fj = j0 - HALO + b;
+      S.x[a * R + b] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
+                                   fj, nxc, nyc);
+    }
+  __syncthreads();
+  for (int s = 0; s < 2 * NU; ++s) S.sweep(1 - (s & 1), s + 1, idx2);
+  for (int e = tid; e < FT * FT; e += FNT) {
+    const int ti = e / FT, tj = e % FT;
+    const int gi = i0 + ti, gj = j0 + tj;
+    if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
   }
 }
 
@@ -461,6 +661,31 @@ __device__ void cta_rbgs(float* x, const float* f, const float* cx, const float*
     x[i * ny + j] += (f[i * ny + j] - ax) / dg[i * ny + j];
   }
   __syncthreads();
+}
+
+// coarsest-level solve: x = A^-1 f with the inverse built at set-up when the
+// level has <= DENSE_MAX_CELLS cells, else symmetric red-black sweep pairs
+__device__ void cta_coarsest(float* x, const float* f, const float* cx, const float* cy,
+                             const float* dg, const float* inv, int nx, int ny, float idx2,
+                             int sweeps) {
+  const int n = nx * ny;
+  if (inv) {
+    for (int k = threadIdx.x; k < n; k += CT) {
+      float v = 0.0f;
+      for (int m = 0; m < n; ++m) v += inv[k * n + m] * f[m];
+      x[k] = v;
+    }
+    __syncthreads();
+    return;
+  }
+  for (int s = 0; s < sweeps; ++s) {
+    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 0);
+    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 1);
+  }
+  for (int s = 0; s < sweeps; ++s) {
+    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 1);
+    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 0);
+  }
 }
 
 __global__ void __launch_bounds__(CT)
@@ -492,19 +717,13 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     }
   }
   __syncthreads();
+  const float* inv = P.cinv >= 0 ? ws_f + P.cinv : nullptr;
   // descend
   for (int l = P.small0; l < P.nlev; ++l) {
     const Level& L = P.L[l];
     const float idx2 = 1.0f / (L.dx * L.dx);
     if (l == P.nlev - 1) {
-      for (int s = 0; s < coarse_sweeps; ++s) {
-        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
-        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
-      }
-      for (int s = 0; s < coarse_sweeps; ++s) {
-        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
-        cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
-      }
+      cta_coarsest(sx[l], sf[l], scx[l], scy[l], sdg[l], inv, L.nx, L.ny, idx2, coarse_sweeps);
       break;
     }
     for (int s = 0; s < nu; ++s) {
@@ -518,18 +737,12 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     }
     __syncthreads();
     const Level& Lc = P.L[l + 1];
+    const float* rl = sr[l];
+    const int nyf = L.ny;
     for (int k = threadIdx.x; k < Lc.nx * Lc.ny; k += CT) {
       const int I = k / Lc.ny, J = k - I * Lc.ny;
-      float s = 0.0f;
-      for (int fi = 2 * I - 1; fi <= 2 * I + 2; ++fi) {
-        if (fi < 0 || fi >= L.nx) continue;
-        for (int fj = 2 * J - 1; fj <= 2 * J + 2; ++fj) {
-          if (fj < 0 || fj >= L.ny) continue;
-          const float w = pweight(fi, fj, I, J, Lc.nx, Lc.ny);
-          if (w != 0.0f) s += w * sr[l][fi * L.ny + fj];
-        }
-      }
-      sf[l + 1][k] = 0.25f * s;
+      sf[l + 1][k] = restrict_at([&](int fi, int fj) { return rl[fi * nyf + fj]; }, I, J, Lc.nx,
+                                 Lc.ny);
     }
     __syncthreads();
   }
@@ -538,19 +751,11 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     const Level& L = P.L[l];
     const Level& Lc = P.L[l + 1];
     const float idx2 = 1.0f / (L.dx * L.dx);
+    const float* ecl = sx[l + 1];
+    const int nyc = Lc.ny;
     for (int k = threadIdx.x; k < L.nx * L.ny; k += CT) {
       const int fi = k / L.ny, fj = k - fi * L.ny;
-      const int ci = fi >> 1, cj = fj >> 1;
-      const int sxg = (fi & 1) ? 1 : -1, syg = (fj & 1) ? 1 : -1;
-      float v = 0.0f;
-      for (int s = 0; s < 4; ++s) {
-        int ii = ci + ((s & 1) ? sxg : 0), jj = cj + ((s & 2) ? syg : 0);
-        float ww = (s == 0) ? 9.0f / 16.0f : ((s == 3) ? 1.0f / 16.0f : 3.0f / 16.0f);
-        if (ii < 0 || ii >= Lc.nx) { ii = ci; ww = -ww; }
-        if (jj < 0 || jj >= Lc.ny) { jj = cj; ww = -ww; }
-        v += ww * sx[l + 1][ii * Lc.ny + jj];
-      }
-      sx[l][k] += v;
+      sx[l][k] += prolong_at([&](int I, int J) { return ecl[I * nyc + J]; }, fi, fj, Lc.nx, Lc.ny);
     }
     __syncthreads();
     for (int s = 0; s < nu; ++s) {
@@ -560,6 +765,53 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
   }
   const Level& L0 = P.L[P.small0];
   for (int k = threadIdx.x; k < L0.nx * L0.ny; k += CT) ws_f[L0.x + k] = sx[P.small0][k];
+}
+
+// dense inverse of the coarsest operator (float64 in-place Gauss-Jordan; the
+// operator is SPD, so no pivoting), stored as float32 for the V-cycle; one CTA
+__global__ void coarse_inverse_kernel(const Plan P, float* ws_f) {
+  __shared__ double a[DENSE_MAX_CELLS][DENSE_MAX_CELLS];
+  __shared__ double fcol[DENSE_MAX_CELLS];
+  const Level& L = P.L[P.nlev - 1];
+  const int nx = L.nx, ny = L.ny, n = nx * ny;
+  const double idx2 = 1.0 / ((double)L.dx * (double)L.dx);
+  const float* cx = ws_f + L.cx;
+  const float* cy = ws_f + L.cy;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[e / n][e % n] = 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        const int k = i * ny + j;
+        const double e = cx[(i + 1) * ny + j], w = cx[i * ny + j];
+        const double nn = cy[i * (ny + 1) + j + 1], ss = cy[i * (ny + 1) + j];
+        double d = (e + w) + (nn + ss);
+        if (i == 0) d += w;
+        if (i == nx - 1) d += e;
+        if (j == 0) d += ss;
+        if (j == ny - 1) d += nn;
+        a[k][k] = d * idx2;
+        if (i + 1 < nx) a[k][k + ny] = -e * idx2;
+        if (i > 0) a[k][k - ny] = -w * idx2;
+        if (j + 1 < ny) a[k][k + 1] = -nn * idx2;
+        if (j > 0) a[k][k - 1] = -ss * idx2;
+      }
+  }
+  __syncthreads();
+  for (int p = 0; p < n; ++p) {
+    const double piv = a[p][p];
+    __syncthreads();
+    for (int c = threadIdx.x; c < n; c += blockDim.x) a[p][c] = (c == p ? 1.0 : a[p][c]) / piv;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) fcol[r] = (r == p) ? 0.0 : a[r][p];
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e % n;
+      if (r != p) a[r][c] = (c == p ? 0.0 : a[r][c]) - fcol[r] * a[p][c];
+    }
+    __syncthreads();
+  }
+  float* inv = ws_f + P.cinv;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) inv[e] = (float)a[e / n][e % n];
 }
 
 static size_t coarse_smem(const Plan& P) {
@@ -581,6 +833,13 @@ static int enable_coarse_smem() {
   if (dev < 32 && !(set_mask & (1u << dev))) {
     ZB_CUDA_TRY(cudaFuncSetAttribute(coarse_vcycle_kernel,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+#define ZB_SMEM_ATTR(K) \
+    ZB_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))
+    ZB_SMEM_ATTR(mg_down_kernel<1>); ZB_SMEM_ATTR(mg_down_kernel<2>);
+    ZB_SMEM_ATTR(mg_down_kernel<3>); ZB_SMEM_ATTR(mg_down_kernel<4>);
+    ZB_SMEM_ATTR(mg_up_kernel<1>); ZB_SMEM_ATTR(mg_up_kernel<2>);
+    ZB_SMEM_ATTR(mg_up_kernel<3>); ZB_SMEM_ATTR(mg_up_kernel<4>);
+#undef ZB_SMEM_ATTR
     set_mask |= 1u << dev;
   }
   return ZB_OK;
@@ -644,7 +903,7 @@ __global__ void correct_kernel(T* __restrict__ qx, T* __restrict__ qy,
 
 static bool valid(const zb_poisson_cfg* c) {
   return c && c->nx >= 2 && c->ny >= 2 && c->dx > 0 && c->cmin > 0 && c->cmax >= c->cmin &&
-         c->nu >= 0 && c->coarse_sweeps >= 1 && c->coarsest >= 2 &&
+         c->nu >= 0 && c->nu <= 4 && c->coarse_sweeps >= 1 && c->coarsest >= 2 &&
          (long long)c->nx * c->ny < (1LL << 31);
 }
 
@@ -659,34 +918,40 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + L0.f, fw + L0.x, n0);
     return zb_launch_check();
   }
+  // fine levels: one fused launch each on the way down
   for (int l = 0; l < P.small0 && l < P.nlev - 1; ++l) {
     const Level& L = P.L[l];
+    const Level& Lc = P.L[l + 1];
     const long long n = (long long)L.nx * L.ny;
     const float idx2 = 1.0f / (L.dx * L.dx);
-    zero32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, n);
     if (l == 0 && precond == 3) {
+      zero32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, n);
       int rc = zb_smoother_apply(smo, fw + L.f, nullptr, fw + L.x, fw + L.cx, fw + L.cy,
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 1, (void*)st);
       if (rc) return rc;
+      residual32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
+                                                    fw + L.r, L.nx, L.ny, idx2);
+      restrict_kernel<<<grid_for((long long)Lc.nx * Lc.ny), NT, 0, st>>>(fw + L.r, fw + Lc.f,
+                                                                          Lc.nx, Lc.ny);
     } else {
-      for (int s = 0; s < P.nu; ++s) {
-        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                        fw + L.dg, L.nx, L.ny, idx2, 0);
-        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                        fw + L.dg, L.nx, L.ny, idx2, 1);
+      const dim3 grid((L.ny + FT - 1) / FT, (L.nx + FT - 1) / FT);
+      const dim3 blk(32, FNT / 32);
+      const size_t sm = fused_smem(2 * P.nu + 2);
+      float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x,
+            *a5 = fw + Lc.f;
+      switch (P.nu) {
+        case 1: mg_down_kernel<1><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
+        case 2: mg_down_kernel<2><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
+        case 3: mg_down_kernel<3><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
+        default: mg_down_kernel<4><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
       }
     }
-    residual32_kernel<<<grid_for(n), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                  fw + L.r, L.nx, L.ny, idx2);
-    const Level& Lc = P.L[l + 1];
-    restrict_kernel<<<grid_for((long long)Lc.nx * Lc.ny), NT, 0, st>>>(fw + L.r, fw + Lc.f, Lc.nx,
-                                                                        Lc.ny);
   }
   if (P.small0 < P.nlev) {
     const size_t smem = coarse_smem(P);
     coarse_vcycle_kernel<<<1, CT, smem, st>>>(P, fw, P.nu, P.coarse_sweeps);
   } else {
-    // no level fits the one-CTA kernel: smooth the coarsest level in place
+    // no level fits the one-CTA kernel: sweep the coarsest level in place
     const Level& L = P.L[P.nlev - 1];
     const long long n = (long long)L.nx * L.ny;
     const float idx2 = 1.0f / (L.dx * L.dx);
@@ -699,22 +964,28 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
                                                       fw + L.dg, L.nx, L.ny, idx2, 1 - c0);
     }
   }
+  // fine levels on the way up: coarse correction + post-smoothing, fused
   for (int l = std::min(P.small0, P.nlev - 1) - 1; l >= 0; --l) {
     const Level& L = P.L[l];
     const Level& Lc = P.L[l + 1];
     const long long n = (long long)L.nx * L.ny;
     const float idx2 = 1.0f / (L.dx * L.dx);
-    prolong_add_kernel<<<grid_for(n), NT, 0, st>>>(fw + Lc.x, fw + L.x, Lc.nx, Lc.ny);
     if (l == 0 && precond == 3) {
+      prolong_add_kernel<<<grid_for(n), NT, 0, st>>>(fw + Lc.x, fw + L.x, Lc.nx, Lc.ny);
       int rc = zb_smoother_apply(smo, fw + L.f, fw + L.x, fw + L.x, fw + L.cx, fw + L.cy,
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 0, (void*)st);
       if (rc) return rc;
     } else {
-      for (int s = 0; s < P.nu; ++s) {
-        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                        fw + L.dg, L.nx, L.ny, idx2, 1);
-        rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                        fw + L.dg, L.nx, L.ny, idx2, 0);
+      const dim3 grid((L.ny + FT - 1) / FT, (L.nx + FT - 1) / FT);
+      const dim3 blk(32, FNT / 32);
+      const size_t sm = fused_smem(2 * P.nu);
+      float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x,
+            *a5 = fw + Lc.x;
+      switch (P.nu) {
+        case 1: mg_up_kernel<1><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
+        case 2: mg_up_kernel<2><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
+        case 3: mg_up_kernel<3><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
+        default: mg_up_kernel<4><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
       }
     }
   }
@@ -776,10 +1047,8 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
     coef_from_h<float><<<grid_for(nf), NT, 0, st>>>((const float*)h, L0.nx, L0.ny, cfg->cmin,
                                                     cfg->cmax, dw + P.cx64, dw + P.cy64,
                                                     fw + L0.cx, fw + L0.cy);
-  if (P.small0 < P.nlev) {
-    if (coarse_smem(P) > 227 * 1024) return ZB_E_TOO_LARGE;
-    if (const int e = enable_coarse_smem()) return e;
-  }
+  if (P.small0 < P.nlev && coarse_smem(P) > 227 * 1024) return ZB_E_TOO_LARGE;
+  if (const int e = enable_coarse_smem()) return e;
   const long long n0 = (long long)L0.nx * L0.ny;
   diag_kernel64<<<grid_for(n0), NT, 0, st>>>(dw + P.cx64, dw + P.cy64, L0.nx, L0.ny,
                                              1.0 / (cfg->dx * cfg->dx), dw + P.dg64);
@@ -794,6 +1063,7 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
     diag_kernel32<<<grid_for((long long)L.nx * L.ny), NT, 0, st>>>(
         fw + L.cx, fw + L.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.dg);
   }
+  if (P.cinv >= 0) coarse_inverse_kernel<<<1, 256, 0, st>>>(P, fw);
   return zb_launch_check();
 }
 

@@ -256,12 +256,17 @@ __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float*
 namespace zb {
 namespace unet {
 
-// per image b: s[b] = sqrt(mean r^2) (tiny floor so a zero residual stays zero)
-__global__ void rms_kernel(const float* __restrict__ r, int B, size_t npix, float* __restrict__ s) {
+// per image b: s[b] = sqrt(mean r^2) (tiny floor so a zero residual stays
+// zero), as a two-stage deterministic reduction: P partial sums per image
+// (grid (P, B)), then one warp per image adds them in a fixed order
+constexpr int RMS_PARTS = 1024;   // partial-sum slots in the workspace
+
+__global__ void rms_part_kernel(const float* __restrict__ r, size_t npix, int P,
+                                float* __restrict__ part) {
   __shared__ float red[NT / 32];
-  const int b = blockIdx.x;
+  const int b = blockIdx.y, p = blockIdx.x;
   float acc = 0.0f;
-  for (size_t k = threadIdx.x; k < npix; k += NT) {
+  for (size_t k = (size_t)p * NT + threadIdx.x; k < npix; k += (size_t)P * NT) {
     const float v = r[(size_t)b * npix + k];
     acc += v * v;
   }
@@ -271,8 +276,24 @@ __global__ void rms_kernel(const float* __restrict__ r, int B, size_t npix, floa
   if (threadIdx.x == 0) {
     float t = 0.0f;
     for (int i = 0; i < NT / 32; ++i) t += red[i];
-    s[b] = fmaxf(sqrtf(t / (float)npix), 1e-30f);
+    part[b * P + p] = t;
   }
+}
+
+__global__ void rms_final_kernel(const float* __restrict__ part, int P, size_t npix,
+                                 float* __restrict__ s) {
+  const int b = blockIdx.x;
+  float t = 0.0f;
+  for (int p = threadIdx.x; p < P; p += 32) t += part[b * P + p];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (threadIdx.x == 0) s[b] = fmaxf(sqrtf(t / (float)npix), 1e-30f);
+}
+
+static void rms(const float* r, int B, size_t npix, float* part, float* s, cudaStream_t st) {
+  int P = (int)std::min<size_t>(256, std::max<size_t>(1, npix / (NT * 16)));
+  P = std::max(1, std::min(P, RMS_PARTS / std::max(1, B)));
+  rms_part_kernel<<<dim3(P, B), NT, 0, st>>>(r, npix, P, part);
+  rms_final_kernel<<<B, 32, 0, st>>>(part, P, npix, s);
 }
 
 // cell coefficient of image b's cell (i, j) from its faces: cx (B, H+1, W),
@@ -553,7 +574,7 @@ static int gridn(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n
 
 // activation buffers (floats) for a batch of B images H x W
 struct Acts {
-  float *in, *e1, *e2, *p, *m1, *m2, *u, *o1, *out, *s;
+  float *in, *e1, *e2, *p, *m1, *m2, *u, *o1, *out, *s, *part;
   // training: gradients and scratch
   float *d_e1, *d_e2, *d_p, *d_m1, *d_m2, *d_cat, *d_o1, *d_out, *res, *lnum, *lden, *tmp;
   __nv_bfloat16* wflip;
@@ -562,7 +583,7 @@ struct Acts {
 static size_t acts_floats(const Net& n, int B, int H, int W, bool train) {
   const size_t N0 = (size_t)B * H * W, N1 = (size_t)B * (H / 2) * (W / 2);
   size_t f = 2 * N0 + 2 * (size_t)n.c1 * N0 + (size_t)n.c1 * N1 + 2 * (size_t)n.c2 * N1 +
-             (size_t)n.c2 * N0 + (size_t)n.c1 * N0 + N0 + 512;
+             (size_t)n.c2 * N0 + (size_t)n.c1 * N0 + N0 + 512 + RMS_PARTS;
   if (train)
     f += 2 * (size_t)n.c1 * N0 + (size_t)n.c1 * N1 + 2 * (size_t)n.c2 * N1 +
          (size_t)(n.c1 + n.c2) * N0 + (size_t)n.c1 * N0 + N0 + N0 + 1024 +
@@ -585,6 +606,7 @@ static Acts acts_split(const Net& n, void* base, int B, int H, int W, bool train
   a.o1 = f; f += (size_t)n.c1 * N0;
   a.out = f; f += N0;
   a.s = f; f += 512;   // per-image RMS, batch <= 512
+  a.part = f; f += RMS_PARTS;
   if (train) {
     a.d_e1 = f; f += (size_t)n.c1 * N0;
     a.d_e2 = f; f += (size_t)n.c1 * N0;
@@ -681,7 +703,7 @@ int zb_smoother_apply(const zb_smoother* smo, const float* f, const float* x_in,
   const float idx2 = (float)(1.0 / (dx * dx));
   const size_t N0 = (size_t)nx * ny;
   patch_residual<<<gridn(N0), NT, 0, st>>>(f, x_in, cx, cy, 1, nx, ny, idx2, r_scratch);
-  rms_kernel<<<1, NT, 0, st>>>(r_scratch, 1, N0, a.s);
+  rms(r_scratch, 1, N0, a.part, a.s, st);
   features_kernel<<<gridn(N0), NT, 0, st>>>(r_scratch, a.s, cx, cy, 1, nx, ny,
                                             1.0f / smo->cmax, a.in);
   int rc = forward(n, a, (const __nv_bfloat16*)smo->w, smo->b, 1, nx, ny, st);
@@ -704,7 +726,7 @@ int zb_unet_forward(const zb_unet_trainer* t, const float* r, const float* cx, c
   const Acts a = acts_split(n, t->act, t->batch, t->n, t->n, true);
   const int B = t->batch, H = t->n, W = t->n;
   const size_t N0 = (size_t)B * H * W;
-  rms_kernel<<<B, NT, 0, st>>>(r, B, (size_t)H * W, a.s);
+  rms(r, B, (size_t)H * W, a.part, a.s, st);
   features_kernel<<<gridn(N0), NT, 0, st>>>(r, a.s, cx, cy, B, H, W, 1.0f / t->cmax, a.in);
   int rc = forward(n, a, (const __nv_bfloat16*)t->w_bf16, t->b_master, B, H, W, st);
   if (rc) return rc;
