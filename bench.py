@@ -178,6 +178,25 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def max_over_ranks(seconds, world, device=None):
+    """The slowest rank's time (the whole job finishes when it does); the
+    identity on one rank.  The collective is the only one of the timing path
+    and every rank calls it in the same order."""
+    if world <= 1:
+        return float(seconds)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells_per_rank, steps, seconds_max, world):
+    """Cell-updates/s of the whole job: every rank advances its own replica
+    of ``cells_per_rank`` cells by ``steps`` steps (weak scaling)."""
+    return world * cells_per_rank * steps / seconds_max
+
+
 def run_gpu(args, rank, world, local_rank):
     import ctypes as C
     import numpy as np
@@ -253,14 +272,8 @@ def run_gpu(args, rank, world, local_rank):
     step_s = sum(st1) + sum(st2)
     c = solver.read_ctrl()
     status_ok = c.status == 0
-    # max over ranks
-    tmax = step_s
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([step_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tmax = float(t.item())
-    value = world * C_cells * K / tmax
+    tmax = max_over_ranks(step_s, world, dev)
+    value = whole_job_rate(C_cells, K, tmax, world)
 
     # roofline of the dominant kernel (stage 2: reads Q1 h/qx/qy + b + Q0
     # h/qx/qy = 7 planes, writes 3 planes), algorithmic bytes per launch
@@ -315,14 +328,9 @@ def run_gpu(args, rank, world, local_rank):
     host_out.copy_(Qd, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_s = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
     state_bytes = 4 * C_cells * es
-    e2e = {"value": world * C_cells * K / e2e_s, "unit": UNIT,
+    e2e = {"value": whole_job_rate(C_cells, K, e2e_s, world), "unit": UNIT,
            "h2d_bytes_per_step": state_bytes // K,
            "d2h_bytes_per_step": L.CTRL_BYTES + state_bytes // K,
            "how": ("public C ABI (zb_swe2d_init/zb_swe2d_step) with pinned host "
@@ -346,7 +354,7 @@ def _ev_ms(fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def run_chorin(local_rank, n=1024, steps=10, warmup=3):
+def run_chorin(local_rank, n=1024, steps=10, warmup=3, train_steps=2000, use_graph=True):
     """The non-hydrostatic configuration: Chorin steps (hyperbolic Euler ->
     pressure Poisson to 1e-8 -> corrector) on an n x n grid, plain multigrid
     FCG against the learned U-Net post-smoother (trained here on the GPU by
@@ -369,7 +377,7 @@ def run_chorin(local_rank, n=1024, steps=10, warmup=3):
         sol = ChorinSolver(pressure_tol=1e-8, pressure_maxit=200, precond=precond,
                            smoother=smoother, compute_dt=zb.timestepping.adaptive(0.45, 2),
                            reconstruction_variables="eta", free_surface_h_index=1,
-                           eps_wet=1e-6, dtype="float32", device=dev)
+                           eps_wet=1e-6, dtype="float32", device=dev, use_graph=use_graph)
         Q, _ = sol.setup_simulation(zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n), nsm)
         return sol, Q
 
@@ -403,13 +411,13 @@ def run_chorin(local_rank, n=1024, steps=10, warmup=3):
         sm = LearnedSmoother(c1, c2, seed=0, device=dev)
         tr = SmootherTrainer(sm, batch=64, n=32, lr=3e-3)
         t0 = time.perf_counter()
-        hist = tr.fit(data, steps=2000, log_every=1000)
+        hist = tr.fit(data, steps=train_steps, log_every=max(1, train_steps // 2))
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
         r = measure("learned", sm)
         r.update({"network": f"U-Net c1={c1} c2={c2}, {sm.n_params} params, bf16 weights, "
                              f"tcgen05 convolutions, fp32 accumulation",
-                  "train_s": round(t_train, 2), "train_steps": 2000,
+                  "train_s": round(t_train, 2), "train_steps": train_steps,
                   "train_loss": [round(v, 4) for _, v in hist],
                   "training_set": f"{data.count} 32x32 patches from 256^2 solver runs "
                                   f"({round(t_data, 2)} s to generate)",
@@ -458,6 +466,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the Chorin and ensemble legs")
+    ap.add_argument("--legs", default="swe,chorin,ensemble",
+                    help="comma-separated legs to run (profiling runs pick one)")
+    ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--chorin-steps", type=int, default=10)
+    ap.add_argument("--chorin-no-graph", action="store_true",
+                    help="drive the pressure iterations from the host (for profilers, which "
+                         "do not list kernels inside conditional graph nodes)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -497,6 +512,22 @@ def main():
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": sample}
 
+    legs = set(args.legs.split(","))
+    if "swe" not in legs:
+        # a single extra leg (profiling): rank 0 only, its own JSON line
+        if rank != 0:
+            return
+        import torch
+        torch.cuda.set_device(local_rank)
+        line = {"legs": sorted(legs)}
+        if "chorin" in legs:
+            line["chorin"] = run_chorin(local_rank, steps=args.chorin_steps,
+                                        train_steps=args.train_steps,
+                                        use_graph=not args.chorin_no_graph)
+        if "ensemble" in legs:
+            line["ensemble"] = run_ensemble(local_rank)
+        print(json.dumps(line), flush=True)
+        return
     if world > 1:
         import datetime
         import torch
@@ -512,8 +543,11 @@ def main():
         return
     extra = {}
     if not args.no_extra:
-        extra["chorin"] = run_chorin(local_rank)
-        extra["ensemble"] = run_ensemble(local_rank)
+        if "chorin" in legs:
+            extra["chorin"] = run_chorin(local_rank, steps=args.chorin_steps,
+                                         train_steps=args.train_steps)
+        if "ensemble" in legs:
+            extra["ensemble"] = run_ensemble(local_rank)
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["ms_per_step"], "higher_is_better": True,

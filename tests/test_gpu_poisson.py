@@ -74,19 +74,24 @@ def test_apply_matches_oracle(nx, ny):
     assert np.array_equal(P.cy32.cpu().numpy().reshape(nx, ny + 1), cy.astype(np.float32))
 
 
-@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 128), (128, 96), (256, 256)])
-def test_vcycle_matches_oracle(nx, ny):
+@pytest.mark.parametrize("nx,ny,nu,coarsest", [
+    (64, 64, 2, 4), (128, 128, 2, 4), (128, 96, 2, 4), (256, 256, 2, 8),
+    (96, 80, 1, 4),       # tiles cut by the domain edge, levels of odd tile counts
+    (512, 512, 3, 8),     # mostly interior tiles (the edge-free path)
+    (200, 136, 2, 8),     # coarsening stops at 25 x 17: no one-CTA level, swept coarsest
+])
+def test_vcycle_matches_oracle(nx, ny, nu, coarsest):
     rng = np.random.default_rng(2)
     h = depth(max(nx, ny))[:nx, :ny]
     dx = 1.0 / nx
-    P = PoissonSolver(nx, ny, dx, coarse_sweeps=8, coarsest=4)
+    P = PoissonSolver(nx, ny, dx, nu=nu, coarse_sweeps=8, coarsest=coarsest)
     P.setup(gpu(h))
     cx, cy = OP.face_coefficients(h)
-    H = OP.Hierarchy(cx, cy, dx, coarsest=4)
+    H = OP.Hierarchy(cx, cy, dx, coarsest=coarsest)
     assert len(H.levels) == P.n_levels
     r = rng.standard_normal((nx, ny))
     z = P.vcycle(gpu(r, torch.float32)).cpu().numpy().astype(np.float64).reshape(nx, ny)
-    zo = OP.vcycle(H, r, nu=2, coarse_sweeps=8)
+    zo = OP.vcycle(H, r, nu=nu, coarse_sweeps=8)
     assert rel_l2(z, zo) <= 2e-5
 
 

@@ -16,10 +16,10 @@
 // with odd reflection at the Dirichlet boundary, restriction R = P^T / 4,
 // red-black Gauss-Seidel (pre red/black, post black/red), a symmetric V-cycle
 // whose coarsest level (at most 64 cells) is solved exactly with an inverse
-// built at set-up.  Each level larger than 32 x 32 costs two launches per
+// built at set-up.  Each level larger than 16 x 16 costs two launches per
 // V-cycle: a fused pre-smooth + residual + restriction kernel on the way down
 // and a fused prolongation + post-smooth kernel on the way up (32 x 32 tiles
-// with a halo in shared memory).  Levels whose side is <= 32 run in ONE CTA
+// with a halo in shared memory).  Levels whose side is <= 16 run in ONE CTA
 // with every array in shared memory (their launches would otherwise be pure
 // latency).  Layout: cell (i, j) at i*ny + j; x-faces (nx+1, ny) at i*ny + j;
 // y-faces (nx, ny+1) at i*(ny+1) + j.
@@ -33,7 +33,7 @@ namespace pois {
 
 constexpr int NT = 256;
 constexpr int MAXL = 16;
-constexpr int SMALL = 32;        // levels with nx, ny <= SMALL go to the one-CTA kernel
+constexpr int SMALL = 16;        // levels with nx, ny <= SMALL go to the one-CTA kernel
 constexpr int RED_BLOCKS = 592;  // 148 SMs x 4
 constexpr int DENSE_MAX_CELLS = 64;   // coarsest levels this small are solved exactly
 
@@ -472,7 +472,7 @@ prolong_add_kernel(const float* __restrict__ ec, float* __restrict__ xf, int nxc
 // expressions as apply_at / rbgs_kernel, so the result is bit-identical to the
 // one-kernel-per-sweep sequence.
 constexpr int FT = 32;
-constexpr int FNT = 256;          // 32 x 8 threads
+constexpr int FNT_MAX = 1024;     // blocks are 32 x 8 (large levels) or 32 x 32 (small levels)
 
 __host__ __device__ inline size_t fused_smem(int halo) {
   const int R = FT + 2 * halo;
@@ -491,41 +491,58 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // Shared-memory image of a level's tile plus a HALO-wide ring: x, f, r, dg
-// (R x R) and the face coefficients cx ((R+1) x R), cy (R x (R+1)).
+// (R x R) and the face coefficients cx ((R+1) x R), cy (R x (R+1)).  A tile
+// whose ring lies wholly inside the level (most of them) takes the EDGE-free
+// path: no domain tests and no Dirichlet ghosts.
 template <int HALO>
 struct Stage {
   static constexpr int R = FT + 2 * HALO;
   int i0, j0, nx, ny;
+  bool interior;
   float *x, *f, *r, *dg, *cx, *cy;
   __device__ bool inside(int a, int b) const {
     const int gi = i0 - HALO + a, gj = j0 - HALO + b;
     return gi >= 0 && gi < nx && gj >= 0 && gj < ny;
   }
+  template <bool EDGE>
   __device__ float ax(int a, int b, float idx2) const {
-    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
     const float xc = x[a * R + b];
     const float ea = cx[(a + 1) * R + b], wa = cx[a * R + b];
     const float nb = cy[a * (R + 1) + b + 1], sb = cy[a * (R + 1) + b];
-    const float xe = gi + 1 < nx ? x[(a + 1) * R + b] : -xc;
-    const float xw = gi > 0 ? x[(a - 1) * R + b] : -xc;
-    const float xn = gj + 1 < ny ? x[a * R + b + 1] : -xc;
-    const float xs = gj > 0 ? x[a * R + b - 1] : -xc;
+    float xe = x[(a + 1) * R + b], xw = x[(a - 1) * R + b];
+    float xn = x[a * R + b + 1], xs = x[a * R + b - 1];
+    if (EDGE) {
+      const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+      if (gi + 1 >= nx) xe = -xc;
+      if (gi <= 0) xw = -xc;
+      if (gj + 1 >= ny) xn = -xc;
+      if (gj <= 0) xs = -xc;
+    }
     return (ea * (xc - xe) + wa * (xc - xw) + nb * (xc - xn) + sb * (xc - xs)) * idx2;
   }
-  // one half-sweep over the cells of `color` at least m cells inside the
-  // staged region; rows over threadIdx.y, same-colour columns over threadIdx.x
-  __device__ void sweep(int color, int m, float idx2) const {
-    for (int a = m + (int)threadIdx.y; a < R - m; a += FNT / 32) {
+  template <bool EDGE>
+  __device__ void sweep_impl(int color, int m, float idx2) const {
+    for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y) {
       const int gi = i0 - HALO + a;
       // first column b >= m with (gi + gj) % 2 == color, gj = j0 - HALO + b
       int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
       for (; b < R - m; b += 64) {
-        if (!inside(a, b)) continue;
-        const float v = ax(a, b, idx2);
+        if (EDGE && !inside(a, b)) continue;
+        const float v = ax<EDGE>(a, b, idx2);
         x[a * R + b] += (f[a * R + b] - v) / dg[a * R + b];
       }
     }
     __syncthreads();
+  }
+  // one half-sweep over the cells of `color` at least m cells inside the
+  // staged region; rows over threadIdx.y, same-colour columns over threadIdx.x
+  __device__ void sweep(int color, int m, float idx2) const {
+    if (interior) sweep_impl<false>(color, m, idx2);
+    else sweep_impl<true>(color, m, idx2);
+  }
+  __device__ float residual(int a, int b, float idx2) const {
+    if (interior) return f[a * R + b] - ax<false>(a, b, idx2);
+    return inside(a, b) ? f[a * R + b] - ax<true>(a, b, idx2) : 0.0f;
   }
 };
 
@@ -537,11 +554,13 @@ __device__ Stage<HALO> stage_level(float* sm, int i0, int j0, int nx, int ny,
   constexpr int R = Stage<HALO>::R;
   Stage<HALO> S;
   S.i0 = i0; S.j0 = j0; S.nx = nx; S.ny = ny;
+  S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
   S.x = sm; S.f = sm + R * R; S.r = sm + 2 * R * R; S.dg = sm + 3 * R * R;
   S.cx = sm + 4 * R * R; S.cy = S.cx + (R + 1) * R;
-  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int nt = (int)(blockDim.x * blockDim.y);
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   // every copy is issued before any is waited for
-  for (int e = tid; e < R * R; e += FNT) {
+  for (int e = tid; e < R * R; e += nt) {
     const int a = e / R, b = e - (e / R) * R;
     const int gi = i0 - HALO + a, gj = j0 - HALO + b;
     const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
@@ -551,7 +570,7 @@ __device__ Stage<HALO> stage_level(float* sm, int i0, int j0, int nx, int ny,
     if (x) cp_async4(S.x + e, x + k, in);
     else S.x[e] = 0.0f;
   }
-  for (int e = tid; e < (R + 1) * R; e += FNT) {
+  for (int e = tid; e < (R + 1) * R; e += nt) {
     {
       const int a = e / R, b = e - (e / R) * R;
       const int gi = i0 - HALO + a, gj = j0 - HALO + b;
@@ -573,7 +592,7 @@ __device__ Stage<HALO> stage_level(float* sm, int i0, int j0, int nx, int ny,
 // pre-smoothing from x = 0 (NU red/black pairs), residual, restriction:
 // writes the tile's x and the coarse right-hand side of its 16 x 16 coarse cells
 template <int NU>
-__global__ void __launch_bounds__(FNT)
+__global__ void __launch_bounds__(FNT_MAX)
 mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
                const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
                float* __restrict__ fc, int nx, int ny, float idx2) {
@@ -581,24 +600,25 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   constexpr int HALO = 2 * NU + 2;
   constexpr int R = Stage<HALO>::R;
   const int i0 = blockIdx.y * FT, j0 = blockIdx.x * FT;
-  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int nt = (int)(blockDim.x * blockDim.y);
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const Stage<HALO> S = stage_level<HALO>(fsm, i0, j0, nx, ny, f, cx, cy, dg, nullptr);
   for (int s = 0; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
   // residual where the sweeps are final and one ring beyond the tile
   {
     constexpr int m = 2 * NU + 1;
-    for (int a = m + (int)threadIdx.y; a < R - m; a += FNT / 32)
+    for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y)
       for (int b = m + (int)threadIdx.x; b < R - m; b += 32)
-        S.r[a * R + b] = S.inside(a, b) ? S.f[a * R + b] - S.ax(a, b, idx2) : 0.0f;
+        S.r[a * R + b] = S.residual(a, b, idx2);
   }
   __syncthreads();
-  for (int e = tid; e < FT * FT; e += FNT) {
+  for (int e = tid; e < FT * FT; e += nt) {
     const int ti = e / FT, tj = e % FT;
     const int gi = i0 + ti, gj = j0 + tj;
     if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
   }
   const int nxc = nx / 2, nyc = ny / 2;
-  for (int e = tid; e < (FT / 2) * (FT / 2); e += FNT) {
+  for (int e = tid; e < (FT / 2) * (FT / 2); e += nt) {
     const int I = i0 / 2 + e / (FT / 2), J = j0 / 2 + e % (FT / 2);
     if (I >= nxc || J >= nyc) continue;
     fc[(long long)I * nyc + J] = restrict_at(
@@ -609,7 +629,7 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
 
 // x += P e (coarse correction), post-smoothing (NU black/red pairs)
 template <int NU>
-__global__ void __launch_bounds__(FNT)
+__global__ void __launch_bounds__(FNT_MAX)
 mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
              const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
              const float* __restrict__ ec, int nx, int ny, float idx2) {
@@ -617,10 +637,11 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   constexpr int HALO = 2 * NU;
   constexpr int R = Stage<HALO>::R;
   const int i0 = blockIdx.y * FT, j0 = blockIdx.x * FT;
-  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int nt = (int)(blockDim.x * blockDim.y);
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const Stage<HALO> S = stage_level<HALO>(fsm, i0, j0, nx, ny, f, cx, cy, dg, x);
   const int nxc = nx / 2, nyc = ny / 2;
-  for (int a = (int)threadIdx.y; a < R; a += FNT / 32)
+  for (int a = (int)threadIdx.y; a < R; a += (int)blockDim.y)
     for (int b = (int)threadIdx.x; b < R; b += 32) {
       if (!S.inside(a, b)) continue;
       const int fi = i0 - HALO + a, fj = j0 - HALO + b;
@@ -629,7 +650,7 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
     }
   __syncthreads();
   for (int s = 0; s < 2 * NU; ++s) S.sweep(1 - (s & 1), s + 1, idx2);
-  for (int e = tid; e < FT * FT; e += FNT) {
+  for (int e = tid; e < FT * FT; e += nt) {
     const int ti = e / FT, tj = e % FT;
     const int gi = i0 + ti, gj = j0 + tj;
     if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
@@ -910,6 +931,10 @@ static bool valid(const zb_poisson_cfg* c) {
 // z32 = M r32 on level 0 (f0 already holds r); precond: 0 none, 1 MG, 2 MG
 // followed by one learned smoothing step on level 0 (x += S(f - A x)), 3 MG
 // with the level-0 red-black smoothing replaced by the learned smoother
+// threads per fused CTA: 32 x 8 when the level has tiles for every SM, else
+// 32 x 32 so that a few CTAs still finish their serial phases quickly
+static int fused_rows(dim3 grid) { return grid.x * grid.y >= 2 * 148 ? 8 : 32; }
+
 static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, cudaStream_t st) {
   float* fw = (float*)((char*)ws + P.fbase);
   const Level& L0 = P.L[0];
@@ -935,7 +960,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
                                                                           Lc.nx, Lc.ny);
     } else {
       const dim3 grid((L.ny + FT - 1) / FT, (L.nx + FT - 1) / FT);
-      const dim3 blk(32, FNT / 32);
+      const dim3 blk(32, fused_rows(grid));
       const size_t sm = fused_smem(2 * P.nu + 2);
       float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x,
             *a5 = fw + Lc.f;
@@ -977,7 +1002,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
       if (rc) return rc;
     } else {
       const dim3 grid((L.ny + FT - 1) / FT, (L.nx + FT - 1) / FT);
-      const dim3 blk(32, FNT / 32);
+      const dim3 blk(32, fused_rows(grid));
       const size_t sm = fused_smem(2 * P.nu);
       float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x,
             *a5 = fw + Lc.x;

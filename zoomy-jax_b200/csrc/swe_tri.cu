@@ -693,21 +693,22 @@ static int run_step(const zb_tri_cfg* cfg, const zb_tri_mesh* m, T* Q, void* ws,
   T *Q1, *S, *Fc;
   ws_split<T>(m, ws, &Q1, &S, &Fc);
   const size_t C = (size_t)m->n_cells;
-  if (ORDER == 1) {
+  if constexpr (ORDER == 1) {
     int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, S, Fc, ctrl, phase,
                                              MODE_EULER, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
     ZB_CUDA_TRY(cudaMemcpyAsync(Q + C, Q1 + C, 3 * C * sizeof(T), cudaMemcpyDeviceToDevice, st));
     return ZB_OK;
+  } else {
+    // stage 1 reads the b plane of Q through Qk = Q; the stage-1 state Q1
+    // holds h, qx, qy in planes 1..3 and Q's b plane is copied once per step
+    ZB_CUDA_TRY(cudaMemcpyAsync(Q1, Q, C * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, S, Fc, ctrl, phase,
+                                             MODE_STEP1, nullptr, nullptr, nullptr, st);
+    if (rc) return rc;
+    return stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q1, Q, Q, S, Fc, ctrl, phase, MODE_STEP2,
+                                           nullptr, nullptr, nullptr, st);
   }
-  // stage 1 reads the b plane of Q through Qk = Q; the stage-1 state Q1 holds
-  // h, qx, qy in planes 1..3 and Q's b plane is copied once per step
-  ZB_CUDA_TRY(cudaMemcpyAsync(Q1, Q, C * sizeof(T), cudaMemcpyDeviceToDevice, st));
-  int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, S, Fc, ctrl, phase,
-                                           MODE_STEP1, nullptr, nullptr, nullptr, st);
-  if (rc) return rc;
-  return stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q1, Q, Q, S, Fc, ctrl, phase, MODE_STEP2,
-                                         nullptr, nullptr, nullptr, st);
 }
 
 }  // namespace tri

@@ -44,7 +44,7 @@ class PoissonSolver:
     finest level) or ``'learned_replace'`` (the U-Net in place of the finest
     level's red-black sweeps)."""
 
-    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
+    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
                  device=None):
         import torch
         L.require_cuda()
@@ -207,6 +207,7 @@ class PoissonSolver:
                 record.append(self.r.float().clone())
             if record_post is not None and rel > tol:
                 record_post.append(self.post_vcycle_residual())
+        self.scal[8].fill_(float(it))     # where the graph solve leaves its count
         return self.x, it, rel
 
 
@@ -219,10 +220,12 @@ class ChorinSolver(HyperbolicSolver):
     Extra parameters: ``pressure_tol`` (1e-8), ``pressure_maxit`` (FCG
     iterations, 200), ``time_order`` (1 or 2), ``precond`` (``'mg'`` |
     ``'learned'`` | ``'none'``), ``smoother`` (a LearnedSmoother), ``cmin``,
-    ``cmax`` (coefficient clip, 0.1 and 2), ``nu`` (smoothing sweeps)."""
+    ``cmax`` (coefficient clip, 0.1 and 2), ``nu`` (smoothing sweeps),
+    ``use_graph`` (False: drive the FCG iterations from the host)."""
 
     def __init__(self, pressure_tol=1e-8, pressure_maxit=200, time_order=1, precond="mg",
-                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4, **kw):
+                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
+                 use_graph=True, **kw):
         super().__init__(**kw)
         if time_order not in (1, 2):
             raise ValueError("time_order is 1 or 2")
@@ -235,6 +238,7 @@ class ChorinSolver(HyperbolicSolver):
         self.smoother = smoother
         self.cmin, self.cmax, self.nu = float(cmin), float(cmax), int(nu)
         self.coarse_sweeps, self.coarsest = int(coarse_sweeps), int(coarsest)
+        self.use_graph = bool(use_graph)
         self.last_elliptic_rel_resid = None
         self.last_elliptic_iterations = None
 
@@ -272,7 +276,13 @@ class ChorinSolver(HyperbolicSolver):
         P.setup(Q[1])
         P.rhs(Q, dt)
         P.x.zero_()
-        P.launch(self.precond, self.smoother, self.pressure_tol, self.pressure_maxit)
+        if self.use_graph:
+            P.launch(self.precond, self.smoother, self.pressure_tol, self.pressure_maxit)
+        else:
+            # host-driven iterations (one sync each): every kernel is an
+            # ordinary launch, which profilers list one by one
+            P.solve_stepwise(None, P.x, self.pressure_tol, self.pressure_maxit, self.precond,
+                             self.smoother)
         if sync:
             s = P.scal[7:9].cpu()
             rel, it = float(s[0]), int(s[1])
