@@ -21,10 +21,11 @@ cannot be installed: it needs jax and zoomy_core, absent here) on the host's
 cores: one process per core, each stepping a 256 x 256 sample of the same
 workload; rank 0 only.
 
-Rank 0 also reports, in the same JSON line, the two other configurations:
+Rank 0 also reports, in the same JSON line, the other configurations:
 "chorin" (1024^2 Chorin steps at a 1e-8 pressure residual, plain multigrid FCG
-against the learned U-Net smoother) and "ensemble" (512 uneven instances in one
-persistent launch per stage); --no-extra skips them.
+against the learned U-Net smoother), "ensemble" (512 uneven instances in one
+persistent launch per stage) and "triangles" (about 4M Delaunay triangles, 500
+steps); --no-extra skips them, --legs picks a subset.
 """
 from __future__ import annotations
 
@@ -426,6 +427,47 @@ def run_chorin(local_rank, n=1024, steps=10, warmup=3, train_steps=2000, use_gra
     return out
 
 
+def run_triangles(local_rank, n_side=1415, steps=500, warmup=3):
+    """The unstructured configuration: a Delaunay triangulation of seeded
+    jittered points (about 2 n_side^2 = 4.0M triangles, int32 connectivity),
+    eta least-squares MUSCL with the Barth-Jespersen limiter, HR-HLL,
+    SSP-RK2, Manning n = 0.03, Gaussian-random-field bathymetry with dry
+    islands, float32 state with float64 mass sums; `steps` steps after
+    `warmup`, timed with CUDA events (mesh building on the host is outside)."""
+    import torch
+    import zoomy_b200 as zb
+    from zoomy_b200.fvm.solver import HyperbolicSolver
+    from zoomy_b200.workloads import grf_dam_state
+    t0 = time.perf_counter()
+    mesh = zb.create_tri(n_side, seed=0)
+    t_mesh = time.perf_counter() - t0
+    state = grf_dam_state(mesh.cell_centers(), seed=0)
+    model = zb.ShallowWater2D(manning_n=0.03, boundary_conditions={t: "wall" for t in
+                                                                  ("left", "right", "bottom",
+                                                                   "top")},
+                              initial_conditions=state)
+    nsm = zb.NumericalSystemModel.from_system_model(
+        model, zb.ReconstructionSpec(2, "barth_jespersen"), "hll_hr")
+    solver = HyperbolicSolver(time_end=math.inf, compute_dt=zb.timestepping.adaptive(0.45, 2),
+                              reconstruction_variables="eta", free_surface_h_index=1,
+                              eps_wet=1e-6, dtype="float32", device=f"cuda:{local_rank}")
+    Q, _ = solver.setup_simulation(mesh, nsm)
+    m0 = solver.mass(Q)
+    solver.init_march(Q)
+    solver.launch_steps(Q, warmup)
+    torch.cuda.synchronize()
+    ms = _ev_ms(lambda: solver.launch_steps(Q, steps), 1) / steps
+    c = solver.read_ctrl()
+    m1 = solver.mass(Q)
+    cells = int(mesh.n_cells)
+    return {"cells": cells, "faces": int(mesh.n_faces), "steps": steps,
+            "ms_per_step": round(ms, 4), "value": cells / (ms * 1e-3),
+            "unit": "cell-updates/s", "kernels_per_step": 6, "device_copies_per_step": 1,
+            "mass_rel_change": abs(m1 - m0) / m0, "status_ok": c.status == 0,
+            "dry_fraction_initial": float((state[1] <= 0).mean()),
+            "mesh_build_s": round(t_mesh, 1)}
+
+
 def run_ensemble(local_rank, steps=2000):
     """The batched configuration: 512 uneven SWE instances (sides log-uniform
     in [64, 512]) advanced together by one persistent launch per stage,
@@ -466,7 +508,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the Chorin and ensemble legs")
-    ap.add_argument("--legs", default="swe,chorin,ensemble",
+    ap.add_argument("--legs", default="swe,chorin,ensemble,triangles",
                     help="comma-separated legs to run (profiling runs pick one)")
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--chorin-steps", type=int, default=10)
@@ -526,6 +568,8 @@ def main():
                                         use_graph=not args.chorin_no_graph)
         if "ensemble" in legs:
             line["ensemble"] = run_ensemble(local_rank)
+        if "triangles" in legs:
+            line["triangles"] = run_triangles(local_rank)
         print(json.dumps(line), flush=True)
         return
     if world > 1:
@@ -548,6 +592,8 @@ def main():
                                          train_steps=args.train_steps)
         if "ensemble" in legs:
             extra["ensemble"] = run_ensemble(local_rank)
+        if "triangles" in legs:
+            extra["triangles"] = run_triangles(local_rank)
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["ms_per_step"], "higher_is_better": True,

@@ -36,6 +36,31 @@ constexpr unsigned TC_SPIN_LIMIT = 1u << 24;
 
 __host__ __device__ constexpr int pad16(int c) { return (c + 15) & ~15; }
 
+// How input channels [0, cin_a) are read: as stored, as the nearest-neighbour
+// 2x upsampling of a half-resolution field (the U-Net's up(m2)), or as the 2x2
+// average of a double-resolution field (pool(e2)); the last two replace the
+// materialised upsampled / pooled activations.  Channels [cin_a, cin) are read
+// as stored from the second source.
+enum { SRC_DIRECT = 0, SRC_UP = 1, SRC_POOL = 2 };
+
+__device__ __forceinline__ float src_at(const float* __restrict__ inA, int cin_a,
+                                        const float* __restrict__ inB, int mode_a, int ci, int b,
+                                        int B, int H, int W, int yy, int xx) {
+  if (ci < cin_a) {
+    if (mode_a == SRC_UP) {
+      const int h = H >> 1, w = W >> 1;
+      return inA[((size_t)ci * B + b) * h * w + (size_t)(yy >> 1) * w + (xx >> 1)];
+    }
+    if (mode_a == SRC_POOL) {
+      const int w = 2 * W;
+      const float* q = inA + ((size_t)ci * B + b) * (size_t)(2 * H) * w + (size_t)(2 * yy) * w + 2 * xx;
+      return 0.25f * (q[0] + q[1] + q[w] + q[w + 1]);
+    }
+    return inA[((size_t)ci * B + b) * H * W + (size_t)yy * W + xx];
+  }
+  return inB[((size_t)(ci - cin_a) * B + b) * H * W + (size_t)yy * W + xx];
+}
+
 __host__ __device__ inline size_t tc_smem_bytes(int cinp, int coutp) {
   return (size_t)cinp * THP * 2 + (size_t)9 * cinp * coutp * 2 + 64;
 }
@@ -108,14 +133,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // out[co][b][y][x] = act(bias[co] + sum_ci sum_tap w[co][ci][tap] in[ci][b][y+dy-1][x+dx-1])
-// with the input channels [0, cin_a) from inA and [cin_a, cin) from inB, the
-// input rounded to bf16, zero padding at the image border.  err (may be null)
+// with the input channels [0, cin_a) from inA (read per mode_a, see src_at)
+// and [cin_a, cin) from inB, the input rounded to bf16, zero padding at the
+// image border.  err (may be null)
 // receives 1 when an mbarrier wait timed out.
 __global__ void __launch_bounds__(TC_THREADS)
 conv3x3_tc(const float* __restrict__ inA, int cin_a, const float* __restrict__ inB, int cin,
            const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
-           float* __restrict__ out, int cout, int B, int H, int W, int act, int tmem_cols,
-           unsigned* err) {
+           float* __restrict__ out, int cout, int B, int H, int W, int act, int mode_a,
+           int tmem_cols, unsigned* err) {
   extern __shared__ __align__(128) unsigned char tc_sm[];
   const int cinp = pad16(cin), coutp = pad16(cout);
   const int nch = cinp / 8;
@@ -176,12 +202,8 @@ conv3x3_tc(const float* __restrict__ inA, int cin_a, const float* __restrict__ i
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int ci = ch * 8 + k;
-        float f = 0.0f;
-        if (inside && ci < cin) {
-          const float* src = ci < cin_a ? inA + (size_t)ci * plane
-                                        : inB + (size_t)(ci - cin_a) * plane;
-          f = src[img + (size_t)yy * W + xx];
-        }
+        const float f = (inside && ci < cin)
+                            ? src_at(inA, cin_a, inB, mode_a, ci, b, B, H, W, yy, xx) : 0.0f;
         v[k] = __float2bfloat16_rn(f);
       }
       *(uint4*)(sA + ((size_t)ch * THP + q) * 16) = *(const uint4*)v;

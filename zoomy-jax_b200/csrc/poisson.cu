@@ -215,12 +215,51 @@ __device__ __forceinline__ void block_sum(double v, double* red, double* out) {
   }
 }
 
+// Grid-wide finish of a two-stage reduction without another launch: every
+// block has stored its partial sums; the last block to arrive (a counter in
+// the workspace) adds the partials in a fixed order -- the same order and
+// arithmetic as a separate reduction kernel, so the result is deterministic --
+// derives the FCG scalar and re-arms the counter.  No block waits on another.
+enum { FIN_NONE = 0, FIN_REL = 1, FIN_ALPHA = 2, FIN_BETA = 3 };
+
+__device__ void finish_scalars(const double* part_a, const double* part_b, unsigned* counter,
+                               double* scal, int dst_a, int dst_b, int what, double* red) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double sa = 0.0, sb = 0.0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += NT) {
+    sa += __ldcg(part_a + k);
+    if (part_b) sb += __ldcg(part_b + k);
+  }
+  block_sum(sa, red, &scal[dst_a]);
+  __syncthreads();
+  if (part_b) block_sum(sb, red, &scal[dst_b]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (what == FIN_REL) {
+      scal[S_REL] = sqrt(scal[S_RR] / scal[S_BB]);
+    } else if (what == FIN_ALPHA) {
+      const double pq = scal[S_PQ];
+      scal[S_ALPHA] = pq != 0.0 ? scal[S_PR] / pq : 0.0;
+    } else if (what == FIN_BETA) {
+      const double pq = scal[S_PQ];
+      scal[S_BETA] = pq != 0.0 ? scal[S_ZQ] / pq : 0.0;
+    }
+    *counter = 0u;
+  }
+}
+
 // q = A p; partial[b] = sum p.q ; partial2[b] = sum p.r
 __global__ void __launch_bounds__(NT)
 apply_dot_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
                  const double* __restrict__ p, const double* __restrict__ r,
                  double* __restrict__ q, int nx, int ny, double idx2, double* part_pq,
-                 double* part_pr) {
+                 double* part_pr, unsigned* counter, double* scal) {
   __shared__ double red[NT / 32];
   double spq = 0.0, spr = 0.0;
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
@@ -239,51 +278,14 @@ apply_dot_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
   block_sum(spq, red, &part_pq[blockIdx.x]);
   __syncthreads();
   if (part_pr) block_sum(spr, red, &part_pr[blockIdx.x]);
-}
-
-// generic dots: part_a[b] = sum a.b, part_c[b] = sum c.d (either may be null)
-__global__ void __launch_bounds__(NT)
-dot2_kernel(const double* __restrict__ a, const double* __restrict__ b,
-            const double* __restrict__ c, const double* __restrict__ d, long long n,
-            double* part_ab, double* part_cd) {
-  __shared__ double red[NT / 32];
-  double s1 = 0.0, s2 = 0.0;
-  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
-    s1 += a[k] * b[k];
-    if (c) s2 += c[k] * d[k];
-  }
-  block_sum(s1, red, &part_ab[blockIdx.x]);
-  __syncthreads();
-  if (part_cd) block_sum(s2, red, &part_cd[blockIdx.x]);
-}
-
-// scal[dst] = sum of partials (fixed order: deterministic)
-__global__ void sum_partials_kernel(const double* part, int n, double* scal, int dst) {
-  __shared__ double red[NT / 32];
-  double s = 0.0;
-  for (int k = threadIdx.x; k < n; k += NT) s += part[k];
-  block_sum(s, red, &scal[dst]);
-}
-
-// scalars of the FCG iteration
-__global__ void fcg_scalar_kernel(double* scal, int what) {
-  if (threadIdx.x != 0) return;
-  if (what == 0) {                       // alpha = p.r / p.q
-    const double pq = scal[S_PQ];
-    scal[S_ALPHA] = pq != 0.0 ? scal[S_PR] / pq : 0.0;
-  } else if (what == 1) {                // rel = sqrt(r.r / b.b)
-    scal[S_REL] = sqrt(scal[S_RR] / scal[S_BB]);
-  } else {                               // beta = z.q / p.q
-    const double pq = scal[S_PQ];
-    scal[S_BETA] = pq != 0.0 ? scal[S_ZQ] / pq : 0.0;
-  }
+  if (counter) finish_scalars(part_pq, part_pr, counter, scal, S_PQ, S_PR, FIN_ALPHA, red);
 }
 
 // x += alpha p ; r -= alpha q ; partial r.r ; r32 = (float) r
 __global__ void __launch_bounds__(NT)
 update_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
-                 const double* __restrict__ q, const double* scal, long long n,
-                 double* part_rr, float* __restrict__ r32) {
+                 const double* __restrict__ q, double* scal, long long n,
+                 double* part_rr, float* __restrict__ r32, unsigned* counter) {
   __shared__ double red[NT / 32];
   const double a = scal[S_ALPHA];
   double s = 0.0;
@@ -295,12 +297,14 @@ update_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* _
     if (r32) r32[k] = (float)rk;
   }
   block_sum(s, red, &part_rr[blockIdx.x]);
+  finish_scalars(part_rr, nullptr, counter, scal, S_RR, 0, FIN_REL, red);
 }
 
 // z = (double) z32 ; partial z.q
 __global__ void __launch_bounds__(NT)
 z_from32_kernel(const float* __restrict__ z32, double* __restrict__ z,
-                const double* __restrict__ q, long long n, double* part_zq) {
+                const double* __restrict__ q, long long n, double* part_zq, unsigned* counter,
+                double* scal) {
   __shared__ double red[NT / 32];
   double s = 0.0;
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
@@ -308,7 +312,10 @@ z_from32_kernel(const float* __restrict__ z32, double* __restrict__ z,
     z[k] = v;
     if (q) s += v * q[k];
   }
-  if (part_zq) block_sum(s, red, &part_zq[blockIdx.x]);
+  if (part_zq) {
+    block_sum(s, red, &part_zq[blockIdx.x]);
+    finish_scalars(part_zq, nullptr, counter, scal, S_ZQ, 0, FIN_BETA, red);
+  }
 }
 
 // p = z - beta p
@@ -324,7 +331,7 @@ __global__ void __launch_bounds__(NT)
 residual64_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
                   const double* __restrict__ x, const double* __restrict__ b,
                   double* __restrict__ r, int nx, int ny, double idx2, double* part_rr,
-                  double* part_bb, float* __restrict__ r32) {
+                  double* part_bb, float* __restrict__ r32, unsigned* counter, double* scal) {
   __shared__ double red[NT / 32];
   double srr = 0.0, sbb = 0.0;
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
@@ -345,6 +352,7 @@ residual64_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
   block_sum(srr, red, &part_rr[blockIdx.x]);
   __syncthreads();
   block_sum(sbb, red, &part_bb[blockIdx.x]);
+  finish_scalars(part_rr, part_bb, counter, scal, S_RR, S_BB, FIN_REL, red);
 }
 
 // ── float32 multigrid kernels ───────────────────────────────────────────────
@@ -793,6 +801,7 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
 __global__ void coarse_inverse_kernel(const Plan P, float* ws_f) {
   __shared__ double a[DENSE_MAX_CELLS][DENSE_MAX_CELLS];
   __shared__ double fcol[DENSE_MAX_CELLS];
+  __shared__ double prow[DENSE_MAX_CELLS];
   const Level& L = P.L[P.nlev - 1];
   const int nx = L.nx, ny = L.ny, n = nx * ny;
   const double idx2 = 1.0 / ((double)L.dx * (double)L.dx);
@@ -819,15 +828,17 @@ __global__ void coarse_inverse_kernel(const Plan P, float* ws_f) {
       }
   }
   __syncthreads();
+  // two phases per pivot, each only reading what the previous phase wrote:
+  // (1) the scaled pivot row and the pivot column go to side arrays, (2) the
+  // rank-one update writes every row
   for (int p = 0; p < n; ++p) {
-    const double piv = a[p][p];
-    __syncthreads();
-    for (int c = threadIdx.x; c < n; c += blockDim.x) a[p][c] = (c == p ? 1.0 : a[p][c]) / piv;
+    for (int c = threadIdx.x; c < n; c += blockDim.x)
+      prow[c] = (c == p ? 1.0 : a[p][c]) / a[p][p];
     for (int r = threadIdx.x; r < n; r += blockDim.x) fcol[r] = (r == p) ? 0.0 : a[r][p];
     __syncthreads();
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
       const int r = e / n, c = e % n;
-      if (r != p) a[r][c] = (c == p ? 0.0 : a[r][c]) - fcol[r] * a[p][c];
+      a[r][c] = (r == p) ? prow[c] : (c == p ? 0.0 : a[r][c]) - fcol[r] * prow[c];
     }
     __syncthreads();
   }
@@ -877,6 +888,10 @@ __global__ void fcg_cond_kernel(double* scal, cudaGraphConditionalHandle h, doub
   const bool go = rel > tol && it < (double)maxit;   // false for NaN
   cudaGraphSetConditional(h, go ? 1u : 0u);
 }
+
+// reduction counters of finish_scalars: four unsigned slots in the last
+// doubles of the scalar block (zeroed at set-up, re-armed by every use)
+static unsigned* counters(double* scal) { return (unsigned*)(scal + 12); }
 
 static int grid_for(long long n) {
   return (int)std::max<long long>(1, std::min<long long>((n + NT - 1) / NT, 148 * 8));
@@ -1089,6 +1104,7 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
         fw + L.cx, fw + L.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.dg);
   }
   if (P.cinv >= 0) coarse_inverse_kernel<<<1, 256, 0, st>>>(P, fw);
+  ZB_CUDA_TRY(cudaMemsetAsync(dw + P.scal, 0, S_COUNT * sizeof(double), st));
   return zb_launch_check();
 }
 
@@ -1100,7 +1116,7 @@ int zb_poisson_apply(const zb_poisson_cfg* cfg, void* ws, const double* p, doubl
   double* dw = (double*)ws;
   apply_dot_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, p, nullptr, q, cfg->nx,
                                               cfg->ny, 1.0 / (cfg->dx * cfg->dx), dw + P.part,
-                                              nullptr);
+                                              nullptr, nullptr, nullptr);
   return zb_launch_check();
 }
 
@@ -1167,15 +1183,14 @@ int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x
   const long long n = (long long)cfg->nx * cfg->ny;
   double* part = dw + P.part;
   double* scal = dw + P.scal;
+  unsigned* ctr = counters(scal);
   residual64_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, x, b, dw + P.vr, cfg->nx,
                                                cfg->ny, 1.0 / (cfg->dx * cfg->dx), part,
-                                               part + RED_BLOCKS, fw + P.L[0].f);
-  sum_partials_kernel<<<1, NT, 0, st>>>(part, RED_BLOCKS, scal, S_RR);
-  sum_partials_kernel<<<1, NT, 0, st>>>(part + RED_BLOCKS, RED_BLOCKS, scal, S_BB);
-  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 1);
+                                               part + RED_BLOCKS, fw + P.L[0].f, ctr, scal);
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
-  z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, nullptr, n, nullptr);
+  z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, nullptr, n, nullptr,
+                                             nullptr, scal);
   p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1);
   return zb_launch_check();
 }
@@ -1191,22 +1206,17 @@ int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
   const long long n = (long long)cfg->nx * cfg->ny;
   double* part = dw + P.part;
   double* scal = dw + P.scal;
+  unsigned* ctr = counters(scal);
   apply_dot_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, dw + P.vp, dw + P.vr,
                                               dw + P.vq, cfg->nx, cfg->ny,
-                                              1.0 / (cfg->dx * cfg->dx), part, part + RED_BLOCKS);
-  sum_partials_kernel<<<1, NT, 0, st>>>(part, RED_BLOCKS, scal, S_PQ);
-  sum_partials_kernel<<<1, NT, 0, st>>>(part + RED_BLOCKS, RED_BLOCKS, scal, S_PR);
-  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 0);
+                                              1.0 / (cfg->dx * cfg->dx), part, part + RED_BLOCKS,
+                                              ctr + 1, scal);
   update_xr_kernel<<<RED_BLOCKS, NT, 0, st>>>(x, dw + P.vr, dw + P.vp, dw + P.vq, scal, n,
-                                              part + 2 * RED_BLOCKS, fw + P.L[0].f);
-  sum_partials_kernel<<<1, NT, 0, st>>>(part + 2 * RED_BLOCKS, RED_BLOCKS, scal, S_RR);
-  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 1);
+                                              part + 2 * RED_BLOCKS, fw + P.L[0].f, ctr + 2);
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
   z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, dw + P.vq, n,
-                                             part + 3 * RED_BLOCKS);
-  sum_partials_kernel<<<1, NT, 0, st>>>(part + 3 * RED_BLOCKS, RED_BLOCKS, scal, S_ZQ);
-  fcg_scalar_kernel<<<1, 32, 0, st>>>(scal, 2);
+                                             part + 3 * RED_BLOCKS, ctr + 3, scal);
   p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0);
   return zb_launch_check();
 }

@@ -42,6 +42,7 @@ constexpr int NT = 256;
 
 enum { ACT_NONE = 0, ACT_TANH = 1 };
 
+
 // out[co][b][y][x] = act(bias[co] + sum_ci sum_tap w[co][ci][tap] in[ci][b][y+dy][x+dx])
 // input channels may come from two planes sets (the concatenation): channels
 // [0, cin_a) from inA, [cin_a, cin) from inB
@@ -49,7 +50,7 @@ template <int COUT>
 __global__ void __launch_bounds__(NTT)
 conv3x3_fwd(const float* __restrict__ inA, int cin_a, const float* __restrict__ inB, int cin,
             const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
-            float* __restrict__ out, int B, int H, int W, int act) {
+            float* __restrict__ out, int B, int H, int W, int act, int mode_a) {
   __shared__ float sin_[CCH][TS + 2][TS + 2];
   __shared__ float sw[COUT][CCH][9];
   const int tx = threadIdx.x % TS, ty = threadIdx.x / TS;
@@ -68,11 +69,8 @@ conv3x3_fwd(const float* __restrict__ inA, int cin_a, const float* __restrict__ 
       const int rr = e - cc * (TS + 2) * (TS + 2);
       const int yy = y0 - 1 + rr / (TS + 2), xx = x0 - 1 + rr % (TS + 2);
       float v = 0.0f;
-      if (cc < nc && yy >= 0 && yy < H && xx >= 0 && xx < W) {
-        const int ci = c0 + cc;
-        const float* src = ci < cin_a ? inA + (size_t)ci * plane : inB + (size_t)(ci - cin_a) * plane;
-        v = src[img + (size_t)yy * W + xx];
-      }
+      if (cc < nc && yy >= 0 && yy < H && xx >= 0 && xx < W)
+        v = src_at(inA, cin_a, inB, mode_a, c0 + cc, b, B, H, W, yy, xx);
       sin_[cc][rr / (TS + 2)][rr % (TS + 2)] = v;
     }
     for (int e = threadIdx.x; e < COUT * CCH * 9; e += NTT) {
@@ -105,7 +103,7 @@ conv3x3_fwd(const float* __restrict__ inA, int cin_a, const float* __restrict__ 
 __global__ void __launch_bounds__(NTT)
 conv3x3_wgrad(const float* __restrict__ inA, int cin_a, const float* __restrict__ inB, int cin,
               const float* __restrict__ dout, int cout, float* __restrict__ dw,
-              float* __restrict__ dbias, int B, int H, int W) {
+              float* __restrict__ dbias, int B, int H, int W, int mode_a) {
   __shared__ float sin_[CCH][TS + 2][TS + 2];
   __shared__ float sd[8][TS * TS];
   const int x0 = blockIdx.x * TS, y0 = blockIdx.y * TS, b = blockIdx.z;
@@ -134,11 +132,8 @@ conv3x3_wgrad(const float* __restrict__ inA, int cin_a, const float* __restrict_
         const int rr = e - cc * (TS + 2) * (TS + 2);
         const int yy = y0 - 1 + rr / (TS + 2), xx = x0 - 1 + rr % (TS + 2);
         float v = 0.0f;
-        if (cc < nc && yy >= 0 && yy < H && xx >= 0 && xx < W) {
-          const int ci = c0 + cc;
-          const float* src = ci < cin_a ? inA + (size_t)ci * plane : inB + (size_t)(ci - cin_a) * plane;
-          v = src[img + (size_t)yy * W + xx];
-        }
+        if (cc < nc && yy >= 0 && yy < H && xx >= 0 && xx < W)
+          v = src_at(inA, cin_a, inB, mode_a, c0 + cc, b, B, H, W, yy, xx);
         sin_[cc][rr / (TS + 2)][rr % (TS + 2)] = v;
       }
       __syncthreads();
@@ -171,21 +166,6 @@ __global__ void tanh_back(float* __restrict__ g, const float* __restrict__ y, si
     g[k] *= 1.0f - y[k] * y[k];
 }
 
-__global__ void avgpool2(const float* __restrict__ in, float* __restrict__ out, int C, int B, int H,
-                         int W) {
-  const int Ho = H / 2, Wo = W / 2;
-  const size_t n = (size_t)C * B * Ho * Wo;
-  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < n; k += (size_t)gridDim.x * NT) {
-    const int xo = (int)(k % Wo);
-    const size_t t = k / Wo;
-    const int yo = (int)(t % Ho);
-    const size_t cb = t / Ho;
-    const float* src = in + cb * (size_t)H * W;
-    out[k] = 0.25f * (src[(size_t)(2 * yo) * W + 2 * xo] + src[(size_t)(2 * yo) * W + 2 * xo + 1] +
-                      src[(size_t)(2 * yo + 1) * W + 2 * xo] + src[(size_t)(2 * yo + 1) * W + 2 * xo + 1]);
-  }
-}
-
 __global__ void avgpool2_back(const float* __restrict__ gout, float* __restrict__ gin, int C,
                               int B, int H, int W) {
   const int Wo = W / 2, Ho = H / 2;
@@ -196,20 +176,6 @@ __global__ void avgpool2_back(const float* __restrict__ gout, float* __restrict_
     const int yy = (int)(t % H);
     const size_t cb = t / H;
     gin[k] = 0.25f * gout[cb * (size_t)Ho * Wo + (size_t)(yy / 2) * Wo + xx / 2];
-  }
-}
-
-__global__ void upsample2(const float* __restrict__ in, float* __restrict__ out, int C, int B,
-                          int H, int W) {
-  // in: (C, B, H/2, W/2) -> out: (C, B, H, W)
-  const int Wi = W / 2, Hi = H / 2;
-  const size_t n = (size_t)C * B * H * W;
-  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < n; k += (size_t)gridDim.x * NT) {
-    const int xx = (int)(k % W);
-    const size_t t = k / W;
-    const int yy = (int)(t % H);
-    const size_t cb = t / H;
-    out[k] = in[cb * (size_t)Hi * Wi + (size_t)(yy / 2) * Wi + xx / 2];
   }
 }
 
@@ -513,7 +479,7 @@ static unsigned* unet_err_word() {
 
 static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin,
                           const __nv_bfloat16* w, const float* bias, float* out, int cout, int B,
-                          int H, int W, int act, cudaStream_t st) {
+                          int H, int W, int act, int mode_a, cudaStream_t st) {
   const int cinp = pad16(cin), coutp = pad16(cout);
   if (coutp > 256 || cinp > 256) return ZB_E_UNSUPPORTED;
   int cols = 32;
@@ -544,18 +510,18 @@ static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin
       (long long)((W + TCX - 1) / TCX) * ((H + TCY - 1) / TCY) * B;
   const int grid = (int)std::max<long long>(1, std::min<long long>(ntiles, (long long)sms[dev] * std::max(1, fit)));
   conv3x3_tc<<<grid, TC_THREADS, smem, st>>>(inA, cin_a, inB, cin, w, bias, out, cout, B, H, W,
-                                             act, cols, unet_err_word());
+                                             act, mode_a, cols, unet_err_word());
   return zb_launch_check();
 }
 
 static int conv(const float* inA, int cin_a, const float* inB, int cin,
                 const __nv_bfloat16* w, const float* bias, float* out, int cout, int B, int H,
-                int W, int act, cudaStream_t st) {
+                int W, int act, cudaStream_t st, int mode_a = SRC_DIRECT) {
   if (g_conv_impl == 1)
-    return conv_tc_launch(inA, cin_a, inB, cin, w, bias, out, cout, B, H, W, act, st);
+    return conv_tc_launch(inA, cin_a, inB, cin, w, bias, out, cout, B, H, W, act, mode_a, st);
   dim3 grid((W + TS - 1) / TS, (H + TS - 1) / TS, B);
   switch (cout) {
-#define ZB_CONV(N) case N: conv3x3_fwd<N><<<grid, NTT, 0, st>>>(inA, cin_a, inB, cin, w, bias, out, B, H, W, act); break;
+#define ZB_CONV(N) case N: conv3x3_fwd<N><<<grid, NTT, 0, st>>>(inA, cin_a, inB, cin, w, bias, out, B, H, W, act, mode_a); break;
     ZB_CONV(1) ZB_CONV(8) ZB_CONV(16) ZB_CONV(24) ZB_CONV(32) ZB_CONV(48) ZB_CONV(72)
 #undef ZB_CONV
     default: return ZB_E_UNSUPPORTED;
@@ -564,9 +530,10 @@ static int conv(const float* inA, int cin_a, const float* inB, int cin,
 }
 
 static int wgrad(const float* inA, int cin_a, const float* inB, int cin, const float* dout,
-                 int cout, float* dw, float* db, int B, int H, int W, cudaStream_t st) {
+                 int cout, float* dw, float* db, int B, int H, int W, cudaStream_t st,
+                 int mode_a = SRC_DIRECT) {
   dim3 grid((W + TS - 1) / TS, (H + TS - 1) / TS, B);
-  conv3x3_wgrad<<<grid, NTT, 0, st>>>(inA, cin_a, inB, cin, dout, cout, dw, db, B, H, W);
+  conv3x3_wgrad<<<grid, NTT, 0, st>>>(inA, cin_a, inB, cin, dout, cout, dw, db, B, H, W, mode_a);
   return zb_launch_check();
 }
 
@@ -574,7 +541,7 @@ static int gridn(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n
 
 // activation buffers (floats) for a batch of B images H x W
 struct Acts {
-  float *in, *e1, *e2, *p, *m1, *m2, *u, *o1, *out, *s, *part;
+  float *in, *e1, *e2, *m1, *m2, *o1, *out, *s, *part;
   // training: gradients and scratch
   float *d_e1, *d_e2, *d_p, *d_m1, *d_m2, *d_cat, *d_o1, *d_out, *res, *lnum, *lden, *tmp;
   __nv_bfloat16* wflip;
@@ -582,8 +549,9 @@ struct Acts {
 
 static size_t acts_floats(const Net& n, int B, int H, int W, bool train) {
   const size_t N0 = (size_t)B * H * W, N1 = (size_t)B * (H / 2) * (W / 2);
-  size_t f = 2 * N0 + 2 * (size_t)n.c1 * N0 + (size_t)n.c1 * N1 + 2 * (size_t)n.c2 * N1 +
-             (size_t)n.c2 * N0 + (size_t)n.c1 * N0 + N0 + 512 + RMS_PARTS;
+  // in (2), e1, e2 (c1 each), m1, m2 (c2 each, half resolution), o1 (c1), out
+  size_t f = 2 * N0 + 2 * (size_t)n.c1 * N0 + 2 * (size_t)n.c2 * N1 + (size_t)n.c1 * N0 + N0 +
+             512 + RMS_PARTS;
   if (train)
     f += 2 * (size_t)n.c1 * N0 + (size_t)n.c1 * N1 + 2 * (size_t)n.c2 * N1 +
          (size_t)(n.c1 + n.c2) * N0 + (size_t)n.c1 * N0 + N0 + N0 + 1024 +
@@ -599,10 +567,8 @@ static Acts acts_split(const Net& n, void* base, int B, int H, int W, bool train
   a.in = f; f += 2 * N0;
   a.e1 = f; f += (size_t)n.c1 * N0;
   a.e2 = f; f += (size_t)n.c1 * N0;
-  a.p = f; f += (size_t)n.c1 * N1;
   a.m1 = f; f += (size_t)n.c2 * N1;
   a.m2 = f; f += (size_t)n.c2 * N1;
-  a.u = f; f += (size_t)n.c2 * N0;
   a.o1 = f; f += (size_t)n.c1 * N0;
   a.out = f; f += N0;
   a.s = f; f += 512;   // per-image RMS, batch <= 512
@@ -632,11 +598,10 @@ static int forward(const Net& n, const Acts& a, const __nv_bfloat16* w, const fl
   int rc;
   if ((rc = conv(a.in, 2, nullptr, 2, w + n.off_w[0], b + n.off_b[0], a.e1, n.c1, B, H, W, ACT_TANH, st))) return rc;
   if ((rc = conv(a.e1, n.c1, nullptr, n.c1, w + n.off_w[1], b + n.off_b[1], a.e2, n.c1, B, H, W, ACT_TANH, st))) return rc;
-  avgpool2<<<gridn((size_t)n.c1 * B * H1 * W1), NT, 0, st>>>(a.e2, a.p, n.c1, B, H, W);
-  if ((rc = conv(a.p, n.c1, nullptr, n.c1, w + n.off_w[2], b + n.off_b[2], a.m1, n.c2, B, H1, W1, ACT_TANH, st))) return rc;
+  // pool(e2) and up(m2) are read through the convolutions' loaders, never stored
+  if ((rc = conv(a.e2, n.c1, nullptr, n.c1, w + n.off_w[2], b + n.off_b[2], a.m1, n.c2, B, H1, W1, ACT_TANH, st, SRC_POOL))) return rc;
   if ((rc = conv(a.m1, n.c2, nullptr, n.c2, w + n.off_w[3], b + n.off_b[3], a.m2, n.c2, B, H1, W1, ACT_TANH, st))) return rc;
-  upsample2<<<gridn((size_t)n.c2 * B * H * W), NT, 0, st>>>(a.m2, a.u, n.c2, B, H, W);
-  if ((rc = conv(a.u, n.c2, a.e2, n.c2 + n.c1, w + n.off_w[4], b + n.off_b[4], a.o1, n.c1, B, H, W, ACT_TANH, st))) return rc;
+  if ((rc = conv(a.m2, n.c2, a.e2, n.c2 + n.c1, w + n.off_w[4], b + n.off_b[4], a.o1, n.c1, B, H, W, ACT_TANH, st, SRC_UP))) return rc;
   if ((rc = conv(a.o1, n.c1, nullptr, n.c1, w + n.off_w[5], b + n.off_b[5], a.out, 1, B, H, W, ACT_NONE, st))) return rc;
   return zb_launch_check();
 }
@@ -775,7 +740,7 @@ int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* targ
   if ((rc = data_grad(n, 5, w, a.wflip, a.d_out, a.d_o1, B, H, W, st))) return rc;
   tanh_back<<<gridn((size_t)n.c1 * N0), NT, 0, st>>>(a.d_o1, a.o1, (size_t)n.c1 * N0);
   // o1 = tanh(conv([u, e2]))
-  if ((rc = wgrad(a.u, n.c2, a.e2, n.c2 + n.c1, a.d_o1, n.c1, gw + n.off_w[4], gb + n.off_b[4], B, H, W, st))) return rc;
+  if ((rc = wgrad(a.m2, n.c2, a.e2, n.c2 + n.c1, a.d_o1, n.c1, gw + n.off_w[4], gb + n.off_b[4], B, H, W, st, SRC_UP))) return rc;
   if ((rc = data_grad(n, 4, w, a.wflip, a.d_o1, a.d_cat, B, H, W, st))) return rc;
   // d_cat = [du (c2), de2_b (c1)]
   upsample2_back<<<gridn((size_t)n.c2 * N1), NT, 0, st>>>(a.d_cat, a.d_m2, n.c2, B, H, W);
@@ -783,7 +748,7 @@ int zb_unet_backward(const zb_unet_trainer* t, const float* r, const float* targ
   if ((rc = wgrad(a.m1, n.c2, nullptr, n.c2, a.d_m2, n.c2, gw + n.off_w[3], gb + n.off_b[3], B, H1, W1, st))) return rc;
   if ((rc = data_grad(n, 3, w, a.wflip, a.d_m2, a.d_m1, B, H1, W1, st))) return rc;
   tanh_back<<<gridn((size_t)n.c2 * N1), NT, 0, st>>>(a.d_m1, a.m1, (size_t)n.c2 * N1);
-  if ((rc = wgrad(a.p, n.c1, nullptr, n.c1, a.d_m1, n.c2, gw + n.off_w[2], gb + n.off_b[2], B, H1, W1, st))) return rc;
+  if ((rc = wgrad(a.e2, n.c1, nullptr, n.c1, a.d_m1, n.c2, gw + n.off_w[2], gb + n.off_b[2], B, H1, W1, st, SRC_POOL))) return rc;
   if ((rc = data_grad(n, 2, w, a.wflip, a.d_m1, a.d_p, B, H1, W1, st))) return rc;
   avgpool2_back<<<gridn((size_t)n.c1 * N0), NT, 0, st>>>(a.d_p, a.d_e2, n.c1, B, H, W);
   add_inplace<<<gridn((size_t)n.c1 * N0), NT, 0, st>>>(a.d_e2, a.d_cat + (size_t)n.c2 * N0,

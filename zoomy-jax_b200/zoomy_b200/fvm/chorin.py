@@ -44,7 +44,7 @@ class PoissonSolver:
     finest level) or ``'learned_replace'`` (the U-Net in place of the finest
     level's red-black sweeps)."""
 
-    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
+    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
                  device=None):
         import torch
         L.require_cuda()
@@ -224,7 +224,7 @@ class ChorinSolver(HyperbolicSolver):
     ``use_graph`` (False: drive the FCG iterations from the host)."""
 
     def __init__(self, pressure_tol=1e-8, pressure_maxit=200, time_order=1, precond="mg",
-                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
+                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
                  use_graph=True, **kw):
         super().__init__(**kw)
         if time_order not in (1, 2):

@@ -23,6 +23,33 @@ def bumps(xc, seed=0, n=16, amp=(0.0, 0.8), width=(0.02, 0.1), domain=(0, 1, 0, 
     return b
 
 
+def gaussian_random_field(xc, seed=0, modes=64, corr=0.08, std=0.35, mean=0.55):
+    """Seeded smooth Gaussian random field on the unit square: a sum of
+    ``modes`` random Fourier modes whose wave vectors are drawn from a
+    Gaussian spectrum of correlation length ``corr`` (random phases), scaled
+    to standard deviation ``std`` around ``mean``; ``xc`` is ``(2, C)``.  With
+    the default level 1 its highs rise above the water (dry islands)."""
+    rng = np.random.default_rng(seed)
+    k = rng.normal(0.0, 1.0 / (2.0 * np.pi * corr), size=(modes, 2)) * 2.0 * np.pi
+    ph = rng.uniform(0.0, 2.0 * np.pi, size=modes)
+    f = np.zeros(xc.shape[1])
+    for m in range(modes):
+        f += np.cos(k[m, 0] * xc[0] + k[m, 1] * xc[1] + ph[m])
+    f *= np.sqrt(2.0 / modes)
+    return mean + std * f
+
+
+def grf_dam_state(xc, seed=0, r0=0.2, h_in=2.0, h_out=1.0):
+    """The unstructured configuration's state: Gaussian-random-field
+    bathymetry, a circular dam (level ``h_in`` inside ``r0``, ``h_out``
+    outside), dry where the bed tops the level, fluid at rest."""
+    b = gaussian_random_field(xc, seed)
+    r = np.sqrt((xc[0] - 0.5) ** 2 + (xc[1] - 0.5) ** 2)
+    level = np.where(r < r0, h_in, h_out)
+    h = np.maximum(level - b, 0.0)
+    return np.stack([b, h, np.zeros_like(b), np.zeros_like(b)])
+
+
 def circular_dam_state(xc, seed=0, r0=0.2, h_in=2.0, h_out=1.0, noise=1e-3,
                        center=(0.5, 0.5), bathymetry=True):
     """Circular dam break over the seeded bumps: level ``h_in`` inside radius
