@@ -44,7 +44,8 @@ enum {
   ZB_E_ARG = -1,      /* invalid argument (size, enum, null pointer) */
   ZB_E_CUDA = -2,     /* CUDA launch / runtime error */
   ZB_E_UNSUPPORTED = -3,
-  ZB_E_TOO_LARGE = -4 /* grid exceeds the fixed scratch of zb_swe2d_step_noalloc */
+  ZB_E_TOO_LARGE = -4,      /* grid exceeds a fixed-size buffer (noalloc step, TMEM) */
+  ZB_E_NOT_CONVERGED = -5   /* an iterative solve missed its tolerance */
 };
 
 /* status bits written by the kernels into zb_ctrl.status */
@@ -401,6 +402,17 @@ int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b,
                         zb_stream_t stream);
 int zb_fcg_graph_launch(zb_fcg_graph* graph, zb_stream_t stream);
 void zb_fcg_graph_destroy(zb_fcg_graph* graph);
+
+/* Synchronous solve for C callers (the shape of the reference's
+ * `jax_gmres(matvec, -b, tol, maxiter)` call plus its residual read-back):
+ * FCG from the x given until |r|/|b| <= tol or maxit iterations, one stream
+ * synchronisation per iteration; iterations and the final relative residual
+ * go to out_iters / out_rel (either may be NULL).  Returns ZB_OK, or
+ * ZB_E_NOT_CONVERGED when the tolerance was missed. */
+int zb_poisson_solve(const zb_poisson_cfg* cfg, void* ws, const double* b,
+                     double* x, double tol, int maxit, int precond,
+                     const zb_smoother* smoother, int* out_iters,
+                     double* out_rel, zb_stream_t stream);
 
 /* ── unstructured triangles ─────────────────────────────────────────────── */
 

@@ -136,6 +136,28 @@ def test_graph_and_stepwise_solves_agree():
     assert it3 == it1 and torch.equal(x3, x1)
 
 
+def test_synchronous_c_solve_matches_the_graph_solve():
+    import ctypes as C
+    n = 128
+    P = PoissonSolver(n, n, 1.0 / n)
+    P.setup(gpu(depth(n, seed=11)))
+    b = gpu(np.random.default_rng(12).standard_normal(n * n))
+    x1, it1, rel1 = P.solve(b, tol=1e-9, maxit=100)
+    x1 = x1.clone()
+    x2 = torch.zeros_like(b)
+    its, rel = C.c_int(), C.c_double()
+    rc = P.lib.zb_poisson_solve(C.byref(P.cfg), L.ptr(P.ws), L.ptr(b), L.ptr(x2), 1e-9, 100,
+                                L.PRECOND["mg"], None, C.byref(its), C.byref(rel),
+                                L.stream_ptr())
+    assert rc == L.ZB_OK and its.value == it1 and rel.value == rel1
+    assert torch.equal(x1, x2)
+    x3 = torch.zeros_like(b)
+    rc = P.lib.zb_poisson_solve(C.byref(P.cfg), L.ptr(P.ws), L.ptr(b), L.ptr(x3), 1e-14, 2,
+                                L.PRECOND["mg"], None, C.byref(its), C.byref(rel),
+                                L.stream_ptr())
+    assert rc == L.ZB_E_NOT_CONVERGED and its.value == 2 and rel.value > 1e-14
+
+
 def test_maxit_stops_the_graph_loop():
     n = 64
     P = PoissonSolver(n, n, 1.0 / n)

@@ -1316,4 +1316,31 @@ void zb_fcg_graph_destroy(zb_fcg_graph* G) {
   delete G;
 }
 
+
+// Synchronous convenience solve for C callers: FCG from the x given until
+// |r| / |b| <= tol or maxit iterations, reading the relative residual after
+// each iteration (one stream synchronisation per iteration).
+int zb_poisson_solve(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x, double tol,
+                     int maxit, int precond, const zb_smoother* smo, int* out_iters,
+                     double* out_rel, zb_stream_t stream) {
+  if (!valid(cfg) || !ws || !b || !x || maxit < 0 || !(tol >= 0.0)) return ZB_E_ARG;
+  const Plan P = make_plan(cfg);
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* rel_dev = (const double*)ws + P.scal + S_REL;
+  int rc = zb_fcg_start(cfg, ws, b, x, precond, smo, stream);
+  if (rc) return rc;
+  double rel = 0.0;
+  int it = 0;
+  for (;;) {
+    ZB_CUDA_TRY(cudaMemcpyAsync(&rel, rel_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+    ZB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!(rel > tol) || it >= maxit) break;
+    if ((rc = zb_fcg_iterate(cfg, ws, x, precond, smo, stream))) return rc;
+    ++it;
+  }
+  if (out_iters) *out_iters = it;
+  if (out_rel) *out_rel = rel;
+  return rel <= tol ? ZB_OK : ZB_E_NOT_CONVERGED;
+}
+
 }  // extern "C"

@@ -14,6 +14,7 @@ LIB_PATH = pathlib.Path(__file__).resolve().parent.parent / "lib" / "libzb.so"
 
 ZB_F32, ZB_F64 = 0, 1
 ZB_OK, ZB_E_ARG, ZB_E_CUDA, ZB_E_UNSUPPORTED, ZB_E_TOO_LARGE = 0, -1, -2, -3, -4
+ZB_E_NOT_CONVERGED = -5
 ZB_NOALLOC_MAX_CELLS = 1 << 20
 ZB_ST_DT_INVALID, ZB_ST_TROUBLED, ZB_ST_NOT_CONVERGED = 1, 2, 4
 BC = {"extrapolation": 0, "wall": 1, "periodic": 2}
@@ -161,6 +162,8 @@ SIGNATURES = [
                                       C.POINTER(C.c_void_p), _P]),
     ("zb_fcg_graph_launch", C.c_int, [_P, _P]),
     ("zb_fcg_graph_destroy", None, [_P]),
+    ("zb_poisson_solve", C.c_int, [_PCFG, _P, _P, _P, C.c_double, C.c_int, C.c_int, _SMO,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double), _P]),
 ]
 
 _lib = None
@@ -192,7 +195,9 @@ class ZbError(RuntimeError):
 def check(rc, what):
     if rc != ZB_OK:
         names = {ZB_E_ARG: "invalid argument", ZB_E_CUDA: "CUDA error",
-                 ZB_E_UNSUPPORTED: "unsupported configuration"}
+                 ZB_E_UNSUPPORTED: "unsupported configuration",
+                 ZB_E_TOO_LARGE: "too large for a fixed-size buffer",
+                 ZB_E_NOT_CONVERGED: "not converged"}
         raise ZbError(f"{what} failed: {names.get(rc, rc)}")
 
 

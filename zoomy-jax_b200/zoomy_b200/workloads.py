@@ -23,20 +23,23 @@ def bumps(xc, seed=0, n=16, amp=(0.0, 0.8), width=(0.02, 0.1), domain=(0, 1, 0, 
     return b
 
 
-def gaussian_random_field(xc, seed=0, modes=64, corr=0.08, std=0.35, mean=0.55):
-    """Seeded smooth Gaussian random field on the unit square: a sum of
-    ``modes`` random Fourier modes whose wave vectors are drawn from a
-    Gaussian spectrum of correlation length ``corr`` (random phases), scaled
-    to standard deviation ``std`` around ``mean``; ``xc`` is ``(2, C)``.  With
-    the default level 1 its highs rise above the water (dry islands)."""
+def gaussian_random_field(xc, seed=0, modes=64, corr=0.05, std=0.35, dry_fraction=0.10,
+                          level=1.0):
+    """Seeded smooth Gaussian random field on the unit square, sampled at the
+    points ``xc (2, C)``: a sum of ``modes`` random Fourier modes whose wave
+    vectors are drawn from the Gaussian spectrum ``exp(-k^2 corr^2)`` (random
+    phases; the spectral form of filtered white noise with correlation length
+    ``corr``), scaled to standard deviation ``std`` and shifted so that a
+    fraction ``dry_fraction`` of the points rises above ``level`` (the dry
+    islands of a lake at that level)."""
     rng = np.random.default_rng(seed)
-    k = rng.normal(0.0, 1.0 / (2.0 * np.pi * corr), size=(modes, 2)) * 2.0 * np.pi
+    k = rng.normal(0.0, 1.0 / (np.sqrt(2.0) * corr), size=(modes, 2))
     ph = rng.uniform(0.0, 2.0 * np.pi, size=modes)
     f = np.zeros(xc.shape[1])
     for m in range(modes):
         f += np.cos(k[m, 0] * xc[0] + k[m, 1] * xc[1] + ph[m])
-    f *= np.sqrt(2.0 / modes)
-    return mean + std * f
+    f *= std * np.sqrt(2.0 / modes)
+    return f + (level - np.quantile(f, 1.0 - dry_fraction))
 
 
 def grf_dam_state(xc, seed=0, r0=0.2, h_in=2.0, h_out=1.0):
