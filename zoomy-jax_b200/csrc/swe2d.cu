@@ -55,6 +55,10 @@ struct SweParams {
   double alpha, beta;       // Shu-Osher coefficients (generic stage)
   double dt_stage;          // generic stage: dt (< 0: read ctrl->dt)
   T inv6dx, inv6dy;         // interior least-squares gradient factors
+  // output region of the interior strip kernel ([fast_i0, fast_i1) x
+  // [fast_j0, fast_j1), empty when fast_i0 >= fast_i1); the tile kernel
+  // leaves these cells alone
+  int fast_i0, fast_i1, fast_j0, fast_j1;
   LsqTable<T> lsq;
 };
 
@@ -501,6 +505,8 @@ __device__ __forceinline__ void stage_tile(
     const int ti = e / TY, tj = e - ti * TY;
     const int gi = i0 + ti, gj = j0 + tj;
     if (gi >= nx || gj >= ny) continue;
+    // cells of the interior strip kernel's region are its to write
+    if (gi >= p.fast_i0 && gi < p.fast_i1 && gj >= p.fast_j0 && gj < p.fast_j1) continue;
     const int fl = ti * TY + tj, fr = fl + TY;
     const int fb = ti * (TY + 1) + tj, ft = fb + 1;
     const T kx = p.kx, ky = p.ky;
@@ -652,11 +658,271 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
       return;
     }
   }
+  // a tile wholly inside the strip kernel's region has nothing to write (the
+  // lead block sits at the corner, outside the region)
+  if (i0 >= p.fast_i0 && i0 + TX <= p.fast_i1 && j0 >= p.fast_j0 && j0 + TY <= p.fast_j1) return;
   stage_tile<T, TX, ORDER, RECON, RIEMANN, MODE>(
       s, red, i0, j0, bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO, ctrl, phase, hinv_src,
       force_o1, trouble_out, p, dtd, blockIdx.x == 0 && blockIdx.y == 0);
 }
 
+
+// ── the interior strip kernel ──────────────────────────────────────────────
+// The same stage arithmetic as stage_tile for cells at least two cells from
+// every boundary (there the boundary conditions, ghosts and boundary
+// least-squares classes never enter), organised for registers instead of
+// shared memory: one warp owns a strip of 32 contiguous columns (28 outputs
+// plus two halo columns on each side) and marches down SX rows.  Each lane
+// keeps a sliding window of three rows of W, the limited slopes of two rows
+// and the last x-face's fluxes in registers; the column neighbours come from
+// warp shuffles.  Every face is still evaluated once and every float
+// expression is the one stage_tile evaluates, so both kernels produce the same
+// bits for a cell.  The tile kernel runs alongside it on the boundary frame and
+// keeps the control-block duties.
+constexpr int SX = 64;          // output rows per work item
+constexpr int SW = 28;          // output columns per strip
+constexpr int STRIP_NT = 128;   // four independent warps per CTA
+
+template <typename T>
+struct RowW {
+  T b, w1, w2, w3, h, hinv;
+  __device__ T w(int v) const { return v == 0 ? b : (v == 1 ? w1 : (v == 2 ? w2 : w3)); }
+};
+
+template <typename T, int RECON>
+__device__ __forceinline__ void strip_trace(const RowW<T>& c, const T* sl, T o, Side<T>& sd) {
+  const T vb = c.b + sl[0] * o, w1 = c.w1 + sl[1] * o;
+  const T w2 = c.w2 + sl[2] * o, w3 = c.w3 + sl[3] * o;
+  sd.b = vb;
+  if (RECON == ZB_RECON_ETA) {
+    const T eta = fmx(w1, vb);
+    const T hf = eta - vb;
+    sd.h = hf;
+    sd.ux = w2;
+    sd.uy = w3;
+    sd.qx = w2 * hf;
+    sd.qy = w3 * hf;
+  } else {
+    sd.h = w1;
+    sd.qx = w2;
+    sd.qy = w3;
+    sd.ux = w2 * c.hinv;
+    sd.uy = w3 * c.hinv;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T shd(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+template <typename T>
+__device__ __forceinline__ T shu(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+
+template <typename T, int RECON, int RIEMANN, int MODE>
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
+swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
+                   const T* __restrict__ qxP, const T* __restrict__ qyP,
+                   const T* __restrict__ h0P, const T* __restrict__ qx0P,
+                   const T* __restrict__ qy0P, T* __restrict__ hO, T* __restrict__ qxO,
+                   T* __restrict__ qyO, zb_ctrl* ctrl, int phase, const SweParams<T> p) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nstrips = (p.fast_j1 - p.fast_j0) / SW;
+  const int nchunks = (p.fast_i1 - p.fast_i0 + SX - 1) / SX;
+  const int item = blockIdx.x * (STRIP_NT / 32) + warp;
+  if (item >= nstrips * nchunks) return;          // warp-uniform; no block barriers below
+  const int strip = item % nstrips, chunk = item / nstrips;
+  const int ny = p.ny;
+  const int cj = p.fast_j0 - 2 + strip * SW + lane;
+  const int r0 = p.fast_i0 + chunk * SX;
+  const int r1 = min(r0 + SX, p.fast_i1);
+  const double t = ctrl->t[phase];
+  const double dtd = dt_from_amax(ctrl->amax[phase], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
+  if (!(isfinite(dtd) && dtd > 0.0)) return;      // no-op step: the tile kernel keeps ctrl
+  const T dt = T(dtd);
+  const T g = p.g, half = T(0.5);
+  const bool out_lane = lane >= 2 && lane < 2 + SW;
+
+  RowW<T> R0, R1, R2;                 // rows r-2, r-1, r
+  T Sx0[4], Sx1[4], Sx2[4];           // (W(j-1) + W(j)) + W(j+1) of those rows
+  T Wm1[4], Wp1[4], Wm2[4], Wp2[4];   // W(j-1), W(j+1) of rows r-1 and r
+  T slA[8], slB[8];                   // [sx0..3, sy0..3] of rows r-2 and r-1
+  T fxh_p = T(0), fxt_p = T(0), fxr_p = T(0);
+  double amax_loc = 0.0;
+  bool bad = false;
+  const int nsteps = (r1 - r0) + 4;
+  // row r + 1 is fetched while row r is processed
+  T nbv, nhv, nqxv, nqyv;
+  {
+    const size_t k = (size_t)(r0 - 2) * ny + cj;
+    nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int r = r0 - 2 + s;
+    // shift the windows and take row r
+    R0 = R1; R1 = R2;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      Sx0[v] = Sx1[v]; Sx1[v] = Sx2[v];
+      Wm1[v] = Wm2[v]; Wp1[v] = Wp2[v];
+    }
+    {
+      const T vb = nbv, vh = nhv, vqx = nqxv, vqy = nqyv;
+      if (s + 1 < nsteps) {
+        const size_t k = (size_t)(r + 1) * ny + cj;
+        nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
+      }
+      const T hinv = kp_hinv(vh, p.eps_kp);
+      R2.b = vb;
+      R2.h = vh;
+      R2.hinv = hinv;
+      if (RECON == ZB_RECON_ETA) {
+        R2.w1 = vb + vh;
+        R2.w2 = vqx * hinv;
+        R2.w3 = vqy * hinv;
+      } else {
+        R2.w1 = vh;
+        R2.w2 = vqx;
+        R2.w3 = vqy;
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const T w = R2.w(v);
+        const T wl = shu(w), wr = shd(w);
+        Wm2[v] = wl;
+        Wp2[v] = wr;
+        Sx2[v] = (wl + w) + wr;
+      }
+    }
+    if (s < 2) continue;
+    // limited slopes of row r-1
+    {
+      T phi[4], gxa[4], gya[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const T u = R1.w(v);
+        const T tc = (R0.w(v) + R1.w(v)) + R2.w(v);
+        const T tl = shu(tc), tr = shd(tc);
+        const T gx = (Sx2[v] - Sx0[v]) * p.inv6dx;
+        const T gy = (tr - tl) * p.inv6dy;
+        const T wp0 = R2.w(v), wm0 = R0.w(v), w0p = Wp1[v], w0m = Wm1[v];
+        const T umax = fmx(fmx(u, wp0), fmx(wm0, fmx(w0p, w0m)));
+        const T umin = fmn(fmn(u, wp0), fmn(wm0, fmn(w0p, w0m)));
+        gxa[v] = gx;
+        gya[v] = gy;
+        phi[v] = limiter_phi(p.limiter, gx, gy, p.half_dx, p.half_dy, umax - u, umin - u,
+                             p.vk_eps2);
+      }
+      if (RECON == ZB_RECON_ETA) {
+        if (p.eps_wet >= T(0) && R1.h < p.eps_wet) {
+          phi[0] = phi[1] = phi[2] = phi[3] = T(0);
+        }
+        phi[0] = zmin(phi[0], phi[1]);
+        phi[2] = zmin(phi[2], phi[1]);
+        phi[3] = zmin(phi[3], phi[1]);
+      }
+#pragma unroll
+      for (int v = 0; v < 8; ++v) slA[v] = slB[v];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        slB[v] = phi[v] * gxa[v];
+        slB[4 + v] = phi[v] * gya[v];
+      }
+    }
+    if (s < 3) continue;
+    // x-face between rows r-2 (A, lower) and r-1 (B, upper)
+    T Fh, Fx, Fy, Dm, Dp;
+    T fxl_n;
+    {
+      Side<T> A, B;
+      strip_trace<T, RECON>(R0, slA, p.half_dx, A);
+      strip_trace<T, RECON>(R1, slB, -p.half_dx, B);
+      riemann<T, RIEMANN, 0>(A, B, T(1), g, Fh, Fx, Fy, Dm, Dp);
+      const T cesA = half * g * (R0.h + A.h) * (A.b - R0.b);
+      const T cesB = -(half * g * (R1.h + B.h) * (B.b - R1.b));
+      fxl_n = Fx + Dm + cesA;
+      const T fxr_n = -Fx + Dp + cesB;
+      if (s == 3) {            // face r0 - 1/2: only the next row needs it
+        fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
+        continue;
+      }
+      // y-faces of row r-2: this lane's top face, the lower lane's one below
+      Side<T> C, D;
+      T Gh, Gx, Gy, Em, Ep;
+      RowW<T> nb;
+      nb.b = shd(R0.b); nb.w1 = shd(R0.w1); nb.w2 = shd(R0.w2); nb.w3 = shd(R0.w3);
+      nb.h = shd(R0.h); nb.hinv = shd(R0.hinv);
+      T sln[8];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) sln[4 + v] = shd(slA[4 + v]);
+      strip_trace<T, RECON>(R0, slA + 4, p.half_dy, C);
+      strip_trace<T, RECON>(nb, sln + 4, -p.half_dy, D);
+      riemann<T, RIEMANN, 1>(C, D, T(1), g, Gh, Gx, Gy, Em, Ep);
+      const T cesC = half * g * (R0.h + C.h) * (C.b - R0.b);
+      const T cesD = -(half * g * (nb.h + D.h) * (D.b - nb.b));
+      const T fyl_t = Gy + Em + cesC;
+      const T fyr_own = -Gy + Ep + cesD;
+      const T fyh_b = shu(Gh), fyt_b = shu(Gx), fyr_b = shu(fyr_own);
+      // update of row r-2
+      const int ro = r - 2;
+      const T kx = p.kx, ky = p.ky;
+      const T dh = -(kx * (Fh - fxh_p) + ky * (Gh - fyh_b));
+      const T dqx = -(kx * (fxl_n + fxr_p) + ky * (Gx - fyt_b));
+      const T dqy = -(kx * (Fy - fxt_p) + ky * (fyl_t + fyr_b));
+      fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
+      if (!out_lane || ro < r0 || ro >= r1) continue;
+      const size_t k = (size_t)ro * ny + cj;
+      const T hk = R0.h;
+      T qxk, qyk;
+      if (RECON == ZB_RECON_ETA) {
+        qxk = qxP[k];
+        qyk = qyP[k];
+      } else {
+        qxk = R0.w2;
+        qyk = R0.w3;
+      }
+      T hn, qxn, qyn;
+      if (MODE == MODE_STEP1) {
+        hn = hk + dt * dh;
+        qxn = qxk + dt * dqx;
+        qyn = qyk + dt * dqy;
+      } else {
+        const T h2 = hk + dt * dh, qx2 = qxk + dt * dqx, qy2 = qyk + dt * dqy;
+        const T h0 = h0P[k], qx0 = qx0P[k], qy0 = qy0P[k];
+        hn = half * (h0 + h2);
+        qxn = half * (qx0 + qx2);
+        qyn = half * (qy0 + qy2);
+        if (p.manning_n != T(0)) {
+          const T hi0 = kp_hinv(h0, p.eps_kp);
+          const T qn = sqrt(qxn * qxn + qyn * qyn);
+          const T kf = (-p.g) * (p.manning_n * p.manning_n) * qn * (hi0 * hi0) * cbrt(hi0);
+          if (p.implicit_source) {
+            const T den = T(1) + dt * (-kf);
+            qxn = qxn / den;
+            qyn = qyn / den;
+          } else {
+            qxn = qxn + dt * (qxn * kf);
+            qyn = qyn + dt * (qyn * kf);
+          }
+        }
+      }
+      hO[k] = hn;
+      qxO[k] = qxn;
+      qyO[k] = qyn;
+      bad = bad || (hn < T(0)) || !isfinite(hn) || !isfinite(qxn) || !isfinite(qyn) ||
+            !isfinite(R0.b);
+      if (MODE == MODE_STEP2) {
+        const T hi = kp_hinv(hn, p.eps_kp);
+        const T c = sqrt(g * fmx(hn, T(0)));
+        const T lx = fabs(qxn * hi) + c, ly = fabs(qyn * hi) + c;
+        amax_loc = nmax(amax_loc, (double)nmax(lx, ly));
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&ctrl->status, (unsigned)ZB_ST_TROUBLED);
+  if (MODE == MODE_STEP2) {
+    for (int o = 16; o > 0; o >>= 1)
+      amax_loc = nmax(amax_loc, __shfl_xor_sync(0xffffffffu, amax_loc, o));
+    if (lane == 0) atomic_max_pos_double(&ctrl->amax[(phase + 1) % 3], amax_loc);
+  }
+}
 
 // ── batched ensemble: one persistent launch per stage over all instances ────
 // Each instance is an independent Cartesian grid with its own size, spacing,
@@ -981,6 +1247,7 @@ static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta
   p.lsq = make_lsq<T>(c->dx, c->dy);
   p.inv6dx = (T)(1.0 / (6.0 * c->dx));
   p.inv6dy = (T)(1.0 / (6.0 * c->dy));
+  p.fast_i0 = p.fast_i1 = p.fast_j0 = p.fast_j1 = 0;
   return p;
 }
 
@@ -1032,14 +1299,37 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
       ZB_CUDA_TRY(cudaMemcpyAsync(h, h1, 3 * C * sizeof(T), cudaMemcpyDeviceToDevice, st));
     return ZB_OK;
   }
+  // the interior (two cells in from every side) goes to the strip kernel,
+  // the boundary frame to the tile kernel
+  SweParams<T> pf = p;
+  const int nstrips = c->ny >= 32 ? (c->ny - 32) / SW + 1 : 0;
+  if (ORDER == 2 && nstrips > 0 && c->nx >= 8) {
+    pf.fast_i0 = 2;
+    pf.fast_i1 = c->nx - 2;
+    pf.fast_j0 = 2;
+    pf.fast_j1 = 2 + SW * nstrips;
+  }
+  const bool strips = pf.fast_i1 > pf.fast_i0;
+  const int nitems = strips ? nstrips * ((pf.fast_i1 - pf.fast_i0 + SX - 1) / SX) : 0;
+  const int sgrid = (nitems + STRIP_NT / 32 - 1) / (STRIP_NT / 32);
   if (part != 1) {
+    if (strips) {
+      swe2d_strip_kernel<T, RECON, RIEMANN, MODE_STEP1><<<sgrid, STRIP_NT, 0, st>>>(
+          b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf);
+      ZB_CUDA_TRY(cudaGetLastError());
+    }
     int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP1>(
-        c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, p, st);
+        c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf, st);
     if (rc) return rc;
   }
   if (part == 0) return ZB_OK;
+  if (strips) {
+    swe2d_strip_kernel<T, RECON, RIEMANN, MODE_STEP2><<<sgrid, STRIP_NT, 0, st>>>(
+        b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, pf);
+    ZB_CUDA_TRY(cudaGetLastError());
+  }
   return launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP2>(
-      c, b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, p, st);
+      c, b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, pf, st);
 }
 
 template <typename T, int ORDER, int RECON, int RIEMANN>
