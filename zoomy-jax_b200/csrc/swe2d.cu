@@ -620,7 +620,28 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
   __shared__ double red[NT / 32];
 
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.y * TX, j0 = blockIdx.x * TY;
+  int i0 = blockIdx.y * TX, j0 = blockIdx.x * TY;
+  if (p.fast_i1 > p.fast_i0) {
+    // frame launch (1-D grid): enumerate only the tiles that hold cells outside
+    // the strip kernel's region -- whole tile rows above and below it, then
+    // the tile columns left and right of it for the rows in between
+    const int ntc = (p.ny + TY - 1) / TY, ntr = (p.nx + TX - 1) / TX;
+    // (bands never overlap: a region narrower than a tile leaves tcb = tca)
+    const int tra = (p.fast_i0 + TX - 1) / TX, trb = max(tra, p.fast_i1 / TX);
+    const int tca = (p.fast_j0 + TY - 1) / TY, tcb = max(tca, p.fast_j1 / TY);
+    const int nside = tca + (ntc - tcb);
+    int b = blockIdx.x;
+    if (b < tra * ntc) {
+      i0 = (b / ntc) * TX; j0 = (b % ntc) * TY;
+    } else if ((b -= tra * ntc) < (ntr - trb) * ntc) {
+      i0 = (trb + b / ntc) * TX; j0 = (b % ntc) * TY;
+    } else {
+      b -= (ntr - trb) * ntc;
+      const int tr = tra + b / nside, k = b % nside;
+      i0 = tr * TX;
+      j0 = (k < tca ? k : tcb + (k - tca)) * TY;
+    }
+  }
 
   // dt of this step
   double dtd;
@@ -1254,7 +1275,17 @@ static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta
 template <typename T>
 constexpr int tile_x() { return sizeof(T) == 4 ? 16 : 8; }
 
-template <typename T, int ORDER, int RECON, int RIEMANN, int MODE>
+// number of frame tiles the tile kernel enumerates when the strip kernel
+// owns the interior (see swe2d_stage_kernel)
+template <int TX>
+static int frame_tiles(int nx, int ny, int fi0, int fi1, int fj0, int fj1) {
+  const int ntc = (ny + TY - 1) / TY, ntr = (nx + TX - 1) / TX;
+  const int tra = (fi0 + TX - 1) / TX, trb = std::max(tra, fi1 / TX);
+  const int tca = (fj0 + TY - 1) / TY, tcb = std::max(tca, fj1 / TY);
+  return tra * ntc + (ntr - trb) * ntc + (trb - tra) * (tca + ntc - tcb);
+}
+
+template <typename T, int ORDER, int RECON, int RIEMANN, int MODE, int TX = tile_x<T>()>
 static int launch_stage(const zb_swe2d_cfg* c, const T* b, const T* h, const T* qx,
                         const T* qy, const T* h0, const T* qx0, const T* qy0,
                         T* ho, T* qxo, T* qyo, zb_ctrl* ctrl, int phase,
@@ -1262,7 +1293,6 @@ static int launch_stage(const zb_swe2d_cfg* c, const T* b, const T* h, const T* 
                         const T* hinv_src = nullptr,
                         const unsigned char* force_o1 = nullptr,
                         unsigned char* trouble_out = nullptr) {
-  constexpr int TX = tile_x<T>();
   auto kern = swe2d_stage_kernel<T, TX, ORDER, RECON, RIEMANN, MODE>;
   const size_t sm = sizeof(Smem<T, TX>);
   static unsigned attr_mask = 0u;   // per instantiation, one bit per device
@@ -1274,6 +1304,8 @@ static int launch_stage(const zb_swe2d_cfg* c, const T* b, const T* h, const T* 
     attr_mask |= 1u << dev;
   }
   dim3 grid((c->ny + TY - 1) / TY, (c->nx + TX - 1) / TX);
+  if (p.fast_i1 > p.fast_i0)
+    grid = dim3(frame_tiles<TX>(c->nx, c->ny, p.fast_i0, p.fast_i1, p.fast_j0, p.fast_j1), 1);
   kern<<<grid, NT, sm, st>>>(b, h, qx, qy, h0, qx0, qy0, ho, qxo, qyo, ctrl, phase,
                              hinv_src, force_o1, trouble_out, p);
   return zb_launch_check();
@@ -1318,7 +1350,8 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
           b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf);
       ZB_CUDA_TRY(cudaGetLastError());
     }
-    int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP1>(
+    // the frame is thin: 8-row tiles waste less of their work on it
+    int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP1, 8>(
         c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf, st);
     if (rc) return rc;
   }
@@ -1328,7 +1361,7 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
         b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, pf);
     ZB_CUDA_TRY(cudaGetLastError());
   }
-  return launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP2>(
+  return launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP2, 8>(
       c, b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, pf, st);
 }
 
