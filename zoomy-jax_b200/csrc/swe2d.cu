@@ -738,7 +738,7 @@ template <typename T>
 __device__ __forceinline__ T shu(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 
 template <typename T, int RECON, int RIEMANN, int MODE>
-__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 5 : 2)
 swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
                    const T* __restrict__ qxP, const T* __restrict__ qyP,
                    const T* __restrict__ h0P, const T* __restrict__ qx0P,
@@ -777,6 +777,16 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
   }
   for (int s = 0; s < nsteps; ++s) {
     const int r = r0 - 2 + s;
+    // the update of row r - 2 at the end of this iteration reads these: issue
+    // the loads now so their latency overlaps the slope and face work
+    const int ro = r - 2;
+    const bool upd = s >= 4 && out_lane && ro >= r0 && ro < r1;
+    T qxk = T(0), qyk = T(0), h0 = T(0), qx0 = T(0), qy0 = T(0);
+    if (upd) {
+      const size_t k = (size_t)ro * ny + cj;
+      if (RECON == ZB_RECON_ETA) { qxk = qxP[k]; qyk = qyP[k]; }
+      if (MODE == MODE_STEP2) { h0 = h0P[k]; qx0 = qx0P[k]; qy0 = qy0P[k]; }
+    }
     // shift the windows and take row r
     R0 = R1; R1 = R2;
 #pragma unroll
@@ -882,20 +892,15 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
       const T fyr_own = -Gy + Ep + cesD;
       const T fyh_b = shu(Gh), fyt_b = shu(Gx), fyr_b = shu(fyr_own);
       // update of row r-2
-      const int ro = r - 2;
       const T kx = p.kx, ky = p.ky;
       const T dh = -(kx * (Fh - fxh_p) + ky * (Gh - fyh_b));
       const T dqx = -(kx * (fxl_n + fxr_p) + ky * (Gx - fyt_b));
       const T dqy = -(kx * (Fy - fxt_p) + ky * (fyl_t + fyr_b));
       fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
-      if (!out_lane || ro < r0 || ro >= r1) continue;
+      if (!upd) continue;
       const size_t k = (size_t)ro * ny + cj;
       const T hk = R0.h;
-      T qxk, qyk;
-      if (RECON == ZB_RECON_ETA) {
-        qxk = qxP[k];
-        qyk = qyP[k];
-      } else {
+      if (RECON != ZB_RECON_ETA) {
         qxk = R0.w2;
         qyk = R0.w3;
       }
@@ -906,7 +911,6 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
         qyn = qyk + dt * dqy;
       } else {
         const T h2 = hk + dt * dh, qx2 = qxk + dt * dqx, qy2 = qyk + dt * dqy;
-        const T h0 = h0P[k], qx0 = qx0P[k], qy0 = qy0P[k];
         hn = half * (h0 + h2);
         qxn = half * (qx0 + qx2);
         qyn = half * (qy0 + qy2);
