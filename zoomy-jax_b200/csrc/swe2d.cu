@@ -737,19 +737,18 @@ __device__ __forceinline__ T shd(T v) { return __shfl_down_sync(0xffffffffu, v, 
 template <typename T>
 __device__ __forceinline__ T shu(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 
+// One warp's work item: strip `strip` (28 output columns) over row chunk
+// `chunk` (SX output rows) of a grid whose interior region is p.fast_*.
 template <typename T, int RECON, int RIEMANN, int MODE>
-__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 5 : 2)
-swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
-                   const T* __restrict__ qxP, const T* __restrict__ qyP,
-                   const T* __restrict__ h0P, const T* __restrict__ qx0P,
-                   const T* __restrict__ qy0P, T* __restrict__ hO, T* __restrict__ qxO,
-                   T* __restrict__ qyO, zb_ctrl* ctrl, int phase, const SweParams<T> p) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nstrips = (p.fast_j1 - p.fast_j0) / SW;
-  const int nchunks = (p.fast_i1 - p.fast_i0 + SX - 1) / SX;
-  const int item = blockIdx.x * (STRIP_NT / 32) + warp;
-  if (item >= nstrips * nchunks) return;          // warp-uniform; no block barriers below
-  const int strip = item % nstrips, chunk = item / nstrips;
+__device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __restrict__ hP,
+                                           const T* __restrict__ qxP, const T* __restrict__ qyP,
+                                           const T* __restrict__ h0P,
+                                           const T* __restrict__ qx0P,
+                                           const T* __restrict__ qy0P, T* __restrict__ hO,
+                                           T* __restrict__ qxO, T* __restrict__ qyO,
+                                           zb_ctrl* ctrl, int phase, const SweParams<T>& p,
+                                           const int strip, const int chunk) {
+  const int lane = threadIdx.x & 31;
   const int ny = p.ny;
   const int cj = p.fast_j0 - 2 + strip * SW + lane;
   const int r0 = p.fast_i0 + chunk * SX;
@@ -949,6 +948,21 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
   }
 }
 
+template <typename T, int RECON, int RIEMANN, int MODE>
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 5 : 2)
+swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
+                   const T* __restrict__ qxP, const T* __restrict__ qyP,
+                   const T* __restrict__ h0P, const T* __restrict__ qx0P,
+                   const T* __restrict__ qy0P, T* __restrict__ hO, T* __restrict__ qxO,
+                   T* __restrict__ qyO, zb_ctrl* ctrl, int phase, const SweParams<T> p) {
+  const int nstrips = (p.fast_j1 - p.fast_j0) / SW;
+  const int nchunks = (p.fast_i1 - p.fast_i0 + SX - 1) / SX;
+  const int item = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5);
+  if (item >= nstrips * nchunks) return;          // warp-uniform; no block barriers below
+  strip_item<T, RECON, RIEMANN, MODE>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO, ctrl,
+                                      phase, p, item % nstrips, item / nstrips);
+}
+
 // ── batched ensemble: one persistent launch per stage over all instances ────
 // Each instance is an independent Cartesian grid with its own size, spacing,
 // Manning coefficient, dt and control block.  The work list holds one item
@@ -966,12 +980,15 @@ struct EnsDesc {
 template <typename T, int TX, int ORDER, int RECON, int RIEMANN, int MODE>
 __global__ void __launch_bounds__(NT)
 ens_stage_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ items,
-                 int n_items, T* Q, T* W, zb_ctrl* ctrls, int phase) {
+                 T* Q, T* W, zb_ctrl* ctrls, int phase) {
   using S = Smem<T, TX>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S& s = *reinterpret_cast<S*>(smem_raw);
   __shared__ double red[NT / 32];
   const int tid = threadIdx.x;
+  // items[0] = {tile items, strip items}; tile items follow
+  const int n_items = items[0].x;
+  items += 1;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int4 w = items[it];
     const EnsDesc<T>* d = desc + w.x;
@@ -1005,6 +1022,35 @@ ens_stage_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ i
           s, red, w.y, w.z, q, ws, ws + C, ws + 2 * C, q + C, q + 2 * C, q + 3 * C, q + C,
           q + 2 * C, q + 3 * C, ctrl, ph, nullptr, nullptr, nullptr, p, dtd, w.w != 0);
     }
+  }
+}
+
+constexpr int ENS_STRIP_CTAS = 4;   // fp32 CTAs per SM (the item loop costs registers)
+
+// The interiors of all instances: persistent warps walk the strip items
+// {instance, strip, row chunk} that follow the tile items.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? ENS_STRIP_CTAS : 2)
+ens_strip_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ items, T* Q,
+                 T* W, zb_ctrl* ctrls, int phase) {
+  const int n_tiles = items[0].x, n_strips = items[0].y;
+  const int4* strips = items + 1 + n_tiles;
+  const int nw = gridDim.x * (STRIP_NT / 32);
+  for (int it = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5); it < n_strips; it += nw) {
+    const int4 w = strips[it];
+    const EnsDesc<T>* d = desc + w.x;
+    const SweParams<T>& p = d->p;
+    const size_t C = (size_t)p.nx * p.ny;
+    T* q = Q + d->q_off;
+    T* ws = W + d->ws_off;
+    if (MODE == MODE_STEP1)
+      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>(
+          q, q + C, q + 2 * C, q + 3 * C, nullptr, nullptr, nullptr, ws, ws + C, ws + 2 * C,
+          ctrls + w.x, phase, p, w.y, w.z);
+    else
+      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>(
+          q, ws, ws + C, ws + 2 * C, q + C, q + 2 * C, q + 3 * C, q + C, q + 2 * C, q + 3 * C,
+          ctrls + w.x, phase, p, w.y, w.z);
   }
 }
 
@@ -1419,8 +1465,40 @@ static size_t ens_desc_bytes(int n_inst) {
   return ((size_t)n_inst * sizeof(EnsDesc<T>) + 255) / 256 * 256;
 }
 
-static int ens_tiles(const zb_ens_instance& in, int tile_x) {
-  return ((in.nx + tile_x - 1) / tile_x) * ((in.ny + TY - 1) / TY);
+// interior region an instance hands to the strip kernel (empty: all tiles)
+struct Fast { int i0, i1, j0, j1, nstrips, nchunks; };
+static Fast fast_region(int nx, int ny) {
+  Fast f{0, 0, 0, 0, 0, 0};
+  const int ns = ny >= 32 ? (ny - 32) / SW + 1 : 0;
+  if (ns > 0 && nx >= 8) {
+    f.i0 = 2; f.i1 = nx - 2; f.j0 = 2; f.j1 = 2 + SW * ns;
+    f.nstrips = ns;
+    f.nchunks = (f.i1 - f.i0 + SX - 1) / SX;
+  }
+  return f;
+}
+
+// tiles of an instance holding at least one cell outside its strip region
+template <typename F>
+static void ens_frame_tiles(const zb_ens_instance& in, int tile_x, F&& visit) {
+  const Fast f = fast_region(in.nx, in.ny);
+  for (int i0 = 0; i0 < in.nx; i0 += tile_x)
+    for (int j0 = 0; j0 < in.ny; j0 += TY) {
+      const bool inside = f.i1 > f.i0 && i0 >= f.i0 && std::min(i0 + tile_x, in.nx) <= f.i1 &&
+                          j0 >= f.j0 && std::min(j0 + TY, in.ny) <= f.j1;
+      if (!inside) visit(i0, j0);
+    }
+}
+
+static void ens_counts(const zb_ens_instance* inst, int n, int tile_x, size_t* tiles,
+                       size_t* strips) {
+  *tiles = 0;
+  *strips = 0;
+  for (int i = 0; i < n; ++i) {
+    ens_frame_tiles(inst[i], tile_x, [&](int, int) { ++*tiles; });
+    const Fast f = fast_region(inst[i].nx, inst[i].ny);
+    *strips += (size_t)f.nstrips * f.nchunks;
+  }
 }
 
 static bool ens_valid(const zb_swe2d_cfg* c, const zb_ens_instance* inst, int n, int tile_x) {
@@ -1445,6 +1523,19 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 32) return ZB_E_UNSUPPORTED;
+  static int sms_cache[32] = {0};
+  if (!sms_cache[dev])
+    ZB_CUDA_TRY(cudaDeviceGetAttribute(&sms_cache[dev], cudaDevAttrMultiProcessorCount, dev));
+  // interiors first (persistent warps over the strip items; a grid that finds
+  // none exits at once), then the frame tiles
+  const int sgrid = sms_cache[dev] * (sizeof(T) == 4 ? ENS_STRIP_CTAS : 2);
+  if (part == 0)
+    ens_strip_kernel<T, MODE_STEP1><<<sgrid, STRIP_NT, 0, st>>>(desc, items, (T*)Q, (T*)W, ctrls,
+                                                               phase);
+  else
+    ens_strip_kernel<T, MODE_STEP2><<<sgrid, STRIP_NT, 0, st>>>(desc, items, (T*)Q, (T*)W, ctrls,
+                                                               phase);
+  ZB_CUDA_TRY(cudaGetLastError());
   static unsigned mask1 = 0u, mask2 = 0u;
   auto k1 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>;
   auto k2 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>;
@@ -1462,9 +1553,9 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   }
   grid = std::min(grid, n_items);
   if (part == 0)
-    k1<<<grid, NT, sm, st>>>(desc, items, n_items, (T*)Q, (T*)W, ctrls, phase);
+    k1<<<grid, NT, sm, st>>>(desc, items, (T*)Q, (T*)W, ctrls, phase);
   else
-    k2<<<grid, NT, sm, st>>>(desc, items, n_items, (T*)Q, (T*)W, ctrls, phase);
+    k2<<<grid, NT, sm, st>>>(desc, items, (T*)Q, (T*)W, ctrls, phase);
   return zb_launch_check();
 }
 
@@ -1655,11 +1746,11 @@ int zb_swe2d_step_noalloc(const zb_swe2d_cfg* cfg, void* Q, zb_ctrl* ctrl, int p
 size_t zb_ens_table_bytes(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
                           int tile_x) {
   if (!ens_valid(common, inst, n_inst, tile_x)) return 0;
-  size_t items = 0;
-  for (int i = 0; i < n_inst; ++i) items += (size_t)ens_tiles(inst[i], tile_x);
+  size_t tiles = 0, strips = 0;
+  ens_counts(inst, n_inst, tile_x, &tiles, &strips);
   const size_t d = common->dtype == ZB_F64 ? ens_desc_bytes<double>(n_inst)
                                            : ens_desc_bytes<float>(n_inst);
-  return d + items * sizeof(int4);
+  return d + (1 + tiles + strips) * sizeof(int4);
 }
 
 int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
@@ -1669,7 +1760,7 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
   auto build = [&](auto tag) -> int {
     using T = decltype(tag);
     std::vector<EnsDesc<T>> desc(n_inst);
-    std::vector<int4> items;
+    std::vector<int4> items(1), strips;   // items[0]: {tile items, strip items}
     for (int i = 0; i < n_inst; ++i) {
       zb_swe2d_cfg c = *common;
       c.nx = inst[i].nx;
@@ -1682,19 +1773,24 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
       desc[i].p = make_params<T>(&c, 0.0, 1.0);
       desc[i].q_off = inst[i].q_offset;
       desc[i].ws_off = inst[i].ws_offset;
-      int first = 1;
-      for (int i0 = 0; i0 < c.nx; i0 += tile_x)
-        for (int j0 = 0; j0 < c.ny; j0 += TY) {
-          items.push_back(make_int4(i, i0, j0, first));
-          first = 0;
-        }
+      const Fast f = fast_region(c.nx, c.ny);
+      desc[i].p.fast_i0 = f.i0; desc[i].p.fast_i1 = f.i1;
+      desc[i].p.fast_j0 = f.j0; desc[i].p.fast_j1 = f.j1;
+      // the corner tile (0, 0) is always a frame tile and keeps the lead duties
+      ens_frame_tiles(inst[i], tile_x, [&](int i0, int j0) {
+        items.push_back(make_int4(i, i0, j0, i0 == 0 && j0 == 0));
+      });
+      for (int ch = 0; ch < f.nchunks; ++ch)
+        for (int st = 0; st < f.nstrips; ++st) strips.push_back(make_int4(i, st, ch, 0));
     }
+    items[0] = make_int4((int)(items.size() - 1), (int)strips.size(), 0, 0);
+    items.insert(items.end(), strips.begin(), strips.end());
     const size_t db = ens_desc_bytes<T>(n_inst);
     ZB_CUDA_TRY(cudaMemcpy(table, desc.data(), desc.size() * sizeof(EnsDesc<T>),
                            cudaMemcpyHostToDevice));
     ZB_CUDA_TRY(cudaMemcpy((char*)table + db, items.data(), items.size() * sizeof(int4),
                            cudaMemcpyHostToDevice));
-    *n_items_out = (int)items.size();
+    *n_items_out = (int)items.size() - 1;
     return ZB_OK;
   };
   return common->dtype == ZB_F64 ? build(double()) : build(float());
