@@ -36,6 +36,32 @@ __device__ __forceinline__ double fmn(double a, double b) { return fmin(a, b); }
 __device__ __forceinline__ float clip01(float x) { return __saturatef(x); }
 __device__ __forceinline__ double clip01(double x) { return fmin(fmax(x, 0.0), 1.0); }
 
+// Division of the shallow-water limiter and flux path.  float: __fdividef
+// (x * approximate 1/y, at most 2 ulp for |y| < 2^126; the ratios here are
+// limiter quotients and the HLL 1/(s_R - s_L)); double: IEEE (float64 parity
+// with the oracle).
+__device__ __forceinline__ float adiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double adiv(double a, double b) { return a / b; }
+
+// Three-operand min / max (NaN-dropping like fmx / fmn; exact, so any grouping
+// gives the same bits).  float: the sm_100 three-input PTX forms.
+__device__ __forceinline__ float fmx3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ double fmx3(double a, double b, double c) {
+  return fmax(fmax(a, b), c);
+}
+__device__ __forceinline__ float fmn3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ double fmn3(double a, double b, double c) {
+  return fmin(fmin(a, b), c);
+}
+
 // KP-desingularised inverse depth: sqrt(2) h / sqrt(h^4 + max(h, eps)^4)
 // (zoomy_jax/fvm/solver_jax.py:291-292).  float: one reciprocal square root;
 // double: IEEE division and square root (float64 parity with the oracle).

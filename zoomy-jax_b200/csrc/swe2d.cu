@@ -55,10 +55,14 @@ struct SweParams {
   double alpha, beta;       // Shu-Osher coefficients (generic stage)
   double dt_stage;          // generic stage: dt (< 0: read ctrl->dt)
   T inv6dx, inv6dy;         // interior least-squares gradient factors
+  T inv4dx, inv4dy;         // 1 / (4 dx), 1 / (4 dy): side-class closed forms
   // output region of the interior strip kernel ([fast_i0, fast_i1) x
   // [fast_j0, fast_j1), empty when fast_i0 >= fast_i1); the tile kernel
   // leaves these cells alone
   int fast_i0, fast_i1, fast_j0, fast_j1;
+  // 1: the strip region is the whole grid (fast_i0 = fast_j0 = 0; the strips
+  // reach the boundary and keep the control block; no tile launch)
+  int strip_full;
   LsqTable<T> lsq;
 };
 
@@ -93,12 +97,13 @@ __device__ __forceinline__ double dt_from_amax(double amax, double t,
 // is monotone in both operands, so the minimum over the four faces is exactly
 // clip(min(dpos, -dneg) / max(|a|, |c|)) whenever max(|a|, |c|) > eps (a pair
 // with |d| <= eps contributes 1 and never the minimum), and 1 otherwise: one
-// division per variable instead of four, bit-identical to the per-face form.
+// division per variable instead of four, bit-identical to the per-face form in
+// float64 (float32 divides with adiv, within its 2 ulp of that form).
 template <typename T>
 __device__ __forceinline__ T phi_clipmin(T a, T c, T dpos, T dneg) {
   const T m = fmx(fabs(a), fabs(c));
   const T dm = fmn(dpos, -dneg);
-  const T r = clip01(dm / m);
+  const T r = clip01(adiv(dm, m));
   return m > T(1e-30) ? r : T(1);
 }
 
@@ -108,11 +113,11 @@ __device__ __forceinline__ T vk_cand(T delta, T dpos, T dneg, T ev2) {
   if (delta > eps) {
     T num = dpos * dpos + ev2 + T(2) * delta * dpos;
     T den = dpos * dpos + T(2) * delta * delta + delta * dpos + ev2;
-    return clip01(num / zmax(den, eps));
+    return clip01(adiv(num, zmax(den, eps)));
   } else if (delta < -eps) {
     T num = dneg * dneg + ev2 + T(2) * delta * dneg;
     T den = dneg * dneg + T(2) * delta * delta + delta * dneg + ev2;
-    return clip01(-num / zmin(den, -eps));
+    return clip01(adiv(-num, zmin(den, -eps)));
   }
   return T(1);
 }
@@ -184,11 +189,11 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R, T sg
     Fqx = half * (FLx + FRx) - hs * (qRx - qLx);
     Fqy = half * (FLy + FRy) - hs * (qRy - qLy);
   } else {
-    const T SL = fmn(unL - cL, unR - cR);
-    const T SR = fmx(unL + cL, unR + cR);
-    const T sl = fmn(SL, T(0)), sr = fmx(SR, T(0));
+    // Davis speeds clipped at zero: s_L = min(uL - cL, uR - cR, 0), s_R likewise
+    const T sl = fmn3(unL - cL, unR - cR, T(0));
+    const T sr = fmx3(unL + cL, unR + cR, T(0));
     const T den = sr - sl;
-    const T inv = den > T(0) ? T(1) / den : T(0);
+    const T inv = den > T(0) ? adiv(T(1), den) : T(0);
     const T slsr = sl * sr;
     Fh = (sr * FLh - sl * FRh + slsr * (hRs - hLs)) * inv;
     Fqx = (sr * FLx - sl * FRx + slsr * (qRx - qLx)) * inv;
@@ -278,8 +283,8 @@ __device__ __forceinline__ void stage_tile(
           const T wpm = W[e2 + S::R2Y - 1], wp0 = W[e2 + S::R2Y], wpp = W[e2 + S::R2Y + 1];
           gx = ((wpm + wp0 + wpp) - (wmm + wm0 + wmp)) * p.inv6dx;
           gy = ((wmp + w0p + wpp) - (wmm + w0m + wpm)) * p.inv6dy;
-          umax = fmx(fmx(umax, wp0), fmx(wm0, fmx(w0p, w0m)));
-          umin = fmn(fmn(umin, wp0), fmn(wm0, fmn(w0p, w0m)));
+          umax = fmx3(umax, wp0, fmx3(wm0, w0p, w0m));
+          umin = fmn3(umin, wp0, fmn3(wm0, w0p, w0m));
         } else {
           // ghost values of this cell's boundary faces (BC at the cell state;
           // a wall negates the normal momentum / velocity; periodic = image)
@@ -737,9 +742,15 @@ __device__ __forceinline__ T shd(T v) { return __shfl_down_sync(0xffffffffu, v, 
 template <typename T>
 __device__ __forceinline__ T shu(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 
-// One warp's work item: strip `strip` (28 output columns) over row chunk
-// `chunk` (SX output rows) of a grid whose interior region is p.fast_*.
-template <typename T, int RECON, int RIEMANN, int MODE>
+// One warp's work item: strip `strip` (28 output columns) over the output rows
+// [r0, r1) of the strip region p.fast_*.  EDGE items touch the
+// grid's boundary (full-coverage mode, wall / extrapolation sides only): rows
+// and columns outside the grid are ghosts that load nothing, boundary cells
+// take the least-squares class weights and the ghost values of their sides, and
+// the faces on the boundary take the side's ghost state -- the expressions of
+// stage_tile's boundary branches.  `lead` (the item at the grid's corner in
+// full-coverage mode, where no tile kernel runs) keeps the control block.
+template <typename T, int RECON, int RIEMANN, int MODE, bool EDGE>
 __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __restrict__ hP,
                                            const T* __restrict__ qxP, const T* __restrict__ qyP,
                                            const T* __restrict__ h0P,
@@ -747,18 +758,34 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
                                            const T* __restrict__ qy0P, T* __restrict__ hO,
                                            T* __restrict__ qxO, T* __restrict__ qyO,
                                            zb_ctrl* ctrl, int phase, const SweParams<T>& p,
-                                           const int strip, const int chunk) {
+                                           const int strip, const int r0, const int r1,
+                                           const bool lead) {
   const int lane = threadIdx.x & 31;
-  const int ny = p.ny;
+  const int nx = p.nx, ny = p.ny;
   const int cj = p.fast_j0 - 2 + strip * SW + lane;
-  const int r0 = p.fast_i0 + chunk * SX;
-  const int r1 = min(r0 + SX, p.fast_i1);
+  const bool colv = !EDGE || (cj >= 0 && cj < ny);
   const double t = ctrl->t[phase];
   const double dtd = dt_from_amax(ctrl->amax[phase], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
-  if (!(isfinite(dtd) && dtd > 0.0)) return;      // no-op step: the tile kernel keeps ctrl
+  const bool ok = isfinite(dtd) && dtd > 0.0;
+  if (lead && lane == 0) {
+    // the duties of the tile kernel's lead block (swe2d_stage_kernel)
+    const int nph = (phase + 1) % 3, nnph = (phase + 2) % 3;
+    if (MODE == MODE_STEP1) {
+      if (!ok && t < p.t_end) atomicOr(&ctrl->status, (unsigned)ZB_ST_DT_INVALID);
+      ctrl->dt = ok ? dtd : 0.0;
+      ctrl->t[nph] = ok ? t + dtd : t;
+      ctrl->amax[nnph] = 0.0;
+      ctrl->troubled = 0u;
+    } else if (!ok) {
+      ctrl->amax[nph] = ctrl->amax[phase];
+    } else {
+      atomicAdd(&ctrl->steps, 1u);
+    }
+  }
+  if (!ok) return;                      // no-op step (t_end reached or dt invalid)
   const T dt = T(dtd);
   const T g = p.g, half = T(0.5);
-  const bool out_lane = lane >= 2 && lane < 2 + SW;
+  const bool out_lane = lane >= 2 && lane < 2 + SW && (!EDGE || cj < ny);
 
   RowW<T> R0, R1, R2;                 // rows r-2, r-1, r
   T Sx0[4], Sx1[4], Sx2[4];           // (W(j-1) + W(j)) + W(j+1) of those rows
@@ -769,8 +796,8 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   bool bad = false;
   const int nsteps = (r1 - r0) + 4;
   // row r + 1 is fetched while row r is processed
-  T nbv, nhv, nqxv, nqyv;
-  {
+  T nbv = T(0), nhv = T(0), nqxv = T(0), nqyv = T(0);
+  if (!EDGE || (colv && r0 - 2 >= 0)) {
     const size_t k = (size_t)(r0 - 2) * ny + cj;
     nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
   }
@@ -796,8 +823,12 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
     {
       const T vb = nbv, vh = nhv, vqx = nqxv, vqy = nqyv;
       if (s + 1 < nsteps) {
-        const size_t k = (size_t)(r + 1) * ny + cj;
-        nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
+        if (!EDGE || (colv && r + 1 >= 0 && r + 1 < nx)) {
+          const size_t k = (size_t)(r + 1) * ny + cj;
+          nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
+        } else {
+          nbv = T(0); nhv = T(0); nqxv = T(0); nqyv = T(0);
+        }
       }
       const T hinv = kp_hinv(vh, p.eps_kp);
       R2.b = vb;
@@ -833,12 +864,85 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
         const T gx = (Sx2[v] - Sx0[v]) * p.inv6dx;
         const T gy = (tr - tl) * p.inv6dy;
         const T wp0 = R2.w(v), wm0 = R0.w(v), w0p = Wp1[v], w0m = Wm1[v];
-        const T umax = fmx(fmx(u, wp0), fmx(wm0, fmx(w0p, w0m)));
-        const T umin = fmn(fmn(u, wp0), fmn(wm0, fmn(w0p, w0m)));
+        const T umax = fmx3(u, wp0, fmx3(wm0, w0p, w0m));
+        const T umin = fmn3(u, wp0, fmn3(wm0, w0p, w0m));
         gxa[v] = gx;
         gya[v] = gy;
         phi[v] = limiter_phi(p.limiter, gx, gy, p.half_dx, p.half_dy, umax - u, umin - u,
                              p.vk_eps2);
+      }
+      if (EDGE) {
+        // row r-1 = m: boundary cells (stage_tile phase B, non-interior
+        // branch) and ghosts (zero slopes)
+        const int m = r - 1;
+        const bool cellv = colv && m >= 0 && m < nx;
+        const bool bnd = cellv && (m == 0 || m == nx - 1 || cj == 0 || cj == ny - 1);
+        if (__any_sync(0xffffffffu, bnd)) {
+          const bool bxl = m == 0, bxh = m == nx - 1, byl = cj == 0, byh = cj == ny - 1;
+          const int cls = (bxl ? 0 : (bxh ? 2 : 1)) * 3 + (byl ? 0 : (byh ? 2 : 1));
+          const T* wx = p.lsq.w[cls][0];
+          const T* wy = p.lsq.w[cls][1];
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const T am = shu(R0.w(v)), ap = shd(R0.w(v));
+            if (bnd) {
+              const T u = R1.w(v);
+              T gx = T(0), gy = T(0), umax = u, umin = u;
+              T gxv = u, gyv = u;
+              if ((bxl || bxh) && p.bc[bxl ? 0 : 1] == ZB_BC_WALL && v == 2) gxv = -u;
+              if ((byl || byh) && p.bc[byl ? 2 : 3] == ZB_BC_WALL && v == 3) gyv = -u;
+              if ((bxl || bxh) && (byl || byh)) {
+                // corner: the class weights (the pseudo-inverse is not diagonal)
+                const T nbr[8] = {am, R0.w(v), ap, Wm1[v], Wp1[v], Wm2[v], R2.w(v), Wp2[v]};
+                int k = 0;
+#pragma unroll
+                for (int a = -1; a <= 1; ++a) {
+#pragma unroll
+                  for (int bb = -1; bb <= 1; ++bb) {
+                    if (a == 0 && bb == 0) continue;
+                    const bool okn = m + a >= 0 && m + a < nx && cj + bb >= 0 && cj + bb < ny;
+                    const T d = okn ? nbr[k] - u : T(0);
+                    gx += wx[k] * d;
+                    gy += wy[k] * d;
+                    ++k;
+                  }
+                }
+                { const T d = gxv - u; gx += wx[8] * d; gy += wy[8] * d; }
+                { const T d = gyv - u; gx += wx[9] * d; gy += wy[9] * d; }
+              } else if (byl || byh) {
+                // side column: the five in-domain neighbours give x the normal
+                // matrix diag(4 dx^2, 3 dy^2); y adds its ghost: diag(4 dx^2,
+                // 4 dy^2) -- the class weights in closed form
+                const T n0 = byl ? ap : am, n1 = byl ? Wp1[v] : Wm1[v];
+                const T n2 = byl ? Wp2[v] : Wm2[v];
+                gx = ((R2.w(v) + n2) - (R0.w(v) + n0)) * p.inv4dx;
+                const T sn = (n0 + n1) + n2;
+                gy = (byl ? (sn - gyv) - T(2) * u : (gyv + T(2) * u) - sn) * p.inv4dy;
+              } else {
+                // side row: the same with the roles of x and y exchanged
+                const T n0 = bxl ? Wm2[v] : am, n1 = bxl ? R2.w(v) : R0.w(v);
+                const T n2 = bxl ? Wp2[v] : ap;
+                gy = ((Wp1[v] + n2) - (Wm1[v] + n0)) * p.inv4dy;
+                const T sn = (n0 + n1) + n2;
+                gx = (bxl ? (sn - gxv) - T(2) * u : (gxv + T(2) * u) - sn) * p.inv4dx;
+              }
+              if (!bxh) { umax = fmx(umax, R2.w(v)); umin = fmn(umin, R2.w(v)); }
+              if (!bxl) { umax = fmx(umax, R0.w(v)); umin = fmn(umin, R0.w(v)); }
+              if (!byh) { umax = fmx(umax, Wp1[v]); umin = fmn(umin, Wp1[v]); }
+              if (!byl) { umax = fmx(umax, Wm1[v]); umin = fmn(umin, Wm1[v]); }
+              if (bxl || bxh) { const T gg = T(2) * gxv - u; umax = fmx(umax, gg); umin = fmn(umin, gg); }
+              if (byl || byh) { const T gg = T(2) * gyv - u; umax = fmx(umax, gg); umin = fmn(umin, gg); }
+              gxa[v] = gx;
+              gya[v] = gy;
+              phi[v] = limiter_phi(p.limiter, gx, gy, p.half_dx, p.half_dy, umax - u, umin - u,
+                                   p.vk_eps2);
+            }
+          }
+        }
+        if (!cellv) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) { phi[v] = T(0); gxa[v] = T(0); gya[v] = T(0); }
+        }
       }
       if (RECON == ZB_RECON_ETA) {
         if (p.eps_wet >= T(0) && R1.h < p.eps_wet) {
@@ -864,11 +968,35 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       Side<T> A, B;
       strip_trace<T, RECON>(R0, slA, p.half_dx, A);
       strip_trace<T, RECON>(R1, slB, -p.half_dx, B);
-      riemann<T, RIEMANN, 0>(A, B, T(1), g, Fh, Fx, Fy, Dm, Dp);
+      // EDGE: a face on the x boundary takes the owner's trace (row 0 below
+      // the face, row nx-1 above it) against its ghost with normal sign sg
+      // (stage_tile's x-face boundary branch)
+      const bool xb = EDGE && (r - 1 == 0 || r - 2 == nx - 1);
+      const bool xlo = EDGE && r - 1 == 0;
+      T sgx = T(1);
+      Side<T> L = A, R = B;
+      if (xb) {
+        L = xlo ? B : A;
+        R = L;
+        if (p.bc[xlo ? 0 : 1] == ZB_BC_WALL) {
+          R.qx = -L.qx;
+          R.ux = -L.ux;
+        }
+        sgx = xlo ? T(-1) : T(1);
+      }
+      riemann<T, RIEMANN, 0>(L, R, sgx, g, Fh, Fx, Fy, Dm, Dp);
       const T cesA = half * g * (R0.h + A.h) * (A.b - R0.b);
       const T cesB = -(half * g * (R1.h + B.h) * (B.b - R1.b));
       fxl_n = Fx + Dm + cesA;
-      const T fxr_n = -Fx + Dp + cesB;
+      T fxr_n = -Fx + Dp + cesB;
+      if (xb) {
+        const T own_n = Fx + Dm * sgx + (xlo ? -cesB : cesA) * sgx;
+        if (xlo) {
+          Fh = -Fh; Fy = -Fy; fxr_n = own_n; fxl_n = T(0);
+        } else {
+          fxl_n = own_n; fxr_n = T(0);
+        }
+      }
       if (s == 3) {            // face r0 - 1/2: only the next row needs it
         fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
         continue;
@@ -884,11 +1012,35 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       for (int v = 0; v < 4; ++v) sln[4 + v] = shd(slA[4 + v]);
       strip_trace<T, RECON>(R0, slA + 4, p.half_dy, C);
       strip_trace<T, RECON>(nb, sln + 4, -p.half_dy, D);
-      riemann<T, RIEMANN, 1>(C, D, T(1), g, Gh, Gx, Gy, Em, Ep);
+      // EDGE: a face on the y boundary takes the owner's trace (the next
+      // lane's cell 0, or this lane's cell ny-1) against its ghost
+      const bool yb = EDGE && (cj == -1 || cj == ny - 1);
+      const bool ylo = EDGE && cj == -1;
+      T sgy = T(1);
+      Side<T> YL = C, YR = D;
+      if (EDGE) {
+        YL.b = ylo ? D.b : C.b; YL.h = ylo ? D.h : C.h; YL.qx = ylo ? D.qx : C.qx;
+        YL.qy = ylo ? D.qy : C.qy; YL.ux = ylo ? D.ux : C.ux; YL.uy = ylo ? D.uy : C.uy;
+        const bool wall = yb && p.bc[ylo ? 2 : 3] == ZB_BC_WALL;
+        YR.b = yb ? YL.b : D.b; YR.h = yb ? YL.h : D.h; YR.qx = yb ? YL.qx : D.qx;
+        YR.ux = yb ? YL.ux : D.ux;
+        YR.qy = yb ? (wall ? -YL.qy : YL.qy) : D.qy;
+        YR.uy = yb ? (wall ? -YL.uy : YL.uy) : D.uy;
+        sgy = ylo ? T(-1) : T(1);
+      }
+      riemann<T, RIEMANN, 1>(YL, YR, sgy, g, Gh, Gx, Gy, Em, Ep);
       const T cesC = half * g * (R0.h + C.h) * (C.b - R0.b);
       const T cesD = -(half * g * (nb.h + D.h) * (D.b - nb.b));
-      const T fyl_t = Gy + Em + cesC;
-      const T fyr_own = -Gy + Ep + cesD;
+      T fyl_t = Gy + Em + cesC;
+      T fyr_own = -Gy + Ep + cesD;
+      if (yb) {
+        const T own_n = Gy + Em * sgy + (ylo ? -cesD : cesC) * sgy;
+        if (ylo) {
+          Gh = -Gh; Gx = -Gx; fyr_own = own_n; fyl_t = T(0);
+        } else {
+          fyl_t = own_n; fyr_own = T(0);
+        }
+      }
       const T fyh_b = shu(Gh), fyt_b = shu(Gx), fyr_b = shu(fyr_own);
       // update of row r-2
       const T kx = p.kx, ky = p.ky;
@@ -948,19 +1100,110 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   }
 }
 
-template <typename T, int RECON, int RIEMANN, int MODE>
-__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 5 : 2)
+// Full-coverage item list of a grid (strips of SW columns from column 0,
+// rows from 0).  Strips whose 32 lanes reach outside the grid (the first, and
+// the last one or two) run the EDGE body on every row and march chunks of SXE
+// rows, so that they end with the others; each middle strip has two EDGE items
+// for the boundary rows [0, 2) and [nx - 2, nx) and marches the rows between
+// in SX-row interior chunks.  Item 0 (strip 0, rows 0..) keeps the control
+// block.  Returns the item count (item = -1), the count of EDGE items, which
+// come first (item = -2), or with item >= 0 fills its strip and rows.
+constexpr int SXE = 8;
+__host__ __device__ inline int full_items(int nx, int ny, int item, int* strip, int* r0,
+                                          int* r1) {
+  const int ns = (ny + SW - 1) / SW;
+  // middle strips: 1 <= s <= mh (lanes 28 s - 2 .. 28 s + 29 inside the grid)
+  int mh = ny >= 30 ? (ny - 30) / SW : 0;
+  if (mh > ns - 1) mh = ns - 1;
+  if (nx < 4) mh = 0;
+  const int nmid = mh, nedge = ns - nmid;
+  const int nce = (nx + SXE - 1) / SXE;
+  const int nci = nx > 4 ? (nx - 4 + SX - 1) / SX : 0;
+  const int total = nedge * nce + nmid * (2 + nci);
+  if (item == -2) return nedge * nce + 2 * nmid;   // the EDGE items come first
+  if (item < 0) return total;
+  int st, a, b;
+  if (item < nedge * nce) {
+    const int e = item / nce;                // edge strips: 0, mh + 1, ..., ns - 1
+    st = e == 0 ? 0 : mh + e;
+    a = (item % nce) * SXE;
+    b = a + SXE;
+  } else if ((item -= nedge * nce) < 2 * nmid) {
+    st = 1 + item / 2;
+    a = (item & 1) ? nx - 2 : 0;
+    b = a + 2;
+  } else {
+    item -= 2 * nmid;
+    st = 1 + item % nmid;
+    a = 2 + (item / nmid) * SX;
+    b = a + SX < nx - 2 ? a + SX : nx - 2;
+  }
+  *strip = st;
+  *r0 = a;
+  *r1 = b < nx ? b : nx;
+  return total;
+}
+
+// an item reaches a boundary or a ghost row or column: the EDGE body
+__host__ __device__ inline bool full_item_edge(int nx, int ny, int strip, int r0, int r1) {
+  const int cj0 = strip * SW - 2;
+  return !(r0 >= 2 && r1 <= nx - 2 && cj0 >= 0 && cj0 + 31 <= ny - 1);
+}
+
+// KIND 0: the interior strips of a grid with a periodic side (the tile kernel
+// takes the frame); KIND 1: the EDGE items of a full-coverage list; KIND 2:
+// its interior items.  Kinds 1 and 2 are separate launches (they run side by
+// side on two streams) so that the EDGE body never raises the interior body's
+// register allocation.
+template <typename T, int RECON, int RIEMANN, int MODE, int KIND>
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? (KIND == 1 ? 4 : 5) : 2)
 swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
                    const T* __restrict__ qxP, const T* __restrict__ qyP,
                    const T* __restrict__ h0P, const T* __restrict__ qx0P,
                    const T* __restrict__ qy0P, T* __restrict__ hO, T* __restrict__ qxO,
                    T* __restrict__ qyO, zb_ctrl* ctrl, int phase, const SweParams<T> p) {
-  const int nstrips = (p.fast_j1 - p.fast_j0) / SW;
-  const int nchunks = (p.fast_i1 - p.fast_i0 + SX - 1) / SX;
-  const int item = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5);
-  if (item >= nstrips * nchunks) return;          // warp-uniform; no block barriers below
-  strip_item<T, RECON, RIEMANN, MODE>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO, ctrl,
-                                      phase, p, item % nstrips, item / nstrips);
+  int item = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5);
+  int strip, r0, r1;
+  if (KIND == 0) {
+    const int nstrips = (p.fast_j1 - p.fast_j0) / SW;
+    if (item >= nstrips * ((p.fast_i1 - p.fast_i0 + SX - 1) / SX)) return;   // warp-uniform
+    strip = item % nstrips;
+    r0 = p.fast_i0 + (item / nstrips) * SX;
+    r1 = min(r0 + SX, p.fast_i1);
+  } else {
+    const int ne = full_items(p.nx, p.ny, -2, nullptr, nullptr, nullptr);
+    if (KIND == 1 && item >= ne) return;
+    if (KIND == 2) {
+      item += ne;
+      if (item >= full_items(p.nx, p.ny, -1, nullptr, nullptr, nullptr)) return;
+    }
+    full_items(p.nx, p.ny, item, &strip, &r0, &r1);
+  }
+  strip_item<T, RECON, RIEMANN, MODE, KIND == 1>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO,
+                                                 qyO, ctrl, phase, p, strip, r0, r1,
+                                                 KIND == 1 && item == 0);
+}
+
+// A second stream per device with a fork and a join event: the EDGE launch of
+// a full-coverage stage runs on it beside the interior launch.
+struct SideStream {
+  cudaStream_t s;
+  cudaEvent_t fork, join;
+};
+static int side_stream(SideStream** out) {
+  static SideStream ss[32];
+  static unsigned made = 0u;
+  int dev = 0;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 32) return ZB_E_UNSUPPORTED;
+  if (!(made & (1u << dev))) {
+    ZB_CUDA_TRY(cudaStreamCreateWithFlags(&ss[dev].s, cudaStreamNonBlocking));
+    ZB_CUDA_TRY(cudaEventCreateWithFlags(&ss[dev].fork, cudaEventDisableTiming));
+    ZB_CUDA_TRY(cudaEventCreateWithFlags(&ss[dev].join, cudaEventDisableTiming));
+    made |= 1u << dev;
+  }
+  *out = &ss[dev];
+  return ZB_OK;
 }
 
 // ── batched ensemble: one persistent launch per stage over all instances ────
@@ -1025,32 +1268,38 @@ ens_stage_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ i
   }
 }
 
-constexpr int ENS_STRIP_CTAS = 4;   // fp32 CTAs per SM (the item loop costs registers)
-
-// The interiors of all instances: persistent warps walk the strip items
-// {instance, strip, row chunk} that follow the tile items.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? ENS_STRIP_CTAS : 2)
+// All instances' strip items: persistent warps walk them.  The work list's
+// header items[0] = {tile items, interior strip items, boundary strip items};
+// the tile items follow it, then the interior strips, then the boundary
+// strips (the EDGE body, a launch of its own so that its extra live values
+// never raise the interior body's register allocation).
+template <typename T, int MODE, bool EDGE>
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
 ens_strip_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ items, T* Q,
                  T* W, zb_ctrl* ctrls, int phase) {
-  const int n_tiles = items[0].x, n_strips = items[0].y;
-  const int4* strips = items + 1 + n_tiles;
+  const int4 hd = items[0];
+  const int4* list = items + 1 + hd.x + (EDGE ? hd.y : 0);
+  const int n = EDGE ? hd.z : hd.y;
   const int nw = gridDim.x * (STRIP_NT / 32);
-  for (int it = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5); it < n_strips; it += nw) {
-    const int4 w = strips[it];
+  for (int it = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5); it < n; it += nw) {
+    // w = {instance, strip, r0, flags | r1 << 2}; flags bit 1 = the item keeps
+    // the instance's control block
+    const int4 w = list[it];
     const EnsDesc<T>* d = desc + w.x;
     const SweParams<T>& p = d->p;
     const size_t C = (size_t)p.nx * p.ny;
     T* q = Q + d->q_off;
     T* ws = W + d->ws_off;
+    const bool lead = EDGE && (w.w & 2) != 0;
+    const int r1 = w.w >> 2;
     if (MODE == MODE_STEP1)
-      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>(
+      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1, EDGE>(
           q, q + C, q + 2 * C, q + 3 * C, nullptr, nullptr, nullptr, ws, ws + C, ws + 2 * C,
-          ctrls + w.x, phase, p, w.y, w.z);
+          ctrls + w.x, phase, p, w.y, w.z, r1, lead);
     else
-      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>(
+      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2, EDGE>(
           q, ws, ws + C, ws + 2 * C, q + C, q + 2 * C, q + 3 * C, q + C, q + 2 * C, q + 3 * C,
-          ctrls + w.x, phase, p, w.y, w.z);
+          ctrls + w.x, phase, p, w.y, w.z, r1, lead);
   }
 }
 
@@ -1318,7 +1567,10 @@ static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta
   p.lsq = make_lsq<T>(c->dx, c->dy);
   p.inv6dx = (T)(1.0 / (6.0 * c->dx));
   p.inv6dy = (T)(1.0 / (6.0 * c->dy));
+  p.inv4dx = (T)(1.0 / (4.0 * c->dx));
+  p.inv4dy = (T)(1.0 / (4.0 * c->dy));
   p.fast_i0 = p.fast_i1 = p.fast_j0 = p.fast_j1 = 0;
+  p.strip_full = 0;
   return p;
 }
 
@@ -1381,36 +1633,88 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
       ZB_CUDA_TRY(cudaMemcpyAsync(h, h1, 3 * C * sizeof(T), cudaMemcpyDeviceToDevice, st));
     return ZB_OK;
   }
-  // the interior (two cells in from every side) goes to the strip kernel,
-  // the boundary frame to the tile kernel
+  // Without a periodic side the strip kernel covers the whole grid (strips
+  // and row chunks that reach the boundary take its EDGE body) and keeps the
+  // control block.  With one, the interior (two cells in from every side)
+  // goes to the strip kernel and the boundary frame to the tile kernel.
   SweParams<T> pf = p;
-  const int nstrips = c->ny >= 32 ? (c->ny - 32) / SW + 1 : 0;
-  if (ORDER == 2 && nstrips > 0 && c->nx >= 8) {
-    pf.fast_i0 = 2;
-    pf.fast_i1 = c->nx - 2;
-    pf.fast_j0 = 2;
-    pf.fast_j1 = 2 + SW * nstrips;
+  int nstrips = 0;
+  if (ORDER == 2) {
+    bool periodic = false;
+    for (int sd = 0; sd < 4; ++sd) periodic = periodic || c->bc[sd] == ZB_BC_PERIODIC;
+    if (!periodic && c->nx >= 4 && c->ny >= 4) {
+      nstrips = (c->ny + SW - 1) / SW;
+      pf.fast_i0 = 0;
+      pf.fast_i1 = c->nx;
+      pf.fast_j0 = 0;
+      pf.fast_j1 = SW * nstrips;
+      pf.strip_full = 1;
+    } else if (c->ny >= 32 && c->nx >= 8) {
+      nstrips = (c->ny - 32) / SW + 1;
+      pf.fast_i0 = 2;
+      pf.fast_i1 = c->nx - 2;
+      pf.fast_j0 = 2;
+      pf.fast_j1 = 2 + SW * nstrips;
+    }
   }
   const bool strips = pf.fast_i1 > pf.fast_i0;
-  const int nitems = strips ? nstrips * ((pf.fast_i1 - pf.fast_i0 + SX - 1) / SX) : 0;
+  const bool tiles = !pf.strip_full;
+  const int nitems = !strips ? 0
+                     : pf.strip_full ? full_items(c->nx, c->ny, -1, nullptr, nullptr, nullptr)
+                                     : nstrips * ((pf.fast_i1 - pf.fast_i0 + SX - 1) / SX);
   const int sgrid = (nitems + STRIP_NT / 32 - 1) / (STRIP_NT / 32);
-  if (part != 1) {
-    if (strips) {
-      swe2d_strip_kernel<T, RECON, RIEMANN, MODE_STEP1><<<sgrid, STRIP_NT, 0, st>>>(
-          b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf);
+  // full coverage: the EDGE items on the side stream, the interior items here
+  SideStream* side = nullptr;
+  int ne = 0, ni = 0;
+  if (pf.strip_full) {
+    int rc = side_stream(&side);
+    if (rc) return rc;
+    ne = full_items(c->nx, c->ny, -2, nullptr, nullptr, nullptr);
+    ni = nitems - ne;
+  }
+  const int wpb = STRIP_NT / 32;
+  auto launch_strips = [&](auto mode, const T* h_, const T* qx_, const T* qy_, const T* h0_,
+                           const T* qx0_, const T* qy0_, T* ho_, T* qxo_, T* qyo_) -> int {
+    constexpr int M = decltype(mode)::value;
+    if (!pf.strip_full) {
+      swe2d_strip_kernel<T, RECON, RIEMANN, M, 0><<<sgrid, STRIP_NT, 0, st>>>(
+          b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
+      return zb_launch_check();
+    }
+    ZB_CUDA_TRY(cudaEventRecord(side->fork, st));
+    ZB_CUDA_TRY(cudaStreamWaitEvent(side->s, side->fork, 0));
+    swe2d_strip_kernel<T, RECON, RIEMANN, M, 1><<<(ne + wpb - 1) / wpb, STRIP_NT, 0, side->s>>>(
+        b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
+    ZB_CUDA_TRY(cudaGetLastError());
+    if (ni > 0) {
+      swe2d_strip_kernel<T, RECON, RIEMANN, M, 2><<<(ni + wpb - 1) / wpb, STRIP_NT, 0, st>>>(
+          b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
       ZB_CUDA_TRY(cudaGetLastError());
     }
-    // the frame is thin: 8-row tiles waste less of their work on it
-    int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP1, 8>(
-        c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf, st);
-    if (rc) return rc;
+    ZB_CUDA_TRY(cudaEventRecord(side->join, side->s));
+    ZB_CUDA_TRY(cudaStreamWaitEvent(st, side->join, 0));
+    return ZB_OK;
+  };
+  using M1 = std::integral_constant<int, MODE_STEP1>;
+  using M2 = std::integral_constant<int, MODE_STEP2>;
+  if (part != 1) {
+    if (strips) {
+      int rc = launch_strips(M1(), h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1);
+      if (rc) return rc;
+    }
+    if (tiles) {
+      // the frame is thin: 8-row tiles waste less of their work on it
+      int rc = launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP1, 8>(
+          c, b, h, qx, qy, nullptr, nullptr, nullptr, h1, qx1, qy1, ctrl, phase, pf, st);
+      if (rc) return rc;
+    }
   }
   if (part == 0) return ZB_OK;
   if (strips) {
-    swe2d_strip_kernel<T, RECON, RIEMANN, MODE_STEP2><<<sgrid, STRIP_NT, 0, st>>>(
-        b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, pf);
-    ZB_CUDA_TRY(cudaGetLastError());
+    int rc = launch_strips(M2(), h1, qx1, qy1, h, qx, qy, h, qx, qy);
+    if (rc) return rc;
   }
+  if (!tiles) return ZB_OK;
   return launch_stage<T, ORDER, RECON, RIEMANN, MODE_STEP2, 8>(
       c, b, h1, qx1, qy1, h, qx, qy, h, qx, qy, ctrl, phase, pf, st);
 }
@@ -1465,29 +1769,39 @@ static size_t ens_desc_bytes(int n_inst) {
   return ((size_t)n_inst * sizeof(EnsDesc<T>) + 255) / 256 * 256;
 }
 
-// interior region an instance hands to the strip kernel (empty: all tiles)
+// strip region of an instance: the whole grid (every instance has wall or
+// extrapolation sides), or empty for a grid too small for strips (all tiles)
 struct Fast { int i0, i1, j0, j1, nstrips, nchunks; };
 static Fast fast_region(int nx, int ny) {
   Fast f{0, 0, 0, 0, 0, 0};
-  const int ns = ny >= 32 ? (ny - 32) / SW + 1 : 0;
-  if (ns > 0 && nx >= 8) {
-    f.i0 = 2; f.i1 = nx - 2; f.j0 = 2; f.j1 = 2 + SW * ns;
-    f.nstrips = ns;
-    f.nchunks = (f.i1 - f.i0 + SX - 1) / SX;
+  if (nx >= 4 && ny >= 4) {
+    f.nstrips = (ny + SW - 1) / SW;
+    f.nchunks = (nx + SX - 1) / SX;
+    f.i1 = nx; f.j1 = SW * f.nstrips;
   }
   return f;
 }
 
-// tiles of an instance holding at least one cell outside its strip region
+// strip items of an instance (the single grid's full-coverage list):
+// {strip, r0, r1, flags}; flags bit 0 = the item reaches the boundary (EDGE
+// body), bit 1 = it keeps the control block
+template <typename F>
+static void ens_strip_items(const zb_ens_instance& in, F&& visit) {
+  if (fast_region(in.nx, in.ny).nstrips == 0) return;
+  const int n = full_items(in.nx, in.ny, -1, nullptr, nullptr, nullptr);
+  for (int it = 0; it < n; ++it) {
+    int st, r0, r1;
+    full_items(in.nx, in.ny, it, &st, &r0, &r1);
+    visit(st, r0, r1, (full_item_edge(in.nx, in.ny, st, r0, r1) ? 1 : 0) | (it == 0 ? 2 : 0));
+  }
+}
+
+// tiles of an instance that the strips do not cover (all of a small grid's)
 template <typename F>
 static void ens_frame_tiles(const zb_ens_instance& in, int tile_x, F&& visit) {
-  const Fast f = fast_region(in.nx, in.ny);
+  if (fast_region(in.nx, in.ny).nstrips > 0) return;
   for (int i0 = 0; i0 < in.nx; i0 += tile_x)
-    for (int j0 = 0; j0 < in.ny; j0 += TY) {
-      const bool inside = f.i1 > f.i0 && i0 >= f.i0 && std::min(i0 + tile_x, in.nx) <= f.i1 &&
-                          j0 >= f.j0 && std::min(j0 + TY, in.ny) <= f.j1;
-      if (!inside) visit(i0, j0);
-    }
+    for (int j0 = 0; j0 < in.ny; j0 += TY) visit(i0, j0);
 }
 
 static void ens_counts(const zb_ens_instance* inst, int n, int tile_x, size_t* tiles,
@@ -1496,8 +1810,8 @@ static void ens_counts(const zb_ens_instance* inst, int n, int tile_x, size_t* t
   *strips = 0;
   for (int i = 0; i < n; ++i) {
     ens_frame_tiles(inst[i], tile_x, [&](int, int) { ++*tiles; });
-    const Fast f = fast_region(inst[i].nx, inst[i].ny);
-    *strips += (size_t)f.nstrips * f.nchunks;
+    if (fast_region(inst[i].nx, inst[i].ny).nstrips > 0)
+      *strips += (size_t)full_items(inst[i].nx, inst[i].ny, -1, nullptr, nullptr, nullptr);
   }
 }
 
@@ -1526,15 +1840,22 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   static int sms_cache[32] = {0};
   if (!sms_cache[dev])
     ZB_CUDA_TRY(cudaDeviceGetAttribute(&sms_cache[dev], cudaDevAttrMultiProcessorCount, dev));
-  // interiors first (persistent warps over the strip items; a grid that finds
-  // none exits at once), then the frame tiles
-  const int sgrid = sms_cache[dev] * (sizeof(T) == 4 ? ENS_STRIP_CTAS : 2);
-  if (part == 0)
-    ens_strip_kernel<T, MODE_STEP1><<<sgrid, STRIP_NT, 0, st>>>(desc, items, (T*)Q, (T*)W, ctrls,
-                                                               phase);
-  else
-    ens_strip_kernel<T, MODE_STEP2><<<sgrid, STRIP_NT, 0, st>>>(desc, items, (T*)Q, (T*)W, ctrls,
-                                                               phase);
+  // boundary strips, interior strips (persistent warps over their items; a
+  // grid that finds none exits at once), then the tiles of grids too small
+  // for strips
+  const int sgrid_e = sms_cache[dev] * (sizeof(T) == 4 ? 4 : 2);
+  const int sgrid_i = sgrid_e;
+  if (part == 0) {
+    ens_strip_kernel<T, MODE_STEP1, true><<<sgrid_e, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
+                                                                       (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP1, false><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
+                                                                        (T*)W, ctrls, phase);
+  } else {
+    ens_strip_kernel<T, MODE_STEP2, true><<<sgrid_e, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
+                                                                       (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP2, false><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
+                                                                        (T*)W, ctrls, phase);
+  }
   ZB_CUDA_TRY(cudaGetLastError());
   static unsigned mask1 = 0u, mask2 = 0u;
   auto k1 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>;
@@ -1760,7 +2081,8 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
   auto build = [&](auto tag) -> int {
     using T = decltype(tag);
     std::vector<EnsDesc<T>> desc(n_inst);
-    std::vector<int4> items(1), strips;   // items[0]: {tile items, strip items}
+    // items[0]: {tile items, interior strip items, boundary strip items}
+    std::vector<int4> items(1), strips, estrips;
     for (int i = 0; i < n_inst; ++i) {
       zb_swe2d_cfg c = *common;
       c.nx = inst[i].nx;
@@ -1776,15 +2098,18 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
       const Fast f = fast_region(c.nx, c.ny);
       desc[i].p.fast_i0 = f.i0; desc[i].p.fast_i1 = f.i1;
       desc[i].p.fast_j0 = f.j0; desc[i].p.fast_j1 = f.j1;
-      // the corner tile (0, 0) is always a frame tile and keeps the lead duties
+      desc[i].p.strip_full = f.nstrips > 0 ? 1 : 0;
+      // tile (0, 0) or strip item (0, 0) keeps the lead duties
       ens_frame_tiles(inst[i], tile_x, [&](int i0, int j0) {
         items.push_back(make_int4(i, i0, j0, i0 == 0 && j0 == 0));
       });
-      for (int ch = 0; ch < f.nchunks; ++ch)
-        for (int st = 0; st < f.nstrips; ++st) strips.push_back(make_int4(i, st, ch, 0));
+      ens_strip_items(inst[i], [&](int st, int r0, int r1, int fl) {
+        ((fl & 1) ? estrips : strips).push_back(make_int4(i, st, r0, fl | (r1 << 2)));
+      });
     }
-    items[0] = make_int4((int)(items.size() - 1), (int)strips.size(), 0, 0);
+    items[0] = make_int4((int)(items.size() - 1), (int)strips.size(), (int)estrips.size(), 0);
     items.insert(items.end(), strips.begin(), strips.end());
+    items.insert(items.end(), estrips.begin(), estrips.end());
     const size_t db = ens_desc_bytes<T>(n_inst);
     ZB_CUDA_TRY(cudaMemcpy(table, desc.data(), desc.size() * sizeof(EnsDesc<T>),
                            cudaMemcpyHostToDevice));
