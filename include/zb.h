@@ -503,6 +503,37 @@ size_t zb_tri_mass_partials(void);
 int zb_tri_mass(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, const void* Q,
                 double* partial, zb_ctrl* ctrl, zb_stream_t stream);
 
+/* ── triangle mesh preparation on the GPU ─────────────────────────────────
+ * Replaces the host conversion LSQMesh -> MeshJAX (zoomy_jax/mesh/mesh.py:
+ * 123-264) and prepare_mesh's index sets (zoomy_jax/fvm/solver2/context.py:
+ * 99-163): faces from matched half-edges, owner / neighbour, interior /
+ * boundary split, normals, lengths, centre offsets, inradius, least-squares
+ * stencils and weights, boundary kinds.  P: [n_vert][2] float64 vertices,
+ * T: [n_cells][3] int32 triangles (either orientation; cell order kept), both
+ * device pointers.  Face numbers follow (owner cell, local edge), the owner
+ * of a shared edge being the lower cell index; boundary faces are numbered in
+ * face order. */
+
+/* Scratch bytes of zb_trimesh_match / zb_trimesh_fill (0: too many cells). */
+size_t zb_trimesh_scratch_bytes(int32_t n_cells);
+
+/* Phase 1: orient, match the half-edges, number the faces.  Writes the face
+ * and boundary-face counts to *n_faces / *n_bf (one stream synchronisation).
+ * ZB_E_ARG for a vertex index out of range, a zero-area triangle or an edge
+ * shared by more than two triangles. */
+int zb_trimesh_match(const double* P, int32_t n_vert, const int32_t* T,
+                     int32_t n_cells, void* scratch, size_t scratch_bytes,
+                     int32_t* n_faces, int32_t* n_bf, zb_stream_t stream);
+
+/* Phase 2: write the arrays of *mesh (allocated by the caller with the counts
+ * of phase 1, geometry in dtype ZB_F32 / ZB_F64, face_inr float64; the
+ * pointers are written through).  bc_kind_by_side: 4 host ints, the ZB_BC_*
+ * of the left, right, bottom and top sides (a boundary face takes the side
+ * its outward normal faces). */
+int zb_trimesh_fill(const double* P, int32_t n_cells, const int32_t* bc_kind_by_side,
+                    int32_t dtype, const void* scratch, size_t scratch_bytes,
+                    zb_tri_mesh* mesh, zb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,9 +8,9 @@ come from PyTorch; nothing runs on the CPU.
 """
 from . import timestepping  # noqa: F401
 from .mesh import CartesianMesh, create_2d  # noqa: F401
-from .trimesh import TriangleMesh, create_tri  # noqa: F401
+from .trimesh import DeviceTriangleMesh, TriangleMesh, create_tri  # noqa: F401
 from .model import (NumericalSystemModel, ReconstructionSpec,  # noqa: F401
                     ShallowWater2D)
 
-__all__ = ["CartesianMesh", "TriangleMesh", "create_2d", "create_tri", "NumericalSystemModel",
+__all__ = ["CartesianMesh", "TriangleMesh", "DeviceTriangleMesh", "create_2d", "create_tri", "NumericalSystemModel",
            "ReconstructionSpec", "ShallowWater2D", "timestepping"]

@@ -138,6 +138,11 @@ SIGNATURES = [
     ("zb_tri_aux", C.c_int, [_TCFG, _TMESH, _P, _P, _P]),
     ("zb_tri_mass_partials", C.c_size_t, []),
     ("zb_tri_mass", C.c_int, [_TCFG, _TMESH, _P, _P, _P, _P]),
+    ("zb_trimesh_scratch_bytes", C.c_size_t, [C.c_int32]),
+    ("zb_trimesh_match", C.c_int, [_P, C.c_int32, _P, C.c_int32, _P, C.c_size_t,
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32), _P]),
+    ("zb_trimesh_fill", C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), C.c_int32, _P,
+                                  C.c_size_t, _TMESH, _P]),
     ("zb_unet_conv_impl", C.c_int, [C.c_int]),
     ("zb_unet_status", C.c_int, [C.c_int]),
     ("zb_unet_param_count", C.c_size_t, [C.c_int, C.c_int, C.POINTER(C.c_size_t),

@@ -21,7 +21,7 @@ import math
 from .. import _lib as L
 from ..mesh import CartesianMesh
 from ..timestepping import Adaptive, Constant, adaptive
-from ..trimesh import TriangleMesh
+from ..trimesh import DeviceTriangleMesh, TriangleMesh
 
 
 class _CartBackend:
@@ -187,7 +187,7 @@ class HyperbolicSolver:
     def _make_cfg(self, mesh, nsm):
         """The libzb config struct for ``mesh`` (Cartesian or triangle)."""
         order, recon, cd = self._scheme(nsm)
-        if isinstance(mesh, TriangleMesh):
+        if isinstance(mesh, (TriangleMesh, DeviceTriangleMesh)):
             kinds = nsm.model.bc_kinds()
             if "periodic" in kinds:
                 raise NotImplementedError("periodic boundaries on the triangle mesh")
@@ -216,11 +216,11 @@ class HyperbolicSolver:
         self.cfg = self._make_cfg(mesh, nsm)
         dev = torch.device(self.device or "cuda")
         td = self._torch_dtype()
-        if isinstance(mesh, TriangleMesh):
+        if isinstance(mesh, (TriangleMesh, DeviceTriangleMesh)):
             self._mesh_arrays = mesh.device_arrays(
                 td, dev, [L.BC[k] for k in nsm.model.bc_kinds()])
             ms = L.ZbTriMesh()
-            ms.n_cells, ms.n_faces, ms.n_bf = mesh.n_cells, mesh.n_faces, len(mesh.bf)
+            ms.n_cells, ms.n_faces, ms.n_bf = mesh.n_cells, mesh.n_faces, mesh.n_bf
             for name in L.TRI_MESH_FIELDS:
                 setattr(ms, name, self._mesh_arrays[name].data_ptr())
             self._mesh_struct = ms

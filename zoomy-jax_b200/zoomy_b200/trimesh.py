@@ -68,6 +68,10 @@ class TriangleMesh:
     def n_faces(self):
         return self.face_cells.shape[1]
 
+    @property
+    def n_bf(self):
+        return len(self.bf)
+
     def cell_centers(self):
         return self.cell_center.T.copy()
 
@@ -77,20 +81,8 @@ class TriangleMesh:
         """Delaunay triangulation of an ``n_side x n_side`` lattice with
         interior points jittered by U[-jitter, jitter] spacings (seeded);
         about ``2 n_side^2`` triangles."""
-        from scipy.spatial import Delaunay
-        rng = np.random.default_rng(seed)
-        x0, x1, y0, y1 = domain
-        hx, hy = (x1 - x0) / (n_side - 1), (y1 - y0) / (n_side - 1)
-        gx, gy = np.meshgrid(np.linspace(x0, x1, n_side), np.linspace(y0, y1, n_side),
-                             indexing="ij")
-        P = np.stack([gx.reshape(-1), gy.reshape(-1)], axis=1)
-        jit = rng.uniform(-jitter, jitter, size=P.shape) * np.array([hx, hy])
-        jit[np.isclose(P[:, 0], x0) | np.isclose(P[:, 0], x1), 0] = 0.0
-        jit[np.isclose(P[:, 1], y0) | np.isclose(P[:, 1], y1), 1] = 0.0
-        P = P + jit
-        T = Delaunay(P).simplices.astype(np.int64)
-        cen = P[T].mean(axis=1)
-        return TriangleMesh.from_points(P, T[_morton(cen)])
+        P, T = lattice_triangulation(n_side, jitter, seed, domain)
+        return TriangleMesh.from_points(P, T)
 
     @staticmethod
     def from_points(P, T):
@@ -198,6 +190,154 @@ class TriangleMesh:
             "bf_kind": i32(kinds), "bf_nx": fl(self.face_normal[0, self.bf]),
             "bf_ny": fl(self.face_normal[1, self.bf]),
         }
+
+
+def lattice_triangulation(n_side, jitter=0.3, seed=0, domain=(0.0, 1.0, 0.0, 1.0)):
+    """Vertices and Morton-ordered triangles of the Delaunay triangulation of
+    an ``n_side x n_side`` lattice with interior points jittered by
+    U[-jitter, jitter] spacings (seeded) -- the mesh generation that
+    :meth:`TriangleMesh.create` and :meth:`DeviceTriangleMesh.create` share."""
+    from scipy.spatial import Delaunay
+    rng = np.random.default_rng(seed)
+    x0, x1, y0, y1 = domain
+    hx, hy = (x1 - x0) / (n_side - 1), (y1 - y0) / (n_side - 1)
+    gx, gy = np.meshgrid(np.linspace(x0, x1, n_side), np.linspace(y0, y1, n_side),
+                         indexing="ij")
+    P = np.stack([gx.reshape(-1), gy.reshape(-1)], axis=1)
+    jit = rng.uniform(-jitter, jitter, size=P.shape) * np.array([hx, hy])
+    jit[np.isclose(P[:, 0], x0) | np.isclose(P[:, 0], x1), 0] = 0.0
+    jit[np.isclose(P[:, 1], y0) | np.isclose(P[:, 1], y1), 1] = 0.0
+    P = P + jit
+    T = Delaunay(P).simplices.astype(np.int64)
+    cen = P[T].mean(axis=1)
+    return P, T[_morton(cen)]
+
+
+class DeviceTriangleMesh:
+    """Triangle mesh whose faces, geometry and least-squares stencils are
+    prepared on the GPU (``zb_trimesh_match`` / ``zb_trimesh_fill``) from
+    vertices and triangles: the host conversion of zoomy_core's ``LSQMesh``
+    into ``MeshJAX`` arrays (``zoomy_jax/mesh/mesh.py:123-264``) and
+    ``prepare_mesh``'s index sets (``zoomy_jax/fvm/solver2/context.py:99-163``)
+    as device kernels.  The solver sees the interface of
+    :class:`TriangleMesh` (``n_cells``, ``n_faces``, ``n_bf``,
+    ``cell_centers()``, ``cell_inradius``, ``device_arrays()``); faces are
+    numbered by (owner cell, local edge), the owner of a shared edge being
+    the lower cell index, so face-indexed arrays differ from the host
+    builder's by that renumbering only."""
+
+    dimension = 2
+
+    def __init__(self, P, T, device="cuda"):
+        import ctypes as C
+        import torch
+        from . import _lib as L
+        L.require_cuda()
+        self.lib = L.load()
+        self.vertices = np.ascontiguousarray(P, dtype=np.float64)
+        self.triangles = np.ascontiguousarray(T, dtype=np.int32)
+        if self.vertices.ndim != 2 or self.vertices.shape[1] != 2:
+            raise ValueError("vertices must be (n, 2)")
+        if self.triangles.ndim != 2 or self.triangles.shape[1] != 3:
+            raise ValueError("triangles must be (C, 3)")
+        dev = torch.device(device)
+        self._P = torch.as_tensor(self.vertices, device=dev)
+        self._T = torch.as_tensor(self.triangles, device=dev)
+        n = len(self.triangles)
+        nb = self.lib.zb_trimesh_scratch_bytes(n)
+        if nb == 0:
+            raise L.ZbError("too many triangles for int32 half-edge numbers")
+        self._scratch = torch.empty(nb, dtype=torch.uint8, device=dev)
+        self._scratch_bytes = nb
+        nf, nbf = C.c_int32(0), C.c_int32(0)
+        L.check(self.lib.zb_trimesh_match(L.ptr(self._P), len(self.vertices), L.ptr(self._T),
+                                          n, L.ptr(self._scratch), C.c_size_t(nb),
+                                          C.byref(nf), C.byref(nbf), L.stream_ptr()),
+                "zb_trimesh_match")
+        self.n_faces, self.n_bf = nf.value, nbf.value
+        self._geo = None
+        self._arrays = {}
+
+    @staticmethod
+    def create(n_side, jitter=0.3, seed=0, domain=(0.0, 1.0, 0.0, 1.0), device="cuda"):
+        """The lattice triangulation of :meth:`TriangleMesh.create`, prepared
+        on the GPU."""
+        P, T = lattice_triangulation(n_side, jitter, seed, domain)
+        return DeviceTriangleMesh(P, T, device)
+
+    @property
+    def n_cells(self):
+        return len(self.triangles)
+
+    n_inner_cells = n_cells
+
+    def _host_geometry(self):
+        # centroid (vertex order after the counter-clockwise flip, as the
+        # device kernels and TriangleMesh.from_points take it) and inradius
+        if self._geo is None:
+            P, T = self.vertices, self.triangles.astype(np.int64)
+            a, b, c = P[T[:, 0]], P[T[:, 1]], P[T[:, 2]]
+            cross = (b[:, 0] - a[:, 0]) * (c[:, 1] - a[:, 1]) - (b[:, 1] - a[:, 1]) * (c[:, 0] - a[:, 0])
+            flip = cross < 0
+            b2 = np.where(flip[:, None], c, b)
+            c2 = np.where(flip[:, None], b, c)
+            area = 0.5 * np.abs(cross)
+            per = (np.hypot(*(b2 - a).T) + np.hypot(*(c2 - b2).T) + np.hypot(*(a - c2).T))
+            self._geo = ((a + b2 + c2) / 3.0, area, 2.0 * area / per)
+        return self._geo
+
+    @property
+    def cell_center(self):
+        return self._host_geometry()[0]
+
+    @property
+    def cell_area(self):
+        return self._host_geometry()[1]
+
+    @property
+    def cell_inradius(self):
+        return self._host_geometry()[2]
+
+    def cell_centers(self):
+        return self.cell_center.T.copy()
+
+    def device_arrays(self, dtype, device, bc_kinds):
+        """Allocate the SoA device arrays the kernels read and fill them on the
+        GPU; ``bc_kinds`` = kind codes of the left, right, bottom and top
+        sides.  Returns a dict of torch tensors (the keys of
+        :meth:`TriangleMesh.device_arrays`)."""
+        import ctypes as C
+        import torch
+        from . import _lib as L
+        dev = torch.device(device)
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError("dtype must be torch.float32 or torch.float64")
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        key = (dtype, str(dev), tuple(int(k) for k in bc_kinds))
+        if key in self._arrays:
+            return self._arrays[key]
+        n, F, nbf = self.n_cells, self.n_faces, self.n_bf
+        i32 = lambda *sh: torch.empty(sh, dtype=torch.int32, device=dev)  # noqa: E731
+        fl = lambda *sh: torch.empty(sh, dtype=dtype, device=dev)  # noqa: E731
+        d = {"lsq_idx": i32(3, n), "lsq_wx": fl(3, n), "lsq_wy": fl(3, n),
+             "cf_rx": fl(3, n), "cf_ry": fl(3, n), "cell_face": i32(3, n),
+             "cell_inv_area": fl(n), "face_a": i32(F), "face_b": i32(F), "face_nx": fl(F),
+             "face_ny": fl(F), "face_len": fl(F), "face_rax": fl(F), "face_ray": fl(F),
+             "face_rbx": fl(F), "face_rby": fl(F),
+             "face_inr": torch.empty(F, dtype=torch.float64, device=dev),
+             "bf_kind": i32(max(nbf, 1)), "bf_nx": fl(max(nbf, 1)), "bf_ny": fl(max(nbf, 1))}
+        ms = L.ZbTriMesh()
+        ms.n_cells, ms.n_faces, ms.n_bf = n, F, nbf
+        for name in L.TRI_MESH_FIELDS:
+            setattr(ms, name, d[name].data_ptr())
+        kinds = (C.c_int32 * 4)(*[int(k) for k in bc_kinds])
+        code = L.ZB_F32 if dtype == torch.float32 else L.ZB_F64
+        L.check(self.lib.zb_trimesh_fill(L.ptr(self._P), n, kinds, code, L.ptr(self._scratch),
+                                         C.c_size_t(self._scratch_bytes), C.byref(ms),
+                                         L.stream_ptr()), "zb_trimesh_fill")
+        self._arrays[key] = d
+        return d
 
 
 def create_tri(n_side, jitter=0.3, seed=0, domain=(0.0, 1.0, 0.0, 1.0)):
