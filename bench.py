@@ -432,7 +432,7 @@ def run_chorin(local_rank, n=1024, steps=10, warmup=3, train_steps=2000, use_gra
     return out
 
 
-def run_triangles(local_rank, n_side=1415, steps=500, warmup=3):
+def run_triangles(local_rank, n_side=1415, steps=500, warmup=3, host_prep=True):
     """The unstructured configuration: a Delaunay triangulation of seeded
     jittered points (about 2 n_side^2 = 4.0M triangles, int32 connectivity),
     eta least-squares MUSCL with the Barth-Jespersen limiter, HR-HLL,
@@ -460,12 +460,14 @@ def run_triangles(local_rank, n_side=1415, steps=500, warmup=3):
     mesh.device_arrays(torch.float32, dev, kinds)
     torch.cuda.synchronize(dev)
     t_prep_gpu = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    hm = TriangleMesh.from_points(P, T)
-    hm.device_arrays(torch.float32, dev, kinds)
-    torch.cuda.synchronize(dev)
-    t_prep_host = time.perf_counter() - t0
-    del hm
+    t_prep_host = None
+    if host_prep:
+        t0 = time.perf_counter()
+        hm = TriangleMesh.from_points(P, T)
+        hm.device_arrays(torch.float32, dev, kinds)
+        torch.cuda.synchronize(dev)
+        t_prep_host = time.perf_counter() - t0
+        del hm
     state = grf_dam_state(mesh.cell_centers(), seed=0)
     model = zb.ShallowWater2D(manning_n=0.03, boundary_conditions={t: "wall" for t in
                                                                   ("left", "right", "bottom",
@@ -507,7 +509,7 @@ def run_triangles(local_rank, n_side=1415, steps=500, warmup=3):
             "dry_fraction_initial": float((state[1] <= 0).mean()),
             "mesh_generation_s": round(t_gen, 1),
             "mesh_prep": {"gpu_ms": round(t_prep_gpu * 1e3, 2),
-                          "host_s": round(t_prep_host, 2),
+                          "host_s": None if t_prep_host is None else round(t_prep_host, 2),
                           "how": ("DeviceTriangleMesh (zb_trimesh_match + zb_trimesh_fill, "
                                   "wall clock incl. one synchronisation) vs TriangleMesh."
                                   "from_points + device_arrays (NumPy, upload included)")}}
@@ -562,6 +564,9 @@ def main():
                     help="comma-separated legs to run (profiling runs pick one)")
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--chorin-steps", type=int, default=10)
+    ap.add_argument("--tri-steps", type=int, default=500)
+    ap.add_argument("--tri-host-prep", type=int, default=1,
+                    help="also time the host mesh builder in the triangles leg (0: skip)")
     ap.add_argument("--chorin-no-graph", action="store_true",
                     help="drive the pressure iterations from the host (for profilers, which "
                          "do not list kernels inside conditional graph nodes)")
@@ -619,7 +624,8 @@ def main():
         if "ensemble" in legs:
             line["ensemble"] = run_ensemble(local_rank)
         if "triangles" in legs:
-            line["triangles"] = run_triangles(local_rank)
+            line["triangles"] = run_triangles(local_rank, steps=args.tri_steps,
+                                              host_prep=bool(args.tri_host_prep))
         print(json.dumps(line), flush=True)
         return
     if world > 1:
@@ -643,7 +649,8 @@ def main():
         if "ensemble" in legs:
             extra["ensemble"] = run_ensemble(local_rank)
         if "triangles" in legs:
-            extra["triangles"] = run_triangles(local_rank)
+            extra["triangles"] = run_triangles(local_rank, steps=args.tri_steps,
+                                               host_prep=bool(args.tri_host_prep))
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["ms_per_step"], "higher_is_better": True,

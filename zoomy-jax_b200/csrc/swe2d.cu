@@ -1845,18 +1845,28 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   // for strips
   const int sgrid_e = sms_cache[dev] * (sizeof(T) == 4 ? 4 : 2);
   const int sgrid_i = sgrid_e;
+  // the boundary items on the library's second stream, beside the interior ones
+  SideStream* side = nullptr;
+  {
+    const int rc = side_stream(&side);
+    if (rc) return rc;
+  }
+  ZB_CUDA_TRY(cudaEventRecord(side->fork, st));
+  ZB_CUDA_TRY(cudaStreamWaitEvent(side->s, side->fork, 0));
   if (part == 0) {
-    ens_strip_kernel<T, MODE_STEP1, true><<<sgrid_e, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
-                                                                       (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP1, true><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+        desc, items, (T*)Q, (T*)W, ctrls, phase);
     ens_strip_kernel<T, MODE_STEP1, false><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
                                                                         (T*)W, ctrls, phase);
   } else {
-    ens_strip_kernel<T, MODE_STEP2, true><<<sgrid_e, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
-                                                                       (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP2, true><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+        desc, items, (T*)Q, (T*)W, ctrls, phase);
     ens_strip_kernel<T, MODE_STEP2, false><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
                                                                         (T*)W, ctrls, phase);
   }
   ZB_CUDA_TRY(cudaGetLastError());
+  ZB_CUDA_TRY(cudaEventRecord(side->join, side->s));
+  ZB_CUDA_TRY(cudaStreamWaitEvent(st, side->join, 0));
   static unsigned mask1 = 0u, mask2 = 0u;
   auto k1 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>;
   auto k2 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>;
