@@ -742,6 +742,86 @@ __device__ __forceinline__ T shd(T v) { return __shfl_down_sync(0xffffffffu, v, 
 template <typename T>
 __device__ __forceinline__ T shu(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 
+// float2 arithmetic on the sm_100 paired-FP32 instructions (one issue slot for
+// two lanes of the same operation)
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {   // a - b, one rounding
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// The x-face (rows r-2 | r-1) and the y-face (row r-2, this lane | next lane)
+// of an interior strip row evaluated together as the two lanes of float2
+// arithmetic: eta traces, the Audusse hydrostatic reconstruction, HLL with
+// Davis speeds, the fluctuations and the cell-edge bed terms of riemann() and
+// strip_trace() for ZB_RECON_ETA / ZB_RIEMANN_HLL_HR in float32.  Lane x is
+// the x-face (normal velocity u, transverse v), lane y the y-face (normal v,
+// transverse u).  Square roots, divisions and min / max stay per lane.
+// Outputs as the scalar path names them: x-face Fh, Fy, fxl_n, fxr_n; y-face
+// Gh, Gx, fyl_t, fyr_own.
+__device__ __forceinline__ void faces_pair(const RowW<float>& R0, const RowW<float>& R1,
+                                           const float* slA, const float* slB,
+                                           const SweParams<float>& p, float& Fh, float& Fy,
+                                           float& fxl_n, float& fxr_n, float& Gh, float& Gx,
+                                           float& fyl_t, float& fyr_own) {
+  const float g = p.g, hg = 0.5f * g;
+  // the next lane's row r-2: the y-face's upper side
+  const float nb_b = shd(R0.b), nb_w1 = shd(R0.w1), nb_w2 = shd(R0.w2), nb_w3 = shd(R0.w3);
+  const float nb_h = shd(R0.h);
+  const float sn4 = shd(slA[4]), sn5 = shd(slA[5]), sn6 = shd(slA[6]), sn7 = shd(slA[7]);
+  const float2 o1 = f2(p.half_dx, p.half_dy), o2 = f2(-p.half_dx, -p.half_dy);
+  // side 1: row r-2 towards +x (x-face) and towards +y (y-face)
+  const float2 b1 = fma2(f2(slA[0], slA[4]), o1, f2(R0.b, R0.b));
+  const float2 e1 = fma2(f2(slA[1], slA[5]), o1, f2(R0.w1, R0.w1));
+  const float2 un1 = fma2(f2(slA[2], slA[7]), o1, f2(R0.w2, R0.w3));
+  const float2 ut1 = fma2(f2(slA[3], slA[6]), o1, f2(R0.w3, R0.w2));
+  const float2 h1 = sub2(f2(fmaxf(e1.x, b1.x), fmaxf(e1.y, b1.y)), b1);   // Audusse clip
+  // side 2: row r-1 towards -x and the next lane's row r-2 towards -y
+  const float2 b2 = fma2(f2(slB[0], sn4), o2, f2(R1.b, nb_b));
+  const float2 e2 = fma2(f2(slB[1], sn5), o2, f2(R1.w1, nb_w1));
+  const float2 un2 = fma2(f2(slB[2], sn7), o2, f2(R1.w2, nb_w3));
+  const float2 ut2 = fma2(f2(slB[3], sn6), o2, f2(R1.w3, nb_w2));
+  const float2 h2 = sub2(f2(fmaxf(e2.x, b2.x), fmaxf(e2.y, b2.y)), b2);
+  // hydrostatic reconstruction
+  const float2 bs = f2(fmaxf(b1.x, b2.x), fmaxf(b1.y, b2.y));
+  const float2 t1 = sub2(add2(h1, b1), bs), t2 = sub2(add2(h2, b2), bs);
+  const float2 hL = f2(fmaxf(0.f, t1.x), fmaxf(0.f, t1.y));
+  const float2 hR = f2(fmaxf(0.f, t2.x), fmaxf(0.f, t2.y));
+  const float2 gg = f2(g, g), hg2 = f2(hg, hg), m1 = f2(-1.f, -1.f);
+  const float2 ghL = mul2(gg, hL), ghR = mul2(gg, hR);
+  const float2 cL = f2(sqrtf(ghL.x), sqrtf(ghL.y)), cR = f2(sqrtf(ghR.x), sqrtf(ghR.y));
+  const float2 FLh = mul2(hL, un1), FRh = mul2(hR, un2);      // normal discharges
+  const float2 qLt = mul2(hL, ut1), qRt = mul2(hR, ut2);      // transverse discharges
+  const float2 FLn = fma2(FLh, un1, mul2(hg2, mul2(hL, hL)));
+  const float2 FRn = fma2(FRh, un2, mul2(hg2, mul2(hR, hR)));
+  const float2 FLt = mul2(qLt, un1), FRt = mul2(qRt, un2);
+  // Davis speeds clipped at zero and the HLL combination
+  const float2 sL1 = sub2(un1, cL), sL2 = sub2(un2, cR), sR1 = add2(un1, cL), sR2 = add2(un2, cR);
+  const float2 sl = f2(fmn3(sL1.x, sL2.x, 0.f), fmn3(sL1.y, sL2.y, 0.f));
+  const float2 sr = f2(fmx3(sR1.x, sR2.x, 0.f), fmx3(sR1.y, sR2.y, 0.f));
+  const float2 den = sub2(sr, sl);
+  const float2 inv = f2(den.x > 0.f ? __fdividef(1.f, den.x) : 0.f,
+                        den.y > 0.f ? __fdividef(1.f, den.y) : 0.f);
+  const float2 slsr = mul2(sl, sr), nsl = mul2(sl, m1);
+  auto hll = [&](float2 FL, float2 FR, float2 d) {
+    return mul2(fma2(slsr, d, fma2(nsl, FR, mul2(sr, FL))), inv);
+  };
+  const float2 Fh2 = hll(FLh, FRh, sub2(hR, hL));
+  const float2 Fn2 = hll(FLn, FRn, sub2(FRh, FLh));
+  const float2 Ft2 = hll(FLt, FRt, sub2(qRt, qLt));
+  // fluctuations of the reconstruction and the cell-edge bed terms
+  const float2 Dm2 = mul2(hg2, fma2(mul2(hL, m1), hL, mul2(h1, h1)));
+  const float2 Dp2 = mul2(f2(-hg, -hg), fma2(mul2(hR, m1), hR, mul2(h2, h2)));
+  const float2 ces1 = mul2(mul2(hg2, add2(f2(R0.h, R0.h), h1)), sub2(b1, f2(R0.b, R0.b)));
+  const float2 ces2 = mul2(mul2(f2(-hg, -hg), add2(f2(R1.h, nb_h), h2)), sub2(b2, f2(R1.b, nb_b)));
+  const float2 fl = add2(add2(Fn2, Dm2), ces1);
+  const float2 fr = add2(sub2(Dp2, Fn2), ces2);
+  Fh = Fh2.x; Fy = Ft2.x; fxl_n = fl.x; fxr_n = fr.x;
+  Gh = Fh2.y; Gx = Ft2.y; fyl_t = fl.y; fyr_own = fr.y;
+}
+
 // One warp's work item: strip `strip` (28 output columns) over the output rows
 // [r0, r1) of the strip region p.fast_*.  EDGE items touch the
 // grid's boundary (full-coverage mode, wall / extrapolation sides only): rows
@@ -786,6 +866,10 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   const T dt = T(dtd);
   const T g = p.g, half = T(0.5);
   const bool out_lane = lane >= 2 && lane < 2 + SW && (!EDGE || cj < ny);
+  // float32 interior rows of the eta / HLL-HR scheme evaluate their two faces
+  // as paired float32 arithmetic (faces_pair)
+  constexpr bool PAIR = std::is_same<T, float>::value && RECON == ZB_RECON_ETA &&
+                        RIEMANN == ZB_RIEMANN_HLL_HR && !EDGE;
 
   RowW<T> R0, R1, R2;                 // rows r-2, r-1, r
   T Sx0[4], Sx1[4], Sx2[4];           // (W(j-1) + W(j)) + W(j+1) of those rows
@@ -962,9 +1046,16 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
     }
     if (s < 3) continue;
     // x-face between rows r-2 (A, lower) and r-1 (B, upper)
-    T Fh, Fx, Fy, Dm, Dp;
-    T fxl_n;
+    T Fh, Fy, fxl_n, fxr_n, Gh, Gx, fyl_t, fyr_own;
     {
+      if constexpr (PAIR) {
+        faces_pair(R0, R1, slA, slB, p, Fh, Fy, fxl_n, fxr_n, Gh, Gx, fyl_t, fyr_own);
+        if (s == 3) {          // face r0 - 1/2: only the next row needs it
+          fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
+          continue;
+        }
+      } else {
+      T Fx, Dm, Dp;
       Side<T> A, B;
       strip_trace<T, RECON>(R0, slA, p.half_dx, A);
       strip_trace<T, RECON>(R1, slB, -p.half_dx, B);
@@ -988,7 +1079,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       const T cesA = half * g * (R0.h + A.h) * (A.b - R0.b);
       const T cesB = -(half * g * (R1.h + B.h) * (B.b - R1.b));
       fxl_n = Fx + Dm + cesA;
-      T fxr_n = -Fx + Dp + cesB;
+      fxr_n = -Fx + Dp + cesB;
       if (xb) {
         const T own_n = Fx + Dm * sgx + (xlo ? -cesB : cesA) * sgx;
         if (xlo) {
@@ -1003,7 +1094,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       }
       // y-faces of row r-2: this lane's top face, the lower lane's one below
       Side<T> C, D;
-      T Gh, Gx, Gy, Em, Ep;
+      T Gy, Em, Ep;
       RowW<T> nb;
       nb.b = shd(R0.b); nb.w1 = shd(R0.w1); nb.w2 = shd(R0.w2); nb.w3 = shd(R0.w3);
       nb.h = shd(R0.h); nb.hinv = shd(R0.hinv);
@@ -1031,8 +1122,8 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       riemann<T, RIEMANN, 1>(YL, YR, sgy, g, Gh, Gx, Gy, Em, Ep);
       const T cesC = half * g * (R0.h + C.h) * (C.b - R0.b);
       const T cesD = -(half * g * (nb.h + D.h) * (D.b - nb.b));
-      T fyl_t = Gy + Em + cesC;
-      T fyr_own = -Gy + Ep + cesD;
+      fyl_t = Gy + Em + cesC;
+      fyr_own = -Gy + Ep + cesD;
       if (yb) {
         const T own_n = Gy + Em * sgy + (ylo ? -cesD : cesC) * sgy;
         if (ylo) {
@@ -1040,6 +1131,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
         } else {
           fyl_t = own_n; fyr_own = T(0);
         }
+      }
       }
       const T fyh_b = shu(Gh), fyt_b = shu(Gx), fyr_b = shu(fyr_own);
       // update of row r-2
@@ -1154,9 +1246,10 @@ __host__ __device__ inline bool full_item_edge(int nx, int ny, int strip, int r0
 // takes the frame); KIND 1: the EDGE items of a full-coverage list; KIND 2:
 // its interior items.  Kinds 1 and 2 are separate launches (they run side by
 // side on two streams) so that the EDGE body never raises the interior body's
-// register allocation.
+// register allocation.  float32: 4 CTAs of 4 warps per SM (128 registers; the
+// paired-face interior body spills at 96).
 template <typename T, int RECON, int RIEMANN, int MODE, int KIND>
-__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? (KIND == 1 ? 4 : 5) : 2)
+__global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
 swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
                    const T* __restrict__ qxP, const T* __restrict__ qyP,
                    const T* __restrict__ h0P, const T* __restrict__ qx0P,
