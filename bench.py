@@ -517,8 +517,10 @@ def run_triangles(local_rank, n_side=1415, steps=500, warmup=3, host_prep=True):
 
 def run_ensemble(local_rank, steps=2000):
     """The batched configuration: 512 uneven SWE instances (sides log-uniform
-    in [64, 512]) advanced together by one persistent launch per stage,
-    autotuned tile height, replayed from a CUDA graph of 30 steps."""
+    in [64, 512]) advanced together: per stage a persistent launch over every
+    instance's boundary strip items beside one over the interior items (the
+    tile fallback for grids narrower than four cells, unused here, keeps its
+    autotuned height), replayed from a CUDA graph of 30 steps."""
     import torch
     from zoomy_b200.ensemble import Ensemble
     from zoomy_b200.workloads import ensemble_512, ensemble_state
