@@ -111,7 +111,9 @@ size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg);
 
 /* Initialise the control block for a march starting at time t0 from state Q:
  * clears status and all slots, sets t[phase] = t0 and amax[phase] = the
- * maximum wave speed of Q.
+ * maximum wave speed of Q.  Also creates, once per device, the library's
+ * second stream that the fused step forks its boundary-strip launch onto
+ * (call it outside stream capture; the steps themselves capture).
  * Replaces the first dt_pass (zoomy_jax/fvm/solver2/blocks.py:36-61). */
 int zb_swe2d_init(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl,
                   int phase, double t0, zb_stream_t stream);
@@ -234,7 +236,8 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
                    int* n_items_out);
 
 /* Reset the n_inst control blocks ctrls[0..n_inst) and seed each instance's
- * wave-speed maximum from its state (zb_swe2d_init per instance). */
+ * wave-speed maximum from its state (zb_swe2d_init per instance; it also
+ * creates the second stream, outside stream capture). */
 int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst,
                 const void* Q, zb_ctrl* ctrls, int phase, double t0,
                 zb_stream_t stream);

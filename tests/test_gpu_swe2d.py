@@ -166,6 +166,31 @@ def test_strip_kernel_matches_tiles(cfg, dtype):
         assert rel_err(Q.cpu().numpy(), ref).max() <= 1e-12
 
 
+def test_fused_steps_replay_from_a_cuda_graph():
+    """Three fused steps captured into a CUDA graph -- each stage forks its
+    boundary-strip launch onto the library's second stream and joins it back
+    -- replay to the bits of the same steps launched eagerly."""
+    domain = (0.0, 1.5, 0.0, 1.0)
+    nx, ny = 150, 100
+    Q0 = moving_dam(nx, ny, domain)
+    solver, Q, Qaux, *_ = make(nx, ny, domain, Q0, dtype="float32", oracle=False, order=2,
+                               recon="eta", riemann="hll_hr", bc="wall", eps_wet=1e-6)
+    Qe = Q.clone()
+    solver.init_march(Qe)
+    solver.launch_steps(Qe, 3)
+    torch.cuda.synchronize()
+    Qg = Q.clone()
+    solver.init_march(Qg)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        solver.launch_steps(Qg, 3)
+    g.replay()
+    torch.cuda.synchronize()
+    assert solver.read_ctrl().status == 0
+    assert torch.equal(Qg, Qe)
+
+
 @pytest.mark.parametrize("nx,ny", [(4, 4), (5, 33), (37, 61), (70, 29), (130, 57), (67, 58)])
 def test_full_coverage_strips_on_ragged_grids(nx, ny):
     """Full-coverage strip lists on grids whose sides are not multiples of the

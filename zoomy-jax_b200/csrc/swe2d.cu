@@ -1,8 +1,8 @@
 // Cartesian 2-D shallow-water finite-volume step for sm_100a.
 //
-// One kernel launch = one explicit stage of zoomy_jax's flux operator fused
-// with the Shu-Osher update (zoomy_jax/fvm/solver_jax.py:722-895 and
-// 990-1074; zoomy_jax/fvm/solver2/blocks.py:129-287, march.py:126-157):
+// One stage = one explicit stage of zoomy_jax's flux operator fused with the
+// Shu-Osher update (zoomy_jax/fvm/solver_jax.py:722-895 and 990-1074;
+// zoomy_jax/fvm/solver2/blocks.py:129-287, march.py:126-157):
 //
 //   halo load -> W = (b, eta, u, v) or (b, h, qx, qy) -> LSQ gradient (3x3
 //   least-squares stencil, boundary ghosts) -> neighbour bounds -> limiter ->
@@ -11,12 +11,16 @@
 //   divergence + cell-edge bed source -> Q_out = a Q0 + (1 - a)(Qk + b dt L).
 //
 // Data layout: SoA planes (the reference's (n_state, n_cells) layout), cell
-// (i, j) at i*ny + j.  A CTA owns a TX x 32 tile (32 cells along the
+// (i, j) at i*ny + j.  Two kernels implement a stage.  The tile kernel
+// (swe2d_stage_kernel): a CTA owns a TX x 32 tile (32 cells along the
 // contiguous y axis = one warp-wide coalesced row) and stages the tile plus a
 // 2-cell halo in shared memory; every face of the tile is evaluated exactly
-// once.  The final stage also folds in Manning friction, the troubled-cell
-// flag and the float64 maximum wave speed that sets the next dt, so a step is
-// two launches (SSP-RK2) with no host synchronisation.
+// once -- the generic stage API, first order, and the frame of grids with a
+// periodic side.  The strip kernel (swe2d_strip_kernel): one warp marches a
+// 32-column strip down its rows in registers -- the fused step (interior and
+// boundary launches side by side).  The final stage also folds in Manning
+// friction, the troubled-cell flag and the float64 maximum wave speed that
+// sets the next dt, so a step queues with no host synchronisation.
 #include <cstdio>
 #include <cstring>
 #include <cmath>
@@ -56,9 +60,9 @@ struct SweParams {
   double dt_stage;          // generic stage: dt (< 0: read ctrl->dt)
   T inv6dx, inv6dy;         // interior least-squares gradient factors
   T inv4dx, inv4dy;         // 1 / (4 dx), 1 / (4 dy): side-class closed forms
-  // output region of the interior strip kernel ([fast_i0, fast_i1) x
-  // [fast_j0, fast_j1), empty when fast_i0 >= fast_i1); the tile kernel
-  // leaves these cells alone
+  // output region of the strip kernel ([fast_i0, fast_i1) x [fast_j0,
+  // fast_j1), empty when fast_i0 >= fast_i1); the tile kernel leaves these
+  // cells alone
   int fast_i0, fast_i1, fast_j0, fast_j1;
   // 1: the strip region is the whole grid (fast_i0 = fast_j0 = 0; the strips
   // reach the boundary and keep the control block; no tile launch)
@@ -693,18 +697,16 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
 }
 
 
-// ── the interior strip kernel ──────────────────────────────────────────────
-// The same stage arithmetic as stage_tile for cells at least two cells from
-// every boundary (there the boundary conditions, ghosts and boundary
-// least-squares classes never enter), organised for registers instead of
+// ── the strip kernel ───────────────────────────────────────────────────────
+// The stage arithmetic of stage_tile organised for registers instead of
 // shared memory: one warp owns a strip of 32 contiguous columns (28 outputs
-// plus two halo columns on each side) and marches down SX rows.  Each lane
+// plus two halo columns on each side) and marches down its rows.  Each lane
 // keeps a sliding window of three rows of W, the limited slopes of two rows
 // and the last x-face's fluxes in registers; the column neighbours come from
-// warp shuffles.  Every face is still evaluated once and every float
-// expression is the one stage_tile evaluates, so both kernels produce the same
-// bits for a cell.  The tile kernel runs alongside it on the boundary frame and
-// keeps the control-block duties.
+// warp shuffles.  Every face is still evaluated once.  Interior items (every
+// cell two cells from every boundary) take the interior body, which for
+// float64 evaluates stage_tile's float expressions (the same bits); items
+// that reach the boundary take the EDGE body (strip_item below).
 constexpr int SX = 64;          // output rows per work item
 constexpr int SW = 28;          // output columns per strip
 constexpr int STRIP_NT = 128;   // four independent warps per CTA
@@ -2001,6 +2003,12 @@ int zb_swe2d_init(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl, int pha
                   double t0, zb_stream_t stream) {
   if (!valid_cfg(cfg) || !Q || !ctrl || phase < 0 || phase > 2) return ZB_E_ARG;
   cudaStream_t st = (cudaStream_t)stream;
+  {
+    // the second stream of the fused step is created here, outside any capture
+    SideStream* side = nullptr;
+    const int rc = side_stream(&side);
+    if (rc) return rc;
+  }
   swe2d_ctrl_init_kernel<<<1, 32, 0, st>>>(ctrl, phase, t0);
   if (cfg->dtype == ZB_F32) return amax_into<float>(cfg, (const float*)Q, &ctrl->amax[phase], st);
   return amax_into<double>(cfg, (const double*)Q, &ctrl->amax[phase], st);
@@ -2228,6 +2236,11 @@ int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst, const
                 zb_ctrl* ctrls, int phase, double t0, zb_stream_t stream) {
   if (!common || !table || !Q || !ctrls || n_inst < 1 || phase < 0 || phase > 2) return ZB_E_ARG;
   cudaStream_t st = (cudaStream_t)stream;
+  {
+    SideStream* side = nullptr;   // created here, outside any capture
+    const int rc = side_stream(&side);
+    if (rc) return rc;
+  }
   const int grid = std::min(n_inst, 148 * 8);
   if (common->dtype == ZB_F64)
     ens_amax_kernel<double><<<grid, NT, 0, st>>>((const EnsDesc<double>*)table, (const double*)Q,
