@@ -942,6 +942,31 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
     // limited slopes of row r-1
     {
       T phi[4], gxa[4], gya[4];
+      if constexpr (PAIR) {
+        // the x and y components of each variable as the two lanes of
+        // paired float32 arithmetic (gradient, limiter increments, bounds)
+        const bool clipmin = p.limiter != ZB_LIM_NONE && p.limiter != ZB_LIM_VENKATAKRISHNAN;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const float u = R1.w(v);
+          const float tc = (R0.w(v) + R1.w(v)) + R2.w(v);
+          const float tl = shu(tc), tr = shd(tc);
+          const float2 gv = mul2(sub2(f2(Sx2[v], tr), f2(Sx0[v], tl)), f2(p.inv6dx, p.inv6dy));
+          const float wp0 = R2.w(v), wm0 = R0.w(v), w0p = Wp1[v], w0m = Wm1[v];
+          const float umax = fmx3(u, wp0, fmx3(wm0, w0p, w0m));
+          const float umin = fmn3(u, wp0, fmn3(wm0, w0p, w0m));
+          const float2 dd = sub2(f2(umax, umin), f2(u, u));          // (dpos, dneg)
+          gxa[v] = gv.x;
+          gya[v] = gv.y;
+          if (clipmin) {
+            const float2 ac = mul2(gv, f2(p.half_dx, p.half_dy));
+            phi[v] = phi_clipmin(ac.x, ac.y, dd.x, dd.y);
+          } else {
+            phi[v] = limiter_phi(p.limiter, gv.x, gv.y, p.half_dx, p.half_dy, dd.x, dd.y,
+                                 p.vk_eps2);
+          }
+        }
+      } else {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const T u = R1.w(v);
@@ -956,6 +981,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
         gya[v] = gy;
         phi[v] = limiter_phi(p.limiter, gx, gy, p.half_dx, p.half_dy, umax - u, umin - u,
                              p.vk_eps2);
+      }
       }
       if (EDGE) {
         // row r-1 = m: boundary cells (stage_tile phase B, non-interior
@@ -1042,8 +1068,14 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       for (int v = 0; v < 8; ++v) slA[v] = slB[v];
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        slB[v] = phi[v] * gxa[v];
-        slB[4 + v] = phi[v] * gya[v];
+        if constexpr (PAIR) {
+          const float2 sv = mul2(f2(phi[v], phi[v]), f2(gxa[v], gya[v]));
+          slB[v] = sv.x;
+          slB[4 + v] = sv.y;
+        } else {
+          slB[v] = phi[v] * gxa[v];
+          slB[4 + v] = phi[v] * gya[v];
+        }
       }
     }
     if (s < 3) continue;
