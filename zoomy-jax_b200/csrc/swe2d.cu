@@ -1994,7 +1994,9 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   ZB_CUDA_TRY(cudaGetLastError());
   ZB_CUDA_TRY(cudaEventRecord(side->join, side->s));
   ZB_CUDA_TRY(cudaStreamWaitEvent(st, side->join, 0));
-  static unsigned mask1 = 0u, mask2 = 0u;
+  // the tile fallback (grids narrower than four cells; its CTAs exit at once
+  // when the work list holds no tile items)
+  static unsigned mask1 = 0u;
   auto k1 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>;
   auto k2 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>;
   if (!(mask1 & (1u << dev))) {
@@ -2002,7 +2004,6 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
     ZB_CUDA_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     mask1 |= 1u << dev;
   }
-  (void)mask2;
   if (grid <= 0) {
     int per_sm = 0, sms = 0;
     ZB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1, NT, sm));
