@@ -33,7 +33,7 @@ namespace pois {
 
 constexpr int NT = 256;
 constexpr int MAXL = 16;
-constexpr int SMALL = 16;        // levels with nx, ny <= SMALL go to the one-CTA kernel
+constexpr int SMALL = 32;        // levels with nx, ny <= SMALL go to the one-CTA kernel
 constexpr int RED_BLOCKS = 592;  // 148 SMs x 4
 constexpr int DENSE_MAX_CELLS = 64;   // coarsest levels this small are solved exactly
 
