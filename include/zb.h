@@ -140,10 +140,9 @@ int zb_swe2d_step(const zb_swe2d_cfg* cfg, void* Q, void* workspace,
 
 /* zb_swe2d_step for callers that cannot allocate device memory.  No
  * counterpart in the reference.  Such callers are plugins inside a framework
- * that owns every device byte (an XLA / JAX FFI custom call declared without
- * a scratch operand, an inference-engine plugin at enqueue time) and code
- * running while a stream is captured into a CUDA graph, where a synchronous
- * cudaMalloc is not allowed.  The caller passes Q and ctrl as for
+ * that owns every device byte and hands them only their operands (an XLA /
+ * JAX FFI custom call declared without a scratch operand, an
+ * inference-engine plugin at enqueue time).  The caller passes Q and ctrl as for
  * zb_swe2d_step; the stage-1 scratch is a file-scope device array inside
  * libzb sized for ZB_NOALLOC_MAX_CELLS cells (24 MiB, held on every GPU that
  * loads the library until the process exits).  Larger grids return

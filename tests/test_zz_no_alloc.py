@@ -1,9 +1,9 @@
 """The allocation-free step against the workspace step.
 
 ``zb_swe2d_step_noalloc`` serves callers that cannot allocate device memory
-(a plugin inside a framework that owns all device memory, or code running
-under CUDA-graph stream capture): its stage scratch is a fixed array inside
-libzb instead of a caller workspace.  This file is named to be collected last
+(a plugin inside a framework that owns all device memory and hands it only
+its operands): its stage scratch is a fixed array inside libzb instead of a
+caller workspace.  This file is named to be collected last
 so that a run stopping at the first failure has run every other test; it
 also passes on its own in a fresh process.
 """

@@ -2166,10 +2166,9 @@ int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux, zb_stream_t
 
 // ── allocation-free step ────────────────────────────────────────────────────
 // Some callers cannot call cudaMalloc: a framework that owns every device
-// byte and hands a plugin only its operands (an XLA / JAX FFI custom call
+// byte hands a plugin only its operands (an XLA / JAX FFI custom call
 // declared without a scratch buffer, an inference-engine plugin at enqueue
-// time), or code running while a stream is being captured into a CUDA graph,
-// where a synchronous cudaMalloc is not permitted.  For them the stage-1
+// time), and the plugin has no way to ask for more.  For them the stage-1
 // state of the fused step lives in this file-scope device array instead of a
 // caller workspace: three planes of up to ZB_NOALLOC_MAX_CELLS cells in
 // float64 (float32 uses the first half), 24 MiB plus 256 bytes of padding.
