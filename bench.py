@@ -259,8 +259,10 @@ def run_gpu(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize(dev)
     wall0 = time.perf_counter()
-    with ClockSampler(local_rank, path=str(ROOT / "gpurun_out" / f"clocks_rank{rank}.csv")
-                      if (ROOT / "gpurun_out").exists() else None) as clk:
+    clock_path = None
+    if args.clock_log:
+        clock_path = args.clock_log if world <= 1 else f"{args.clock_log}.rank{rank}"
+    with ClockSampler(local_rank, path=clock_path) as clk:
         for k in range(K):
             flush.zero_()
             ev[k][0].record(stream)
@@ -573,6 +575,9 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--clock-log", default=None,
+                    help="also write the raw nvidia-smi clock samples of the timed region "
+                         "to this CSV (the JSON line always carries their summary)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the Chorin and ensemble legs")
     ap.add_argument("--legs", default="swe,chorin,ensemble,triangles",
