@@ -662,7 +662,9 @@ def main():
     if rank != 0:
         return
     extra = {}
-    if not args.no_extra:
+    # the extra legs are single-GPU configurations: measured at N = 1 only, so
+    # a scaling run holds its N GPUs for the replicated SWE leg alone
+    if not args.no_extra and world == 1:
         if "chorin" in legs:
             extra["chorin"] = run_chorin(local_rank, steps=args.chorin_steps,
                                          train_steps=args.train_steps)
