@@ -106,14 +106,16 @@ class HyperbolicSolver:
     ``dtype`` (``float64`` default, as the reference enables x64, or
     ``float32``), ``eps_wet`` (the emitted dry-cell demotion threshold of the
     eta reconstruction, ``None`` = off) and ``implicit_source`` (point-implicit
-    Manning, the IMEX local solve).
+    Manning, the IMEX local solve); ``output_path`` and ``output_snapshots``
+    (the reference's ``settings.output`` file and snapshot count) for
+    ``run_simulation(write_output=True)``.
     """
 
     def __init__(self, time_end=1.0, compute_dt=None, free_surface_h_index=None,
                  free_surface_b_index=0, free_surface_momentum_indices=None,
                  reconstruction_variables="conservative", positivity_method="",
                  front_theta_tol=None, mood=False, dtype="float64", eps_wet=None,
-                 implicit_source=False, device=None):
+                 implicit_source=False, device=None, output_path=None, output_snapshots=2):
         self.time_end = float(time_end)
         self.compute_dt = compute_dt if compute_dt is not None else adaptive(0.45, 2)
         self.free_surface_h_index = free_surface_h_index
@@ -131,6 +133,8 @@ class HyperbolicSolver:
         self.eps_wet = eps_wet
         self.implicit_source = bool(implicit_source)
         self.device = device
+        self.output_path = output_path
+        self.output_snapshots = int(output_snapshots)
 
     # ── configuration ─────────────────────────────────────────────────────
     def _torch_dtype(self):
@@ -354,7 +358,40 @@ class HyperbolicSolver:
         ``time_end`` a queued step takes dt = 0 and leaves the state unchanged.
         With MOOD the host drives ``compute_timestep`` / ``step`` /
         ``post_step`` per step (the redo decision needs the troubled mask).
-        The state is returned with its aux."""
+        The state is returned with its aux.
+
+        ``write_output``: snapshots to ``output_path`` as the reference writes
+        them -- snapshot 0 before the first step, snapshot ``i`` after the
+        first step whose time reaches ``i * time_end / (output_snapshots -
+        1)``, at most one per step -- through an asynchronous
+        :class:`~zoomy_b200.snapshots.SnapshotWriter` (the march pays a
+        device-to-device copy per snapshot).  Near an output time the
+        device-resident loop queues single steps so that it stops on the same
+        step as the reference."""
+        writer = None
+        if write_output:
+            if self.output_path is None:
+                raise ValueError("write_output needs the solver's output_path")
+            from ..snapshots import SnapshotWriter
+            writer = SnapshotWriter(self.output_path)
+        try:
+            return self._march(Q, Qaux, writer, max_steps)
+        finally:
+            if writer is not None:
+                writer.close()
+
+    def _march(self, Q, Qaux, writer, max_steps):
+        from ..snapshots import snapshot_times
+        stamps = snapshot_times(self.time_end, self.output_snapshots) if writer else []
+        i_snap = 0
+
+        def snap(t, Qs, As=None):
+            nonlocal i_snap
+            writer.save(i_snap, t, Qs, As if As is not None else self.update_qaux(Qs))
+            i_snap += 1
+
+        if writer is not None:
+            snap(0.0, Q, Qaux)
         if self.mood:
             t, n = 0.0, 0
             while t < self.time_end:
@@ -366,6 +403,8 @@ class HyperbolicSolver:
                 Q, Qaux = self.post_step(t + dt, dt, Qn, Q, Qaux)
                 t += dt
                 n += 1
+                if i_snap < len(stamps) and t >= stamps[i_snap]:
+                    snap(t, Q, Qaux)
                 if n >= max_steps:
                     raise FloatingPointError(f"march exceeded max_steps = {max_steps}")
             self.time, self.steps_taken = t, n
@@ -378,11 +417,15 @@ class HyperbolicSolver:
             t = c.t[self._n % 3]
             if c.status & L.ZB_ST_DT_INVALID:
                 self._raise_dt(Q, t)
+            if i_snap < len(stamps) and t >= stamps[i_snap]:
+                snap(t, Q)
             if t >= self.time_end:
                 break
             if self._n >= max_steps:
                 raise FloatingPointError(f"march exceeded max_steps = {max_steps}")
             batch = min(batch * 2, 64)
+            if i_snap < len(stamps) and c.dt > 0.0 and stamps[i_snap] - t <= 4.0 * batch * c.dt:
+                batch = 1
         self.time = t
         self.steps_taken = int(c.steps)
         return Q, self.update_qaux(Q)
