@@ -21,11 +21,13 @@ cannot be installed: it needs jax and zoomy_core, absent here) on the host's
 cores: one process per core, each stepping a 256 x 256 sample of the same
 workload; rank 0 only.
 
-Rank 0 also reports, in the same JSON line, the other configurations:
-"chorin" (1024^2 Chorin steps at a 1e-8 pressure residual, plain multigrid FCG
-against the learned U-Net smoother), "ensemble" (512 uneven instances in one
-persistent launch per stage) and "triangles" (about 4M Delaunay triangles, 500
-steps); --no-extra skips them, --legs picks a subset.
+At N = 1 the same JSON line also reports the other configurations: "chorin"
+(1024^2 Chorin steps at a 1e-8 pressure residual, plain multigrid FCG against
+the learned U-Net smoother), "ensemble" (512 uneven instances, boundary and
+interior strip launches per stage), "triangles" (about 4M Delaunay triangles,
+500 steps, with the GPU mesh preparation) and "snapshots" (the 2048^2 march
+with asynchronous snapshot output); --no-extra skips them, --legs picks a
+subset.
 """
 from __future__ import annotations
 
@@ -530,6 +532,63 @@ def run_triangles(local_rank, n_side=1415, steps=500, warmup=3, host_prep=True):
                                   "from_points + device_arrays (NumPy, upload included)")}}
 
 
+def run_snapshots(local_rank, n=2048, steps=200, snapshots=5):
+    """Snapshot output while marching: the 2048^2 float32 workload, `steps`
+    fused steps queued without host synchronisation, against the same steps
+    with `snapshots` snapshots (state + 7 aux rows each) handed to the
+    asynchronous writer at even intervals; wall clock from the first launch
+    to the last file closed.  Files go to a temporary directory."""
+    import math as _m
+    import tempfile
+    import torch
+    import zoomy_b200 as zb
+    from zoomy_b200.fvm.solver import HyperbolicSolver
+    from zoomy_b200.snapshots import SnapshotWriter
+    dev = torch.device("cuda", local_rank)
+    Q_host = workload_state(n, seed=0)
+    model = zb.ShallowWater2D(wet_dry_eps=1e-6, initial_conditions=Q_host,
+                              boundary_conditions={t: "wall" for t in
+                                                   ("left", "right", "bottom", "top")})
+    nsm = zb.NumericalSystemModel.from_system_model(
+        model, zb.ReconstructionSpec(2, "minmod"), "hll_hr")
+    solver = HyperbolicSolver(time_end=_m.inf, compute_dt=zb.timestepping.adaptive(0.45, 2),
+                              reconstruction_variables="eta", free_surface_h_index=1,
+                              eps_wet=1e-6, dtype="float32", device=f"cuda:{local_rank}")
+    Q, _ = solver.setup_simulation(zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n), nsm)
+    Q0 = Q.clone()
+    every = max(1, steps // snapshots)
+
+    def march(writer):
+        Q.copy_(Q0)
+        solver.init_march(Q)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        k = 0
+        for i in range(steps):
+            solver.launch_steps(Q, 1)
+            if writer is not None and (i + 1) % every == 0 and k < snapshots:
+                writer.save(k, float(i + 1), Q, solver.update_qaux(Q))
+                k += 1
+        if writer is not None:
+            writer.close()
+        torch.cuda.synchronize(dev)
+        return time.perf_counter() - t0
+
+    march(None)                                  # warm-up
+    t_plain = march(None)
+    with tempfile.TemporaryDirectory() as d:
+        t_snap = march(SnapshotWriter(os.path.join(d, "run.h5")))
+    per_snap = 4 * n * n * 4 + 7 * n * n * 4
+    return {"grid": [n, n], "steps": steps, "snapshots": snapshots,
+            "bytes_per_snapshot": per_snap,
+            "march_s": round(t_plain, 4), "march_with_snapshots_s": round(t_snap, 4),
+            "overhead_per_snapshot_ms": round((t_snap - t_plain) / snapshots * 1e3, 2),
+            "how": ("wall clock of the march, steps queued without host synchronisation; "
+                    "snapshots staged device-to-device, copied to a pinned ring on a side "
+                    "stream and written by a writer thread (.npy files: no HDF5 library "
+                    "in the image); includes closing the writer")}
+
+
 def run_ensemble(local_rank, steps=2000):
     """The batched configuration: 512 uneven SWE instances (sides log-uniform
     in [64, 512]) advanced together: per stage a persistent launch over every
@@ -580,7 +639,7 @@ def main():
                          "to this CSV (the JSON line always carries their summary)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the Chorin and ensemble legs")
-    ap.add_argument("--legs", default="swe,chorin,ensemble,triangles",
+    ap.add_argument("--legs", default="swe,chorin,ensemble,triangles,snapshots",
                     help="comma-separated legs to run (profiling runs pick one)")
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--chorin-steps", type=int, default=10)
@@ -646,6 +705,8 @@ def main():
         if "triangles" in legs:
             line["triangles"] = run_triangles(local_rank, steps=args.tri_steps,
                                               host_prep=bool(args.tri_host_prep))
+        if "snapshots" in legs:
+            line["snapshots"] = run_snapshots(local_rank)
         print(json.dumps(line), flush=True)
         return
     if world > 1:
@@ -673,6 +734,8 @@ def main():
         if "triangles" in legs:
             extra["triangles"] = run_triangles(local_rank, steps=args.tri_steps,
                                                host_prep=bool(args.tri_host_prep))
+        if "snapshots" in legs:
+            extra["snapshots"] = run_snapshots(local_rank)
     line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["ms_per_step"], "higher_is_better": True,
