@@ -37,6 +37,7 @@ from zoomy_b200.fvm.chorin import (ChorinSolver, EllipticSolveError,  # noqa: E4
                                    PoissonSolver)
 from zoomy_b200.learned import (LearnedSmoother, PatchSet, SmootherTrainer,  # noqa: E402
                                 solver_training_set)
+from zoomy_b200.fvm.solver import HyperbolicSolver  # noqa: E402
 from zoomy_b200.workloads import cartesian_centers  # noqa: E402
 
 DEV = torch.device("cuda")
@@ -442,3 +443,33 @@ def test_missed_tolerance_raises():
     dt = solver.compute_timestep(Q)
     with pytest.raises(EllipticSolveError, match="did NOT converge"):
         solver.step(dt, 0.0, Q)
+
+
+def test_run_simulation_marches_chorin_cycles():
+    """run_simulation on a ChorinSolver advances through its own step (the
+    Chorin cycle), as the reference's _advance calls self.step: its result is
+    the manual loop of compute_timestep / step / post_step, and it differs
+    from the hyperbolic march alone (the pressure projection acts)."""
+    n = 64
+    solver, Q, _ = _chorin(n)
+    solver.time_end = 3e-3
+    Q0 = Q.clone()
+    Qr, _ = solver.run_simulation(Q.clone(), None)
+    t, Qm = 0.0, Q0.clone()
+    Am = solver.update_qaux(Qm)
+    while t < solver.time_end:
+        dt = solver.compute_timestep(Qm, Am, time=t)
+        Qn = solver.step(dt, t, Qm, Am)
+        Qm, Am = solver.post_step(t + dt, dt, Qn, Qm, Am)
+        t += dt
+    assert torch.equal(Qr, Qm)
+    hyp = HyperbolicSolver(time_end=3e-3, compute_dt=zb.timestepping.adaptive(0.45, 2),
+                           reconstruction_variables="eta", free_surface_h_index=1,
+                           eps_wet=1e-6, dtype="float64")
+    model = zb.ShallowWater2D(boundary_conditions={tg: "wall" for tg in TAGS},
+                              initial_conditions=Q0.cpu().numpy())
+    nsm = zb.NumericalSystemModel.from_system_model(model, zb.ReconstructionSpec(2, "minmod"),
+                                                    "hll_hr")
+    Qh, Ah = hyp.setup_simulation(zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n), nsm)
+    Qh, _ = hyp.run_simulation(Qh, Ah)
+    assert not torch.allclose(Qh, Qr)

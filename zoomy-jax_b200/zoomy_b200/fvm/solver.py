@@ -356,9 +356,11 @@ class HyperbolicSolver:
         Without MOOD the loop is device-resident: fused steps are queued in
         growing batches and the host only polls the control block; after
         ``time_end`` a queued step takes dt = 0 and leaves the state unchanged.
-        With MOOD the host drives ``compute_timestep`` / ``step`` /
-        ``post_step`` per step (the redo decision needs the troubled mask).
-        The state is returned with its aux.
+        With MOOD, or in a subclass that overrides ``step`` (the Chorin
+        projection), the host drives ``compute_timestep`` / ``step`` /
+        ``post_step`` per step as the reference's ``_advance`` does (the MOOD
+        redo decision needs the troubled mask; a subclass's step is not the
+        fused kernel).  The state is returned with its aux.
 
         ``write_output``: snapshots to ``output_path`` as the reference writes
         them -- snapshot 0 before the first step, snapshot ``i`` after the
@@ -392,7 +394,7 @@ class HyperbolicSolver:
 
         if writer is not None:
             snap(0.0, Q, Qaux)
-        if self.mood:
+        if self.mood or type(self).step is not HyperbolicSolver.step:
             t, n = 0.0, 0
             while t < self.time_end:
                 dt = self.compute_timestep(Q, Qaux, time=t)
