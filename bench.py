@@ -98,6 +98,32 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
+def reference_sample_side(total_steps, budget_s=120.0):
+    """Side of the per-core sample that lets `total_steps` oracle steps fit
+    `budget_s`: one 128^2 step is timed here (single-threaded NumPy, as in
+    the workers) and the cost scaled by the cell count; clamped to [32, 256]
+    and rounded to a multiple of 8."""
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ.setdefault(k, "1")
+    sys.path.insert(0, str(ROOT))
+    from oracle import mesh as OM
+    from oracle import swe as OS
+    n0 = 128
+    m = OM.create_2d(0.0, 1.0, 0.0, 1.0, n0, n0)
+    Q = workload_state(n0, 0)
+    params = OS.Params(wet_dry_eps=1e-6)
+    scheme = OS.Scheme(order=2, limiter="minmod", recon="eta", riemann="hll_hr",
+                       eps_wet=1e-6, cfl=0.45,
+                       bc={t: "wall" for t in ("left", "right", "bottom", "top")})
+    kind = OS.bc_kinds(m, scheme)
+    t0 = time.perf_counter()
+    OS.step(m, Q, OS.compute_dt(m, Q, params, scheme), params, scheme, kind)
+    per_cell = (time.perf_counter() - t0) / (n0 * n0)
+    cells = budget_s / max(1, total_steps) / per_cell
+    side = int(math.sqrt(max(cells, 1.0))) // 8 * 8
+    return max(32, min(CPU_SAMPLE_N, side))
+
+
 def run_cpu(warmup, steps, n=CPU_SAMPLE_N, procs=None):
     """All host cores, one oracle process each (spawn context).  Returns
     (cell-updates/s, cores, per-step seconds, sample text)."""
@@ -665,8 +691,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        value, cores, mean_step, sample = run_cpu(max(1, min(args.warmup, 1)),
-                                                  max(1, min(args.steps, 3)))
+        # all W + K steps, each on a per-core sample sized so that the run
+        # ends within about two minutes
+        side = reference_sample_side(args.warmup + args.steps)
+        value, cores, mean_step, sample = run_cpu(args.warmup, args.steps, n=side)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": mean_step * 1e3, "higher_is_better": True,
