@@ -878,7 +878,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   T Wm1[4], Wp1[4], Wm2[4], Wp2[4];   // W(j-1), W(j+1) of rows r-1 and r
   T slA[8], slB[8];                   // [sx0..3, sy0..3] of rows r-2 and r-1
   T fxh_p = T(0), fxt_p = T(0), fxr_p = T(0);
-  double amax_loc = 0.0;
+  T amax_loc = T(0);   // reduced in T; float -> double is exact and monotone
   bool bad = false;
   const int nsteps = (r1 - r0) + 4;
   // row r + 1 is fetched while row r is processed
@@ -1208,13 +1208,16 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       hO[k] = hn;
       qxO[k] = qxn;
       qyO[k] = qyn;
-      bad = bad || (hn < T(0)) || !isfinite(hn) || !isfinite(qxn) || !isfinite(qyn) ||
-            !isfinite(R0.b);
+      // troubled: h < 0 or a non-finite value (one non-finite term makes
+      // the sum's difference with itself NaN; finite states that overflow
+      // the sum, |q| ~ 1e38, would flag too)
+      const T chk = (hn + qxn) + (qyn + R0.b);
+      bad = bad || !(hn >= T(0)) || !(chk - chk == T(0));
       if (MODE == MODE_STEP2) {
         const T hi = kp_hinv(hn, p.eps_kp);
         const T c = sqrt(g * fmx(hn, T(0)));
         const T lx = fabs(qxn * hi) + c, ly = fabs(qyn * hi) + c;
-        amax_loc = nmax(amax_loc, (double)nmax(lx, ly));
+        amax_loc = nmax(amax_loc, nmax(lx, ly));
       }
     }
   }
@@ -1222,7 +1225,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   if (MODE == MODE_STEP2) {
     for (int o = 16; o > 0; o >>= 1)
       amax_loc = nmax(amax_loc, __shfl_xor_sync(0xffffffffu, amax_loc, o));
-    if (lane == 0) atomic_max_pos_double(&ctrl->amax[(phase + 1) % 3], amax_loc);
+    if (lane == 0) atomic_max_pos_double(&ctrl->amax[(phase + 1) % 3], (double)amax_loc);
   }
 }
 
