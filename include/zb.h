@@ -227,9 +227,11 @@ size_t zb_ens_table_bytes(const zb_swe2d_cfg* common,
 /* Build the per-instance parameter blocks (spacing, least-squares weights,
  * Manning, t_end) and the work list, and copy them to the device table
  * (synchronous host-to-device copies: call at set-up, outside stream
- * capture).  The work list holds (instance, tile) items for the cells near
- * each instance's boundary and (instance, strip, row chunk) items for its
- * interior.  *n_items_out receives the work-list length (tiles + strips). */
+ * capture).  The work list holds every instance's (instance, strip, row
+ * chunk) items of the single grid's full-coverage list (interior, boundary-
+ * column and boundary-row bodies), and (instance, tile) items for grids
+ * narrower than four cells.  *n_items_out receives the work-list length
+ * (tiles + strips). */
 int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
                    int n_inst, int tile_x, void* table, size_t table_bytes,
                    int* n_items_out);
@@ -242,10 +244,13 @@ int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst,
                 zb_stream_t stream);
 
 /* One SSP-RK2 step of every instance: part 0 = the first stage, 1 = the
- * second, -1 = both.  Each stage is two persistent kernels: warps walking the
- * interior strip items, then CTAs walking the boundary tiles (grid <= 0 picks
- * SMs x occupancy for the latter).  Each instance takes its own CFL dt
- * (zb_swe2d_step semantics per instance). */
+ * second, -1 = both.  Each stage is four persistent kernels: warps walking the
+ * boundary-column and then the boundary-row strip items on the library's
+ * second stream beside warps walking the interior strip items on `stream`,
+ * then CTAs walking the tiles of grids narrower than four cells (grid <= 0
+ * picks SMs x occupancy for the latter; with no such grid they exit at
+ * once).  Each instance takes its own CFL dt (zb_swe2d_step semantics per
+ * instance). */
 int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst,
                      int n_items, int tile_x, int grid, void* Q, void* W,
                      zb_ctrl* ctrls, int phase, int part, zb_stream_t stream);

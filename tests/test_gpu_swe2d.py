@@ -211,6 +211,29 @@ def test_full_coverage_strips_on_ragged_grids(nx, ny):
     assert rel_err(Q.cpu().numpy(), ref).max() <= 1e-12
 
 
+@pytest.mark.parametrize("bc", ["wall", ("extrapolation", "extrapolation", "wall", "wall")],
+                         ids=["walls", "y-walls"])
+@pytest.mark.parametrize("nx,ny", [(5, 33), (37, 61), (70, 29), (130, 57), (67, 58)])
+def test_float32_column_edge_strips_match_tiles(nx, ny, bc):
+    """In float32 the strips whose lanes reach a y-boundary column march the
+    rows between the boundary rows with the paired-float interior arithmetic
+    and recompute the boundary column's slopes and its boundary y-face with the
+    boundary expressions (walls mirror q_y there).  One fused step against the
+    tile kernel's host-dt step with the same dt, on ragged grids."""
+    domain = (0.0, 1.0, 0.0, 1.0)
+    Q0 = moving_dam(nx, ny, domain)
+    solver, Q, Qaux, *_ = make(nx, ny, domain, Q0, dtype="float32", oracle=False, bc=bc,
+                               eps_wet=1e-6)
+    Qa = Q.clone()
+    solver.init_march(Q)
+    solver.launch_steps(Q, 1)
+    c = solver.read_ctrl()
+    assert c.status == 0
+    ref = solver.step(c.dt, 0.0, Qa, Qaux)
+    err = rel_err(Q.double().cpu().numpy(), ref.double().cpu().numpy())
+    assert err.max() <= 2e-6, err
+
+
 @pytest.mark.parametrize("cfg", CONFIGS[3:7], ids=lambda c: "-".join(str(v) for v in c.values()))
 def test_host_dt_step_matches_oracle(cfg):
     """``step(dt, t, Q, Qaux)`` with a host dt (the reference's call shape)."""

@@ -706,7 +706,9 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
 // warp shuffles.  Every face is still evaluated once.  Interior items (every
 // cell two cells from every boundary) take the interior body, which for
 // float64 evaluates stage_tile's float expressions (the same bits); items
-// that reach the boundary take the EDGE body (strip_item below).
+// that reach the boundary rows take the EDGE body, items whose rows are inside
+// but whose lanes reach a boundary column the column-EDGE body (strip_item
+// below).
 constexpr int SX = 64;          // output rows per work item
 constexpr int SW = 28;          // output columns per strip
 constexpr int STRIP_NT = 128;   // four independent warps per CTA
@@ -763,16 +765,25 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 // transverse u).  Square roots, divisions and min / max stay per lane.
 // Outputs as the scalar path names them: x-face Fh, Fy, fxl_n, fxr_n; y-face
 // Gh, Gx, fyl_t, fyr_own.
+// The next lane's row r-2 (the y-face's upper side): W, h and the y-slopes.
+struct NextRow {
+  float b, w1, w2, w3, h, s4, s5, s6, s7;
+};
+__device__ __forceinline__ NextRow next_row(const RowW<float>& R0, const float* slA) {
+  NextRow n;
+  n.b = shd(R0.b); n.w1 = shd(R0.w1); n.w2 = shd(R0.w2); n.w3 = shd(R0.w3); n.h = shd(R0.h);
+  n.s4 = shd(slA[4]); n.s5 = shd(slA[5]); n.s6 = shd(slA[6]); n.s7 = shd(slA[7]);
+  return n;
+}
+
 __device__ __forceinline__ void faces_pair(const RowW<float>& R0, const RowW<float>& R1,
                                            const float* slA, const float* slB,
-                                           const SweParams<float>& p, float& Fh, float& Fy,
-                                           float& fxl_n, float& fxr_n, float& Gh, float& Gx,
-                                           float& fyl_t, float& fyr_own) {
+                                           const NextRow& nx_, const SweParams<float>& p,
+                                           float& Fh, float& Fy, float& fxl_n, float& fxr_n,
+                                           float& Gh, float& Gx, float& fyl_t, float& fyr_own) {
   const float g = p.g, hg = 0.5f * g;
-  // the next lane's row r-2: the y-face's upper side
-  const float nb_b = shd(R0.b), nb_w1 = shd(R0.w1), nb_w2 = shd(R0.w2), nb_w3 = shd(R0.w3);
-  const float nb_h = shd(R0.h);
-  const float sn4 = shd(slA[4]), sn5 = shd(slA[5]), sn6 = shd(slA[6]), sn7 = shd(slA[7]);
+  const float nb_b = nx_.b, nb_w1 = nx_.w1, nb_w2 = nx_.w2, nb_w3 = nx_.w3, nb_h = nx_.h;
+  const float sn4 = nx_.s4, sn5 = nx_.s5, sn6 = nx_.s6, sn7 = nx_.s7;
   const float2 o1 = f2(p.half_dx, p.half_dy), o2 = f2(-p.half_dx, -p.half_dy);
   // side 1: row r-2 towards +x (x-face) and towards +y (y-face)
   const float2 b1 = fma2(f2(slA[0], slA[4]), o1, f2(R0.b, R0.b));
@@ -825,14 +836,21 @@ __device__ __forceinline__ void faces_pair(const RowW<float>& R0, const RowW<flo
 }
 
 // One warp's work item: strip `strip` (28 output columns) over the output rows
-// [r0, r1) of the strip region p.fast_*.  EDGE items touch the
-// grid's boundary (full-coverage mode, wall / extrapolation sides only): rows
-// and columns outside the grid are ghosts that load nothing, boundary cells
-// take the least-squares class weights and the ghost values of their sides, and
-// the faces on the boundary take the side's ghost state -- the expressions of
-// stage_tile's boundary branches.  `lead` (the item at the grid's corner in
-// full-coverage mode, where no tile kernel runs) keeps the control block.
-template <typename T, int RECON, int RIEMANN, int MODE, bool EDGE>
+// [r0, r1) of the strip region p.fast_*.  EK selects the body:
+//   0  interior: every lane's cell two cells or more from every boundary;
+//   1  EDGE (full-coverage mode, wall / extrapolation sides only): rows and
+//      columns outside the grid are ghosts that load nothing, boundary cells
+//      take the least-squares class weights and the ghost values of their
+//      sides, and the faces on the boundary take the side's ghost state -- the
+//      expressions of stage_tile's boundary branches;
+//   2  column EDGE: the rows [r0 - 2, r1 + 2) lie inside the grid (r0 >= 2,
+//      r1 <= nx - 2) but the strip's lanes reach a boundary column: the
+//      interior body with guarded column loads, then the boundary column's
+//      slopes and its boundary y-face recomputed by the EDGE expressions on
+//      the lanes that hold them.
+// `lead` (one item of the grid in full-coverage mode, where no tile kernel
+// runs) keeps the control block.
+template <typename T, int RECON, int RIEMANN, int MODE, int EK>
 __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __restrict__ hP,
                                            const T* __restrict__ qxP, const T* __restrict__ qyP,
                                            const T* __restrict__ h0P,
@@ -842,10 +860,12 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
                                            zb_ctrl* ctrl, int phase, const SweParams<T>& p,
                                            const int strip, const int r0, const int r1,
                                            const bool lead) {
+  constexpr bool EDGE = EK == 1;   // row and column guards
+  constexpr bool CG = EK != 0;     // column guards
   const int lane = threadIdx.x & 31;
   const int nx = p.nx, ny = p.ny;
   const int cj = p.fast_j0 - 2 + strip * SW + lane;
-  const bool colv = !EDGE || (cj >= 0 && cj < ny);
+  const bool colv = !CG || (cj >= 0 && cj < ny);
   const double t = ctrl->t[phase];
   const double dtd = dt_from_amax(ctrl->amax[phase], t, p.cfl2r, p.den_fac, p.dt_max, p.t_end);
   const bool ok = isfinite(dtd) && dtd > 0.0;
@@ -867,7 +887,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   if (!ok) return;                      // no-op step (t_end reached or dt invalid)
   const T dt = T(dtd);
   const T g = p.g, half = T(0.5);
-  const bool out_lane = lane >= 2 && lane < 2 + SW && (!EDGE || cj < ny);
+  const bool out_lane = lane >= 2 && lane < 2 + SW && (!CG || cj < ny);
   // float32 interior rows of the eta / HLL-HR scheme evaluate their two faces
   // as paired float32 arithmetic (faces_pair)
   constexpr bool PAIR = std::is_same<T, float>::value && RECON == ZB_RECON_ETA &&
@@ -883,7 +903,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   const int nsteps = (r1 - r0) + 4;
   // row r + 1 is fetched while row r is processed
   T nbv = T(0), nhv = T(0), nqxv = T(0), nqyv = T(0);
-  if (!EDGE || (colv && r0 - 2 >= 0)) {
+  if (!CG || (colv && (!EDGE || r0 - 2 >= 0))) {
     const size_t k = (size_t)(r0 - 2) * ny + cj;
     nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
   }
@@ -909,7 +929,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
     {
       const T vb = nbv, vh = nhv, vqx = nqxv, vqy = nqyv;
       if (s + 1 < nsteps) {
-        if (!EDGE || (colv && r + 1 >= 0 && r + 1 < nx)) {
+        if (!CG || (colv && (!EDGE || (r + 1 >= 0 && r + 1 < nx)))) {
           const size_t k = (size_t)(r + 1) * ny + cj;
           nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
         } else {
@@ -983,14 +1003,16 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
                              p.vk_eps2);
       }
       }
-      if (EDGE) {
+      if (CG) {
         // row r-1 = m: boundary cells (stage_tile phase B, non-interior
-        // branch) and ghosts (zero slopes)
+        // branch) and ghosts (zero slopes); a column-EDGE item's rows are
+        // never boundary rows
         const int m = r - 1;
-        const bool cellv = colv && m >= 0 && m < nx;
-        const bool bnd = cellv && (m == 0 || m == nx - 1 || cj == 0 || cj == ny - 1);
+        const bool cellv = colv && (!EDGE || (m >= 0 && m < nx));
+        const bool bxl = EDGE && m == 0, bxh = EDGE && m == nx - 1;
+        const bool byl = cj == 0, byh = cj == ny - 1;
+        const bool bnd = cellv && (bxl || bxh || byl || byh);
         if (__any_sync(0xffffffffu, bnd)) {
-          const bool bxl = m == 0, bxh = m == nx - 1, byl = cj == 0, byh = cj == ny - 1;
           const int cls = (bxl ? 0 : (bxh ? 2 : 1)) * 3 + (byl ? 0 : (byh ? 2 : 1));
           const T* wx = p.lsq.w[cls][0];
           const T* wy = p.lsq.w[cls][1];
@@ -1083,10 +1105,40 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
     T Fh, Fy, fxl_n, fxr_n, Gh, Gx, fyl_t, fyr_own;
     {
       if constexpr (PAIR) {
-        faces_pair(R0, R1, slA, slB, p, Fh, Fy, fxl_n, fxr_n, Gh, Gx, fyl_t, fyr_own);
+        const NextRow nv = next_row(R0, slA);
+        faces_pair(R0, R1, slA, slB, nv, p, Fh, Fy, fxl_n, fxr_n, Gh, Gx, fyl_t, fyr_own);
         if (s == 3) {          // face r0 - 1/2: only the next row needs it
           fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
           continue;
+        }
+        if (EK == 2 && (cj == -1 || cj == ny - 1)) {
+          // the y-face on the boundary (the lane below column 0, or column
+          // ny - 1): the owner's trace against its ghost with normal sign sgy,
+          // as the EDGE body evaluates it
+          RowW<T> nb;
+          nb.b = nv.b; nb.w1 = nv.w1; nb.w2 = nv.w2; nb.w3 = nv.w3; nb.h = nv.h; nb.hinv = T(0);
+          const T sln[4] = {nv.s4, nv.s5, nv.s6, nv.s7};
+          Side<T> C, D;
+          strip_trace<T, RECON>(R0, slA + 4, p.half_dy, C);
+          strip_trace<T, RECON>(nb, sln, -p.half_dy, D);
+          const bool ylo = cj == -1;
+          const Side<T> YL = ylo ? D : C;
+          Side<T> YR = YL;
+          if (p.bc[ylo ? 2 : 3] == ZB_BC_WALL) {
+            YR.qy = -YL.qy;
+            YR.uy = -YL.uy;
+          }
+          const T sgy = ylo ? T(-1) : T(1);
+          T Gy, Em, Ep;
+          riemann<T, RIEMANN, 1>(YL, YR, sgy, g, Gh, Gx, Gy, Em, Ep);
+          const T cesC = half * g * (R0.h + C.h) * (C.b - R0.b);
+          const T cesD = -(half * g * (nb.h + D.h) * (D.b - nb.b));
+          const T own_n = Gy + Em * sgy + (ylo ? -cesD : cesC) * sgy;
+          if (ylo) {
+            Gh = -Gh; Gx = -Gx; fyr_own = own_n; fyl_t = T(0);
+          } else {
+            fyl_t = own_n; fyr_own = T(0);
+          }
         }
       } else {
       T Fx, Dm, Dp;
@@ -1139,11 +1191,11 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       strip_trace<T, RECON>(nb, sln + 4, -p.half_dy, D);
       // EDGE: a face on the y boundary takes the owner's trace (the next
       // lane's cell 0, or this lane's cell ny-1) against its ghost
-      const bool yb = EDGE && (cj == -1 || cj == ny - 1);
-      const bool ylo = EDGE && cj == -1;
+      const bool yb = CG && (cj == -1 || cj == ny - 1);
+      const bool ylo = CG && cj == -1;
       T sgy = T(1);
       Side<T> YL = C, YR = D;
-      if (EDGE) {
+      if (CG) {
         YL.b = ylo ? D.b : C.b; YL.h = ylo ? D.h : C.h; YL.qx = ylo ? D.qx : C.qx;
         YL.qy = ylo ? D.qy : C.qy; YL.ux = ylo ? D.ux : C.ux; YL.uy = ylo ? D.uy : C.uy;
         const bool wall = yb && p.bc[ylo ? 2 : 3] == ZB_BC_WALL;
@@ -1229,62 +1281,71 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   }
 }
 
-// Full-coverage item list of a grid (strips of SW columns from column 0,
-// rows from 0).  Strips whose 32 lanes reach outside the grid (the first, and
-// the last one or two) run the EDGE body on every row and march chunks of SXE
-// rows, so that they end with the others; each middle strip has two EDGE items
-// for the boundary rows [0, 2) and [nx - 2, nx) and marches the rows between
-// in SX-row interior chunks.  Item 0 (strip 0, rows 0..) keeps the control
-// block.  Returns the item count (item = -1), the count of EDGE items, which
-// come first (item = -2), or with item >= 0 fills its strip and rows.
-constexpr int SXE = 8;
+// Full-coverage item list of a grid with nx, ny >= 4 (strips of SW columns
+// from column 0, rows from 0).  Every strip has two EDGE items for the
+// boundary rows [0, 2) and [nx - 2, nx).  The rows between go in chunks: SX
+// rows for the middle strips (lanes 28 s - 2 .. 28 s + 29 inside the grid,
+// the interior body), sxc rows for the strips whose lanes reach outside the
+// grid (the first, and the last one or two: the column-EDGE body).  Order:
+// the column-EDGE items, the EDGE items (these two kinds form the boundary
+// launch), then the interior items.  Item 0 keeps the control block.  Returns
+// the item count (item = -1), the count of boundary-launch items (item = -2),
+// or with item >= 0 fills its strip, rows and kind (the strip_item EK).
+// Column-EDGE chunk heights (B200, 2048^2 and the 512-instance ensemble): a
+// single grid's boundary launch shares the SMs with one wave of interior
+// items and fills their tail best with short chunks (8 rows: 0.189 ms per
+// step; 16: 0.213; 32: 0.261); the ensemble's persistent launches walk their
+// lists one after another and lose less to halo rows with 16 (2.28 ms per
+// step; 8: 2.33; 32: 2.30).
+constexpr int SXC_GRID = 8;
+constexpr int SXC_ENS = 16;
 __host__ __device__ inline int full_items(int nx, int ny, int item, int* strip, int* r0,
-                                          int* r1) {
+                                          int* r1, int* kind, int sxc) {
+  const int SXC = sxc;
   const int ns = (ny + SW - 1) / SW;
-  // middle strips: 1 <= s <= mh (lanes 28 s - 2 .. 28 s + 29 inside the grid)
+  // middle strips: 1 <= s <= mh
   int mh = ny >= 30 ? (ny - 30) / SW : 0;
   if (mh > ns - 1) mh = ns - 1;
-  if (nx < 4) mh = 0;
   const int nmid = mh, nedge = ns - nmid;
-  const int nce = (nx + SXE - 1) / SXE;
   const int nci = nx > 4 ? (nx - 4 + SX - 1) / SX : 0;
-  const int total = nedge * nce + nmid * (2 + nci);
-  if (item == -2) return nedge * nce + 2 * nmid;   // the EDGE items come first
+  const int ncc = nx > 4 ? (nx - 4 + SXC - 1) / SXC : 0;
+  const int nside = nedge * ncc + 2 * ns;
+  const int total = nside + nmid * nci;
+  if (item == -2) return nside;
   if (item < 0) return total;
-  int st, a, b;
-  if (item < nedge * nce) {
-    const int e = item / nce;                // edge strips: 0, mh + 1, ..., ns - 1
+  int st, a, b, k;
+  if (item < nedge * ncc) {
+    const int e = item / ncc;                // edge strips: 0, mh + 1, ..., ns - 1
     st = e == 0 ? 0 : mh + e;
-    a = (item % nce) * SXE;
-    b = a + SXE;
-  } else if ((item -= nedge * nce) < 2 * nmid) {
-    st = 1 + item / 2;
+    a = 2 + (item % ncc) * SXC;
+    b = a + SXC < nx - 2 ? a + SXC : nx - 2;
+    k = 2;
+  } else if ((item -= nedge * ncc) < 2 * ns) {
+    st = item >> 1;
     a = (item & 1) ? nx - 2 : 0;
     b = a + 2;
+    k = 1;
   } else {
-    item -= 2 * nmid;
+    item -= 2 * ns;
     st = 1 + item % nmid;
     a = 2 + (item / nmid) * SX;
     b = a + SX < nx - 2 ? a + SX : nx - 2;
+    k = 0;
   }
   *strip = st;
   *r0 = a;
-  *r1 = b < nx ? b : nx;
+  *r1 = b;
+  *kind = k;
   return total;
 }
 
-// an item reaches a boundary or a ghost row or column: the EDGE body
-__host__ __device__ inline bool full_item_edge(int nx, int ny, int strip, int r0, int r1) {
-  const int cj0 = strip * SW - 2;
-  return !(r0 >= 2 && r1 <= nx - 2 && cj0 >= 0 && cj0 + 31 <= ny - 1);
-}
-
 // KIND 0: the interior strips of a grid with a periodic side (the tile kernel
-// takes the frame); KIND 1: the EDGE items of a full-coverage list; KIND 2:
-// its interior items.  Kinds 1 and 2 are separate launches (they run side by
-// side on two streams) so that the EDGE body never raises the interior body's
-// register allocation.  float32: 4 CTAs of 4 warps per SM (128 registers; the
-// paired-face interior body spills at 96).
+// takes the frame); KIND 1: the boundary items of a full-coverage list
+// (column-EDGE and EDGE); KIND 2: its interior items.  Kinds 1 and 2 are
+// separate launches (they run side by side on two streams) so that the
+// boundary bodies never raise the interior body's register allocation.
+// float32: 4 CTAs of 4 warps per SM (128 registers; the paired-face interior
+// body spills at 96).
 template <typename T, int RECON, int RIEMANN, int MODE, int KIND>
 __global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
 swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
@@ -1293,7 +1354,7 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
                    const T* __restrict__ qy0P, T* __restrict__ hO, T* __restrict__ qxO,
                    T* __restrict__ qyO, zb_ctrl* ctrl, int phase, const SweParams<T> p) {
   int item = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5);
-  int strip, r0, r1;
+  int strip, r0, r1, kind = 0;
   if (KIND == 0) {
     const int nstrips = (p.fast_j1 - p.fast_j0) / SW;
     if (item >= nstrips * ((p.fast_i1 - p.fast_i0 + SX - 1) / SX)) return;   // warp-uniform
@@ -1301,17 +1362,27 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
     r0 = p.fast_i0 + (item / nstrips) * SX;
     r1 = min(r0 + SX, p.fast_i1);
   } else {
-    const int ne = full_items(p.nx, p.ny, -2, nullptr, nullptr, nullptr);
+    const int ne = full_items(p.nx, p.ny, -2, nullptr, nullptr, nullptr, nullptr, SXC_GRID);
     if (KIND == 1 && item >= ne) return;
     if (KIND == 2) {
       item += ne;
-      if (item >= full_items(p.nx, p.ny, -1, nullptr, nullptr, nullptr)) return;
+      const int n = full_items(p.nx, p.ny, -1, nullptr, nullptr, nullptr, nullptr, SXC_GRID);
+      if (item >= n) return;
     }
-    full_items(p.nx, p.ny, item, &strip, &r0, &r1);
+    full_items(p.nx, p.ny, item, &strip, &r0, &r1, &kind, SXC_GRID);
   }
-  strip_item<T, RECON, RIEMANN, MODE, KIND == 1>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO,
-                                                 qyO, ctrl, phase, p, strip, r0, r1,
-                                                 KIND == 1 && item == 0);
+  if (KIND == 1) {
+    // warp-uniform: the item's kind
+    if (kind == 2)
+      strip_item<T, RECON, RIEMANN, MODE, 2>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO,
+                                             ctrl, phase, p, strip, r0, r1, item == 0);
+    else
+      strip_item<T, RECON, RIEMANN, MODE, 1>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO,
+                                             ctrl, phase, p, strip, r0, r1, item == 0);
+  } else {
+    strip_item<T, RECON, RIEMANN, MODE, 0>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO,
+                                           ctrl, phase, p, strip, r0, r1, false);
+  }
 }
 
 // A second stream per device with a fork and a join event: the EDGE launch of
@@ -1359,7 +1430,7 @@ ens_stage_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ i
   S& s = *reinterpret_cast<S*>(smem_raw);
   __shared__ double red[NT / 32];
   const int tid = threadIdx.x;
-  // items[0] = {tile items, strip items}; tile items follow
+  // items[0].x = the tile item count; the tile items follow the header
   const int n_items = items[0].x;
   items += 1;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -1398,38 +1469,44 @@ ens_stage_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ i
   }
 }
 
-// All instances' strip items: persistent warps walk them.  The work list's
-// header items[0] = {tile items, interior strip items, boundary strip items};
-// the tile items follow it, then the interior strips, then the boundary
-// strips (the EDGE body, a launch of its own so that its extra live values
-// never raise the interior body's register allocation).
-template <typename T, int MODE, bool EDGE>
+// One strip item of an instance: stage 1 reads Q and writes the stage buffer,
+// stage 2 reads the stage buffer and Q0 = Q and writes Q.
+template <typename T, int MODE, int EK>
+__device__ __forceinline__ void ens_item(const EnsDesc<T>* d, T* Q, T* W, zb_ctrl* ctrl,
+                                         int phase, int strip, int r0, int r1, bool lead) {
+  const SweParams<T>& p = d->p;
+  const size_t C = (size_t)p.nx * p.ny;
+  T* q = Q + d->q_off;
+  T* ws = W + d->ws_off;
+  if (MODE == MODE_STEP1)
+    strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1, EK>(
+        q, q + C, q + 2 * C, q + 3 * C, nullptr, nullptr, nullptr, ws, ws + C, ws + 2 * C,
+        ctrl, phase, p, strip, r0, r1, lead);
+  else
+    strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2, EK>(
+        q, ws, ws + C, ws + 2 * C, q + C, q + 2 * C, q + 3 * C, q + C, q + 2 * C, q + 3 * C,
+        ctrl, phase, p, strip, r0, r1, lead);
+}
+
+// All instances' strip items of one body (EK, as strip_item): persistent warps
+// walk them.  The work list's header items[0] = {tile items, interior strip
+// items, EDGE strip items, column-EDGE strip items}; the lists follow it in
+// that order.  Each body is a launch of its own, so that the boundary bodies'
+// extra live values never raise another body's register allocation.
+template <typename T, int MODE, int EK>
 __global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
 ens_strip_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ items, T* Q,
                  T* W, zb_ctrl* ctrls, int phase) {
   const int4 hd = items[0];
-  const int4* list = items + 1 + hd.x + (EDGE ? hd.y : 0);
-  const int n = EDGE ? hd.z : hd.y;
+  const int4* list = items + 1 + hd.x + (EK >= 1 ? hd.y : 0) + (EK == 2 ? hd.z : 0);
+  const int n = EK == 0 ? hd.y : (EK == 1 ? hd.z : hd.w);
   const int nw = gridDim.x * (STRIP_NT / 32);
   for (int it = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5); it < n; it += nw) {
-    // w = {instance, strip, r0, flags | r1 << 2}; flags bit 1 = the item keeps
+    // w = {instance, strip, r0, flags | r1 << 3}; flags bit 1 = the item keeps
     // the instance's control block
     const int4 w = list[it];
-    const EnsDesc<T>* d = desc + w.x;
-    const SweParams<T>& p = d->p;
-    const size_t C = (size_t)p.nx * p.ny;
-    T* q = Q + d->q_off;
-    T* ws = W + d->ws_off;
-    const bool lead = EDGE && (w.w & 2) != 0;
-    const int r1 = w.w >> 2;
-    if (MODE == MODE_STEP1)
-      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1, EDGE>(
-          q, q + C, q + 2 * C, q + 3 * C, nullptr, nullptr, nullptr, ws, ws + C, ws + 2 * C,
-          ctrls + w.x, phase, p, w.y, w.z, r1, lead);
-    else
-      strip_item<T, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2, EDGE>(
-          q, ws, ws + C, ws + 2 * C, q + C, q + 2 * C, q + 3 * C, q + C, q + 2 * C, q + 3 * C,
-          ctrls + w.x, phase, p, w.y, w.z, r1, lead);
+    ens_item<T, MODE, EK>(desc + w.x, Q, W, ctrls + w.x, phase, w.y, w.z, w.w >> 3,
+                          (w.w & 2) != 0);
   }
 }
 
@@ -1790,16 +1867,17 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
   const bool strips = pf.fast_i1 > pf.fast_i0;
   const bool tiles = !pf.strip_full;
   const int nitems = !strips ? 0
-                     : pf.strip_full ? full_items(c->nx, c->ny, -1, nullptr, nullptr, nullptr)
+                     : pf.strip_full ? full_items(c->nx, c->ny, -1, nullptr, nullptr, nullptr,
+                                                       nullptr, SXC_GRID)
                                      : nstrips * ((pf.fast_i1 - pf.fast_i0 + SX - 1) / SX);
   const int sgrid = (nitems + STRIP_NT / 32 - 1) / (STRIP_NT / 32);
-  // full coverage: the EDGE items on the side stream, the interior items here
+  // full coverage: the boundary items on the side stream, the interior items here
   SideStream* side = nullptr;
   int ne = 0, ni = 0;
   if (pf.strip_full) {
     int rc = side_stream(&side);
     if (rc) return rc;
-    ne = full_items(c->nx, c->ny, -2, nullptr, nullptr, nullptr);
+    ne = full_items(c->nx, c->ny, -2, nullptr, nullptr, nullptr, nullptr, SXC_GRID);
     ni = nitems - ne;
   }
   const int wpb = STRIP_NT / 32;
@@ -1913,16 +1991,16 @@ static Fast fast_region(int nx, int ny) {
 }
 
 // strip items of an instance (the single grid's full-coverage list):
-// {strip, r0, r1, flags}; flags bit 0 = the item reaches the boundary (EDGE
-// body), bit 1 = it keeps the control block
+// {strip, r0, r1, flags}; flags bit 0 = a boundary-launch item, bit 1 = it
+// keeps the control block, bit 2 = a column-EDGE item (else EDGE, when bit 0)
 template <typename F>
 static void ens_strip_items(const zb_ens_instance& in, F&& visit) {
   if (fast_region(in.nx, in.ny).nstrips == 0) return;
-  const int n = full_items(in.nx, in.ny, -1, nullptr, nullptr, nullptr);
+  const int n = full_items(in.nx, in.ny, -1, nullptr, nullptr, nullptr, nullptr, SXC_ENS);
   for (int it = 0; it < n; ++it) {
-    int st, r0, r1;
-    full_items(in.nx, in.ny, it, &st, &r0, &r1);
-    visit(st, r0, r1, (full_item_edge(in.nx, in.ny, st, r0, r1) ? 1 : 0) | (it == 0 ? 2 : 0));
+    int st, r0, r1, kind;
+    full_items(in.nx, in.ny, it, &st, &r0, &r1, &kind, SXC_ENS);
+    visit(st, r0, r1, (kind != 0 ? 1 : 0) | (it == 0 ? 2 : 0) | (kind == 2 ? 4 : 0));
   }
 }
 
@@ -1941,7 +2019,8 @@ static void ens_counts(const zb_ens_instance* inst, int n, int tile_x, size_t* t
   for (int i = 0; i < n; ++i) {
     ens_frame_tiles(inst[i], tile_x, [&](int, int) { ++*tiles; });
     if (fast_region(inst[i].nx, inst[i].ny).nstrips > 0)
-      *strips += (size_t)full_items(inst[i].nx, inst[i].ny, -1, nullptr, nullptr, nullptr);
+      *strips += (size_t)full_items(inst[i].nx, inst[i].ny, -1, nullptr, nullptr, nullptr,
+                                          nullptr, SXC_ENS);
   }
 }
 
@@ -1983,16 +2062,21 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   }
   ZB_CUDA_TRY(cudaEventRecord(side->fork, st));
   ZB_CUDA_TRY(cudaStreamWaitEvent(side->s, side->fork, 0));
+  // the column-EDGE items (longer) before the EDGE items on the second stream
   if (part == 0) {
-    ens_strip_kernel<T, MODE_STEP1, true><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+    ens_strip_kernel<T, MODE_STEP1, 2><<<sgrid_e, STRIP_NT, 0, side->s>>>(
         desc, items, (T*)Q, (T*)W, ctrls, phase);
-    ens_strip_kernel<T, MODE_STEP1, false><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
-                                                                        (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP1, 1><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+        desc, items, (T*)Q, (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP1, 0><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
+                                                                    (T*)W, ctrls, phase);
   } else {
-    ens_strip_kernel<T, MODE_STEP2, true><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+    ens_strip_kernel<T, MODE_STEP2, 2><<<sgrid_e, STRIP_NT, 0, side->s>>>(
         desc, items, (T*)Q, (T*)W, ctrls, phase);
-    ens_strip_kernel<T, MODE_STEP2, false><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
-                                                                        (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP2, 1><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+        desc, items, (T*)Q, (T*)W, ctrls, phase);
+    ens_strip_kernel<T, MODE_STEP2, 0><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
+                                                                    (T*)W, ctrls, phase);
   }
   ZB_CUDA_TRY(cudaGetLastError());
   ZB_CUDA_TRY(cudaEventRecord(side->join, side->s));
@@ -2227,8 +2311,9 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
   auto build = [&](auto tag) -> int {
     using T = decltype(tag);
     std::vector<EnsDesc<T>> desc(n_inst);
-    // items[0]: {tile items, interior strip items, boundary strip items}
-    std::vector<int4> items(1), strips, estrips;
+    // items[0]: {tile items, interior strip items, EDGE strip items,
+    // column-EDGE strip items}
+    std::vector<int4> items(1), strips, estrips, cstrips;
     for (int i = 0; i < n_inst; ++i) {
       zb_swe2d_cfg c = *common;
       c.nx = inst[i].nx;
@@ -2250,12 +2335,15 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
         items.push_back(make_int4(i, i0, j0, i0 == 0 && j0 == 0));
       });
       ens_strip_items(inst[i], [&](int st, int r0, int r1, int fl) {
-        ((fl & 1) ? estrips : strips).push_back(make_int4(i, st, r0, fl | (r1 << 2)));
+        std::vector<int4>& to = (fl & 4) ? cstrips : ((fl & 1) ? estrips : strips);
+        to.push_back(make_int4(i, st, r0, fl | (r1 << 3)));
       });
     }
-    items[0] = make_int4((int)(items.size() - 1), (int)strips.size(), (int)estrips.size(), 0);
+    items[0] = make_int4((int)(items.size() - 1), (int)strips.size(), (int)estrips.size(),
+                         (int)cstrips.size());
     items.insert(items.end(), strips.begin(), strips.end());
     items.insert(items.end(), estrips.begin(), estrips.end());
+    items.insert(items.end(), cstrips.begin(), cstrips.end());
     const size_t db = ens_desc_bytes<T>(n_inst);
     ZB_CUDA_TRY(cudaMemcpy(table, desc.data(), desc.size() * sizeof(EnsDesc<T>),
                            cudaMemcpyHostToDevice));

@@ -1,13 +1,15 @@
-"""Batched ensemble of independent 2-D SWE instances in one launch per stage.
+"""Batched ensemble of independent 2-D SWE instances in shared launches.
 
 Each instance is its own Cartesian grid (own size, spacing, Manning
 coefficient, CFL dt and control block).  All instances' states live in one
-device array; a persistent libzb kernel walks an (instance, tile) work list,
-so one launch advances every instance by one stage and one SSP-RK2 step is two
-launches regardless of the number of instances.  The tile height and the
-persistent grid size are picked by a small autotuner that times the
-candidates on the actual ensemble; the steps can be captured into a CUDA
-graph and replayed.
+device array; persistent libzb kernels walk one work list of every
+instance's strip items (interior, boundary-column and boundary-row bodies,
+one launch each) and the tiles of grids narrower than four cells, so a fixed
+set of four launches advances every instance by one stage, whatever the
+number of instances.  The tile height and the persistent grid size of the
+tile fallback are picked by a small autotuner that times the candidates on
+the actual ensemble; the steps can be captured into a CUDA graph and
+replayed.
 """
 from __future__ import annotations
 
