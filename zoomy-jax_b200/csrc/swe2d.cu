@@ -2339,6 +2339,16 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
         to.push_back(make_int4(i, st, r0, fl | (r1 << 3)));
       });
     }
+    // longest items first: the persistent warps take items round-robin, so
+    // each warp's k-th item is about as long as every other warp's k-th
+    auto longest_first = [](std::vector<int4>& v) {
+      std::stable_sort(v.begin(), v.end(), [](const int4& a, const int4& b) {
+        return (a.w >> 3) - a.z > (b.w >> 3) - b.z;
+      });
+    };
+    longest_first(strips);
+    longest_first(estrips);
+    longest_first(cstrips);
     items[0] = make_int4((int)(items.size() - 1), (int)strips.size(), (int)estrips.size(),
                          (int)cstrips.size());
     items.insert(items.end(), strips.begin(), strips.end());
