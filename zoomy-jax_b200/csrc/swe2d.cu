@@ -1295,10 +1295,10 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
 // single grid's boundary launch shares the SMs with one wave of interior
 // items and fills their tail best with short chunks (8 rows: 0.189 ms per
 // step; 16: 0.213; 32: 0.261); the ensemble's persistent launches walk their
-// lists one after another and lose less to halo rows with 16 (2.28 ms per
-// step; 8: 2.33; 32: 2.30).
+// longest-first lists one after another and lose less to halo rows with 32
+// (2.094 ms per step; 8: 2.21; 16: 2.127; 64: 2.136).
 constexpr int SXC_GRID = 8;
-constexpr int SXC_ENS = 16;
+constexpr int SXC_ENS = 32;
 __host__ __device__ inline int full_items(int nx, int ny, int item, int* strip, int* r0,
                                           int* r1, int* kind, int sxc) {
   const int SXC = sxc;
