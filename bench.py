@@ -320,8 +320,9 @@ def run_gpu(args, rank, world, local_rank):
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
             "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
             "traffic": None,
-            "kernel": ("swe2d_strip_kernel<MODE_STEP2>: interior and EDGE launches side by "
-                       "side on two streams, timed together (stage 2)"),
+            "kernel": ("swe2d_strip_kernel<MODE_STEP2>: the interior launch and the boundary "
+                       "launch (column-EDGE and EDGE items) side by side on two streams, "
+                       "timed together (stage 2)"),
             "algorithmic_bytes_per_launch": bytes2,
             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "stage1": {"ms": round(mean1 * 1e3, 4),
