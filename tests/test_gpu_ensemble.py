@@ -70,6 +70,26 @@ def test_ensemble_matches_single_grids(tile):
         assert ci.t[5 % 3] == pytest.approx(c.t[5 % 3], rel=1e-14)
 
 
+def test_float32_ensemble_matches_single_grids():
+    """float32 runs the boundary strips' inner rows in the paired column-EDGE
+    body (32-row chunks in the ensemble's lists, 8-row chunks in a single
+    grid's): every instance -- a grid too small for strips (tile fallback),
+    grids without inner rows or middle strips, grids with one and several
+    middle strips -- agrees with the same grid run alone after 5 steps (the
+    two kernels may contract a few products differently: 1e-5 relative)."""
+    sides = [3, 4, 5, 6, 29, 30, 31, 57, 58, 60, 85]
+    ens, heights, manning = make_ens(sides, "float32", 16)
+    ens.init()
+    ens.launch_steps(5)
+    assert ens.status_any() == 0
+    for i, n in enumerate(sides):
+        ref, c = single_run(n, heights[i], manning[i], 5, "float32")
+        got = ens.instance(i).double().cpu().numpy()
+        scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-30
+        assert (np.abs(got - ref) / scale).max() <= 1e-5, f"instance {i} (n={n})"
+        assert ens.ctrl(i).t[5 % 3] == pytest.approx(c.t[5 % 3], rel=1e-5)
+
+
 def test_ensemble_instance_matches_oracle_per_step():
     ens, heights, manning = make_ens([40, 56], "float64", 16)
     ens.init()

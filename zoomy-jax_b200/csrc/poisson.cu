@@ -479,11 +479,12 @@ prolong_add_kernel(const float* __restrict__ ec, float* __restrict__ xf, int nxc
 // level-wide sweeps produce.  The operator and update are the same float
 // expressions as apply_at / rbgs_kernel, so the result is bit-identical to the
 // one-kernel-per-sweep sequence.
-constexpr int FT = 32;
-constexpr int FNT_MAX = 1024;     // blocks are 32 x 8 (large levels) or 32 x 32 (small levels)
+constexpr int FT = 32;            // tile side of the levels with a tile for every SM
+constexpr int FTS = 16;           // tile side of the smaller levels
+constexpr int FNT_MAX = 1024;
 
-__host__ __device__ inline size_t fused_smem(int halo) {
-  const int R = FT + 2 * halo;
+__host__ __device__ inline size_t fused_smem(int halo, int tile) {
+  const int R = tile + 2 * halo;
   return (size_t)(4 * R * R + 2 * (R + 1) * R) * sizeof(float);
 }
 
@@ -502,9 +503,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // (R x R) and the face coefficients cx ((R+1) x R), cy (R x (R+1)).  A tile
 // whose ring lies wholly inside the level (most of them) takes the EDGE-free
 // path: no domain tests and no Dirichlet ghosts.
-template <int HALO>
+template <int HALO, int TT>
 struct Stage {
-  static constexpr int R = FT + 2 * HALO;
+  static constexpr int R = TT + 2 * HALO;
   int i0, j0, nx, ny;
   bool interior;
   float *x, *f, *r, *dg, *cx, *cy;
@@ -534,7 +535,7 @@ struct Stage {
       const int gi = i0 - HALO + a;
       // first column b >= m with (gi + gj) % 2 == color, gj = j0 - HALO + b
       int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
-      for (; b < R - m; b += 64) {
+      for (; b < R - m; b += 2 * (int)blockDim.x) {
         if (EDGE && !inside(a, b)) continue;
         const float v = ax<EDGE>(a, b, idx2);
         x[a * R + b] += (f[a * R + b] - v) / dg[a * R + b];
@@ -554,13 +555,13 @@ struct Stage {
   }
 };
 
-template <int HALO>
-__device__ Stage<HALO> stage_level(float* sm, int i0, int j0, int nx, int ny,
-                                   const float* __restrict__ f, const float* __restrict__ cx,
-                                   const float* __restrict__ cy, const float* __restrict__ dg,
-                                   const float* __restrict__ x) {
-  constexpr int R = Stage<HALO>::R;
-  Stage<HALO> S;
+template <int HALO, int TT>
+__device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny,
+                                       const float* __restrict__ f, const float* __restrict__ cx,
+                                       const float* __restrict__ cy, const float* __restrict__ dg,
+                                       const float* __restrict__ x) {
+  constexpr int R = Stage<HALO, TT>::R;
+  Stage<HALO, TT> S;
   S.i0 = i0; S.j0 = j0; S.nx = nx; S.ny = ny;
   S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
   S.x = sm; S.f = sm + R * R; S.r = sm + 2 * R * R; S.dg = sm + 3 * R * R;
@@ -598,36 +599,37 @@ __device__ Stage<HALO> stage_level(float* sm, int i0, int j0, int nx, int ny,
 }
 
 // pre-smoothing from x = 0 (NU red/black pairs), residual, restriction:
-// writes the tile's x and the coarse right-hand side of its 16 x 16 coarse cells
-template <int NU>
+// writes the tile's x and the coarse right-hand side of its TT/2 x TT/2
+// coarse cells
+template <int NU, int TT>
 __global__ void __launch_bounds__(FNT_MAX)
 mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
                const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
                float* __restrict__ fc, int nx, int ny, float idx2) {
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU + 2;
-  constexpr int R = Stage<HALO>::R;
-  const int i0 = blockIdx.y * FT, j0 = blockIdx.x * FT;
+  constexpr int R = Stage<HALO, TT>::R;
+  const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const Stage<HALO> S = stage_level<HALO>(fsm, i0, j0, nx, ny, f, cx, cy, dg, nullptr);
+  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, dg, nullptr);
   for (int s = 0; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
   // residual where the sweeps are final and one ring beyond the tile
   {
     constexpr int m = 2 * NU + 1;
     for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y)
-      for (int b = m + (int)threadIdx.x; b < R - m; b += 32)
+      for (int b = m + (int)threadIdx.x; b < R - m; b += (int)blockDim.x)
         S.r[a * R + b] = S.residual(a, b, idx2);
   }
   __syncthreads();
-  for (int e = tid; e < FT * FT; e += nt) {
-    const int ti = e / FT, tj = e % FT;
+  for (int e = tid; e < TT * TT; e += nt) {
+    const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
     if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
   }
   const int nxc = nx / 2, nyc = ny / 2;
-  for (int e = tid; e < (FT / 2) * (FT / 2); e += nt) {
-    const int I = i0 / 2 + e / (FT / 2), J = j0 / 2 + e % (FT / 2);
+  for (int e = tid; e < (TT / 2) * (TT / 2); e += nt) {
+    const int I = i0 / 2 + e / (TT / 2), J = j0 / 2 + e % (TT / 2);
     if (I >= nxc || J >= nyc) continue;
     fc[(long long)I * nyc + J] = restrict_at(
         [&](int fi, int fj) { return S.r[(fi - i0 + HALO) * R + (fj - j0 + HALO)]; }, I, J, nxc,
@@ -636,21 +638,21 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
 }
 
 // x += P e (coarse correction), post-smoothing (NU black/red pairs)
-template <int NU>
+template <int NU, int TT>
 __global__ void __launch_bounds__(FNT_MAX)
 mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
              const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
              const float* __restrict__ ec, int nx, int ny, float idx2) {
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU;
-  constexpr int R = Stage<HALO>::R;
-  const int i0 = blockIdx.y * FT, j0 = blockIdx.x * FT;
+  constexpr int R = Stage<HALO, TT>::R;
+  const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const Stage<HALO> S = stage_level<HALO>(fsm, i0, j0, nx, ny, f, cx, cy, dg, x);
+  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, dg, x);
   const int nxc = nx / 2, nyc = ny / 2;
   for (int a = (int)threadIdx.y; a < R; a += (int)blockDim.y)
-    for (int b = (int)threadIdx.x; b < R; b += 32) {
+    for (int b = (int)threadIdx.x; b < R; b += (int)blockDim.x) {
       if (!S.inside(a, b)) continue;
       const int fi = i0 - HALO + a, fj = j0 - HALO + b;
       S.x[a * R + b] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
@@ -658,8 +660,8 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
     }
   __syncthreads();
   for (int s = 0; s < 2 * NU; ++s) S.sweep(1 - (s & 1), s + 1, idx2);
-  for (int e = tid; e < FT * FT; e += nt) {
-    const int ti = e / FT, tj = e % FT;
+  for (int e = tid; e < TT * TT; e += nt) {
+    const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
     if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
   }
@@ -867,10 +869,14 @@ static int enable_coarse_smem() {
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
 #define ZB_SMEM_ATTR(K) \
     ZB_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))
-    ZB_SMEM_ATTR(mg_down_kernel<1>); ZB_SMEM_ATTR(mg_down_kernel<2>);
-    ZB_SMEM_ATTR(mg_down_kernel<3>); ZB_SMEM_ATTR(mg_down_kernel<4>);
-    ZB_SMEM_ATTR(mg_up_kernel<1>); ZB_SMEM_ATTR(mg_up_kernel<2>);
-    ZB_SMEM_ATTR(mg_up_kernel<3>); ZB_SMEM_ATTR(mg_up_kernel<4>);
+    ZB_SMEM_ATTR((mg_down_kernel<1, FT>)); ZB_SMEM_ATTR((mg_down_kernel<2, FT>));
+    ZB_SMEM_ATTR((mg_down_kernel<3, FT>)); ZB_SMEM_ATTR((mg_down_kernel<4, FT>));
+    ZB_SMEM_ATTR((mg_up_kernel<1, FT>)); ZB_SMEM_ATTR((mg_up_kernel<2, FT>));
+    ZB_SMEM_ATTR((mg_up_kernel<3, FT>)); ZB_SMEM_ATTR((mg_up_kernel<4, FT>));
+    ZB_SMEM_ATTR((mg_down_kernel<1, FTS>)); ZB_SMEM_ATTR((mg_down_kernel<2, FTS>));
+    ZB_SMEM_ATTR((mg_down_kernel<3, FTS>)); ZB_SMEM_ATTR((mg_down_kernel<4, FTS>));
+    ZB_SMEM_ATTR((mg_up_kernel<1, FTS>)); ZB_SMEM_ATTR((mg_up_kernel<2, FTS>));
+    ZB_SMEM_ATTR((mg_up_kernel<3, FTS>)); ZB_SMEM_ATTR((mg_up_kernel<4, FTS>));
 #undef ZB_SMEM_ATTR
     set_mask |= 1u << dev;
   }
@@ -946,9 +952,44 @@ static bool valid(const zb_poisson_cfg* c) {
 // z32 = M r32 on level 0 (f0 already holds r); precond: 0 none, 1 MG, 2 MG
 // followed by one learned smoothing step on level 0 (x += S(f - A x)), 3 MG
 // with the level-0 red-black smoothing replaced by the learned smoother
-// threads per fused CTA: 32 x 8 when the level has tiles for every SM, else
-// 32 x 32 so that a few CTAs still finish their serial phases quickly
-static int fused_rows(dim3 grid) { return grid.x * grid.y >= 2 * 148 ? 8 : 32; }
+// One fused level launch (down: pre-smoothing, residual, restriction into the
+// coarse right-hand side `to`; up: coarse correction from `to`, post-smoothing)
+// with TT x TT tiles.
+template <int TT>
+static void fused_level(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
+                        dim3 blk, cudaStream_t st) {
+  const dim3 grid((L.ny + TT - 1) / TT, (L.nx + TT - 1) / TT);
+  const size_t sm = fused_smem(down ? 2 * nu + 2 : 2 * nu, TT);
+  float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x;
+#define ZB_FUSED(K) K<<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2)
+  if (down) {
+    switch (nu) {
+      case 1: ZB_FUSED((mg_down_kernel<1, TT>)); break;
+      case 2: ZB_FUSED((mg_down_kernel<2, TT>)); break;
+      case 3: ZB_FUSED((mg_down_kernel<3, TT>)); break;
+      default: ZB_FUSED((mg_down_kernel<4, TT>)); break;
+    }
+  } else {
+    switch (nu) {
+      case 1: ZB_FUSED((mg_up_kernel<1, TT>)); break;
+      case 2: ZB_FUSED((mg_up_kernel<2, TT>)); break;
+      case 3: ZB_FUSED((mg_up_kernel<3, TT>)); break;
+      default: ZB_FUSED((mg_up_kernel<4, TT>)); break;
+    }
+  }
+#undef ZB_FUSED
+}
+
+// 32 x 32 tiles with 32 x 8 threads when the level has two tiles for every
+// SM; else 16 x 16 tiles with 16 x 32 threads (four times the CTAs, one
+// staged row per thread and phase), so that the few CTAs of a small level
+// finish their serial phases sooner
+static void fused(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
+                  cudaStream_t st) {
+  const bool big = ((L.ny + FT - 1) / FT) * ((L.nx + FT - 1) / FT) >= 2 * 148;
+  if (big) fused_level<FT>(down, nu, L, fw, to, idx2, dim3(32, 8), st);
+  else fused_level<FTS>(down, nu, L, fw, to, idx2, dim3(FTS, 32), st);
+}
 
 static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, cudaStream_t st) {
   float* fw = (float*)((char*)ws + P.fbase);
@@ -974,17 +1015,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
       restrict_kernel<<<grid_for((long long)Lc.nx * Lc.ny), NT, 0, st>>>(fw + L.r, fw + Lc.f,
                                                                           Lc.nx, Lc.ny);
     } else {
-      const dim3 grid((L.ny + FT - 1) / FT, (L.nx + FT - 1) / FT);
-      const dim3 blk(32, fused_rows(grid));
-      const size_t sm = fused_smem(2 * P.nu + 2);
-      float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x,
-            *a5 = fw + Lc.f;
-      switch (P.nu) {
-        case 1: mg_down_kernel<1><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-        case 2: mg_down_kernel<2><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-        case 3: mg_down_kernel<3><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-        default: mg_down_kernel<4><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-      }
+      fused(true, P.nu, L, fw, fw + Lc.f, idx2, st);
     }
   }
   if (P.small0 < P.nlev) {
@@ -1016,17 +1047,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 0, (void*)st);
       if (rc) return rc;
     } else {
-      const dim3 grid((L.ny + FT - 1) / FT, (L.nx + FT - 1) / FT);
-      const dim3 blk(32, fused_rows(grid));
-      const size_t sm = fused_smem(2 * P.nu);
-      float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x,
-            *a5 = fw + Lc.x;
-      switch (P.nu) {
-        case 1: mg_up_kernel<1><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-        case 2: mg_up_kernel<2><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-        case 3: mg_up_kernel<3><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-        default: mg_up_kernel<4><<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, a5, L.nx, L.ny, idx2); break;
-      }
+      fused(false, P.nu, L, fw, fw + Lc.x, idx2, st);
     }
   }
   if (precond == 2) {

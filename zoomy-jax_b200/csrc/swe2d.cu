@@ -1394,9 +1394,11 @@ struct SideStream {
 static int side_stream(SideStream** out) {
   static SideStream ss[32];
   static unsigned made = 0u;
+  static std::mutex mu;   // host threads that set up solvers at once share one stream per device
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 32) return ZB_E_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(mu);
   if (!(made & (1u << dev))) {
     ZB_CUDA_TRY(cudaStreamCreateWithFlags(&ss[dev].s, cudaStreamNonBlocking));
     ZB_CUDA_TRY(cudaEventCreateWithFlags(&ss[dev].fork, cudaEventDisableTiming));
