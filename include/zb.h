@@ -202,6 +202,15 @@ int zb_swe2d_mass(const zb_swe2d_cfg* cfg, const void* Q, double* partial,
 int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux,
                  zb_stream_t stream);
 
+/* Diagnostic with no counterpart in the reference: the float64 quotient
+ * a[i] / b[i], square root sqrt(b[i]) and reciprocal square root
+ * 1 / sqrt(b[i]) as the float64 shallow-water kernels compute them (Newton
+ * refinement of the hardware approximations), into out[0..n), out[n..2n) and
+ * out[2n..3n) (device pointers; b > 0), for their accuracy test against IEEE
+ * arithmetic. */
+int zb_newton_check_f64(const double* a, const double* b, double* out, int64_t n,
+                        zb_stream_t stream);
+
 /* ── batched ensemble of Cartesian instances ─────────────────────────────── */
 
 /* One independent instance of the ensemble (host description).  Its state

@@ -161,7 +161,7 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R, T sg
   const T unL = sg * (AXIS == 0 ? L.ux : L.uy);
   const T unR = sg * (AXIS == 0 ? R.ux : R.uy);
   if (RIEMANN == ZB_RIEMANN_RUSANOV) {
-    const T cL = sqrt(g * L.h), cR = sqrt(g * R.h);
+    const T cL = asqrt(g * L.h), cR = asqrt(g * R.h);
     const T s = fmx(fabs(unL) + cL, fabs(unR) + cR);
     const T qnL = sg * (AXIS == 0 ? L.qx : L.qy);
     const T qnR = sg * (AXIS == 0 ? R.qx : R.qy);
@@ -179,7 +179,7 @@ __device__ __forceinline__ void riemann(const Side<T>& L, const Side<T>& R, T sg
   const T bs = fmx(L.b, R.b);
   const T hLs = fmx(T(0), L.h + L.b - bs);
   const T hRs = fmx(T(0), R.h + R.b - bs);
-  const T cL = sqrt(g * hLs), cR = sqrt(g * hRs);
+  const T cL = asqrt(g * hLs), cR = asqrt(g * hRs);
   const T qLx = hLs * L.ux, qLy = hLs * L.uy;
   const T qRx = hRs * R.ux, qRy = hRs * R.uy;
   const T FLh = hLs * unL, FRh = hRs * unR;
@@ -556,7 +556,7 @@ __device__ __forceinline__ void stage_tile(
         // solver2 adds the source to the stage residual at Qk with the step's
         // aux (solver2/blocks.py:241-287, march.py:120-124)
         const T hi = hinv_src[k];
-        const T qn = sqrt(qxk * qxk + qyk * qyk);
+        const T qn = asqrt(qxk * qxk + qyk * qyk);
         const T kf = (-p.g) * (p.manning_n * p.manning_n) * qn * (hi * hi) * cbrt(hi);
         sqx = dqx + qxk * kf;
         sqy = dqy + qyk * kf;
@@ -576,7 +576,7 @@ __device__ __forceinline__ void stage_tile(
       // (zoomy_jax/fvm/solver_jax.py:1129; ode.py:14-18)
       const T h0 = (MODE == MODE_STEP2) ? h0P[k] : hk;
       const T hi0 = kp_hinv(h0, p.eps_kp);
-      const T qn = sqrt(qxn * qxn + qyn * qyn);
+      const T qn = asqrt(qxn * qxn + qyn * qyn);
       const T kf = (-p.g) * (p.manning_n * p.manning_n) * qn * (hi0 * hi0) * cbrt(hi0);
       if (p.implicit_source) {
         const T den = T(1) + dt * (-kf);
@@ -596,7 +596,7 @@ __device__ __forceinline__ void stage_tile(
     if (trouble_out != nullptr) trouble_out[k] = tr ? 1 : 0;
     if (MODE == MODE_STEP2 || MODE == MODE_EULER) {
       const T hi = kp_hinv(hn, p.eps_kp);
-      const T c = sqrt(g * fmx(hn, T(0)));
+      const T c = asqrt(g * fmx(hn, T(0)));
       const T lx = fabs(qxn * hi) + c, ly = fabs(qyn * hi) + c;
       amax_loc = nmax(amax_loc, (double)nmax(lx, ly));
     }
@@ -1245,7 +1245,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
         qyn = half * (qy0 + qy2);
         if (p.manning_n != T(0)) {
           const T hi0 = kp_hinv(h0, p.eps_kp);
-          const T qn = sqrt(qxn * qxn + qyn * qyn);
+          const T qn = asqrt(qxn * qxn + qyn * qyn);
           const T kf = (-p.g) * (p.manning_n * p.manning_n) * qn * (hi0 * hi0) * cbrt(hi0);
           if (p.implicit_source) {
             const T den = T(1) + dt * (-kf);
@@ -1267,7 +1267,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       bad = bad || !(hn >= T(0)) || !(chk - chk == T(0));
       if (MODE == MODE_STEP2) {
         const T hi = kp_hinv(hn, p.eps_kp);
-        const T c = sqrt(g * fmx(hn, T(0)));
+        const T c = asqrt(g * fmx(hn, T(0)));
         const T lx = fabs(qxn * hi) + c, ly = fabs(qyn * hi) + c;
         amax_loc = nmax(amax_loc, nmax(lx, ly));
       }
@@ -1525,7 +1525,7 @@ ens_amax_kernel(const EnsDesc<T>* __restrict__ desc, const T* __restrict__ Q, zb
     for (size_t k = threadIdx.x; k < C; k += NT) {
       const T h = q[C + k];
       const T hi = kp_hinv(h, eps);
-      const T c = sqrt(g * nmax(h, T(0)));
+      const T c = asqrt(g * nmax(h, T(0)));
       m = nmax(m, (double)nmax(fabs(q[2 * C + k] * hi) + c, fabs(q[3 * C + k] * hi) + c));
     }
     __syncthreads();
@@ -1555,7 +1555,7 @@ swe2d_amax_kernel(const T* __restrict__ hP, const T* __restrict__ qxP,
        k += (size_t)gridDim.x * NT) {
     const T h = hP[k];
     const T hi = kp_hinv(h, eps_kp);
-    const T c = sqrt(g * nmax(h, T(0)));
+    const T c = asqrt(g * nmax(h, T(0)));
     const T lx = fabs(qxP[k] * hi) + c, ly = fabs(qyP[k] * hi) + c;
     m = nmax(m, (double)nmax(lx, ly));
   }
@@ -1669,7 +1669,7 @@ swe2d_source_kernel(T* __restrict__ qx, T* __restrict__ qy, const T* __restrict_
        k += (size_t)gridDim.x * NT) {
     const T hi0 = hinv0[k];
     T a = qx[k], b = qy[k];
-    const T qn = sqrt(a * a + b * b);
+    const T qn = asqrt(a * a + b * b);
     const T kf = (-g) * (n * n) * qn * (hi0 * hi0) * cbrt(hi0);
     if (implicit) {
       const T den = T(1) + dt * (-kf);
@@ -1681,6 +1681,19 @@ swe2d_source_kernel(T* __restrict__ qx, T* __restrict__ qy, const T* __restrict_
     }
     qx[k] = a;
     qy[k] = b;
+  }
+}
+
+// the float64 quotient, square root and reciprocal square root of the
+// kernels above, for their accuracy test (zb_newton_check_f64)
+__global__ void __launch_bounds__(NT)
+newton_check_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                    double* __restrict__ out, long long n) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n;
+       k += (long long)gridDim.x * NT) {
+    out[k] = ndiv(a[k], b[k]);
+    out[n + k] = nsqrt(b[k]);
+    out[2 * n + k] = nrsqrt(b[k]);
   }
 }
 
@@ -2250,6 +2263,15 @@ int zb_swe2d_aux(const zb_swe2d_cfg* cfg, const void* Q, void* Qaux, zb_stream_t
     swe2d_aux_kernel<double><<<blocks, NT, 0, st>>>((const double*)Q, (double*)Qaux, cfg->nx,
                                                     cfg->ny, cfg->wet_dry_eps,
                                                     make_lsq<double>(cfg->dx, cfg->dy));
+  return zb_launch_check();
+}
+
+int zb_newton_check_f64(const double* a, const double* b, double* out, int64_t n,
+                        zb_stream_t stream) {
+  if (!a || !b || !out || n < 0) return ZB_E_ARG;
+  if (n == 0) return ZB_OK;
+  const int blocks = (int)std::min<long long>((n + NT - 1) / NT, 148 * 8);
+  newton_check_kernel<<<blocks, NT, 0, (cudaStream_t)stream>>>(a, b, out, (long long)n);
   return zb_launch_check();
 }
 

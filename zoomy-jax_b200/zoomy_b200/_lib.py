@@ -122,6 +122,7 @@ SIGNATURES = [
     ("zb_swe2d_mass_partials", C.c_size_t, [_CFG]),
     ("zb_swe2d_mass", C.c_int, [_CFG, _P, _P, _P, _P]),
     ("zb_swe2d_aux", C.c_int, [_CFG, _P, _P, _P]),
+    ("zb_newton_check_f64", C.c_int, [_P, _P, _P, C.c_int64, _P]),
     ("zb_ens_table_bytes", C.c_size_t, [_CFG, _P, C.c_int, C.c_int]),
     ("zb_ens_prepare", C.c_int, [_CFG, _P, C.c_int, C.c_int, _P, C.c_size_t,
                                  C.POINTER(C.c_int)]),
