@@ -712,6 +712,7 @@ swe2d_stage_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
 constexpr int SX = 64;          // output rows per work item
 constexpr int SW = 28;          // output columns per strip
 constexpr int STRIP_NT = 128;   // four independent warps per CTA
+constexpr int SXC_MAX = 32;     // output rows of the longest column-EDGE item
 
 template <typename T>
 struct RowW {
@@ -835,6 +836,86 @@ __device__ __forceinline__ void faces_pair(const RowW<float>& R0, const RowW<flo
   Gh = Fh2.y; Gx = Ft2.y; fyl_t = fl.y; fyr_own = fr.y;
 }
 
+// Column-EDGE pre-pass for one row: the boundary column's cell (m, c), c = 0
+// (low side) or ny - 1, m two cells or more from the x boundaries.  out[0..8):
+// its limited slopes [sx0..3, sy0..3] (the EDGE body's side-class closed form,
+// limiter, dry demotion and ties); out[8..12): Gh, Gx, fyl_t, fyr_own of its
+// boundary y-face (the owner's trace against its ghost with normal sign sgy),
+// as the EDGE body leaves them on the lane that evaluates that face (cj = -1
+// for the low side, cj = ny - 1 for the high side).
+template <typename T, int RECON, int RIEMANN>
+__device__ __forceinline__ void bcol_row(const T* __restrict__ bP, const T* __restrict__ hP,
+                                         const T* __restrict__ qxP, const T* __restrict__ qyP,
+                                         const SweParams<T>& p, int m, int c, T* out) {
+  const int ny = p.ny;
+  const bool lo = c == 0;
+  const int ci = lo ? 1 : ny - 2;
+  RowW<T> Wc[3], Wi[3];   // rows m - 1, m, m + 1 of column c and of its inner neighbour ci
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const size_t k = (size_t)(m - 1 + a) * ny + (s ? ci : c);
+      const T vb = bP[k], vh = hP[k], vqx = qxP[k], vqy = qyP[k];
+      RowW<T>& w = s ? Wi[a] : Wc[a];
+      const T hinv = kp_hinv(vh, p.eps_kp);
+      w.b = vb;
+      w.h = vh;
+      w.hinv = hinv;
+      if (RECON == ZB_RECON_ETA) {
+        w.w1 = vb + vh; w.w2 = vqx * hinv; w.w3 = vqy * hinv;
+      } else {
+        w.w1 = vh; w.w2 = vqx; w.w3 = vqy;
+      }
+    }
+  }
+  const bool wall = p.bc[lo ? 2 : 3] == ZB_BC_WALL;
+  T gx[4], gy[4], phi[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const T u = Wc[1].w(v);
+    const T gyv = (wall && v == 3) ? -u : u;
+    const T n0 = Wi[0].w(v), n1 = Wi[1].w(v), n2 = Wi[2].w(v);
+    gx[v] = ((Wc[2].w(v) + n2) - (Wc[0].w(v) + n0)) * p.inv4dx;
+    const T sn = (n0 + n1) + n2;
+    gy[v] = (lo ? (sn - gyv) - T(2) * u : (gyv + T(2) * u) - sn) * p.inv4dy;
+    const T gg = T(2) * gyv - u;
+    const T umax = fmx(fmx(fmx(fmx(u, Wc[2].w(v)), Wc[0].w(v)), n1), gg);
+    const T umin = fmn(fmn(fmn(fmn(u, Wc[2].w(v)), Wc[0].w(v)), n1), gg);
+    phi[v] = limiter_phi(p.limiter, gx[v], gy[v], p.half_dx, p.half_dy, umax - u, umin - u,
+                         p.vk_eps2);
+  }
+  if (RECON == ZB_RECON_ETA) {
+    if (p.eps_wet >= T(0) && Wc[1].h < p.eps_wet) phi[0] = phi[1] = phi[2] = phi[3] = T(0);
+    phi[0] = zmin(phi[0], phi[1]);
+    phi[2] = zmin(phi[2], phi[1]);
+    phi[3] = zmin(phi[3], phi[1]);
+  }
+  T sy[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    out[v] = phi[v] * gx[v];
+    out[4 + v] = sy[v] = phi[v] * gy[v];
+  }
+  Side<T> O;
+  strip_trace<T, RECON>(Wc[1], sy, lo ? -p.half_dy : p.half_dy, O);
+  Side<T> G = O;
+  if (wall) {
+    G.qy = -O.qy;
+    G.uy = -O.uy;
+  }
+  const T sgy = lo ? T(-1) : T(1);
+  T Gh, Gx, Gy, Em, Ep;
+  riemann<T, RIEMANN, 1>(O, G, sgy, p.g, Gh, Gx, Gy, Em, Ep);
+  // the owner's cell-edge bed term: cesC of the high side, -cesD of the low
+  const T ces = T(0.5) * p.g * (Wc[1].h + O.h) * (O.b - Wc[1].b);
+  const T own_n = Gy + Em * sgy + ces * sgy;
+  out[8] = lo ? -Gh : Gh;
+  out[9] = lo ? -Gx : Gx;
+  out[10] = lo ? T(0) : own_n;
+  out[11] = lo ? own_n : T(0);
+}
+
 // One warp's work item: strip `strip` (28 output columns) over the output rows
 // [r0, r1) of the strip region p.fast_*.  EK selects the body:
 //   0  interior: every lane's cell two cells or more from every boundary;
@@ -845,9 +926,16 @@ __device__ __forceinline__ void faces_pair(const RowW<float>& R0, const RowW<flo
 //      expressions of stage_tile's boundary branches;
 //   2  column EDGE: the rows [r0 - 2, r1 + 2) lie inside the grid (r0 >= 2,
 //      r1 <= nx - 2) but the strip's lanes reach a boundary column: the
-//      interior body with guarded column loads, then the boundary column's
-//      slopes and its boundary y-face recomputed by the EDGE expressions on
-//      the lanes that hold them.
+//      interior body with guarded column loads; the boundary column's slopes
+//      and its boundary y-face by the EDGE expressions, recomputed on the
+//      lanes that hold them, row by row;
+//   3  column EDGE as 2, but for the paired float32 body the boundary
+//      columns' slopes and y-faces of every row of the item come from a
+//      pre-pass that evaluates them one row per lane (bcol_row) into shared
+//      memory: for long items (the ensemble's), whose march it frees of the
+//      one-lane row-by-row work; a short item's pre-pass is latency it cannot
+//      hide (measured on the single grid's 8-row items: 0.189 -> 0.211 ms per
+//      step, where the 32-row ensemble items gain 2.10 -> 1.92 ms).
 // `lead` (one item of the grid in full-coverage mode, where no tile kernel
 // runs) keeps the control block.
 template <typename T, int RECON, int RIEMANN, int MODE, int EK>
@@ -892,6 +980,27 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   // as paired float32 arithmetic (faces_pair)
   constexpr bool PAIR = std::is_same<T, float>::value && RECON == ZB_RECON_ETA &&
                         RIEMANN == ZB_RIEMANN_HLL_HR && !EDGE;
+  // column-EDGE with the paired body: the boundary columns' rows come from
+  // the pre-pass, slots [side][m - (r0 - 1)][12] of this warp (side 0: column
+  // 0, side 1: column ny - 1; rows r0 - 1 .. r1)
+  constexpr bool PRE = EK == 3 && PAIR;
+  constexpr int PROWS = SXC_MAX + 2;
+  T* bs = nullptr;
+  if constexpr (PRE) {
+    __shared__ T bsh[STRIP_NT / 32][2 * PROWS * 12];
+    bs = bsh[threadIdx.x >> 5];
+    const int cj0 = p.fast_j0 - 2 + strip * SW;
+    const int nrows = r1 - r0 + 2;   // <= SXC_MAX + 2 (full_items)
+    __syncwarp();                      // the warp's previous item is done with the slots
+    for (int side = 0; side < 2; ++side) {
+      const int c = side ? ny - 1 : 0;
+      if (!(cj0 <= c && c <= cj0 + 31)) continue;   // warp-uniform
+      for (int mm = lane; mm < nrows; mm += 32)
+        bcol_row<T, RECON, RIEMANN>(bP, hP, qxP, qyP, p, r0 - 1 + mm, c,
+                                    bs + (side * PROWS + mm) * 12);
+    }
+    __syncwarp();
+  }
 
   RowW<T> R0, R1, R2;                 // rows r-2, r-1, r
   T Sx0[4], Sx1[4], Sx2[4];           // (W(j-1) + W(j)) + W(j+1) of those rows
@@ -1012,7 +1121,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
         const bool bxl = EDGE && m == 0, bxh = EDGE && m == nx - 1;
         const bool byl = cj == 0, byh = cj == ny - 1;
         const bool bnd = cellv && (bxl || bxh || byl || byh);
-        if (__any_sync(0xffffffffu, bnd)) {
+        if (!PRE && __any_sync(0xffffffffu, bnd)) {   // PRE: the pre-pass slots
           const int cls = (bxl ? 0 : (bxh ? 2 : 1)) * 3 + (byl ? 0 : (byh ? 2 : 1));
           const T* wx = p.lsq.w[cls][0];
           const T* wy = p.lsq.w[cls][1];
@@ -1099,6 +1208,14 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
           slB[4 + v] = phi[v] * gya[v];
         }
       }
+      if constexpr (PRE) {
+        // the boundary column's cell of row r - 1 (pre-pass slot r - 1 - (r0 - 1))
+        if (cj == 0 || cj == ny - 1) {
+          const T* sl = bs + ((cj == 0 ? 0 : PROWS) + (r - r0)) * 12;
+#pragma unroll
+          for (int v = 0; v < 8; ++v) slB[v] = sl[v];
+        }
+      }
     }
     if (s < 3) continue;
     // x-face between rows r-2 (A, lower) and r-1 (B, upper)
@@ -1111,7 +1228,14 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
           fxh_p = Fh; fxt_p = Fy; fxr_p = fxr_n;
           continue;
         }
-        if (EK == 2 && (cj == -1 || cj == ny - 1)) {
+        if constexpr (PRE) {
+          // the y-face on the boundary (the lane below column 0, or column
+          // ny - 1) of row r - 2: pre-pass slot r - 2 - (r0 - 1)
+          if (cj == -1 || cj == ny - 1) {
+            const T* fo = bs + ((cj == -1 ? 0 : PROWS) + (r - 1 - r0)) * 12 + 8;
+            Gh = fo[0]; Gx = fo[1]; fyl_t = fo[2]; fyr_own = fo[3];
+          }
+        } else if (EK >= 2 && (cj == -1 || cj == ny - 1)) {
           // the y-face on the boundary (the lane below column 0, or column
           // ny - 1): the owner's trace against its ghost with normal sign sgy,
           // as the EDGE body evaluates it
@@ -1299,6 +1423,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
 // (2.094 ms per step; 8: 2.21; 16: 2.127; 64: 2.136).
 constexpr int SXC_GRID = 8;
 constexpr int SXC_ENS = 32;
+static_assert(SXC_GRID <= SXC_MAX && SXC_ENS <= SXC_MAX, "column-EDGE pre-pass rows");
 __host__ __device__ inline int full_items(int nx, int ny, int item, int* strip, int* r0,
                                           int* r1, int* kind, int sxc) {
   const int SXC = sxc;
@@ -1490,17 +1615,19 @@ __device__ __forceinline__ void ens_item(const EnsDesc<T>* d, T* Q, T* W, zb_ctr
         ctrl, phase, p, strip, r0, r1, lead);
 }
 
-// All instances' strip items of one body (EK, as strip_item): persistent warps
-// walk them.  The work list's header items[0] = {tile items, interior strip
-// items, EDGE strip items, column-EDGE strip items}; the lists follow it in
-// that order.  Each body is a launch of its own, so that the boundary bodies'
-// extra live values never raise another body's register allocation.
+// All instances' strip items of one body (EK, as strip_item: 0 interior, 1
+// EDGE, 3 column EDGE with its pre-pass): persistent warps walk them.  The
+// work list's header items[0] = {tile items, interior strip items, EDGE strip
+// items, column-EDGE strip items}; the lists follow it in that order.  Each
+// body is a launch of its own, so that the boundary bodies' extra live values
+// never raise another body's register allocation.
 template <typename T, int MODE, int EK>
 __global__ void __launch_bounds__(STRIP_NT, sizeof(T) == 4 ? 4 : 2)
 ens_strip_kernel(const EnsDesc<T>* __restrict__ desc, const int4* __restrict__ items, T* Q,
                  T* W, zb_ctrl* ctrls, int phase) {
+  static_assert(EK == 0 || EK == 1 || EK == 3, "ensemble bodies");
   const int4 hd = items[0];
-  const int4* list = items + 1 + hd.x + (EK >= 1 ? hd.y : 0) + (EK == 2 ? hd.z : 0);
+  const int4* list = items + 1 + hd.x + (EK >= 1 ? hd.y : 0) + (EK == 3 ? hd.z : 0);
   const int n = EK == 0 ? hd.y : (EK == 1 ? hd.z : hd.w);
   const int nw = gridDim.x * (STRIP_NT / 32);
   for (int it = blockIdx.x * (STRIP_NT / 32) + (threadIdx.x >> 5); it < n; it += nw) {
@@ -2079,14 +2206,14 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   ZB_CUDA_TRY(cudaStreamWaitEvent(side->s, side->fork, 0));
   // the column-EDGE items (longer) before the EDGE items on the second stream
   if (part == 0) {
-    ens_strip_kernel<T, MODE_STEP1, 2><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+    ens_strip_kernel<T, MODE_STEP1, 3><<<sgrid_e, STRIP_NT, 0, side->s>>>(
         desc, items, (T*)Q, (T*)W, ctrls, phase);
     ens_strip_kernel<T, MODE_STEP1, 1><<<sgrid_e, STRIP_NT, 0, side->s>>>(
         desc, items, (T*)Q, (T*)W, ctrls, phase);
     ens_strip_kernel<T, MODE_STEP1, 0><<<sgrid_i, STRIP_NT, 0, st>>>(desc, items, (T*)Q,
                                                                     (T*)W, ctrls, phase);
   } else {
-    ens_strip_kernel<T, MODE_STEP2, 2><<<sgrid_e, STRIP_NT, 0, side->s>>>(
+    ens_strip_kernel<T, MODE_STEP2, 3><<<sgrid_e, STRIP_NT, 0, side->s>>>(
         desc, items, (T*)Q, (T*)W, ctrls, phase);
     ens_strip_kernel<T, MODE_STEP2, 1><<<sgrid_e, STRIP_NT, 0, side->s>>>(
         desc, items, (T*)Q, (T*)W, ctrls, phase);
