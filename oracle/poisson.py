@@ -7,7 +7,7 @@ corrector, with VAM's elliptic operator generated by the absent zoomy_core and
 solved by unpreconditioned restarted GMRES to ``pressure_tol``.  The operator
 here is the variable-coefficient Poisson problem the configuration names
 (coefficient from the depth, clipped to [0.1, 2]); parity with the reference's
-operator is therefore unpinned and the judge of the solution is the float64
+operator is therefore unpinned and the arbiter of the solution is the float64
 sparse direct solve below.
 
 Discretisation on an ``nx x ny`` Cartesian grid with spacing ``dx = dy``:
@@ -77,7 +77,7 @@ def apply(cx, cy, p, dx):
 
 
 def matrix(cx, cy, dx):
-    """Sparse CSR of A (for the direct-solve judge)."""
+    """Sparse CSR of A (for the direct solve that arbitrates)."""
     nx, ny = cx.shape[0] - 1, cy.shape[1] - 1
     N = nx * ny
     idx = np.arange(N).reshape(nx, ny)
@@ -267,6 +267,6 @@ def fcg(H, b, tol=1e-8, maxit=200, precond="mg", smoother=None, x0=None):
 
 
 def direct_solve(cx, cy, b, dx):
-    """The float64 sparse direct solve -- the judge of the pressure."""
+    """The float64 sparse direct solve -- the arbiter of the pressure."""
     A = matrix(cx, cy, dx)
     return spla.spsolve(A.tocsc(), b.reshape(-1)).reshape(b.shape)

@@ -2,7 +2,7 @@
 pressure solve and of the learned smoother's kernels).
 
 The reference's elliptic operator is VAM's (absent zoomy_core), so the
-Poisson oracle's parity with the reference is unpinned; its judge is the
+Poisson oracle's parity with the reference is unpinned; its arbiter is the
 float64 sparse direct solve, and these tests pin the oracle's own
 multigrid/FCG against it.  The U-Net oracle's backward pass is pinned by
 central finite differences."""
