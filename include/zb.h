@@ -111,9 +111,12 @@ size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg);
 
 /* Initialise the control block for a march starting at time t0 from state Q:
  * clears status and all slots, sets t[phase] = t0 and amax[phase] = the
- * maximum wave speed of Q.  Also creates, once per device, the library's
- * second stream that the fused step forks its boundary-strip launch onto
- * (call it outside stream capture; the steps themselves capture).
+ * maximum wave speed of Q.  Also creates, once per device and host thread,
+ * the library's second stream that the fused step forks its boundary-strip
+ * launch onto (call it outside stream capture, on the thread that will step
+ * or capture; the steps themselves capture).  Each host thread has its own
+ * second stream and fork / join events, so host threads may step different
+ * solvers on one device at once.
  * Replaces the first dt_pass (zoomy_jax/fvm/solver2/blocks.py:36-61). */
 int zb_swe2d_init(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl,
                   int phase, double t0, zb_stream_t stream);
@@ -153,7 +156,9 @@ int zb_swe2d_step(const zb_swe2d_cfg* cfg, void* Q, void* workspace,
  * array and it keeps the last call's contents (the step overwrites every
  * scratch cell it reads, so nothing needs clearing); calls that overlap on
  * the GPU -- concurrent streams, or several host threads on one device --
- * race on it and must be serialised by the caller. */
+ * race on it and must be serialised by the caller.  The looked-up address is
+ * kept for the life of the process: do not use the library across a
+ * cudaDeviceReset. */
 int zb_swe2d_step_noalloc(const zb_swe2d_cfg* cfg, void* Q, zb_ctrl* ctrl,
                           int phase, zb_stream_t stream);
 
@@ -234,10 +239,11 @@ size_t zb_ens_table_bytes(const zb_swe2d_cfg* common,
                           const zb_ens_instance* inst, int n_inst, int tile_x);
 
 /* Build the per-instance parameter blocks (spacing, least-squares weights,
- * Manning, t_end) and the work list, and copy them to the device table
- * (synchronous host-to-device copies: call at set-up, outside stream
- * capture).  The work list holds every instance's (instance, strip, row
- * chunk) items of the single grid's full-coverage list (interior, boundary-
+ * Manning, t_end) and the work list, and copy them to the device table.  The
+ * call waits for all work on the current device before it copies (a table
+ * that steps in flight still read is not overwritten under them) and returns
+ * once the copy has landed: call at set-up, outside stream capture.  The
+ * work list holds every instance's (instance, strip, row chunk) items of the single grid's full-coverage list (interior, boundary-
  * column and boundary-row bodies), and (instance, tile) items for grids
  * narrower than four cells.  *n_items_out receives the work-list length
  * (tiles + strips). */

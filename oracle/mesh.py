@@ -200,7 +200,14 @@ def create_1d(x0, x1, n):
              shape=(n,), spacing=(dx,), origin=(x0,))
     m.bf_partner = np.full(2, -1, dtype=np.int64)
     m.extra["periodic_partner"] = lambda k, b: (n - 1 if k == 0 else 0)
+    # interior cells: the two face neighbours; an end cell, which has only one,
+    # takes the next cell beyond it as well (one-sided pair + its boundary
+    # ghost) -- pinned by the derivative rows of the reference's bc_wall,
+    # bc_periodic and bc_inflow goldens (tests/runtime/test_bc_runtime.py).
     nbrs = [[j for j in (i - 1, i + 1) if 0 <= j < n] for i in range(n)]
+    if n >= 3:
+        nbrs[0] = [1, 2]
+        nbrs[n - 1] = [n - 2, n - 3]
     _lsq_weights(m, nbrs)
     _cell_faces(m)
     return m

@@ -46,7 +46,8 @@ class Scheme:
     eps_wet: Optional[float] = None      # eta: dry-cell demotion (emitted wet_dry_eps)
     positivity: Optional[str] = None     # eta: None | "zhang_shu"
     front_tol: Optional[float] = None    # eta: front pre-detector
-    mood: bool = False                   # a-posteriori per-cell order-1 redo
+    mood: bool = False                   # a-posteriori order-1 redo
+    mood_mode: str = "cell"              # cell: demote the troubled cells | step: whole step
     cfl: float = 0.9
     dt_max: float = np.inf
     degree: int = 0                      # (2k+1) factor of the CFL law
@@ -555,7 +556,11 @@ def step(mesh, Q, dt, params, scheme, kind=None, return_troubled=False):
     Qn = advance(None)
     trouble = troubled_cells(Qn)
     if scheme.mood and trouble.any():
-        Qn = advance(trouble)
+        # production MOOD demotes the troubled cells (solver_jax.py:1055-1071);
+        # solver2's sanctioned body redoes the whole step at order 1 with the
+        # same stage loop (solver2/blocks.py:304-323)
+        Qn = advance(trouble if scheme.mood_mode == "cell"
+                     else np.ones(Q.shape[1], dtype=bool))
     if params.manning_n != 0.0:
         if scheme.source == "implicit":
             # point-implicit Manning (IMEX local implicit source,

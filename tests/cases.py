@@ -24,3 +24,9 @@ def gaussian_pulse_2d(x):
 
 
 from zoomy_b200.workloads import bumps, circular_dam_state  # noqa: E402,F401
+
+
+def tilted_ic(x):
+    """The reference's tilted free surface on [0, 1] (its ``tests/cases.py``
+    ``tilted_ic``), the initial state of the BC goldens."""
+    return np.array([0.0, 0.5 + 0.05 * (float(x) - 0.5), 0.0])

@@ -413,24 +413,60 @@ def test_march_solver_matches_hyperbolic_solver():
     assert err.max() <= 1e-13, err
 
 
-def test_mood_redo_matches_oracle():
-    """Per-cell MOOD (production): with a dt three times the CFL limit the
-    order-2 candidate goes negative at the dry front; the troubled cells are
-    demoted to first order and the step is re-run, as the oracle does."""
-    domain = (0.0, 1.0, 0.0, 1.0)
-    m = zb.create_2d(domain, 48, 48)
+def _island_under_flow(n):
+    """A Gaussian island (peak 0.8) that emerges from a 0.5-deep layer moving
+    in x: with the eta reconstruction and no dry-cell demotion the order-2
+    candidate leaves negative depth at the island's shore at the plain CFL dt
+    (the oracle troubles 32 cells of 48^2)."""
+    m = zb.create_2d((0.0, 1.0, 0.0, 1.0), n, n)
     xc = m.cell_centers()
     Q0 = np.zeros((4, m.n_cells))
-    Q0[1] = np.where(xc[0] < 0.5, 1.0, 0.0)
+    Q0[0] = 0.8 * np.exp(-((xc[0] - 0.5) ** 2 + (xc[1] - 0.5) ** 2) / 0.02)
+    Q0[1] = np.maximum(0.5 - Q0[0], 0.0)
+    Q0[2] = 0.5 * Q0[1]
+    return Q0
+
+
+def test_mood_redo_matches_oracle():
+    """Per-cell MOOD (production ``solver_jax.py:1055-1071``): the troubled
+    cells of the order-2 candidate are demoted to first order and the step is
+    re-run.  The case troubles cells by construction (asserted first)."""
+    domain = (0.0, 1.0, 0.0, 1.0)
+    Q0 = _island_under_flow(48)
     solver, Q, Qaux, om, scheme, params = make(48, 48, domain, Q0, mood=True)
     q0 = Q.double().cpu().numpy()
-    dt = 3.0 * OS.compute_dt(om, q0, params, scheme)
+    dt = OS.compute_dt(om, q0, params, scheme)
     ref_plain, trouble = OS.step(om, q0, dt, params,
                                  OS.Scheme(**{**scheme.__dict__, "mood": False}),
                                  return_troubled=True)
-    if not trouble.any():
-        pytest.skip("no troubled cell at this dt")
+    assert trouble.sum() > 0 and ref_plain[1].min() < 0.0
     got = solver.step(dt, 0.0, Q, Qaux).double().cpu().numpy()
     ref = OS.step(om, q0, dt, params, scheme)
     assert rel_err(got, ref).max() <= 1e-12
+    assert got[1].min() >= 0.0
     assert not np.allclose(got, ref_plain)
+    # mass is conserved through the redo (shared face fluxes)
+    assert abs(got[1].sum() - q0[1].sum()) <= 1e-12 * q0[1].sum()
+
+
+def test_march_solver_whole_step_redo_matches_oracle():
+    """solver2's MOOD (``solver2/blocks.py:304-323``): when any cell is
+    troubled the whole step is replayed with the constant reconstruction
+    through the same SSP-RK2 stage loop."""
+    domain = (0.0, 1.0, 0.0, 1.0)
+    Q0 = _island_under_flow(48)
+    _, _, _, om, scheme, params = make(48, 48, domain, Q0, mood=True)
+    model = zb.ShallowWater2D(boundary_conditions={t: "wall" for t in TAGS},
+                              initial_conditions=Q0)
+    nsm = zb.NumericalSystemModel.from_system_model(
+        model, zb.ReconstructionSpec(2, "minmod"), "hll_hr")
+    ms = MarchSolver(mood_redo=True, reconstruction_variables="eta", free_surface_h_index=1)
+    S = ms.setup_march(zb.create_2d(domain, 48, 48), nsm, CFL=0.45)
+    _, _, dt = ms.step_head(S)
+    assert dt == pytest.approx(OS.compute_dt(om, Q0, params, scheme), rel=1e-14)
+    S1, troubled = ms.hyperbolic_step(S, dt)
+    assert troubled
+    ref = OS.step(om, Q0, dt, params, OS.Scheme(**{**scheme.__dict__, "mood_mode": "step"}))
+    got = S1.Q.double().cpu().numpy()
+    assert rel_err(got, ref).max() <= 1e-12
+    assert got[1].min() >= 0.0

@@ -24,8 +24,11 @@ INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -prec-div/-prec-sqrt/-ftz affect single precision only: the float kernels
-# use fast division and square root (stated tolerance), the double kernels stay
-# IEEE (float64 parity with the oracle to 1e-12)
+# use fast division and square root (stated tolerance).  These flags leave
+# double arithmetic IEEE; the Cartesian float64 kernels nonetheless divide and
+# take square roots through their own Newton-refined routines (ndiv / nsqrt /
+# nrsqrt in csrc/common.cuh, within 1 ulp of IEEE), and float64 parity with
+# the oracle stays at 1e-12
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-prec-div=false", "-prec-sqrt=false", "-ftz=true",
          "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]

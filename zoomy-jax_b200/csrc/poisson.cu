@@ -25,6 +25,7 @@
 // y-faces (nx, ny+1) at i*(ny+1) + j.
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 
@@ -861,10 +862,10 @@ static size_t coarse_smem(const Plan& P) {
 // opt the one-CTA kernel into the full 227 KB of shared memory (once per
 // device; called from set-up, never inside a stream capture)
 static int enable_coarse_smem() {
-  static unsigned set_mask = 0u;
+  static std::atomic<unsigned> set_mask{0u};
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 32 && !(set_mask & (1u << dev))) {
+  if (dev >= 0 && dev < 32 && !(set_mask.load() & (1u << dev))) {
     ZB_CUDA_TRY(cudaFuncSetAttribute(coarse_vcycle_kernel,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
 #define ZB_SMEM_ATTR(K) \
@@ -878,7 +879,7 @@ static int enable_coarse_smem() {
     ZB_SMEM_ATTR((mg_up_kernel<1, FTS>)); ZB_SMEM_ATTR((mg_up_kernel<2, FTS>));
     ZB_SMEM_ATTR((mg_up_kernel<3, FTS>)); ZB_SMEM_ATTR((mg_up_kernel<4, FTS>));
 #undef ZB_SMEM_ATTR
-    set_mask |= 1u << dev;
+    set_mask.fetch_or(1u << dev);
   }
   return ZB_OK;
 }

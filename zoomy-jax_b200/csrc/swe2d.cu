@@ -25,6 +25,7 @@
 #include <cstring>
 #include <cmath>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <type_traits>
 #include <vector>
@@ -1511,19 +1512,22 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
 }
 
 // A second stream per device with a fork and a join event: the EDGE launch of
-// a full-coverage stage runs on it beside the interior launch.
+// a full-coverage stage runs on it beside the interior launch.  Each host
+// thread has its own (thread_local), so the fork / join records of calls from
+// different threads never interleave and a stream capture on one thread never
+// pulls in another thread's launches.  Calls from one thread are ordered by
+// the host; on the side stream they run in call order, whatever the caller's
+// stream.
 struct SideStream {
   cudaStream_t s;
   cudaEvent_t fork, join;
 };
 static int side_stream(SideStream** out) {
-  static SideStream ss[32];
-  static unsigned made = 0u;
-  static std::mutex mu;   // host threads that set up solvers at once share one stream per device
+  thread_local SideStream ss[32];
+  thread_local unsigned made = 0u;
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev >= 32) return ZB_E_UNSUPPORTED;
-  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 32) return ZB_E_UNSUPPORTED;
   if (!(made & (1u << dev))) {
     ZB_CUDA_TRY(cudaStreamCreateWithFlags(&ss[dev].s, cudaStreamNonBlocking));
     ZB_CUDA_TRY(cudaEventCreateWithFlags(&ss[dev].fork, cudaEventDisableTiming));
@@ -1946,13 +1950,13 @@ static int launch_stage(const zb_swe2d_cfg* c, const T* b, const T* h, const T* 
                         unsigned char* trouble_out = nullptr) {
   auto kern = swe2d_stage_kernel<T, TX, ORDER, RECON, RIEMANN, MODE>;
   const size_t sm = sizeof(Smem<T, TX>);
-  static unsigned attr_mask = 0u;   // per instantiation, one bit per device
+  static std::atomic<unsigned> attr_mask{0u};   // per instantiation, one bit per device
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev >= 32) return ZB_E_UNSUPPORTED;
-  if (!(attr_mask & (1u << dev))) {
+  if (dev < 0 || dev >= 32) return ZB_E_UNSUPPORTED;
+  if (!(attr_mask.load() & (1u << dev))) {
     ZB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    attr_mask |= 1u << dev;
+    attr_mask.fetch_or(1u << dev);
   }
   dim3 grid((c->ny + TY - 1) / TY, (c->nx + TX - 1) / TX);
   if (p.fast_i1 > p.fast_i0)
@@ -2187,14 +2191,17 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   const size_t sm = sizeof(Smem<T, TX>);
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev >= 32) return ZB_E_UNSUPPORTED;
-  static int sms_cache[32] = {0};
-  if (!sms_cache[dev])
-    ZB_CUDA_TRY(cudaDeviceGetAttribute(&sms_cache[dev], cudaDevAttrMultiProcessorCount, dev));
+  if (dev < 0 || dev >= 32) return ZB_E_UNSUPPORTED;
+  static std::atomic<int> sms_cache[32];
+  if (!sms_cache[dev].load()) {
+    int v = 0;
+    ZB_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    sms_cache[dev].store(v);
+  }
   // boundary strips, interior strips (persistent warps over their items; a
   // grid that finds none exits at once), then the tiles of grids too small
   // for strips
-  const int sgrid_e = sms_cache[dev] * (sizeof(T) == 4 ? 4 : 2);
+  const int sgrid_e = sms_cache[dev].load() * (sizeof(T) == 4 ? 4 : 2);
   const int sgrid_i = sgrid_e;
   // the boundary items on the library's second stream, beside the interior ones
   SideStream* side = nullptr;
@@ -2225,13 +2232,13 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   ZB_CUDA_TRY(cudaStreamWaitEvent(st, side->join, 0));
   // the tile fallback (grids narrower than four cells; its CTAs exit at once
   // when the work list holds no tile items)
-  static unsigned mask1 = 0u;
+  static std::atomic<unsigned> mask1{0u};
   auto k1 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP1>;
   auto k2 = ens_stage_kernel<T, TX, 2, ZB_RECON_ETA, ZB_RIEMANN_HLL_HR, MODE_STEP2>;
-  if (!(mask1 & (1u << dev))) {
+  if (!(mask1.load() & (1u << dev))) {
     ZB_CUDA_TRY(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     ZB_CUDA_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    mask1 |= 1u << dev;
+    mask1.fetch_or(1u << dev);
   }
   if (grid <= 0) {
     int per_sm = 0, sms = 0;
@@ -2506,10 +2513,14 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
     items.insert(items.end(), estrips.begin(), estrips.end());
     items.insert(items.end(), cstrips.begin(), cstrips.end());
     const size_t db = ens_desc_bytes<T>(n_inst);
+    // the table may still be read by steps in flight on any stream: wait for
+    // the device, copy, and return only once the copy has landed
+    ZB_CUDA_TRY(cudaDeviceSynchronize());
     ZB_CUDA_TRY(cudaMemcpy(table, desc.data(), desc.size() * sizeof(EnsDesc<T>),
                            cudaMemcpyHostToDevice));
     ZB_CUDA_TRY(cudaMemcpy((char*)table + db, items.data(), items.size() * sizeof(int4),
                            cudaMemcpyHostToDevice));
+    ZB_CUDA_TRY(cudaDeviceSynchronize());
     *n_items_out = (int)items.size() - 1;
     return ZB_OK;
   };

@@ -28,6 +28,7 @@
 
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 #include "conv_tc.cuh"
@@ -466,15 +467,15 @@ static int g_conv_impl = 1;
 static __device__ unsigned g_unet_err;
 
 static unsigned* unet_err_word() {
-  static unsigned* ptrs[64] = {nullptr};
+  static std::atomic<unsigned*> ptrs[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  if (!ptrs[dev]) {
+  if (!ptrs[dev].load()) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_unet_err) != cudaSuccess) return nullptr;
-    ptrs[dev] = (unsigned*)p;
+    ptrs[dev].store((unsigned*)p);
   }
-  return ptrs[dev];
+  return ptrs[dev].load();
 }
 
 static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin,
@@ -484,16 +485,20 @@ static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin
   if (coutp > 256 || cinp > 256) return ZB_E_UNSUPPORTED;
   int cols = 32;
   while (cols < coutp) cols *= 2;
-  static int sms[64] = {0};
-  static bool attr[64] = {false};
+  static std::atomic<int> sms[64];
+  static std::atomic<bool> attr[64];
   int dev = 0;
   ZB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return ZB_E_CUDA;
-  if (!sms[dev]) ZB_CUDA_TRY(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
-  if (!attr[dev]) {
+  if (!sms[dev].load()) {
+    int v = 0;
+    ZB_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    sms[dev].store(v);
+  }
+  if (!attr[dev].load()) {
     ZB_CUDA_TRY(cudaFuncSetAttribute(conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024));
-    attr[dev] = true;
+    attr[dev].store(true);
   }
   // resident CTAs of one SM must never ask for more than its 512 TMEM
   // columns: pad the shared memory so that at most 512 / cols fit
