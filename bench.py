@@ -21,7 +21,8 @@ cannot be installed: it needs jax and zoomy_core, absent here) on the host's
 cores: one process per core, each stepping a 256 x 256 sample of the same
 workload; rank 0 only.
 
-At N = 1 the same JSON line also reports the other configurations: "chorin"
+At N = 1 the same JSON line also reports the other configurations: "fp64"
+(the same 2048^2 step with a float64 state), "chorin"
 (1024^2 Chorin steps at a 1e-8 pressure residual, plain multigrid FCG against
 the learned U-Net smoother), "ensemble" (512 uneven instances, boundary and
 interior strip launches per stage), "triangles" (about 4M Delaunay triangles,
@@ -144,7 +145,46 @@ def run_cpu(warmup, steps, n=CPU_SAMPLE_N, procs=None):
 
 
 # ── clocks ──────────────────────────────────────────────────────────────────
+# A child process polls NVML (query only: SM clock, its maximum and the active
+# clock-event reasons) every millisecond and prints one line per sample with a
+# CLOCK_MONOTONIC stamp; the parent marks the timed region on the same clock.
+# A separate process keeps the polling off the launching thread's interpreter.
+_NVML_POLLER = r"""
+import sys, time
+import pynvml as N
+N.nvmlInit()
+key = sys.argv[1]
+h = (N.nvmlDeviceGetHandleByUUID(key) if key.startswith("GPU-")
+     else N.nvmlDeviceGetHandleByPciBusId(key))
+reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+    N.nvmlDeviceGetCurrentClocksThrottleReasons
+mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+out = sys.stdout
+while True:
+    t = time.monotonic()
+    sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+    r = reasons(h)
+    out.write(f"{t:.6f} {sm} {mx} {r}\n")
+    out.flush()
+    time.sleep(0.001)
+"""
+
+# NVML clock-event reason bits (nvml.h)
+_REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+
+
 class ClockSampler:
+    """SM clocks and throttle reasons DURING the timed region.
+
+    ``start()`` launches the NVML poller for the torch device ``index`` (found
+    by UUID, else by PCI bus id) and waits for its first sample; ``mark()``
+    stamps the start and the end of the timed region; ``stop()`` ends the
+    poller.  ``summary()`` reports the samples inside the region; a region too
+    short to hold one (20 steps of 0.2 ms) reports the nearest sample on each
+    side and says so.  Without NVML it falls back to ``nvidia-smi -lms 50``
+    over the whole bracket."""
+
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -153,34 +193,105 @@ class ClockSampler:
         self.index = index
         self.path = path
         self.proc = None
-        self.lines = []
+        self.kind = None
+        self.samples = []       # (t, sm, max, reasons bitmask)
+        self.smi_lines = []
+        self.window = [None, None]
 
-    def __enter__(self):
+    def _device_key(self):
+        import torch
+        p = torch.cuda.get_device_properties(self.index)
+        u = str(getattr(p, "uuid", "") or "")
+        if u:
+            return u if u.startswith("GPU-") else "GPU-" + u
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+
+    def start(self):
+        try:
+            import pynvml  # noqa: F401
+            key = self._device_key()
+            self.proc = subprocess.Popen([sys.executable, "-c", _NVML_POLLER, key],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True, bufsize=1)
+            import select
+            ready, _, _ = select.select([self.proc.stdout], [], [], 20.0)
+            first = self.proc.stdout.readline() if ready else ""
+            if first.strip():
+                self.kind = "nvml"
+                self._lines = [first]
+                return self
+            self.proc.kill()
+            self.proc.wait()
+        except Exception:
+            self.proc = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                  "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.kind = "nvidia-smi"
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
 
-    def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+    def mark(self, which):
+        self.window[0 if which == "start" else 1] = time.monotonic()
+
+    def stop(self):
+        if self.proc is None:
+            return
+        time.sleep(0.01)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        if self.kind == "nvml":
+            for ln in self._lines + out.splitlines():
+                f = ln.split()
+                if len(f) == 4:
+                    try:
+                        self.samples.append((float(f[0]), float(f[1]), float(f[2]), int(f[3])))
+                    except ValueError:
+                        pass
             if self.path:
-                pathlib.Path(self.path).write_text("\n".join(self.lines) + "\n")
+                pathlib.Path(self.path).write_text(
+                    "t_monotonic,sm_mhz,sm_max_mhz,reasons\n" +
+                    "".join(f"{t:.6f},{a:.0f},{b:.0f},{r:#x}\n" for t, a, b, r in self.samples))
+        else:
+            self.smi_lines = [ln for ln in out.splitlines() if ln.strip()]
+            if self.path:
+                pathlib.Path(self.path).write_text("\n".join(self.smi_lines) + "\n")
+
+    def __enter__(self):
+        self.start()
+        self.mark("start")
+        return self
+
+    def __exit__(self, *exc):
+        self.mark("end")
+        self.stop()
 
     def summary(self):
+        if self.kind == "nvml" and self.samples:
+            t0, t1 = self.window
+            inside = [s for s in self.samples if t0 is not None and t0 <= s[0] <= (t1 or t0)]
+            where = "inside the timed region"
+            if not inside:
+                before = [s for s in self.samples if s[0] < t0]
+                after = [s for s in self.samples if s[0] > (t1 or t0)]
+                inside = before[-1:] + after[:1]
+                where = ("the nearest sample on each side of the timed region "
+                         f"({(t1 - t0) * 1e3:.1f} ms, shorter than the 1 ms poll)")
+            reasons = sorted({nm for _, _, _, r in inside for nm, b in _REASON_BITS.items()
+                              if r & b})
+            return {"sm_mhz": statistics.median(s[1] for s in inside),
+                    "sm_max_mhz": inside[-1][2], "reasons": reasons,
+                    "samples": len(inside), "source": "NVML, " + where}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.smi_lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -195,7 +306,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 # ── GPU leg ──────────────────────────────────────────────────────────────────
@@ -226,7 +337,7 @@ def whole_job_rate(cells_per_rank, steps, seconds_max, world):
     return world * cells_per_rank * steps / seconds_max
 
 
-def run_gpu(args, rank, world, local_rank):
+def run_gpu(args, rank, world, local_rank, dtype_key=None, with_e2e=True):
     import ctypes as C
     import numpy as np
     import torch
@@ -238,7 +349,8 @@ def run_gpu(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     n = args.n
     C_cells = n * n
-    dtype = "float32" if args.dtype == "fp32" else "float64"
+    dtype_key = dtype_key or args.dtype
+    dtype = "float32" if dtype_key == "fp32" else "float64"
     es = 4 if dtype == "float32" else 8
     Q_host = workload_state(n, seed=0)
     model = zb.ShallowWater2D(wet_dry_eps=1e-6, initial_conditions=Q_host,
@@ -270,6 +382,10 @@ def run_gpu(args, rank, world, local_rank):
         if rc != 0:
             L.check(rc, "zb_swe2d_step_part")
 
+    clock_path = None
+    if args.clock_log:
+        clock_path = args.clock_log if world <= 1 else f"{args.clock_log}.rank{rank}"
+    clk = ClockSampler(local_rank, path=clock_path).start()
     # warm-up
     solver.init_march(Q, 0.0)
     for k in range(args.warmup):
@@ -287,18 +403,17 @@ def run_gpu(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize(dev)
     wall0 = time.perf_counter()
-    clock_path = None
-    if args.clock_log:
-        clock_path = args.clock_log if world <= 1 else f"{args.clock_log}.rank{rank}"
-    with ClockSampler(local_rank, path=clock_path) as clk:
-        for k in range(K):
-            flush.zero_()
-            ev[k][0].record(stream)
-            part(k0 + k, 0)
-            ev[k][1].record(stream)
-            part(k0 + k, 1)
-            ev[k][2].record(stream)
-        torch.cuda.synchronize(dev)
+    clk.mark("start")
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record(stream)
+        part(k0 + k, 0)
+        ev[k][1].record(stream)
+        part(k0 + k, 1)
+        ev[k][2].record(stream)
+    torch.cuda.synchronize(dev)
+    clk.mark("end")
+    clk.stop()
     barrier()
     wall = time.perf_counter() - wall0
     st1 = [ev[k][0].elapsed_time(ev[k][1]) * 1e-3 for k in range(K)]
@@ -331,13 +446,18 @@ def run_gpu(args, rank, world, local_rank):
             "stage2_ms": round(mean2 * 1e3, 4),
             "step_bytes_per_cell_update": 17 * es,
             "step_achieved": round(17 * es * C_cells * K / step_s / 1e9, 1)}
-    traffic_file = ROOT / "profiles" / f"traffic_{args.dtype}.json"
+    traffic_file = ROOT / "profiles" / f"traffic_{dtype_key}.json"
     if traffic_file.exists():
         try:
             roof["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch")
         except ValueError:
             pass
 
+    out = {"value": value, "ms_per_step": tmax / K * 1e3, "roofline": roof,
+           "clocks": clk.summary(), "gpu_launches": launches_per_step * K,
+           "status_ok": status_ok, "sim_time": float(c.t[(k0 + K) % 3]), "wall_s": wall}
+    if not with_e2e:
+        return out
     # e2e through the public C ABI with host buffers: upload the state from
     # pinned host memory, K fused steps each followed by a device->host read
     # of the step's control block (dt, time, status) that the host checks,
@@ -386,11 +506,8 @@ def run_gpu(args, rank, world, local_rank):
                    "buffers: state upload, K steps each followed by a D2H read of the "
                    "step's control block that the host checks while the next step runs, "
                    "state download")}
-    return {
-        "value": value, "ms_per_step": tmax / K * 1e3, "roofline": roof, "e2e": e2e,
-        "clocks": clk.summary(), "gpu_launches": launches_per_step * K, "status_ok": status_ok,
-        "sim_time": float(c.t[(k0 + K) % 3]), "wall_s": wall,
-    }
+    out["e2e"] = e2e
+    return out
 
 
 def _ev_ms(fn, reps):
@@ -402,6 +519,25 @@ def _ev_ms(fn, reps):
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def poisson_solve_bytes(cells, iterations, levels):
+    """Algorithmic bytes of one multigrid-FCG pressure solve on ``cells`` fine
+    cells: what the kernels must stream per cell.  Per FCG iteration (float64
+    vectors, float64 level-0 face coefficients): q = A p with the p.q and p.r
+    dots reads p, r, cx, cy and writes q (40 B); x += a p, r -= a q reads x,
+    p, r, q and writes x, r and the float32 copy of r (52 B); z = z32 with z.q
+    reads z32, q and writes z (20 B); p = z - b p reads z, p and writes p
+    (24 B); the V-cycle (float32) per level reads f, cx, cy, dg and writes x
+    and a quarter-size coarse right-hand side on the way down (21 B), reads
+    f, cx, cy, dg, x and the quarter-size correction and writes x on the way
+    up (25 B), over levels shrinking 4x (46 B x 4/3).  The start is one
+    residual (x, b, cx, cy read; r, r32 written: 44 B), one V-cycle, z = z32
+    and p = z (12 + 16 B)."""
+    vcycle = 46.0 * (1.0 - 0.25 ** levels) / 0.75
+    per_it = 40 + 52 + 20 + 24 + vcycle
+    start = 44 + vcycle + 12 + 16
+    return int(cells * (start + iterations * per_it))
 
 
 def run_chorin(local_rank, n=1024, steps=10, warmup=3, train_steps=2000, use_graph=True):
@@ -445,8 +581,31 @@ def run_chorin(local_rank, n=1024, steps=10, warmup=3, train_steps=2000, use_gra
         ms = _ev_ms(one, steps)
         rel = float(sol._max_rel.item())
         its = float(sol._iters.item()) / steps
-        return {"ms_per_step": round(ms, 4), "fcg_iterations_per_solve": its,
-                "max_rel_residual": rel, "gate_ok": rel <= elliptic_accept(1e-8)}
+        out = {"ms_per_step": round(ms, 4), "fcg_iterations_per_solve": its,
+               "max_rel_residual": rel, "gate_ok": rel <= elliptic_accept(1e-8)}
+        # the pressure solve alone (the last step's right-hand side, from x = 0)
+        P = sol.poisson
+
+        def solve():
+            P.x.zero_()
+            P.launch(sol.precond, sol.smoother, sol.pressure_tol, sol.pressure_maxit)
+        solve()
+        torch.cuda.synchronize()
+        ms_solve = _ev_ms(solve, steps)
+        it_solve = int(P.scal[8].item())
+        out["solve_ms"] = round(ms_solve, 4)
+        out["solve_iterations"] = it_solve
+        if precond == "mg":
+            b_alg = poisson_solve_bytes(n * n, it_solve, P.n_levels)
+            hbm_peak, peak_kind = peaks()
+            ach = b_alg / (ms_solve * 1e-3) / 1e9
+            out["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak,
+                               "unit": "GB/s", "frac": round(ach / hbm_peak, 4),
+                               "algorithmic_bytes_per_solve": b_alg,
+                               "peak_kind": peak_kind,
+                               "what": "one pressure solve (FCG start + iterations), "
+                                       "bytes per poisson_solve_bytes()"}
+        return out
 
     out = {"grid": [n, n], "tol": 1e-8, "steps": steps, "warmup": warmup,
            "step": "hyperbolic Euler (eta-MUSCL + HR-HLL) + pressure FCG + corrector, fp32 "
@@ -671,7 +830,7 @@ def main():
                          "to this CSV (the JSON line always carries their summary)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the Chorin and ensemble legs")
-    ap.add_argument("--legs", default="swe,chorin,ensemble,triangles,snapshots",
+    ap.add_argument("--legs", default="swe,fp64,chorin,ensemble,triangles,snapshots",
                     help="comma-separated legs to run (profiling runs pick one)")
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--chorin-steps", type=int, default=10)
@@ -760,6 +919,14 @@ def main():
     # the extra legs are single-GPU configurations: measured at N = 1 only, so
     # a scaling run holds its N GPUs for the replicated SWE leg alone
     if not args.no_extra and world == 1:
+        if "fp64" in legs and args.dtype == "fp32":
+            # the same 2048^2 configuration with a float64 state (its other run)
+            r64 = run_gpu(args, rank, world, local_rank, dtype_key="fp64", with_e2e=False)
+            extra["fp64"] = {"value": r64["value"], "unit": UNIT,
+                             "ms_per_step": r64["ms_per_step"], "steps": args.steps,
+                             "roofline": r64["roofline"], "clocks": r64["clocks"],
+                             "gpu_launches": r64["gpu_launches"],
+                             "status_ok": r64["status_ok"]}
         if "chorin" in legs:
             extra["chorin"] = run_chorin(local_rank, steps=args.chorin_steps,
                                          train_steps=args.train_steps)

@@ -328,6 +328,33 @@ def test_fp32_drift_after_1000_steps():
     assert np.abs(q32[1] - q64[1]).max() / np.abs(q64[1]).max() <= 2e-2
 
 
+def test_fp32_1000_steps_against_the_float64_oracle():
+    """The float32 GPU march of 1000 steps at 256^2 (the 2048^2 configuration's
+    scheme and case family: noisy circular dam break over 16 seeded bumps,
+    eta-MUSCL minmod + HR-HLL, SSP-RK2, walls, dry-cell demotion 1e-6, CFL
+    0.45) against the float64 ORACLE's own march of the same 1000 steps
+    (``tests/golden/march_256_1000.npz``, made by ``make_march_fixture.py``).
+    Stated tolerance: relative L1 of h <= 2e-3, of each momentum row <= 2e-2,
+    relative L-infinity of h <= 2e-2, end times within 1e-4 relative."""
+    import pathlib
+    fx = np.load(pathlib.Path(__file__).parent / "golden" / "march_256_1000.npz")
+    n, steps = int(fx["n"]), int(fx["steps"])
+    domain = (0.0, 1.0, 0.0, 1.0)
+    m = zb.create_2d(domain, n, n)
+    Q0 = circular_dam_state(m.cell_centers(), seed=int(fx["seed"]))
+    solver, Q, Qaux, *_ = make(n, n, domain, Q0, dtype="float32", eps_wet=1e-6, oracle=False)
+    solver.init_march(Q)
+    solver.launch_steps(Q, steps)
+    c = solver.read_ctrl()
+    assert c.status == 0
+    got = Q.double().cpu().numpy()[1:]
+    ref = fx["Q"].astype(np.float64)
+    assert c.t[steps % 3] == pytest.approx(float(fx["t"]), rel=1e-4)
+    assert _l1(got[0], ref[0]) <= 2e-3
+    assert max(_l1(got[1], ref[1]), _l1(got[2], ref[2])) <= 2e-2
+    assert np.abs(got[0] - ref[0]).max() / np.abs(ref[0]).max() <= 2e-2
+
+
 def test_fp64_short_march_tracks_oracle():
     """20 steps of the wet-dry dam break: float64 GPU against the oracle's
     own march (own dt each step) stays within 1e-9 relative L-infinity."""
