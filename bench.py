@@ -784,15 +784,17 @@ def run_ensemble(local_rank, steps=2000):
     in [64, 512]) advanced together: per stage persistent launches over every
     instance's column-EDGE and EDGE strip items beside one over the interior
     items, and the tile fallback for grids narrower than four cells (unused
-    here; it keeps its autotuned height): four launches per stage, replayed
-    from a CUDA graph of 30 steps."""
+    here): four launches per stage, replayed from a CUDA graph of 30 steps.
+    The launch shape (strip CTAs per SM, column-EDGE and interior chunk
+    heights per size class of instance) is autotuned first on the ensemble
+    itself, and the tuned shape is the one timed."""
     import torch
     from zoomy_b200.ensemble import Ensemble
     from zoomy_b200.workloads import ensemble_512, ensemble_state
     sides, heights, manning = ensemble_512(seed=0)
     ens = Ensemble(sides, manning, dtype="float32", device=f"cuda:{local_rank}")
     ens.setup([ensemble_state(int(k), h) for k, h in zip(sides, heights)])
-    tuned = ens.autotune(steps=6)
+    tuned = ens.autotune(steps=8)
     ens.init()
     chunk = 30
     ens.capture(chunk)
@@ -810,8 +812,10 @@ def run_ensemble(local_rank, steps=2000):
                          "bytes_per_cell_update": 68},
             "ms_per_step": round(ms / chunk, 4),
             "value": cells * chunk / (ms * 1e-3), "unit": "cell-updates/s",
-            "launches_per_step": 8, "autotune_ms_per_step": {f"tile{t}_grid{g}": round(v, 4)
-                                                            for (t, g), v in tuned.items()},
+            "launches_per_step": 8,
+            "autotune_ms_per_step": {k: round(v, 4) for k, v in tuned.items()},
+            "launch_shape": ens.tuned_shape,
+            "class_instances_cells": ens.class_sizes(),
             "status_ok": ens.status_any() == 0}
 
 
@@ -835,6 +839,9 @@ def main():
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--chorin-steps", type=int, default=10)
     ap.add_argument("--tri-steps", type=int, default=500)
+    ap.add_argument("--tri-side", type=int, default=1415,
+                    help="lattice side of the triangle mesh (2 side^2 triangles; profiling "
+                         "captures use a smaller mesh)")
     ap.add_argument("--tri-host-prep", type=int, default=1,
                     help="also time the host mesh builder in the triangles leg (0: skip)")
     ap.add_argument("--chorin-no-graph", action="store_true",
@@ -896,7 +903,7 @@ def main():
         if "ensemble" in legs:
             line["ensemble"] = run_ensemble(local_rank)
         if "triangles" in legs:
-            line["triangles"] = run_triangles(local_rank, steps=args.tri_steps,
+            line["triangles"] = run_triangles(local_rank, n_side=args.tri_side, steps=args.tri_steps,
                                               host_prep=bool(args.tri_host_prep))
         if "snapshots" in legs:
             line["snapshots"] = run_snapshots(local_rank)
@@ -933,7 +940,7 @@ def main():
         if "ensemble" in legs:
             extra["ensemble"] = run_ensemble(local_rank)
         if "triangles" in legs:
-            extra["triangles"] = run_triangles(local_rank, steps=args.tri_steps,
+            extra["triangles"] = run_triangles(local_rank, n_side=args.tri_side, steps=args.tri_steps,
                                                host_prep=bool(args.tri_host_prep))
         if "snapshots" in legs:
             extra["snapshots"] = run_snapshots(local_rank)

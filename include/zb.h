@@ -231,6 +231,27 @@ typedef struct {
   double t_end;
 } zb_ens_instance;
 
+/* Launch shape of the ensemble step: what zb_ens_prepare_tuned lays into the
+ * work list and zb_ens_step_part_tuned launches.  No counterpart in the
+ * reference (its ensemble is a Python loop over solvers); the autotuner of
+ * the host package picks it by timing candidates on the actual ensemble.
+ *   tile_x          tile height of the small-grid fallback (8 or 16)
+ *   ctas_per_sm     persistent strip CTAs per SM: 1..4 (float32), 1..2 (float64)
+ *   n_classes       size classes of instances (1..4); an instance of side
+ *                   max(nx, ny) belongs to the first class whose
+ *                   class_max_side is >= that side (the last class takes
+ *                   every larger one); class_max_side increases
+ *   edge_rows       column-EDGE chunk height per class (4..32 rows)
+ *   interior_rows   interior chunk height per class (8..1024 rows) */
+typedef struct {
+  int32_t tile_x;
+  int32_t ctas_per_sm;
+  int32_t n_classes;
+  int32_t class_max_side[4];
+  int32_t edge_rows[4];
+  int32_t interior_rows[4];
+} zb_ens_tuning;
+
 /* Device bytes of the instance table + work list for a tile height of
  * tile_x (8 or 16) cells; 0 if the configuration is not supported (the
  * ensemble runs the order-2 eta reconstruction with HR-HLL, wall or
@@ -251,6 +272,15 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
                    int n_inst, int tile_x, void* table, size_t table_bytes,
                    int* n_items_out);
 
+/* zb_ens_table_bytes / zb_ens_prepare with an explicit launch shape (the
+ * untuned calls use one class with 32-row column-EDGE chunks, 64-row interior
+ * chunks and 4 (float32) or 2 (float64) strip CTAs per SM). */
+size_t zb_ens_table_bytes_tuned(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
+                                int n_inst, const zb_ens_tuning* tuning);
+int zb_ens_prepare_tuned(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
+                         int n_inst, const zb_ens_tuning* tuning, void* table,
+                         size_t table_bytes, int* n_items_out);
+
 /* Reset the n_inst control blocks ctrls[0..n_inst) and seed each instance's
  * wave-speed maximum from its state (zb_swe2d_init per instance; it also
  * creates the second stream, outside stream capture). */
@@ -269,6 +299,12 @@ int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst,
 int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst,
                      int n_items, int tile_x, int grid, void* Q, void* W,
                      zb_ctrl* ctrls, int phase, int part, zb_stream_t stream);
+
+/* zb_ens_step_part with the launch shape the table was prepared with. */
+int zb_ens_step_part_tuned(const zb_swe2d_cfg* common, const void* table, int n_inst,
+                           int n_items, const zb_ens_tuning* tuning, int grid, void* Q,
+                           void* W, zb_ctrl* ctrls, int phase, int part,
+                           zb_stream_t stream);
 
 /* ── Chorin pressure solve ─────────────────────────────────────────────────
  * Variable-coefficient Poisson -div(c grad p) = f on an nx x ny Cartesian grid

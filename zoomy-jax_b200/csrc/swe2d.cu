@@ -1426,8 +1426,9 @@ constexpr int SXC_GRID = 8;
 constexpr int SXC_ENS = 32;
 static_assert(SXC_GRID <= SXC_MAX && SXC_ENS <= SXC_MAX, "column-EDGE pre-pass rows");
 __host__ __device__ inline int full_items(int nx, int ny, int item, int* strip, int* r0,
-                                          int* r1, int* kind, int sxc) {
+                                          int* r1, int* kind, int sxc, int sx = SX) {
   const int SXC = sxc;
+  const int SX = sx;
   const int ns = (ny + SW - 1) / SW;
   // middle strips: 1 <= s <= mh
   int mh = ny >= 30 ? (ny - 30) / SW : 0;
@@ -2139,13 +2140,25 @@ static Fast fast_region(int nx, int ny) {
 // strip items of an instance (the single grid's full-coverage list):
 // {strip, r0, r1, flags}; flags bit 0 = a boundary-launch item, bit 1 = it
 // keeps the control block, bit 2 = a column-EDGE item (else EDGE, when bit 0)
+// the chunk heights of an instance's size class (zb_ens_tuning)
+static void ens_class_rows(const zb_ens_tuning& t, const zb_ens_instance& in, int* sxc,
+                           int* sx) {
+  const int side = std::max(in.nx, in.ny);
+  int c = 0;
+  while (c < t.n_classes - 1 && side > t.class_max_side[c]) ++c;
+  *sxc = t.edge_rows[c];
+  *sx = t.interior_rows[c];
+}
+
 template <typename F>
-static void ens_strip_items(const zb_ens_instance& in, F&& visit) {
+static void ens_strip_items(const zb_ens_instance& in, const zb_ens_tuning& t, F&& visit) {
   if (fast_region(in.nx, in.ny).nstrips == 0) return;
-  const int n = full_items(in.nx, in.ny, -1, nullptr, nullptr, nullptr, nullptr, SXC_ENS);
+  int sxc, sx;
+  ens_class_rows(t, in, &sxc, &sx);
+  const int n = full_items(in.nx, in.ny, -1, nullptr, nullptr, nullptr, nullptr, sxc, sx);
   for (int it = 0; it < n; ++it) {
     int st, r0, r1, kind;
-    full_items(in.nx, in.ny, it, &st, &r0, &r1, &kind, SXC_ENS);
+    full_items(in.nx, in.ny, it, &st, &r0, &r1, &kind, sxc, sx);
     visit(st, r0, r1, (kind != 0 ? 1 : 0) | (it == 0 ? 2 : 0) | (kind == 2 ? 4 : 0));
   }
 }
@@ -2158,16 +2171,46 @@ static void ens_frame_tiles(const zb_ens_instance& in, int tile_x, F&& visit) {
     for (int j0 = 0; j0 < in.ny; j0 += TY) visit(i0, j0);
 }
 
-static void ens_counts(const zb_ens_instance* inst, int n, int tile_x, size_t* tiles,
-                       size_t* strips) {
+static void ens_counts(const zb_ens_instance* inst, int n, const zb_ens_tuning& t,
+                       size_t* tiles, size_t* strips) {
   *tiles = 0;
   *strips = 0;
   for (int i = 0; i < n; ++i) {
-    ens_frame_tiles(inst[i], tile_x, [&](int, int) { ++*tiles; });
-    if (fast_region(inst[i].nx, inst[i].ny).nstrips > 0)
+    ens_frame_tiles(inst[i], t.tile_x, [&](int, int) { ++*tiles; });
+    if (fast_region(inst[i].nx, inst[i].ny).nstrips > 0) {
+      int sxc, sx;
+      ens_class_rows(t, inst[i], &sxc, &sx);
       *strips += (size_t)full_items(inst[i].nx, inst[i].ny, -1, nullptr, nullptr, nullptr,
-                                          nullptr, SXC_ENS);
+                                    nullptr, sxc, sx);
+    }
   }
+}
+
+// the launch shape of the untuned entry points: one size class, 32-row
+// column-EDGE chunks, 64-row interior chunks, 4 (float) or 2 (double) strip
+// CTAs per SM
+static zb_ens_tuning ens_default_tuning(const zb_swe2d_cfg* c, int tile_x) {
+  zb_ens_tuning t;
+  std::memset(&t, 0, sizeof(t));
+  t.tile_x = tile_x;
+  t.ctas_per_sm = c && c->dtype == ZB_F64 ? 2 : 4;
+  t.n_classes = 1;
+  t.class_max_side[0] = 1 << 30;
+  t.edge_rows[0] = SXC_ENS;
+  t.interior_rows[0] = SX;
+  return t;
+}
+
+static bool ens_tuning_valid(const zb_swe2d_cfg* c, const zb_ens_tuning* t) {
+  if (!c || !t || (t->tile_x != 8 && t->tile_x != 16)) return false;
+  if (t->ctas_per_sm < 1 || t->ctas_per_sm > (c->dtype == ZB_F64 ? 2 : 4)) return false;
+  if (t->n_classes < 1 || t->n_classes > 4) return false;
+  for (int k = 0; k < t->n_classes; ++k) {
+    if (t->edge_rows[k] < 4 || t->edge_rows[k] > SXC_MAX) return false;
+    if (t->interior_rows[k] < 8 || t->interior_rows[k] > 1024) return false;
+    if (k > 0 && t->class_max_side[k] <= t->class_max_side[k - 1]) return false;
+  }
+  return true;
 }
 
 static bool ens_valid(const zb_swe2d_cfg* c, const zb_ens_instance* inst, int n, int tile_x) {
@@ -2184,8 +2227,9 @@ static bool ens_valid(const zb_swe2d_cfg* c, const zb_ens_instance* inst, int n,
 }
 
 template <typename T, int TX>
-static int ens_launch(int part, const void* table, int n_inst, int n_items, int grid, void* Q,
-                      void* W, zb_ctrl* ctrls, int phase, cudaStream_t st) {
+static int ens_launch(int part, const void* table, int n_inst, int n_items, int grid,
+                      int ctas_per_sm, void* Q, void* W, zb_ctrl* ctrls, int phase,
+                      cudaStream_t st) {
   const EnsDesc<T>* desc = (const EnsDesc<T>*)table;
   const int4* items = (const int4*)((const char*)table + ens_desc_bytes<T>(n_inst));
   const size_t sm = sizeof(Smem<T, TX>);
@@ -2201,7 +2245,7 @@ static int ens_launch(int part, const void* table, int n_inst, int n_items, int 
   // boundary strips, interior strips (persistent warps over their items; a
   // grid that finds none exits at once), then the tiles of grids too small
   // for strips
-  const int sgrid_e = sms_cache[dev].load() * (sizeof(T) == 4 ? 4 : 2);
+  const int sgrid_e = sms_cache[dev].load() * ctas_per_sm;
   const int sgrid_i = sgrid_e;
   // the boundary items on the library's second stream, beside the interior ones
   SideStream* side = nullptr;
@@ -2452,20 +2496,38 @@ int zb_swe2d_step_noalloc(const zb_swe2d_cfg* cfg, void* Q, zb_ctrl* ctrl, int p
 
 
 // ── ensemble C ABI ──────────────────────────────────────────────────────────
-size_t zb_ens_table_bytes(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
-                          int tile_x) {
-  if (!ens_valid(common, inst, n_inst, tile_x)) return 0;
+size_t zb_ens_table_bytes_tuned(const zb_swe2d_cfg* common, const zb_ens_instance* inst,
+                                int n_inst, const zb_ens_tuning* tuning) {
+  if (!ens_tuning_valid(common, tuning)) return 0;
+  if (!ens_valid(common, inst, n_inst, tuning->tile_x)) return 0;
   size_t tiles = 0, strips = 0;
-  ens_counts(inst, n_inst, tile_x, &tiles, &strips);
+  ens_counts(inst, n_inst, *tuning, &tiles, &strips);
   const size_t d = common->dtype == ZB_F64 ? ens_desc_bytes<double>(n_inst)
                                            : ens_desc_bytes<float>(n_inst);
   return d + (1 + tiles + strips) * sizeof(int4);
 }
 
+size_t zb_ens_table_bytes(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
+                          int tile_x) {
+  if (!common) return 0;
+  const zb_ens_tuning t = ens_default_tuning(common, tile_x);
+  return zb_ens_table_bytes_tuned(common, inst, n_inst, &t);
+}
+
 int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
                    int tile_x, void* table, size_t table_bytes, int* n_items_out) {
+  if (!common) return ZB_E_ARG;
+  const zb_ens_tuning t = ens_default_tuning(common, tile_x);
+  return zb_ens_prepare_tuned(common, inst, n_inst, &t, table, table_bytes, n_items_out);
+}
+
+int zb_ens_prepare_tuned(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int n_inst,
+                         const zb_ens_tuning* tuning, void* table, size_t table_bytes,
+                         int* n_items_out) {
+  if (!ens_tuning_valid(common, tuning)) return ZB_E_ARG;
+  const int tile_x = tuning->tile_x;
   if (!ens_valid(common, inst, n_inst, tile_x) || !table || !n_items_out) return ZB_E_ARG;
-  if (table_bytes < zb_ens_table_bytes(common, inst, n_inst, tile_x)) return ZB_E_ARG;
+  if (table_bytes < zb_ens_table_bytes_tuned(common, inst, n_inst, tuning)) return ZB_E_ARG;
   auto build = [&](auto tag) -> int {
     using T = decltype(tag);
     std::vector<EnsDesc<T>> desc(n_inst);
@@ -2492,7 +2554,7 @@ int zb_ens_prepare(const zb_swe2d_cfg* common, const zb_ens_instance* inst, int 
       ens_frame_tiles(inst[i], tile_x, [&](int i0, int j0) {
         items.push_back(make_int4(i, i0, j0, i0 == 0 && j0 == 0));
       });
-      ens_strip_items(inst[i], [&](int st, int r0, int r1, int fl) {
+      ens_strip_items(inst[i], *tuning, [&](int st, int r0, int r1, int fl) {
         std::vector<int4>& to = (fl & 4) ? cstrips : ((fl & 1) ? estrips : strips);
         to.push_back(make_int4(i, st, r0, fl | (r1 << 3)));
       });
@@ -2548,24 +2610,36 @@ int zb_ens_init(const zb_swe2d_cfg* common, const void* table, int n_inst, const
   return zb_launch_check();
 }
 
-int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst, int n_items,
-                     int tile_x, int grid, void* Q, void* W, zb_ctrl* ctrls, int phase,
-                     int part, zb_stream_t stream) {
+int zb_ens_step_part_tuned(const zb_swe2d_cfg* common, const void* table, int n_inst,
+                           int n_items, const zb_ens_tuning* tuning, int grid, void* Q, void* W,
+                           zb_ctrl* ctrls, int phase, int part, zb_stream_t stream) {
   if (!common || !table || !Q || !W || !ctrls || n_inst < 1 || n_items < 1) return ZB_E_ARG;
   if (phase < 0 || phase > 2 || part < -1 || part > 1) return ZB_E_ARG;
-  if (tile_x != 8 && tile_x != 16) return ZB_E_ARG;
+  if (!ens_tuning_valid(common, tuning)) return ZB_E_ARG;
+  const int tile_x = tuning->tile_x, cps = tuning->ctas_per_sm;
   cudaStream_t st = (cudaStream_t)stream;
   for (int pt = (part == 1 ? 1 : 0); pt <= (part == 0 ? 0 : 1); ++pt) {
     int rc;
     if (common->dtype == ZB_F64)
-      rc = tile_x == 8 ? ens_launch<double, 8>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st)
-                       : ens_launch<double, 16>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st);
+      rc = tile_x == 8
+               ? ens_launch<double, 8>(pt, table, n_inst, n_items, grid, cps, Q, W, ctrls, phase, st)
+               : ens_launch<double, 16>(pt, table, n_inst, n_items, grid, cps, Q, W, ctrls, phase, st);
     else
-      rc = tile_x == 8 ? ens_launch<float, 8>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st)
-                       : ens_launch<float, 16>(pt, table, n_inst, n_items, grid, Q, W, ctrls, phase, st);
+      rc = tile_x == 8
+               ? ens_launch<float, 8>(pt, table, n_inst, n_items, grid, cps, Q, W, ctrls, phase, st)
+               : ens_launch<float, 16>(pt, table, n_inst, n_items, grid, cps, Q, W, ctrls, phase, st);
     if (rc) return rc;
   }
   return ZB_OK;
+}
+
+int zb_ens_step_part(const zb_swe2d_cfg* common, const void* table, int n_inst, int n_items,
+                     int tile_x, int grid, void* Q, void* W, zb_ctrl* ctrls, int phase,
+                     int part, zb_stream_t stream) {
+  if (!common || (tile_x != 8 && tile_x != 16)) return ZB_E_ARG;
+  const zb_ens_tuning t = ens_default_tuning(common, tile_x);
+  return zb_ens_step_part_tuned(common, table, n_inst, n_items, &t, grid, Q, W, ctrls, phase,
+                                part, stream);
 }
 
 }  // extern "C"

@@ -64,6 +64,12 @@ class ZbEnsInstance(C.Structure):
                 ("manning_n", C.c_double), ("t_end", C.c_double)]
 
 
+class ZbEnsTuning(C.Structure):
+    _fields_ = [("tile_x", C.c_int32), ("ctas_per_sm", C.c_int32), ("n_classes", C.c_int32),
+                ("class_max_side", C.c_int32 * 4), ("edge_rows", C.c_int32 * 4),
+                ("interior_rows", C.c_int32 * 4)]
+
+
 class ZbPoissonCfg(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("dx", C.c_double),
                 ("cmin", C.c_double), ("cmax", C.c_double), ("nu", C.c_int32),
@@ -126,6 +132,11 @@ SIGNATURES = [
     ("zb_ens_table_bytes", C.c_size_t, [_CFG, _P, C.c_int, C.c_int]),
     ("zb_ens_prepare", C.c_int, [_CFG, _P, C.c_int, C.c_int, _P, C.c_size_t,
                                  C.POINTER(C.c_int)]),
+    ("zb_ens_table_bytes_tuned", C.c_size_t, [_CFG, _P, C.c_int, C.POINTER(ZbEnsTuning)]),
+    ("zb_ens_prepare_tuned", C.c_int, [_CFG, _P, C.c_int, C.POINTER(ZbEnsTuning), _P,
+                                       C.c_size_t, C.POINTER(C.c_int)]),
+    ("zb_ens_step_part_tuned", C.c_int, [_CFG, _P, C.c_int, C.c_int, C.POINTER(ZbEnsTuning),
+                                         C.c_int, _P, _P, _P, C.c_int, C.c_int, _P]),
     ("zb_ens_init", C.c_int, [_CFG, _P, C.c_int, _P, _P, C.c_int, C.c_double, _P]),
     ("zb_ens_step_part", C.c_int, [_CFG, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P,
                                    _P, C.c_int, C.c_int, _P]),

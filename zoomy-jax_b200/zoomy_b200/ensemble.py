@@ -6,10 +6,11 @@ device array; persistent libzb kernels walk one work list of every
 instance's strip items (interior, boundary-column and boundary-row bodies,
 one launch each) and the tiles of grids narrower than four cells, so a fixed
 set of four launches advances every instance by one stage, whatever the
-number of instances.  The tile height and the persistent grid size of the
-tile fallback are picked by a small autotuner that times the candidates on
-the actual ensemble; the steps can be captured into a CUDA graph and
-replayed.
+number of instances.  The launch shape -- strip CTAs per SM and, per size
+class of instance, the row-chunk heights of the column-EDGE and interior
+items -- is picked by an autotuner that times the candidates on the actual
+ensemble (coordinate descent from the untuned shape); the steps can be
+captured into a CUDA graph and replayed.
 """
 from __future__ import annotations
 
@@ -21,7 +22,11 @@ import numpy as np
 
 from . import _lib as L
 
-TILE_CANDIDATES = (8, 16)
+# size classes of instances by side (the last class takes every larger one)
+CLASS_MAX_SIDE = (128, 256, 1 << 30)
+CTAS_CANDIDATES = (2, 3, 4)
+EDGE_ROWS_CANDIDATES = (8, 16, 24, 32)
+INTERIOR_ROWS_CANDIDATES = (32, 64, 128, 256)
 
 
 class Ensemble:
@@ -66,6 +71,15 @@ class Ensemble:
         self.inst = inst
         self.tile_x = 16
         self.grid = 0
+        t = L.ZbEnsTuning()
+        t.tile_x = self.tile_x
+        t.ctas_per_sm = 2 if dtype == "float64" else 4
+        t.n_classes = len(CLASS_MAX_SIDE)
+        for k, side in enumerate(CLASS_MAX_SIDE):
+            t.class_max_side[k] = side
+            t.edge_rows[k] = 32
+            t.interior_rows[k] = 64
+        self.tuning = t
         self._n = 0
 
     @property
@@ -86,21 +100,32 @@ class Ensemble:
         self.W = torch.empty(3 * self.total_cells, dtype=td, device=self.device)
         self.ctrls = torch.zeros(self.n_inst * L.CTRL_BYTES, dtype=torch.uint8,
                                  device=self.device)
-        self._build_table(self.tile_x)
+        self._build_table()
         return self.Q
 
-    def _build_table(self, tile_x):
+    def _build_table(self):
         import torch
-        nb = self.lib.zb_ens_table_bytes(C.byref(self.cfg), self.inst, self.n_inst, tile_x)
+        t = C.byref(self.tuning)
+        nb = self.lib.zb_ens_table_bytes_tuned(C.byref(self.cfg), self.inst, self.n_inst, t)
         if nb == 0:
             raise L.ZbError("unsupported ensemble configuration")
         self.table = torch.empty(nb, dtype=torch.uint8, device=self.device)
         n_items = C.c_int(0)
-        L.check(self.lib.zb_ens_prepare(C.byref(self.cfg), self.inst, self.n_inst, tile_x,
-                                        L.ptr(self.table), C.c_size_t(nb), C.byref(n_items)),
-                "zb_ens_prepare")
+        L.check(self.lib.zb_ens_prepare_tuned(C.byref(self.cfg), self.inst, self.n_inst, t,
+                                              L.ptr(self.table), C.c_size_t(nb),
+                                              C.byref(n_items)),
+                "zb_ens_prepare_tuned")
         self.n_items = n_items.value
-        self.tile_x = tile_x
+
+    def class_sizes(self):
+        """(instances, cells) per size class."""
+        out = []
+        lo = 0
+        for side in CLASS_MAX_SIDE:
+            m = (self.sides > lo) & (self.sides <= side)
+            out.append((int(m.sum()), int(self.cells[m].sum())))
+            lo = side
+        return out
 
     def instance(self, i):
         """Device view ``(4, n*n)`` of instance ``i``'s state."""
@@ -116,12 +141,12 @@ class Ensemble:
 
     def launch_part(self, part, phase=None):
         ph = self._n % 3 if phase is None else phase
-        rc = self.lib.zb_ens_step_part(C.byref(self.cfg), L.ptr(self.table), self.n_inst,
-                                       self.n_items, self.tile_x, self.grid, L.ptr(self.Q),
-                                       L.ptr(self.W), L.ptr(self.ctrls), ph, part,
-                                       L.stream_ptr())
+        rc = self.lib.zb_ens_step_part_tuned(C.byref(self.cfg), L.ptr(self.table), self.n_inst,
+                                             self.n_items, C.byref(self.tuning), self.grid,
+                                             L.ptr(self.Q), L.ptr(self.W), L.ptr(self.ctrls), ph,
+                                             part, L.stream_ptr())
         if rc != L.ZB_OK:
-            L.check(rc, "zb_ens_step_part")
+            L.check(rc, "zb_ens_step_part_tuned")
 
     def launch_steps(self, n):
         for _ in range(n):
@@ -139,33 +164,81 @@ class Ensemble:
         return int(np.bitwise_or.reduce(st))
 
     # ── autotuner ─────────────────────────────────────────────────────────
-    def autotune(self, steps=6, grids=(0,), tiles=TILE_CANDIDATES):
-        """Time ``steps`` steps for every (tile height, persistent grid)
-        candidate on a scratch copy of the state and keep the fastest.
-        Returns ``{(tile, grid): ms_per_step}``."""
+    def shape(self):
+        """The current launch shape as a plain dict."""
+        t = self.tuning
+        return {"ctas_per_sm": int(t.ctas_per_sm),
+                "edge_rows": [int(t.edge_rows[k]) for k in range(t.n_classes)],
+                "interior_rows": [int(t.interior_rows[k]) for k in range(t.n_classes)],
+                "class_max_side": [int(t.class_max_side[k]) for k in range(t.n_classes)]}
+
+    def _time_shape(self, saved_q, steps):
         import torch
+        self._build_table()
+        self.Q.copy_(saved_q)
+        self.init()
+        self.launch_steps(2)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        self.launch_steps(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def autotune(self, steps=8):
+        """Coordinate descent over the launch shape from the untuned one:
+        strip CTAs per SM, then per populated size class the column-EDGE and
+        the interior chunk heights; each candidate is timed over ``steps``
+        steps (after two untimed ones) on a scratch copy of the state and
+        replaces the incumbent only when it is faster.  Returns ``{candidate:
+        ms_per_step}`` for every candidate timed and keeps the best shape
+        (``self.tuned_shape``, ``self.tuned_ms``) for the steps that follow."""
         saved_q = self.Q.clone()
+        t = self.tuning
         results = {}
-        for tile in tiles:
-            self._build_table(tile)
-            for grid in grids:
-                self.grid = grid
-                self.Q.copy_(saved_q)
-                self.init()
-                self.launch_steps(2)
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                self.launch_steps(steps)
-                e1.record()
-                torch.cuda.synchronize()
-                results[(tile, grid)] = e0.elapsed_time(e1) / steps
-        best = min(results, key=results.get)
-        self._build_table(best[0])
-        self.grid = best[1]
+        best = self._time_shape(saved_q, steps)
+        results["untuned"] = best
+
+        def trial(key, set_, undo):
+            nonlocal best
+            set_()
+            ms = self._time_shape(saved_q, steps)
+            results[key] = ms
+            if ms < best:
+                best = ms
+            else:
+                undo()
+
+        for cps in CTAS_CANDIDATES:
+            if cps == t.ctas_per_sm or (self.dtype == "float64" and cps > 2):
+                continue
+            old = t.ctas_per_sm
+            trial(f"ctas_per_sm={cps}", lambda v=cps: setattr(t, "ctas_per_sm", v),
+                  lambda v=old: setattr(t, "ctas_per_sm", v))
+        for k, (n_inst, _) in enumerate(self.class_sizes()):
+            if n_inst == 0:
+                continue
+            for rows in EDGE_ROWS_CANDIDATES:
+                if rows == t.edge_rows[k]:
+                    continue
+                old = t.edge_rows[k]
+                trial(f"class{k}.edge_rows={rows}",
+                      lambda v=rows, k=k: t.edge_rows.__setitem__(k, v),
+                      lambda v=old, k=k: t.edge_rows.__setitem__(k, v))
+            for rows in INTERIOR_ROWS_CANDIDATES:
+                if rows == t.interior_rows[k]:
+                    continue
+                old = t.interior_rows[k]
+                trial(f"class{k}.interior_rows={rows}",
+                      lambda v=rows, k=k: t.interior_rows.__setitem__(k, v),
+                      lambda v=old, k=k: t.interior_rows.__setitem__(k, v))
+        self._build_table()
         self.Q.copy_(saved_q)
         self.init()
         self.tuned = results
+        self.tuned_shape = self.shape()
+        self.tuned_ms = best
         return results
 
     # ── CUDA graph ────────────────────────────────────────────────────────
