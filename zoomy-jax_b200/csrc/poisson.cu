@@ -328,6 +328,29 @@ __global__ void p_update_kernel(double* __restrict__ p, const double* __restrict
     p[k] = first ? z[k] : z[k] - b * p[k];
 }
 
+// loop control of the graph solve: counts the iteration and keeps the WHILE
+// node running while the relative residual is above tol (NaN stops it)
+__device__ __forceinline__ void fcg_loop_control(double* scal, cudaGraphConditionalHandle h,
+                                                 double tol, int maxit, int first) {
+  const double it = first ? 0.0 : scal[S_ITER] + 1.0;
+  scal[S_ITER] = it;
+  const double rel = scal[S_REL];
+  const bool go = rel > tol && it < (double)maxit;   // false for NaN
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// p_update with the graph solve's loop control folded in (block 0, thread 0;
+// it reads S_REL, set by update_xr before the V-cycle, and writes S_ITER,
+// which p_update does not touch): one launch fewer per iteration
+__global__ void p_update_cond_kernel(double* __restrict__ p, const double* __restrict__ z,
+                                     double* scal, long long n, int first,
+                                     cudaGraphConditionalHandle h, double tol, int maxit) {
+  const double b = first ? 0.0 : scal[S_BETA];
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
+    p[k] = first ? z[k] : z[k] - b * p[k];
+  if (blockIdx.x == 0 && threadIdx.x == 0) fcg_loop_control(scal, h, tol, maxit, first);
+}
+
 // r = b - A x ; partial r.r and b.b ; r32
 __global__ void __launch_bounds__(NT)
 residual64_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
@@ -1123,17 +1146,13 @@ static int enable_coarse_smem() {
   return ZB_OK;
 }
 
-// loop control of the graph solve: counts the iteration and keeps the WHILE
-// node running while the relative residual is above tol (NaN stops it)
-__global__ void fcg_cond_kernel(double* scal, cudaGraphConditionalHandle h, double tol, int maxit,
-                                int first) {
-  if (threadIdx.x != 0) return;
-  const double it = first ? 0.0 : scal[S_ITER] + 1.0;
-  scal[S_ITER] = it;
-  const double rel = scal[S_REL];
-  const bool go = rel > tol && it < (double)maxit;   // false for NaN
-  cudaGraphSetConditional(h, go ? 1u : 0u);
-}
+// the graph solve's loop control, folded into the last kernel of the start
+// and of every iteration (nullptr: none, the host drives the loop)
+struct LoopCtl {
+  cudaGraphConditionalHandle h;
+  double tol;
+  int maxit;
+};
 
 // reduction counters of finish_scalars: four unsigned slots in the last
 // doubles of the scalar block (zeroed at set-up, re-armed by every use)
@@ -1442,8 +1461,9 @@ int zb_poisson_correct(const zb_poisson_cfg* cfg, void* ws, void* Q, int dtype, 
   return zb_launch_check();
 }
 
-int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x, int precond,
-                 const zb_smoother* smo, zb_stream_t stream) {
+static int fcg_start_impl(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x,
+                          int precond, const zb_smoother* smo, zb_stream_t stream,
+                          const LoopCtl* lc) {
   if (!valid(cfg) || !ws || !b || !x || precond < 0 || precond > 3) return ZB_E_ARG;
   if (precond >= 2 && !smo) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
@@ -1461,12 +1481,21 @@ int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x
   if (rc) return rc;
   z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, nullptr, n, nullptr,
                                              nullptr, scal);
-  p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1);
+  if (lc)
+    p_update_cond_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1, lc->h,
+                                                     lc->tol, lc->maxit);
+  else
+    p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1);
   return zb_launch_check();
 }
 
-int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
-                   const zb_smoother* smo, zb_stream_t stream) {
+int zb_fcg_start(const zb_poisson_cfg* cfg, void* ws, const double* b, double* x, int precond,
+                 const zb_smoother* smo, zb_stream_t stream) {
+  return fcg_start_impl(cfg, ws, b, x, precond, smo, stream, nullptr);
+}
+
+static int fcg_iterate_impl(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
+                            const zb_smoother* smo, zb_stream_t stream, const LoopCtl* lc) {
   if (!valid(cfg) || !ws || !x || precond < 0 || precond > 3) return ZB_E_ARG;
   if (precond >= 2 && !smo) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
@@ -1487,8 +1516,17 @@ int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
   if (rc) return rc;
   z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, dw + P.vq, n,
                                              part + 3 * RED_BLOCKS, ctr + 3, scal);
-  p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0);
+  if (lc)
+    p_update_cond_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0, lc->h,
+                                                     lc->tol, lc->maxit);
+  else
+    p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0);
   return zb_launch_check();
+}
+
+int zb_fcg_iterate(const zb_poisson_cfg* cfg, void* ws, double* x, int precond,
+                   const zb_smoother* smo, zb_stream_t stream) {
+  return fcg_iterate_impl(cfg, ws, x, precond, smo, stream, nullptr);
 }
 
 
@@ -1530,9 +1568,8 @@ int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b, do
     if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr) != cudaSuccess) { rc = ZB_E_CUDA; break; }
     cudaGraphConditionalHandle h;
     if (cudaGraphConditionalHandleCreate(&h, g, 0u, cudaGraphCondAssignDefault) != cudaSuccess) { rc = ZB_E_CUDA; break; }
-    if ((rc = zb_fcg_start(cfg, ws, b, x, precond, smo, (void*)st))) break;
-    fcg_cond_kernel<<<1, 32, 0, st>>>(scal, h, tol, maxit, 1);
-    if (cudaGetLastError() != cudaSuccess) { rc = ZB_E_CUDA; break; }
+    const LoopCtl lc = {h, tol, maxit};
+    if ((rc = fcg_start_impl(cfg, ws, b, x, precond, smo, (void*)st, &lc))) break;
     if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess) { rc = ZB_E_CUDA; break; }
     cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
     np.conditional.handle = h;
@@ -1543,8 +1580,7 @@ int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b, do
     cudaGraph_t bg = np.conditional.phGraph_out[0];
     if (cudaStreamBeginCaptureToGraph(body, bg, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal) != cudaSuccess) { rc = ZB_E_CUDA; break; }
-    int rb = zb_fcg_iterate(cfg, ws, x, precond, smo, (void*)body);
-    fcg_cond_kernel<<<1, 32, 0, body>>>(scal, h, tol, maxit, 0);
+    int rb = fcg_iterate_impl(cfg, ws, x, precond, smo, (void*)body, &lc);
     cudaGraph_t bg2 = nullptr;
     const cudaError_t eb = cudaStreamEndCapture(body, &bg2);
     if (rb) { rc = rb; break; }
