@@ -1549,7 +1549,6 @@ int zb_fcg_graph_create(const zb_poisson_cfg* cfg, void* ws, const double* b, do
   *out = nullptr;
   (void)stream;   // capture runs on private streams; nothing executes here
   const Plan P = make_plan(cfg);
-  double* scal = (double*)ws + P.scal;
   cudaStream_t st = nullptr, body = nullptr;
   ZB_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   if (cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking) != cudaSuccess) {
