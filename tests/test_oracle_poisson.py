@@ -127,3 +127,37 @@ def test_unet_output_is_homogeneous_in_the_residual():
     y2, _ = OU.forward(Ws, bs, 7.0 * r, cx, cy, 0.1, 2.0)
     assert np.allclose(y2, 7.0 * y1, rtol=1e-12, atol=0)
     assert OU.param_counts(24, 48) == (52488, 169)
+
+
+def test_coefficient_variation_costs_at_most_one_iteration():
+    """How much room a coefficient-aware learned component has: on a Chorin
+    pressure problem (the first stage of the seeded dam break over bumps,
+    128^2, c = clip(h, 0.1, 2) from 0.21 to 1.97) multigrid FCG needs 8
+    iterations to 1e-8, and the same right-hand side with the coefficient
+    replaced by a constant still needs 7.  A smoother or transfer operator
+    that learned the coefficient field perfectly could therefore save about
+    one iteration of eight; halving the count needs a V-cycle that contracts
+    ~100x instead of ~7x, i.e. a stronger cycle, not a coefficient-aware one."""
+    import sys
+    import pathlib
+    sys.path.insert(0, str(pathlib.Path(__file__).resolve().parent.parent / "zoomy-jax_b200"))
+    from oracle import mesh as OM
+    from oracle import swe as OS
+    from zoomy_b200.workloads import cartesian_centers, circular_dam_state
+    n = 128
+    tags = ("left", "right", "bottom", "top")
+    Q0 = circular_dam_state(cartesian_centers(n), seed=0)
+    om = OM.create_2d(0.0, 1.0, 0.0, 1.0, n, n)
+    sc = OS.Scheme(order=2, recon="eta", riemann="hll_hr", cfl=0.45,
+                   bc={t: "wall" for t in tags}, eps_wet=1e-6)
+    p = OS.Params(wet_dry_eps=1e-6)
+    dt = OS.compute_dt(om, Q0, p, sc)
+    Qs = Q0 + dt * OS.flux_operator(om, Q0, sc, p, OS.bc_kinds(om, sc))
+    dx = 1.0 / n
+    b = OP.divergence_rhs(Qs[2].reshape(n, n), Qs[3].reshape(n, n), dt, dx)
+    cx, cy = OP.face_coefficients(Qs[1].reshape(n, n))
+    _, it_var, rel_var = OP.fcg(OP.Hierarchy(cx, cy, dx, coarsest=4), b, tol=1e-8)
+    ones = (np.ones_like(cx), np.ones_like(cy))
+    _, it_const, rel_const = OP.fcg(OP.Hierarchy(*ones, dx, coarsest=4), b, tol=1e-8)
+    assert rel_var <= 1e-8 and rel_const <= 1e-8
+    assert it_var == 8 and it_const == 7, (it_var, it_const)
