@@ -582,6 +582,19 @@ struct Stage {
     }
     __syncthreads();
   }
+  // the first half-sweep of a V-cycle's way down starts from x = 0, where
+  // A x = 0 exactly: the update x += (f - A x) / dg is x = f / dg, bit for bit
+  __device__ void sweep_from_zero(int color, int m) const {
+    for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y) {
+      const int gi = i0 - HALO + a;
+      int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
+      for (; b < R - m; b += 2 * (int)blockDim.x) {
+        if (!interior && !inside(a, b)) continue;
+        x[a * R + b] = f[a * R + b] / dg[a * R + b];
+      }
+    }
+    __syncthreads();
+  }
   // one half-sweep over the cells of `color` at least m cells inside the
   // staged region; rows over threadIdx.y, same-colour columns over threadIdx.x
   __device__ void sweep(int color, int m, float idx2) const {
@@ -652,7 +665,8 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, dg, nullptr);
-  for (int s = 0; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
+  if (NU > 0) S.sweep_from_zero(0, 1);
+  for (int s = 1; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
   // residual where the sweeps are final and one ring beyond the tile
   {
     constexpr int m = 2 * NU + 1;
