@@ -26,7 +26,6 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
-#include <cooperative_groups.h>
 
 #include "common.cuh"
 
@@ -851,244 +850,6 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
   for (int k = threadIdx.x; k < L0.nx * L0.ny; k += CT) ws_f[L0.x + k] = sx[P.small0][k];
 }
 
-// ── the cluster V-cycle (levels cl0 .. nlev-1 in distributed shared memory) ─
-// The coarse part of the V-cycle as ONE launch of a thread-block cluster
-// (16 CTAs where the device allows non-portable clusters, else 8).  Every
-// level from cl0 down is split into blocks of rows, one block per CTA, held in
-// that CTA's shared memory (x, f, r, the diagonal and its faces); a cell
-// whose stencil, restriction or prolongation reaches a row of another block
-// reads it from the owning CTA's shared memory (distributed shared memory),
-// and every phase ends with a cluster barrier instead of a kernel boundary.
-// The arithmetic is the one-CTA kernel's (the same expressions in the same
-// order), so both give the same V-cycle.
-namespace cgr = cooperative_groups;
-constexpr int CLT = 1024;                 // threads per cluster CTA
-constexpr int CL_SMEM_MAX = 200 * 1024;   // shared memory per CTA for the levels
-
-__host__ __device__ inline int cl_rows(int nx, int ncl) { return (nx + ncl - 1) / ncl; }
-__host__ __device__ inline long long cl_level_floats(int nx, int ny, int ncl) {
-  const long long rp = cl_rows(nx, ncl);
-  return 4 * rp * ny + (rp + 1) * ny + rp * (ny + 1);
-}
-
-struct ClLev {
-  int nx, ny, rp, lo, hi;     // rows per CTA; this CTA's rows [lo, hi)
-  float idx2;
-  float *x, *f, *r, *dg, *cx, *cy;   // this CTA's block (same offsets in every CTA)
-};
-
-// value of `arr` (a per-level array of cells) at row i, column j of the level,
-// from whichever CTA owns row i
-__device__ __forceinline__ float cl_at(const ClLev& L, float* arr, int i, int j, unsigned me) {
-  const int q = i / L.rp;
-  float* base = (unsigned)q == me ? arr : cgr::this_cluster().map_shared_rank(arr, q);
-  return base[(i - q * L.rp) * L.ny + j];
-}
-
-// (A x)_k of a cell of this CTA's block (apply_at's expression and order)
-__device__ __forceinline__ float cl_ax(const ClLev& L, int li, int j, unsigned me) {
-  const int rows = L.hi - L.lo, ny = L.ny, i = L.lo + li;
-  const int k = li * ny + j;
-  const float xc = L.x[k];
-  const float a = L.cx[(li + 1) * ny + j], b = L.cx[li * ny + j];
-  const float c = L.cy[li * (ny + 1) + j + 1], d = L.cy[li * (ny + 1) + j];
-  const float xe = i + 1 >= L.nx ? -xc : (li + 1 < rows ? L.x[k + ny] : cl_at(L, L.x, i + 1, j, me));
-  const float xw = i <= 0 ? -xc : (li > 0 ? L.x[k - ny] : cl_at(L, L.x, i - 1, j, me));
-  const float xn = j + 1 >= ny ? -xc : L.x[k + 1];
-  const float xs = j <= 0 ? -xc : L.x[k - 1];
-  return (a * (xc - xe) + b * (xc - xw) + c * (xc - xn) + d * (xc - xs)) * L.idx2;
-}
-
-// one red-black half sweep over this CTA's rows (rbgs_kernel's update), then
-// the cluster barrier
-__device__ void cl_sweep(const ClLev& L, int color, unsigned me) {
-  const int rows = L.hi - L.lo, ny = L.ny;
-  const int half = (ny + 1) / 2;
-  for (int t = threadIdx.x; t < rows * half; t += CLT) {
-    const int li = t / half, m = t - li * half;
-    const int j = 2 * m + ((L.lo + li + color) & 1);
-    if (j >= ny) continue;
-    const int k = li * ny + j;
-    const float v = cl_ax(L, li, j, me);
-    L.x[k] += (L.f[k] - v) / L.dg[k];
-  }
-  cgr::this_cluster().sync();
-}
-
-__device__ void cl_residual(const ClLev& L, unsigned me) {
-  const int rows = L.hi - L.lo, ny = L.ny;
-  for (int t = threadIdx.x; t < rows * ny; t += CLT) {
-    const int li = t / ny, j = t - li * ny;
-    L.r[t] = L.f[t] - cl_ax(L, li, j, me);
-  }
-  cgr::this_cluster().sync();
-}
-
-__global__ void __launch_bounds__(CLT, 1)
-cluster_vcycle_kernel(const Plan P, float* ws_f, int l0, int ncl) {
-  extern __shared__ float sm[];
-  const unsigned me = cgr::this_cluster().block_rank();
-  ClLev Lv[MAXL];
-  long long o = 0;
-  for (int l = l0; l < P.nlev; ++l) {
-    const Level& G = P.L[l];
-    ClLev& L = Lv[l];
-    L.nx = G.nx; L.ny = G.ny; L.rp = cl_rows(G.nx, ncl);
-    L.lo = min(G.nx, (int)me * L.rp);
-    L.hi = min(G.nx, L.lo + L.rp);
-    L.idx2 = 1.0f / (G.dx * G.dx);
-    const long long nb = (long long)L.rp * L.ny;
-    L.x = sm + o; o += nb;
-    L.f = sm + o; o += nb;
-    L.r = sm + o; o += nb;
-    L.dg = sm + o; o += nb;
-    L.cx = sm + o; o += (long long)(L.rp + 1) * L.ny;
-    L.cy = sm + o; o += (long long)L.rp * (L.ny + 1);
-  }
-  // stage this CTA's rows of every level: diagonal, faces, x = 0; f of level l0
-  for (int l = l0; l < P.nlev; ++l) {
-    const Level& G = P.L[l];
-    const ClLev& L = Lv[l];
-    const int rows = L.hi - L.lo, ny = L.ny;
-    const long long c0 = (long long)L.lo * ny;
-    for (int k = threadIdx.x; k < rows * ny; k += CLT) {
-      L.dg[k] = ws_f[G.dg + c0 + k];
-      L.x[k] = 0.0f;
-      if (l == l0) L.f[k] = ws_f[G.f + c0 + k];
-    }
-    if (rows > 0) {
-      for (int k = threadIdx.x; k < (rows + 1) * ny; k += CLT) L.cx[k] = ws_f[G.cx + c0 + k];
-      const long long y0 = (long long)L.lo * (ny + 1);
-      for (int k = threadIdx.x; k < rows * (ny + 1); k += CLT) L.cy[k] = ws_f[G.cy + y0 + k];
-    }
-  }
-  cgr::this_cluster().sync();
-  const int nu = P.nu;
-  // descend
-  for (int l = l0; l < P.nlev; ++l) {
-    const ClLev& L = Lv[l];
-    if (l == P.nlev - 1) {
-      const int n = L.nx * L.ny;
-      const int rows = L.hi - L.lo;
-      if (P.cinv >= 0) {
-        // x = A^-1 f with the inverse built at set-up (cta_coarsest's order)
-        const float* inv = ws_f + P.cinv;
-        for (int t = threadIdx.x; t < rows * L.ny; t += CLT) {
-          const int kg = (L.lo + t / L.ny) * L.ny + t % L.ny;
-          float v = 0.0f;
-          for (int m = 0; m < n; ++m) v += inv[kg * n + m] * cl_at(L, L.f, m / L.ny, m % L.ny, me);
-          L.x[t] = v;
-        }
-        cgr::this_cluster().sync();
-      } else {
-        for (int s = 0; s < P.coarse_sweeps; ++s) { cl_sweep(L, 0, me); cl_sweep(L, 1, me); }
-        for (int s = 0; s < P.coarse_sweeps; ++s) { cl_sweep(L, 1, me); cl_sweep(L, 0, me); }
-      }
-      break;
-    }
-    for (int s = 0; s < nu; ++s) { cl_sweep(L, 0, me); cl_sweep(L, 1, me); }
-    cl_residual(L, me);
-    const ClLev& C = Lv[l + 1];
-    const int rc = C.hi - C.lo;
-    for (int t = threadIdx.x; t < rc * C.ny; t += CLT) {
-      const int I = C.lo + t / C.ny, J = t % C.ny;
-      C.f[t] = restrict_at([&](int fi, int fj) { return cl_at(L, L.r, fi, fj, me); }, I, J,
-                           C.nx, C.ny);
-    }
-    cgr::this_cluster().sync();
-  }
-  // ascend
-  for (int l = P.nlev - 2; l >= l0; --l) {
-    const ClLev& L = Lv[l];
-    const ClLev& C = Lv[l + 1];
-    const int rows = L.hi - L.lo;
-    for (int t = threadIdx.x; t < rows * L.ny; t += CLT) {
-      const int fi = L.lo + t / L.ny, fj = t % L.ny;
-      L.x[t] += prolong_at([&](int I, int J) { return cl_at(C, C.x, I, J, me); }, fi, fj, C.nx,
-                           C.ny);
-    }
-    cgr::this_cluster().sync();
-    for (int s = 0; s < nu; ++s) { cl_sweep(L, 1, me); cl_sweep(L, 0, me); }
-  }
-  // level l0's x back to the workspace (own rows only: no remote access after
-  // the last barrier)
-  const ClLev& L = Lv[l0];
-  const long long c0 = (long long)L.lo * L.ny;
-  for (int k = threadIdx.x; k < (L.hi - L.lo) * L.ny; k += CLT) ws_f[P.L[l0].x + c0 + k] = L.x[k];
-}
-
-static long long cl_smem(const Plan& P, int l0, int ncl) {
-  long long o = 0;
-  for (int l = l0; l < P.nlev; ++l) o += cl_level_floats(P.L[l].nx, P.L[l].ny, ncl);
-  return o * (long long)sizeof(float);
-}
-
-// The cluster size this device runs the cluster V-cycle with (16, 8, or 0 =
-// not at all), probed once per device outside stream capture: the kernel is
-// given the shared-memory limit and non-portable cluster sizes, and the
-// occupancy query says whether a cluster of that size fits.
-static int cluster_capability() {
-  static std::atomic<int> cap[32];   // 0 unknown, -1 none, else the size
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 32) return 0;
-  int c = cap[dev].load();
-  if (c != 0) return c > 0 ? c : 0;
-  c = -1;
-  if (cudaFuncSetAttribute(cluster_vcycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           CL_SMEM_MAX) == cudaSuccess &&
-      cudaFuncSetAttribute(cluster_vcycle_kernel,
-                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
-    for (int ncl : {16, 8}) {
-      cudaLaunchConfig_t lc = {};
-      lc.gridDim = dim3(ncl);
-      lc.blockDim = dim3(CLT);
-      lc.dynamicSmemBytes = CL_SMEM_MAX;
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = ncl;
-      at[0].val.clusterDim.y = 1;
-      at[0].val.clusterDim.z = 1;
-      lc.attrs = at;
-      lc.numAttrs = 1;
-      int nclusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&nclusters, cluster_vcycle_kernel, &lc) == cudaSuccess &&
-          nclusters >= 1) {
-        c = ncl;
-        break;
-      }
-    }
-  }
-  cudaGetLastError();
-  cap[dev].store(c);
-  return c > 0 ? c : 0;
-}
-
-// First level of the cluster part: the finest level below level 0 whose
-// levels down to the coarsest fit the CTAs' shared memory (P.nlev: none)
-static int cluster_first_level(const Plan& P, int ncl) {
-  if (ncl <= 0) return P.nlev;
-  for (int l = 1; l < P.nlev; ++l)
-    if (cl_smem(P, l, ncl) <= CL_SMEM_MAX) return l;
-  return P.nlev;
-}
-
-static int launch_cluster_vcycle(const Plan& P, float* fw, int l0, int ncl, cudaStream_t st) {
-  cudaLaunchConfig_t lc = {};
-  lc.gridDim = dim3(ncl);
-  lc.blockDim = dim3(CLT);
-  lc.dynamicSmemBytes = (size_t)cl_smem(P, l0, ncl);
-  lc.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = ncl;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  lc.attrs = at;
-  lc.numAttrs = 1;
-  ZB_CUDA_TRY(cudaLaunchKernelEx(&lc, cluster_vcycle_kernel, P, fw, l0, ncl));
-  return ZB_OK;
-}
-
 // dense inverse of the coarsest operator (float64 in-place Gauss-Jordan; the
 // operator is SPD, so no pivoting), stored as float32 for the V-cycle; one CTA
 __global__ void coarse_inverse_kernel(const Plan P, float* ws_f) {
@@ -1286,14 +1047,8 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + L0.f, fw + L0.x, n0);
     return zb_launch_check();
   }
-  // the coarse part runs in one cluster launch where the device allows it
-  // (levels cl0 ..), else in the one-CTA kernel (levels small0 ..)
-  const int ncl = cluster_capability();
-  const int cl0 = cluster_first_level(P, ncl);
-  const bool use_cluster = cl0 < P.nlev;
-  const int split = use_cluster ? cl0 : P.small0;
   // fine levels: one fused launch each on the way down
-  for (int l = 0; l < split && l < P.nlev - 1; ++l) {
+  for (int l = 0; l < P.small0 && l < P.nlev - 1; ++l) {
     const Level& L = P.L[l];
     const Level& Lc = P.L[l + 1];
     const long long n = (long long)L.nx * L.ny;
@@ -1311,9 +1066,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
       fused(true, P.nu, L, fw, fw + Lc.f, idx2, st);
     }
   }
-  if (use_cluster) {
-    if (const int rc = launch_cluster_vcycle(P, fw, cl0, ncl, st)) return rc;
-  } else if (P.small0 < P.nlev) {
+  if (P.small0 < P.nlev) {
     const size_t smem = coarse_smem(P);
     coarse_vcycle_kernel<<<1, CT, smem, st>>>(P, fw, P.nu, P.coarse_sweeps);
   } else {
@@ -1331,7 +1084,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     }
   }
   // fine levels on the way up: coarse correction + post-smoothing, fused
-  for (int l = std::min(split, P.nlev - 1) - 1; l >= 0; --l) {
+  for (int l = std::min(P.small0, P.nlev - 1) - 1; l >= 0; --l) {
     const Level& L = P.L[l];
     const Level& Lc = P.L[l + 1];
     const long long n = (long long)L.nx * L.ny;
@@ -1405,7 +1158,6 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
                                                     fw + L0.cx, fw + L0.cy);
   if (P.small0 < P.nlev && coarse_smem(P) > 227 * 1024) return ZB_E_TOO_LARGE;
   if (const int e = enable_coarse_smem()) return e;
-  (void)cluster_capability();   // probed here, outside any stream capture
   const long long n0 = (long long)L0.nx * L0.ny;
   diag_kernel64<<<grid_for(n0), NT, 0, st>>>(dw + P.cx64, dw + P.cy64, L0.nx, L0.ny,
                                              1.0 / (cfg->dx * cfg->dx), dw + P.dg64);
