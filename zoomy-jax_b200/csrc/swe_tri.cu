@@ -83,38 +83,9 @@ __device__ __forceinline__ void to_w(T b, T h, T qx, T qy, T eps, T w[4], T& hin
 }
 
 // ── gradient + limiter ──────────────────────────────────────────────────────
-// Per-cell record that the face kernel gathers (RW values of T, one record per
-// cell, 64-byte aligned for float): W (4), the limited slopes [s0x, s0y, ..,
-// s3x, s3y] (8), h, hinv, two pad values.  A face side is then two 32-byte
-// sectors instead of twelve scattered planes.
-constexpr int RW = 16;
-// Per-face record of the face kernel's results (FW values): the owner's
-// (Fh, Fx, Fy), a pad, the neighbour's (Fh, Fx, Fy), a pad -- one 32-byte
-// sector for float, read by the update kernel as one vector per side.
-constexpr int FW = 8;
-
-template <typename T>
-struct Vec4;
-template <>
-struct Vec4<float> { using type = float4; };
-template <>
-struct Vec4<double> { using type = double4; };
-
-template <typename T>
-__device__ __forceinline__ void st4(T* p, T a, T b, T c, T d) {
-  using V = typename Vec4<T>::type;
-  V v;
-  v.x = a; v.y = b; v.z = c; v.w = d;
-  *reinterpret_cast<V*>(p) = v;
-}
-template <typename T>
-__device__ __forceinline__ typename Vec4<T>::type ld4(const T* p) {
-  return *reinterpret_cast<const typename Vec4<T>::type*>(p);
-}
-
 template <typename T, int RECON>
 __global__ void __launch_bounds__(NT)
-tri_grad_kernel(const T* __restrict__ Q, T* __restrict__ Rec, const Geo<T> geo,
+tri_grad_kernel(const T* __restrict__ Q, T* __restrict__ S, const Geo<T> geo,
                 const Prm<T> p, const unsigned char* __restrict__ force_o1) {
   const int C = geo.C;
   const int c = blockIdx.x * NT + threadIdx.x;
@@ -200,11 +171,11 @@ tri_grad_kernel(const T* __restrict__ Q, T* __restrict__ Rec, const Geo<T> geo,
     phi[3] = fmn(phi[3], phi[1]);
   }
   if (force_o1 != nullptr && force_o1[c]) phi[0] = phi[1] = phi[2] = phi[3] = T(0);
-  T* r = Rec + (size_t)c * RW;
-  st4<T>(r, wc[0], wc[1], wc[2], wc[3]);
-  st4<T>(r + 4, phi[0] * gx[0], phi[0] * gy[0], phi[1] * gx[1], phi[1] * gy[1]);
-  st4<T>(r + 8, phi[2] * gx[2], phi[2] * gy[2], phi[3] * gx[3], phi[3] * gy[3]);
-  st4<T>(r + 12, hc, hic, T(0), T(0));
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    S[(2 * v) * Cs + c] = phi[v] * gx[v];
+    S[(2 * v + 1) * Cs + c] = phi[v] * gy[v];
+  }
 }
 
 // ── face kernel ─────────────────────────────────────────────────────────────
@@ -214,26 +185,18 @@ struct Side {
 };
 
 template <typename T, int ORDER, int RECON>
-__device__ __forceinline__ void face_trace(const T* __restrict__ Q, const T* __restrict__ Rec,
+__device__ __forceinline__ void face_trace(const T* __restrict__ Q, const T* __restrict__ S,
                                            int c, size_t Cs, T rx, T ry, T eps,
                                            Side<T>& sd, T& hc, T& bcell) {
+  const T b = Q[c], h = Q[Cs + c], qx = Q[2 * Cs + c], qy = Q[3 * Cs + c];
+  hc = h;
+  bcell = b;
   T w[4], hinv;
+  to_w<T, RECON>(b, h, qx, qy, eps, w, hinv);
   if (ORDER >= 2) {
-    // the cell's record: W, limited slopes, h, hinv (tri_grad_kernel)
-    const T* r = Rec + (size_t)c * RW;
-    const auto a0 = ld4<T>(r), a1 = ld4<T>(r + 4), a2 = ld4<T>(r + 8), a3 = ld4<T>(r + 12);
-    hc = a3.x;
-    hinv = a3.y;
-    bcell = a0.x;
-    w[0] = a0.x + (a1.x * rx + a1.y * ry);
-    w[1] = a0.y + (a1.z * rx + a1.w * ry);
-    w[2] = a0.z + (a2.x * rx + a2.y * ry);
-    w[3] = a0.w + (a2.z * rx + a2.w * ry);
-  } else {
-    const T b = Q[c], h = Q[Cs + c], qx = Q[2 * Cs + c], qy = Q[3 * Cs + c];
-    hc = h;
-    bcell = b;
-    to_w<T, RECON>(b, h, qx, qy, eps, w, hinv);
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      w[v] = w[v] + (S[(2 * v) * Cs + c] * rx + S[(2 * v + 1) * Cs + c] * ry);
   }
   sd.b = w[0];
   if (RECON == ZB_RECON_ETA) {
@@ -303,11 +266,11 @@ __device__ __forceinline__ void riemann_n(const Side<T>& L, const Side<T>& R, T 
 
 template <typename T, int ORDER, int RECON, int RIEMANN, bool DT>
 __global__ void __launch_bounds__(NT)
-tri_face_kernel(const T* __restrict__ Q, const T* __restrict__ Rec, T* __restrict__ Fc,
+tri_face_kernel(const T* __restrict__ Q, const T* __restrict__ S, T* __restrict__ Fc,
                 const Geo<T> geo, const Prm<T> p, double* dt_slot, unsigned* status) {
   __shared__ double red[NT / 32];
   const int F = geo.F;
-  const size_t Cs = (size_t)geo.C;
+  const size_t Cs = (size_t)geo.C, Fs = (size_t)F;
   const int f = blockIdx.x * NT + threadIdx.x;
   double loc = INFINITY;
   if (f < F) {
@@ -315,10 +278,9 @@ tri_face_kernel(const T* __restrict__ Q, const T* __restrict__ Rec, T* __restric
     const T nx = geo.face_nx[f], ny = geo.face_ny[f];
     Side<T> A, B;
     T hA, bA, hB, bB;
-    face_trace<T, ORDER, RECON>(Q, Rec, a, Cs, geo.face_rax[f], geo.face_ray[f], p.eps_kp, A, hA,
-                                bA);
+    face_trace<T, ORDER, RECON>(Q, S, a, Cs, geo.face_rax[f], geo.face_ray[f], p.eps_kp, A, hA, bA);
     if (bcode >= 0) {
-      face_trace<T, ORDER, RECON>(Q, Rec, bcode, Cs, geo.face_rbx[f], geo.face_rby[f], p.eps_kp, B,
+      face_trace<T, ORDER, RECON>(Q, S, bcode, Cs, geo.face_rbx[f], geo.face_rby[f], p.eps_kp, B,
                                   hB, bB);
     } else {
       // boundary: Q_R = BC(Q_L) at the reconstructed face state
@@ -344,28 +306,21 @@ tri_face_kernel(const T* __restrict__ Q, const T* __restrict__ Rec, T* __restric
       gB = T(0.5) * p.g * (hB + B.h) * (B.b - bB);
     }
     // owner: F + (Dm + gA) n ; neighbour: -F + (Dp - gB) n
-    T* fr = Fc + (size_t)f * FW;
-    st4<T>(fr, Fh, Fx + (Dm + gA) * nx, Fy + (Dm + gA) * ny, T(0));
-    st4<T>(fr + 4, -Fh, -Fx + (Dp - gB) * nx, -Fy + (Dp - gB) * ny, T(0));
+    Fc[0 * Fs + f] = Fh;
+    Fc[1 * Fs + f] = Fx + (Dm + gA) * nx;
+    Fc[2 * Fs + f] = Fy + (Dm + gA) * ny;
+    Fc[3 * Fs + f] = -Fh;
+    Fc[4 * Fs + f] = -Fx + (Dp - gB) * nx;
+    Fc[5 * Fs + f] = -Fy + (Dp - gB) * ny;
     if (DT) {
       // CFL law over faces at the CELL states, owner on both sides of a
       // boundary face (solver2/blocks.py:36-95, context.py:111-117)
       const int bc2 = bcode >= 0 ? bcode : a;
-      T lA, lB;
-      if (ORDER >= 2 && RECON == ZB_RECON_ETA) {
-        // the records hold u = q hinv and v = q hinv of the cells already
-        // (the same products), and h
-        const T* ra = Rec + (size_t)a * RW;
-        const T* rb = Rec + (size_t)bc2 * RW;
-        lA = fabs(ra[2] * nx + ra[3] * ny) + sqrt(p.g * fmx(ra[12], T(0)));
-        lB = fabs(rb[2] * nx + rb[3] * ny) + sqrt(p.g * fmx(rb[12], T(0)));
-      } else {
-        const T hia = kp_hinv(Q[Cs + a], p.eps_kp), hib = kp_hinv(Q[Cs + bc2], p.eps_kp);
-        lA = fabs(Q[2 * Cs + a] * hia * nx + Q[3 * Cs + a] * hia * ny) +
-             sqrt(p.g * fmx(Q[Cs + a], T(0)));
-        lB = fabs(Q[2 * Cs + bc2] * hib * nx + Q[3 * Cs + bc2] * hib * ny) +
-             sqrt(p.g * fmx(Q[Cs + bc2], T(0)));
-      }
+      const T hia = kp_hinv(Q[Cs + a], p.eps_kp), hib = kp_hinv(Q[Cs + bc2], p.eps_kp);
+      const T lA = fabs(Q[2 * Cs + a] * hia * nx + Q[3 * Cs + a] * hia * ny) +
+                   sqrt(p.g * fmx(Q[Cs + a], T(0)));
+      const T lB = fabs(Q[2 * Cs + bc2] * hib * nx + Q[3 * Cs + bc2] * hib * ny) +
+                   sqrt(p.g * fmx(Q[Cs + bc2], T(0)));
       const double am = (double)nmax(lA, lB);
       loc = (p.cfl2 * geo.face_inr[f]) / (p.den_fac * am);
       if (loc != loc) loc = -1.0;   // non-finite state: poison the minimum
@@ -399,7 +354,7 @@ tri_update_kernel(const T* __restrict__ Qk, const T* Q0, T* Qo, const T* __restr
                   const Geo<T> geo, const Prm<T> p, zb_ctrl* ctrl, int phase,
                   const T* __restrict__ hinv_src, unsigned char* __restrict__ trouble_out) {
   const int C = geo.C;
-  const size_t Cs = (size_t)C;
+  const size_t Cs = (size_t)C, Fs = (size_t)geo.F;
   const int c = blockIdx.x * NT + threadIdx.x;
   double dtd;
   if (MODE == MODE_STAGE) {
@@ -427,10 +382,8 @@ tri_update_kernel(const T* __restrict__ Qk, const T* Q0, T* Qo, const T* __restr
     const int code = geo.cell_face[k * Cs + c];
     const int f = code >> 1, side = code & 1;
     const T lw = geo.face_len[f] * ia;
-    const auto fv = ld4<T>(Fc + (size_t)f * FW + 4 * side);
-    dq[0] -= lw * fv.x;
-    dq[1] -= lw * fv.y;
-    dq[2] -= lw * fv.z;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) dq[v] -= lw * Fc[(3 * side + v) * Fs + f];
   }
   const T hk = Qk[Cs + c], qxk = Qk[2 * Cs + c], qyk = Qk[3 * Cs + c];
   T hn, qxn, qyn;
@@ -670,19 +623,19 @@ static Prm<T> make_prm(const zb_tri_cfg* c, double alpha, double beta, double dt
 
 template <typename T, int ORDER, int RECON, int RIEMANN>
 static int stage(const zb_tri_cfg* cfg, const Geo<T>& geo, const Prm<T>& p, const T* Qk,
-                 const T* Q0, T* Qo, T* Rec, T* Fc, zb_ctrl* ctrl, int phase, int mode,
+                 const T* Q0, T* Qo, T* S, T* Fc, zb_ctrl* ctrl, int phase, int mode,
                  const T* hinv_src, const unsigned char* force_o1, unsigned char* trouble,
                  cudaStream_t st) {
   const int gc = (geo.C + NT - 1) / NT, gf = (geo.F + NT - 1) / NT;
-  if (ORDER >= 2) tri_grad_kernel<T, RECON><<<gc, NT, 0, st>>>(Qk, Rec, geo, p, force_o1);
+  if (ORDER >= 2) tri_grad_kernel<T, RECON><<<gc, NT, 0, st>>>(Qk, S, geo, p, force_o1);
   const bool dt = mode == MODE_STEP1 || mode == MODE_EULER;
   double* slot = &ctrl->amax[phase < 3 ? phase : 0];
   if (dt)
     tri_face_kernel<T, ORDER, RECON, RIEMANN, true>
-        <<<gf, NT, 0, st>>>(Qk, Rec, Fc, geo, p, slot, &ctrl->status);
+        <<<gf, NT, 0, st>>>(Qk, S, Fc, geo, p, slot, &ctrl->status);
   else
     tri_face_kernel<T, ORDER, RECON, RIEMANN, false>
-        <<<gf, NT, 0, st>>>(Qk, Rec, Fc, geo, p, slot, &ctrl->status);
+        <<<gf, NT, 0, st>>>(Qk, S, Fc, geo, p, slot, &ctrl->status);
   switch (mode) {
     case MODE_STEP1:
       tri_update_kernel<T, MODE_STEP1><<<gc, NT, 0, st>>>(Qk, Q0, Qo, Fc, geo, p, ctrl, phase,
@@ -720,25 +673,16 @@ static int dispatch(const zb_tri_cfg* c, Fn&& f) {
   return ZB_E_UNSUPPORTED;
 }
 
-// workspace layout: Q1 (4 planes of T, b unused), the per-cell records (RW
-// values each) and the per-face records (FW values each), every part starting
-// on a 256-byte boundary (the workspace start is rounded up to one)
-static size_t ws_round(size_t b) { return (b + 255) / 256 * 256; }
+// workspace layout (elements of T): Q1 (4 planes, b unused), slopes (8
+// planes over cells), face contributions (6 planes over faces)
 template <typename T>
-static size_t ws_bytes(const zb_tri_mesh* m) {
+static void ws_split(const zb_tri_mesh* m, void* ws, T** Q1, T** S, T** Fc) {
+  T* base = (T*)ws;
   const size_t C = (size_t)m->n_cells, F = (size_t)m->n_faces;
-  return ws_round(4 * C * sizeof(T)) + ws_round(RW * C * sizeof(T)) +
-         ws_round(FW * F * sizeof(T)) + 256;
-}
-template <typename T>
-static void ws_split(const zb_tri_mesh* m, void* ws, T** Q1, T** Rec, T** Fc) {
-  const size_t C = (size_t)m->n_cells;
-  char* base = (char*)(((uintptr_t)ws + 255) / 256 * 256);
-  *Q1 = (T*)base;
-  base += ws_round(4 * C * sizeof(T));
-  *Rec = (T*)base;
-  base += ws_round(RW * C * sizeof(T));
-  *Fc = (T*)base;
+  *Q1 = base;
+  *S = base + 4 * C;
+  *Fc = base + 12 * C;
+  (void)F;
 }
 
 template <typename T, int ORDER, int RECON, int RIEMANN>
@@ -746,11 +690,11 @@ static int run_step(const zb_tri_cfg* cfg, const zb_tri_mesh* m, T* Q, void* ws,
                     zb_ctrl* ctrl, int phase, cudaStream_t st) {
   const Geo<T> geo = make_geo<T>(m);
   const Prm<T> p = make_prm<T>(cfg, 0.0, 1.0, -1.0);
-  T *Q1, *Rec, *Fc;
-  ws_split<T>(m, ws, &Q1, &Rec, &Fc);
+  T *Q1, *S, *Fc;
+  ws_split<T>(m, ws, &Q1, &S, &Fc);
   const size_t C = (size_t)m->n_cells;
   if constexpr (ORDER == 1) {
-    int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, Rec, Fc, ctrl, phase,
+    int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, S, Fc, ctrl, phase,
                                              MODE_EULER, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
     ZB_CUDA_TRY(cudaMemcpyAsync(Q + C, Q1 + C, 3 * C * sizeof(T), cudaMemcpyDeviceToDevice, st));
@@ -759,10 +703,10 @@ static int run_step(const zb_tri_cfg* cfg, const zb_tri_mesh* m, T* Q, void* ws,
     // stage 1 reads the b plane of Q through Qk = Q; the stage-1 state Q1
     // holds h, qx, qy in planes 1..3 and Q's b plane is copied once per step
     ZB_CUDA_TRY(cudaMemcpyAsync(Q1, Q, C * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, Rec, Fc, ctrl, phase,
+    int rc = stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q, Q, Q1, S, Fc, ctrl, phase,
                                              MODE_STEP1, nullptr, nullptr, nullptr, st);
     if (rc) return rc;
-    return stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q1, Q, Q, Rec, Fc, ctrl, phase, MODE_STEP2,
+    return stage<T, ORDER, RECON, RIEMANN>(cfg, geo, p, Q1, Q, Q, S, Fc, ctrl, phase, MODE_STEP2,
                                            nullptr, nullptr, nullptr, st);
   }
 }
@@ -777,7 +721,8 @@ extern "C" {
 
 size_t zb_tri_workspace_bytes(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh) {
   if (!valid(cfg, mesh)) return 0;
-  return cfg->dtype == ZB_F64 ? ws_bytes<double>(mesh) : ws_bytes<float>(mesh);
+  const size_t es = cfg->dtype == ZB_F64 ? 8 : 4;
+  return (12 * (size_t)mesh->n_cells + 6 * (size_t)mesh->n_faces) * es + 256;
 }
 
 int zb_tri_init(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, zb_ctrl* ctrl, int phase,
@@ -815,10 +760,10 @@ int zb_tri_stage(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, const void* Qk,
     using T = decltype(tag);
     const Geo<T> geo = make_geo<T>(mesh);
     const Prm<T> p = make_prm<T>(cfg, alpha, beta, dt);
-    T *Q1, *Rec, *Fc;
-    ws_split<T>(mesh, workspace, &Q1, &Rec, &Fc);
+    T *Q1, *S, *Fc;
+    ws_split<T>(mesh, workspace, &Q1, &S, &Fc);
     return stage<T, decltype(O)::value, decltype(R)::value, decltype(M)::value>(
-        cfg, geo, p, (const T*)Qk, (const T*)Q0, (T*)Q_out, Rec, Fc, ctrl, 0, MODE_STAGE,
+        cfg, geo, p, (const T*)Qk, (const T*)Q0, (T*)Q_out, S, Fc, ctrl, 0, MODE_STAGE,
         (const T*)hinv_src, force_o1, trouble_out, st);
   };
   if (cfg->dtype == ZB_F32)
@@ -838,11 +783,11 @@ int zb_tri_dt(const zb_tri_cfg* cfg, const zb_tri_mesh* mesh, const void* Q, voi
     using T = decltype(tag);
     const Geo<T> geo = make_geo<T>(mesh);
     Prm<T> p = make_prm<T>(cfg, 0.0, 1.0, -1.0);
-    T *Q1, *Rec, *Fc;
-    ws_split<T>(mesh, workspace, &Q1, &Rec, &Fc);
+    T *Q1, *S, *Fc;
+    ws_split<T>(mesh, workspace, &Q1, &S, &Fc);
     const int gf = (geo.F + NT - 1) / NT;
     tri_face_kernel<T, 1, ZB_RECON_CONSTANT, ZB_RIEMANN_RUSANOV_HR, true>
-        <<<gf, NT, 0, st>>>((const T*)Q, Rec, Fc, geo, p, &ctrl->reserved[0], &ctrl->status);
+        <<<gf, NT, 0, st>>>((const T*)Q, S, Fc, geo, p, &ctrl->reserved[0], &ctrl->status);
     return zb_launch_check();
   };
   int rc = cfg->dtype == ZB_F32 ? go(float()) : go(double());
