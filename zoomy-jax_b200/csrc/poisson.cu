@@ -26,6 +26,7 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
+#include <utility>
 
 #include "common.cuh"
 
@@ -57,6 +58,33 @@ struct Plan {
   int nu, coarse_sweeps;
   double dx;
 };
+
+// Programmatic dependent launch: the kernels of a solve iteration and of the
+// V-cycle are launched with programmatic stream serialisation, so the next
+// kernel's launch overlaps the tail of this one.  Each of them first waits for
+// its predecessor's completion and memory (griddepcontrol.wait, before any
+// global read or write), then lets its own successor launch; launched without
+// the attribute, both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t pdl_launch(void (*k)(KArgs...), dim3 g, dim3 b, size_t sm, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t c = {};
+  c.gridDim = g;
+  c.blockDim = b;
+  c.dynamicSmemBytes = sm;
+  c.stream = st;
+  cudaLaunchAttribute a[1];
+  a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  a[0].val.programmaticStreamSerializationAllowed = 1;
+  c.attrs = a;
+  c.numAttrs = 1;
+  return cudaLaunchKernelEx(&c, k, std::forward<Args>(args)...);
+}
 
 // scalars (doubles) at plan.scal
 enum { S_BB = 0, S_RR, S_PQ, S_PR, S_ZQ, S_ALPHA, S_BETA, S_REL, S_ITER, S_COUNT = 16 };
@@ -261,6 +289,7 @@ apply_dot_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
                  const double* __restrict__ p, const double* __restrict__ r,
                  double* __restrict__ q, int nx, int ny, double idx2, double* part_pq,
                  double* part_pr, unsigned* counter, double* scal) {
+  pdl_enter();
   __shared__ double red[NT / 32];
   double spq = 0.0, spr = 0.0;
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
@@ -287,6 +316,7 @@ __global__ void __launch_bounds__(NT)
 update_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                  const double* __restrict__ q, double* scal, long long n,
                  double* part_rr, float* __restrict__ r32, unsigned* counter) {
+  pdl_enter();
   __shared__ double red[NT / 32];
   const double a = scal[S_ALPHA];
   double s = 0.0;
@@ -306,6 +336,7 @@ __global__ void __launch_bounds__(NT)
 z_from32_kernel(const float* __restrict__ z32, double* __restrict__ z,
                 const double* __restrict__ q, long long n, double* part_zq, unsigned* counter,
                 double* scal) {
+  pdl_enter();
   __shared__ double red[NT / 32];
   double s = 0.0;
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
@@ -322,6 +353,7 @@ z_from32_kernel(const float* __restrict__ z32, double* __restrict__ z,
 // p = z - beta p
 __global__ void p_update_kernel(double* __restrict__ p, const double* __restrict__ z,
                                 const double* scal, long long n, int first) {
+  pdl_enter();
   const double b = first ? 0.0 : scal[S_BETA];
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
     p[k] = first ? z[k] : z[k] - b * p[k];
@@ -344,6 +376,7 @@ __device__ __forceinline__ void fcg_loop_control(double* scal, cudaGraphConditio
 __global__ void p_update_cond_kernel(double* __restrict__ p, const double* __restrict__ z,
                                      double* scal, long long n, int first,
                                      cudaGraphConditionalHandle h, double tol, int maxit) {
+  pdl_enter();
   const double b = first ? 0.0 : scal[S_BETA];
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
     p[k] = first ? z[k] : z[k] - b * p[k];
@@ -356,6 +389,7 @@ residual64_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
                   const double* __restrict__ x, const double* __restrict__ b,
                   double* __restrict__ r, int nx, int ny, double idx2, double* part_rr,
                   double* part_bb, float* __restrict__ r32, unsigned* counter, double* scal) {
+  pdl_enter();
   __shared__ double red[NT / 32];
   double srr = 0.0, sbb = 0.0;
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
@@ -657,6 +691,7 @@ __global__ void __launch_bounds__(FNT_MAX)
 mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
                const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
                float* __restrict__ fc, int nx, int ny, float idx2) {
+  pdl_enter();
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU + 2;
   constexpr int R = Stage<HALO, TT>::R;
@@ -695,6 +730,7 @@ __global__ void __launch_bounds__(FNT_MAX)
 mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
              const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
              const float* __restrict__ ec, int nx, int ny, float idx2) {
+  pdl_enter();
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU;
   constexpr int R = Stage<HALO, TT>::R;
@@ -773,6 +809,7 @@ __device__ void cta_coarsest(float* x, const float* f, const float* cx, const fl
 
 __global__ void __launch_bounds__(CT)
 coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
+  pdl_enter();
   extern __shared__ float sm[];
   // shared copies of x, f, r, cx, cy, dg for every small level
   float* sx[MAXL]; float* sf[MAXL]; float* sr[MAXL];
@@ -1004,12 +1041,13 @@ static bool valid(const zb_poisson_cfg* c) {
 // coarse right-hand side `to`; up: coarse correction from `to`, post-smoothing)
 // with TT x TT tiles.
 template <int TT>
-static void fused_level(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
-                        dim3 blk, cudaStream_t st) {
+static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
+                       dim3 blk, cudaStream_t st) {
   const dim3 grid((L.ny + TT - 1) / TT, (L.nx + TT - 1) / TT);
   const size_t sm = fused_smem(down ? 2 * nu + 2 : 2 * nu, TT);
   float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x;
-#define ZB_FUSED(K) K<<<grid, blk, sm, st>>>(a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2)
+#define ZB_FUSED(K) e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2)
+  cudaError_t e = cudaSuccess;
   if (down) {
     switch (nu) {
       case 1: ZB_FUSED((mg_down_kernel<1, TT>)); break;
@@ -1026,17 +1064,18 @@ static void fused_level(bool down, int nu, const Level& L, float* fw, float* to,
     }
   }
 #undef ZB_FUSED
+  return e == cudaSuccess ? ZB_OK : ZB_E_CUDA;
 }
 
 // 32 x 32 tiles with 32 x 8 threads when the level has two tiles for every
 // SM; else 16 x 16 tiles with 16 x 32 threads (four times the CTAs, one
 // staged row per thread and phase), so that the few CTAs of a small level
 // finish their serial phases sooner
-static void fused(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
-                  cudaStream_t st) {
+static int fused(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
+                 cudaStream_t st) {
   const bool big = ((L.ny + FT - 1) / FT) * ((L.nx + FT - 1) / FT) >= 2 * 148;
-  if (big) fused_level<FT>(down, nu, L, fw, to, idx2, dim3(32, 8), st);
-  else fused_level<FTS>(down, nu, L, fw, to, idx2, dim3(FTS, 32), st);
+  if (big) return fused_level<FT>(down, nu, L, fw, to, idx2, dim3(32, 8), st);
+  return fused_level<FTS>(down, nu, L, fw, to, idx2, dim3(FTS, 32), st);
 }
 
 static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, cudaStream_t st) {
@@ -1063,12 +1102,13 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
       restrict_kernel<<<grid_for((long long)Lc.nx * Lc.ny), NT, 0, st>>>(fw + L.r, fw + Lc.f,
                                                                           Lc.nx, Lc.ny);
     } else {
-      fused(true, P.nu, L, fw, fw + Lc.f, idx2, st);
+      if (const int rc = fused(true, P.nu, L, fw, fw + Lc.f, idx2, st)) return rc;
     }
   }
   if (P.small0 < P.nlev) {
     const size_t smem = coarse_smem(P);
-    coarse_vcycle_kernel<<<1, CT, smem, st>>>(P, fw, P.nu, P.coarse_sweeps);
+    ZB_CUDA_TRY(pdl_launch(coarse_vcycle_kernel, dim3(1), dim3(CT), smem, st, P, fw, P.nu,
+                           P.coarse_sweeps));
   } else {
     // no level fits the one-CTA kernel: sweep the coarsest level in place
     const Level& L = P.L[P.nlev - 1];
@@ -1095,7 +1135,7 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 0, (void*)st);
       if (rc) return rc;
     } else {
-      fused(false, P.nu, L, fw, fw + Lc.x, idx2, st);
+      if (const int rc = fused(false, P.nu, L, fw, fw + Lc.x, idx2, st)) return rc;
     }
   }
   if (precond == 2) {
@@ -1254,18 +1294,22 @@ static int fcg_start_impl(const zb_poisson_cfg* cfg, void* ws, const double* b, 
   double* part = dw + P.part;
   double* scal = dw + P.scal;
   unsigned* ctr = counters(scal);
-  residual64_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, x, b, dw + P.vr, cfg->nx,
-                                               cfg->ny, 1.0 / (cfg->dx * cfg->dx), part,
-                                               part + RED_BLOCKS, fw + P.L[0].f, ctr, scal);
+  ZB_CUDA_TRY(pdl_launch(residual64_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
+                         (const double*)(dw + P.cx64), (const double*)(dw + P.cy64),
+                         (const double*)x, b, dw + P.vr, cfg->nx, cfg->ny,
+                         1.0 / (cfg->dx * cfg->dx), part, part + RED_BLOCKS, fw + P.L[0].f, ctr,
+                         scal));
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
-  z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, nullptr, n, nullptr,
-                                             nullptr, scal);
+  ZB_CUDA_TRY(pdl_launch(z_from32_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
+                         (const float*)(fw + P.L[0].x), dw + P.vz, (const double*)nullptr, n,
+                         (double*)nullptr, (unsigned*)nullptr, scal));
   if (lc)
-    p_update_cond_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1, lc->h,
-                                                     lc->tol, lc->maxit);
+    ZB_CUDA_TRY(pdl_launch(p_update_cond_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
+                           (const double*)(dw + P.vz), scal, n, 1, lc->h, lc->tol, lc->maxit));
   else
-    p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 1);
+    ZB_CUDA_TRY(pdl_launch(p_update_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
+                           (const double*)(dw + P.vz), (const double*)scal, n, 1));
   return zb_launch_check();
 }
 
@@ -1286,21 +1330,25 @@ static int fcg_iterate_impl(const zb_poisson_cfg* cfg, void* ws, double* x, int 
   double* part = dw + P.part;
   double* scal = dw + P.scal;
   unsigned* ctr = counters(scal);
-  apply_dot_kernel<<<RED_BLOCKS, NT, 0, st>>>(dw + P.cx64, dw + P.cy64, dw + P.vp, dw + P.vr,
-                                              dw + P.vq, cfg->nx, cfg->ny,
-                                              1.0 / (cfg->dx * cfg->dx), part, part + RED_BLOCKS,
-                                              ctr + 1, scal);
-  update_xr_kernel<<<RED_BLOCKS, NT, 0, st>>>(x, dw + P.vr, dw + P.vp, dw + P.vq, scal, n,
-                                              part + 2 * RED_BLOCKS, fw + P.L[0].f, ctr + 2);
+  ZB_CUDA_TRY(pdl_launch(apply_dot_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
+                         (const double*)(dw + P.cx64), (const double*)(dw + P.cy64),
+                         (const double*)(dw + P.vp), (const double*)(dw + P.vr), dw + P.vq, cfg->nx,
+                         cfg->ny, 1.0 / (cfg->dx * cfg->dx), part, part + RED_BLOCKS, ctr + 1,
+                         scal));
+  ZB_CUDA_TRY(pdl_launch(update_xr_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st, x, dw + P.vr,
+                         (const double*)(dw + P.vp), (const double*)(dw + P.vq), scal, n,
+                         part + 2 * RED_BLOCKS, fw + P.L[0].f, ctr + 2));
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
-  z_from32_kernel<<<RED_BLOCKS, NT, 0, st>>>(fw + P.L[0].x, dw + P.vz, dw + P.vq, n,
-                                             part + 3 * RED_BLOCKS, ctr + 3, scal);
+  ZB_CUDA_TRY(pdl_launch(z_from32_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
+                         (const float*)(fw + P.L[0].x), dw + P.vz, (const double*)(dw + P.vq), n,
+                         part + 3 * RED_BLOCKS, ctr + 3, scal));
   if (lc)
-    p_update_cond_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0, lc->h,
-                                                     lc->tol, lc->maxit);
+    ZB_CUDA_TRY(pdl_launch(p_update_cond_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
+                           (const double*)(dw + P.vz), scal, n, 0, lc->h, lc->tol, lc->maxit));
   else
-    p_update_kernel<<<grid_for(n), NT, 0, st>>>(dw + P.vp, dw + P.vz, scal, n, 0);
+    ZB_CUDA_TRY(pdl_launch(p_update_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
+                           (const double*)(dw + P.vz), (const double*)scal, n, 0));
   return zb_launch_check();
 }
 
