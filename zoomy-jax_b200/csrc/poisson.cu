@@ -43,6 +43,7 @@ struct Level {
   int nx, ny;
   float dx;
   long long cx, cy, dg, x, f, r;   // float offsets into the workspace
+  long long xo;                    // the level's V-cycle result (see mg_up_kernel)
 };
 
 struct Plan {
@@ -111,6 +112,7 @@ static Plan make_plan(const zb_poisson_cfg* c) {
     L.x = f; f += (long long)nx * ny;
     L.f = f; f += (long long)nx * ny;
     L.r = f; f += (long long)nx * ny;
+    L.xo = f; f += (long long)nx * ny;
     if (P.small0 < 0 && nx <= SMALL && ny <= SMALL) P.small0 = l;
     ++l;
     if (nx <= c->coarsest || ny <= c->coarsest || (nx & 1) || (ny & 1)) break;
@@ -724,12 +726,17 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   }
 }
 
-// x += P e (coarse correction), post-smoothing (NU black/red pairs)
+// x += P e (coarse correction), post-smoothing (NU black/red pairs).  The
+// tile stages its halo from `x` (the way down's result, which neighbouring
+// tiles also read) and writes the level's result to the separate `xo`: a tile
+// that finished before a neighbour staged its halo must not have overwritten
+// what that neighbour reads (a level with more tiles than one wave of CTAs)
 template <int NU, int TT>
 __global__ void __launch_bounds__(FNT_MAX)
 mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
-             const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
-             const float* __restrict__ ec, int nx, int ny, float idx2) {
+             const float* __restrict__ cy, const float* __restrict__ dg,
+             const float* __restrict__ x, const float* __restrict__ ec, float* __restrict__ xo,
+             int nx, int ny, float idx2) {
   pdl_enter();
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU;
@@ -751,7 +758,7 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   for (int e = tid; e < TT * TT; e += nt) {
     const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
-    if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
+    if (gi < nx && gj < ny) xo[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
   }
 }
 
@@ -884,7 +891,7 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     }
   }
   const Level& L0 = P.L[P.small0];
-  for (int k = threadIdx.x; k < L0.nx * L0.ny; k += CT) ws_f[L0.x + k] = sx[P.small0][k];
+  for (int k = threadIdx.x; k < L0.nx * L0.ny; k += CT) ws_f[L0.xo + k] = sx[P.small0][k];
 }
 
 // dense inverse of the coarsest operator (float64 in-place Gauss-Jordan; the
@@ -1043,10 +1050,17 @@ static bool valid(const zb_poisson_cfg* c) {
 template <int TT>
 static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
                        dim3 blk, cudaStream_t st) {
+  // down: `to` = the coarse right-hand side it restricts into; up: `to` =
+  // the coarse level's result it prolongs from
   const dim3 grid((L.ny + TT - 1) / TT, (L.nx + TT - 1) / TT);
   const size_t sm = fused_smem(down ? 2 * nu + 2 : 2 * nu, TT);
-  float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg, *a4 = fw + L.x;
+  const float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg;
+  float* a4 = fw + L.x;
+  float* a5 = fw + L.xo;
 #define ZB_FUSED(K) e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2)
+#define ZB_FUSED_UP(K) \
+  e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, (const float*)a4, (const float*)to, a5, \
+                 L.nx, L.ny, idx2)
   cudaError_t e = cudaSuccess;
   if (down) {
     switch (nu) {
@@ -1057,13 +1071,14 @@ static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, 
     }
   } else {
     switch (nu) {
-      case 1: ZB_FUSED((mg_up_kernel<1, TT>)); break;
-      case 2: ZB_FUSED((mg_up_kernel<2, TT>)); break;
-      case 3: ZB_FUSED((mg_up_kernel<3, TT>)); break;
-      default: ZB_FUSED((mg_up_kernel<4, TT>)); break;
+      case 1: ZB_FUSED_UP((mg_up_kernel<1, TT>)); break;
+      case 2: ZB_FUSED_UP((mg_up_kernel<2, TT>)); break;
+      case 3: ZB_FUSED_UP((mg_up_kernel<3, TT>)); break;
+      default: ZB_FUSED_UP((mg_up_kernel<4, TT>)); break;
     }
   }
 #undef ZB_FUSED
+#undef ZB_FUSED_UP
   return e == cudaSuccess ? ZB_OK : ZB_E_CUDA;
 }
 
@@ -1083,9 +1098,15 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
   const Level& L0 = P.L[0];
   const long long n0 = (long long)L0.nx * L0.ny;
   if (precond == 0) {
-    copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + L0.f, fw + L0.x, n0);
+    copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + L0.f, fw + L0.xo, n0);
     return zb_launch_check();
   }
+  // where a level's result lands: the fused up launch and the one-CTA kernel
+  // write xo; the in-place sweeps of the coarsest level (no level fits the
+  // one-CTA kernel) leave it in x
+  auto result = [&](int l) -> float* {
+    return (P.small0 >= P.nlev && l == P.nlev - 1) ? fw + P.L[l].x : fw + P.L[l].xo;
+  };
   // fine levels: one fused launch each on the way down
   for (int l = 0; l < P.small0 && l < P.nlev - 1; ++l) {
     const Level& L = P.L[l];
@@ -1130,16 +1151,18 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     const long long n = (long long)L.nx * L.ny;
     const float idx2 = 1.0f / (L.dx * L.dx);
     if (l == 0 && precond == 3) {
-      prolong_add_kernel<<<grid_for(n), NT, 0, st>>>(fw + Lc.x, fw + L.x, Lc.nx, Lc.ny);
-      int rc = zb_smoother_apply(smo, fw + L.f, fw + L.x, fw + L.x, fw + L.cx, fw + L.cy,
+      prolong_add_kernel<<<grid_for(n), NT, 0, st>>>(result(l + 1), fw + L.x, Lc.nx, Lc.ny);
+      int rc = zb_smoother_apply(smo, fw + L.f, fw + L.x, fw + L.xo, fw + L.cx, fw + L.cy,
                                  fw + L.r, L.nx, L.ny, (double)L.dx, 0, (void*)st);
       if (rc) return rc;
     } else {
-      if (const int rc = fused(false, P.nu, L, fw, fw + Lc.x, idx2, st)) return rc;
+      if (const int rc = fused(false, P.nu, L, fw, result(l + 1), idx2, st)) return rc;
     }
   }
+  if (result(0) != fw + L0.xo)   // a single level swept in place
+    copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + L0.x, fw + L0.xo, n0);
   if (precond == 2) {
-    int rc = zb_smoother_apply(smo, fw + L0.f, fw + L0.x, fw + L0.x, fw + L0.cx, fw + L0.cy,
+    int rc = zb_smoother_apply(smo, fw + L0.f, fw + L0.xo, fw + L0.xo, fw + L0.cx, fw + L0.cy,
                                fw + L0.r, L0.nx, L0.ny, (double)L0.dx, 0, (void*)st);
     if (rc) return rc;
   }
@@ -1162,14 +1185,14 @@ size_t zb_poisson_workspace_bytes(const zb_poisson_cfg* cfg) {
 int zb_poisson_layout(const zb_poisson_cfg* cfg, int64_t* out) {
   if (!valid(cfg) || !out) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
-  // byte offsets: r, z, p, q (float64 Krylov vectors), scalars, level-0 float
-  // arrays x and f, number of levels, first one-CTA level
+  // byte offsets: r, z, p, q (float64 Krylov vectors), scalars, the V-cycle's
+  // float result on level 0 and level-0 f, number of levels, first one-CTA level
   out[0] = P.vr * 8;
   out[1] = P.vz * 8;
   out[2] = P.vp * 8;
   out[3] = P.vq * 8;
   out[4] = P.scal * 8;
-  out[5] = P.fbase + P.L[0].x * 4;
+  out[5] = P.fbase + P.L[0].xo * 4;
   out[6] = P.fbase + P.L[0].f * 4;
   out[7] = P.nlev;
   out[8] = P.small0;
@@ -1240,7 +1263,7 @@ int zb_poisson_vcycle(const zb_poisson_cfg* cfg, void* ws, const float* r, float
   copy32_kernel<<<grid_for(n0), NT, 0, st>>>(r, fw + P.L[0].f, n0);
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
-  copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + P.L[0].x, z, n0);
+  copy32_kernel<<<grid_for(n0), NT, 0, st>>>(fw + P.L[0].xo, z, n0);
   return zb_launch_check();
 }
 
@@ -1302,7 +1325,7 @@ static int fcg_start_impl(const zb_poisson_cfg* cfg, void* ws, const double* b, 
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
   ZB_CUDA_TRY(pdl_launch(z_from32_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
-                         (const float*)(fw + P.L[0].x), dw + P.vz, (const double*)nullptr, n,
+                         (const float*)(fw + P.L[0].xo), dw + P.vz, (const double*)nullptr, n,
                          (double*)nullptr, (unsigned*)nullptr, scal));
   if (lc)
     ZB_CUDA_TRY(pdl_launch(p_update_cond_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
@@ -1341,7 +1364,7 @@ static int fcg_iterate_impl(const zb_poisson_cfg* cfg, void* ws, double* x, int 
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
   ZB_CUDA_TRY(pdl_launch(z_from32_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
-                         (const float*)(fw + P.L[0].x), dw + P.vz, (const double*)(dw + P.vq), n,
+                         (const float*)(fw + P.L[0].xo), dw + P.vz, (const double*)(dw + P.vq), n,
                          part + 3 * RED_BLOCKS, ctr + 3, scal));
   if (lc)
     ZB_CUDA_TRY(pdl_launch(p_update_cond_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
