@@ -83,7 +83,12 @@ static cudaError_t pdl_launch(void (*k)(KArgs...), dim3 g, dim3 b, size_t sm, cu
   a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   a[0].val.programmaticStreamSerializationAllowed = 1;
   c.attrs = a;
-  c.numAttrs = 1;
+  // only on launches outside stream capture: inside the FCG graph's
+  // conditional body the programmatic edges measured slower than plain ones
+  // (1024^2 pressure solve, 8 iterations: 1.655 ms against 1.628 ms)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+  c.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
   return cudaLaunchKernelEx(&c, k, std::forward<Args>(args)...);
 }
 
