@@ -100,6 +100,13 @@ typedef struct {
   double t_end;            /* t_end clamp (+inf: none)                     */
   int32_t degree;          /* k of the (2k+1) CFL factor                   */
   int32_t dtype;           /* ZB_F32 / ZB_F64                              */
+  /* NULL, or the planes zb_swe2d_bed_prepare wrote for the b row of every
+   * state stepped with this config (device memory).  Read by the fused steps
+   * of the float32 order-2 eta / HLL-HR scheme on grids without a periodic
+   * side (ignored by every other scheme, by the stage API and by the
+   * ensemble); the results are the same bits either way.  The caller owns
+   * the promise that b has not changed since the planes were prepared. */
+  const void* bed;
 } zb_swe2d_cfg;
 
 /* Library version / build info. */
@@ -108,6 +115,21 @@ const char* zb_version(void);
 /* Bytes of device workspace zb_swe2d_step needs (one stage buffer of three
  * planes plus alignment padding). */
 size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg);
+
+/* Bytes of the bed planes of cfg's scheme (0 when the scheme does not read
+ * them: see zb_swe2d_cfg.bed). */
+size_t zb_swe2d_bed_bytes(const zb_swe2d_cfg* cfg);
+
+/* The bathymetry's interior least-squares gradient (x, y) and limiter value,
+ * three float32 planes laid out like a state row, from the b row of Q.  b is
+ * constant in time (the reference steps it with a zero update), so a march
+ * prepares them once and the interior body of every step reads them instead
+ * of re-evaluating b's slope each stage (the reference's reconstruction
+ * evaluates the gradient and limiter of every variable, b included, on every
+ * call: zoomy_jax/fvm/reconstruction_jax.py:524-533, 695-708).  ZB_E_ARG for
+ * a scheme without bed planes. */
+int zb_swe2d_bed_prepare(const zb_swe2d_cfg* cfg, const void* Q, void* bed,
+                         size_t bed_bytes, zb_stream_t stream);
 
 /* Initialise the control block for a march starting at time t0 from state Q:
  * clears status and all slots, sets t[phase] = t0 and amax[phase] = the

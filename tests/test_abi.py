@@ -45,6 +45,29 @@ def test_struct_layouts_match_header():
     assert L.ZbSwe2dCfg.bc.offset == 56
 
 
+def test_cfg_struct_matches_the_c_compiler(tmp_path):
+    """Every field offset of the ctypes mirror of zb_swe2d_cfg and its size,
+    against what gcc lays out from the header."""
+    import shutil
+    import subprocess
+    from zoomy_b200 import _lib as L
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    names = [f[0] for f in L.ZbSwe2dCfg._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include "zb.h"\nint main(void) {\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(zb_swe2d_cfg, {n}));\n'
+                             for n in names)
+                   + '  printf("%zu\\n", sizeof(zb_swe2d_cfg));\n  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    want = [getattr(L.ZbSwe2dCfg, n).offset for n in names] + [ctypes.sizeof(L.ZbSwe2dCfg)]
+    assert got == want
+
+
 def test_version_string():
     from zoomy_b200 import _lib as L
     assert b"sm_100a" in L.load().zb_version()

@@ -68,6 +68,10 @@ struct SweParams {
   // 1: the strip region is the whole grid (fast_i0 = fast_j0 = 0; the strips
   // reach the boundary and keep the control block; no tile launch)
   int strip_full;
+  // the bed's interior gradient and limiter value (planes gx, gy, phi of
+  // zb_swe2d_bed_prepare), read by the float32 eta / HLL-HR interior strip
+  // body; nullptr: evaluated from b like every other variable
+  const T* bed;
   LsqTable<T> lsq;
 };
 
@@ -939,7 +943,7 @@ __device__ __forceinline__ void bcol_row(const T* __restrict__ bP, const T* __re
 //      step, where the 32-row ensemble items gain 2.10 -> 1.92 ms).
 // `lead` (one item of the grid in full-coverage mode, where no tile kernel
 // runs) keeps the control block.
-template <typename T, int RECON, int RIEMANN, int MODE, int EK>
+template <typename T, int RECON, int RIEMANN, int MODE, int EK, bool BEDT = false>
 __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __restrict__ hP,
                                            const T* __restrict__ qxP, const T* __restrict__ qyP,
                                            const T* __restrict__ h0P,
@@ -985,6 +989,12 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   // the pre-pass, slots [side][m - (r0 - 1)][12] of this warp (side 0: column
   // 0, side 1: column ny - 1; rows r0 - 1 .. r1)
   constexpr bool PRE = EK == 3 && PAIR;
+  // BEDT: float32 interior items read b's gradient and limiter value from the
+  // planes swe2d_bed_kernel prepared (b never changes) instead of evaluating
+  // them; the planes are laid out like the state's
+  constexpr bool BED = BEDT && PAIR && EK == 0;
+  const T* __restrict__ bedP = p.bed;
+  const size_t bed_plane = (size_t)nx * ny;
   constexpr int PROWS = SXC_MAX + 2;
   T* bs = nullptr;
   if constexpr (PRE) {
@@ -1013,6 +1023,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   const int nsteps = (r1 - r0) + 4;
   // row r + 1 is fetched while row r is processed
   T nbv = T(0), nhv = T(0), nqxv = T(0), nqyv = T(0);
+  T nbgx = T(0), nbgy = T(0), nbphi = T(0);   // BED: the next slope row's bed values
   if (!CG || (colv && (!EDGE || r0 - 2 >= 0))) {
     const size_t k = (size_t)(r0 - 2) * ny + cj;
     nbv = bP[k]; nhv = hP[k]; nqxv = qxP[k]; nqyv = qyP[k];
@@ -1028,6 +1039,15 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       const size_t k = (size_t)ro * ny + cj;
       if (RECON == ZB_RECON_ETA) { qxk = qxP[k]; qyk = qyP[k]; }
       if (MODE == MODE_STEP2) { h0 = h0P[k]; qx0 = qx0P[k]; qy0 = qy0P[k]; }
+    }
+    // the bed slopes of row r - 1 (the slope block below), fetched in the
+    // previous iteration; fetch row r's for the next one
+    const T bgx = nbgx, bgy = nbgy, bphi = nbphi;
+    if (BED && s >= 1 && r <= r1) {
+      const size_t k = (size_t)r * ny + cj;   // BED: EK == 0, no guards
+      nbgx = __ldg(bedP + k);
+      nbgy = __ldg(bedP + bed_plane + k);
+      nbphi = __ldg(bedP + 2 * bed_plane + k);
     }
     // shift the windows and take row r
     R0 = R1; R1 = R2;
@@ -1061,6 +1081,7 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       }
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
+        if (v == 0 && BED) continue;   // b's windows feed only its slope
         const T w = R2.w(v);
         const T wl = shu(w), wr = shd(w);
         Wm2[v] = wl;
@@ -1078,6 +1099,12 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
         const bool clipmin = p.limiter != ZB_LIM_NONE && p.limiter != ZB_LIM_VENKATAKRISHNAN;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
+          if (v == 0 && BED) {
+            gxa[0] = bgx;
+            gya[0] = bgy;
+            phi[0] = bphi;
+            continue;
+          }
           const float u = R1.w(v);
           const float tc = (R0.w(v) + R1.w(v)) + R2.w(v);
           const float tl = shu(tc), tr = shd(tc);
@@ -1468,7 +1495,8 @@ __host__ __device__ inline int full_items(int nx, int ny, int item, int* strip, 
 
 // KIND 0: the interior strips of a grid with a periodic side (the tile kernel
 // takes the frame); KIND 1: the boundary items of a full-coverage list
-// (column-EDGE and EDGE); KIND 2: its interior items.  Kinds 1 and 2 are
+// (column-EDGE and EDGE); KIND 2: its interior items; KIND 3: its interior
+// items reading the prepared bed planes (p.bed).  Kinds 1 and 2 are
 // separate launches (they run side by side on two streams) so that the
 // boundary bodies never raise the interior body's register allocation.
 // float32: 4 CTAs of 4 warps per SM (128 registers; the paired-face interior
@@ -1491,7 +1519,7 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
   } else {
     const int ne = full_items(p.nx, p.ny, -2, nullptr, nullptr, nullptr, nullptr, SXC_GRID);
     if (KIND == 1 && item >= ne) return;
-    if (KIND == 2) {
+    if (KIND >= 2) {
       item += ne;
       const int n = full_items(p.nx, p.ny, -1, nullptr, nullptr, nullptr, nullptr, SXC_GRID);
       if (item >= n) return;
@@ -1507,8 +1535,9 @@ swe2d_strip_kernel(const T* __restrict__ bP, const T* __restrict__ hP,
       strip_item<T, RECON, RIEMANN, MODE, 1>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO,
                                              ctrl, phase, p, strip, r0, r1, item == 0);
   } else {
-    strip_item<T, RECON, RIEMANN, MODE, 0>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO, qxO, qyO,
-                                           ctrl, phase, p, strip, r0, r1, false);
+    strip_item<T, RECON, RIEMANN, MODE, 0, KIND == 3>(bP, hP, qxP, qyP, h0P, qx0P, qy0P, hO,
+                                                      qxO, qyO, ctrl, phase, p, strip, r0, r1,
+                                                      false);
   }
 }
 
@@ -1693,6 +1722,51 @@ swe2d_amax_kernel(const T* __restrict__ hP, const T* __restrict__ qxP,
   }
   m = block_max_double(m, red);
   if (threadIdx.x == 0) atomic_max_pos_double(out, m);
+}
+
+// The bed's interior least-squares gradient and limiter value, one thread per
+// cell: the float32 paired slope block of strip_item for variable 0 (b), in
+// the same operations and order ((left + centre) + right sums, paired
+// difference and scaling, three-input bounds, the limiter), so the strip body
+// that reads these planes produces the same bits as the one that evaluates
+// them.  Cells on the domain boundary get zeros (the interior body never
+// reads them; boundary cells take the boundary classes).
+__global__ void __launch_bounds__(NT)
+swe2d_bed_kernel(const float* __restrict__ b, float* __restrict__ bed,
+                 const SweParams<float> p) {
+  const int nx = p.nx, ny = p.ny;
+  const size_t n = (size_t)nx * ny;
+  const bool clipmin = p.limiter != ZB_LIM_NONE && p.limiter != ZB_LIM_VENKATAKRISHNAN;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k / (size_t)ny), j = (int)(k % (size_t)ny);
+    float gx = 0.f, gy = 0.f, phi = 0.f;
+    if (i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1) {
+      const float* rm = b + (k - ny);   // row i - 1
+      const float* rc = b + k;          // row i
+      const float* rp = b + (k + ny);   // row i + 1
+      const float u = rc[0];
+      const float sx0 = (rm[-1] + rm[0]) + rm[1];   // row sums of rows i -/+ 1
+      const float sx2 = (rp[-1] + rp[0]) + rp[1];
+      const float tl = (rm[-1] + rc[-1]) + rp[-1];  // column sums of columns j -/+ 1
+      const float tr = (rm[1] + rc[1]) + rp[1];
+      const float2 gv = mul2(sub2(f2(sx2, tr), f2(sx0, tl)), f2(p.inv6dx, p.inv6dy));
+      const float umax = fmx3(u, rp[0], fmx3(rm[0], rc[1], rc[-1]));
+      const float umin = fmn3(u, rp[0], fmn3(rm[0], rc[1], rc[-1]));
+      const float2 dd = sub2(f2(umax, umin), f2(u, u));
+      gx = gv.x;
+      gy = gv.y;
+      if (clipmin) {
+        const float2 ac = mul2(gv, f2(p.half_dx, p.half_dy));
+        phi = phi_clipmin(ac.x, ac.y, dd.x, dd.y);
+      } else {
+        phi = limiter_phi(p.limiter, gv.x, gv.y, p.half_dx, p.half_dy, dd.x, dd.y, p.vk_eps2);
+      }
+    }
+    bed[k] = gx;
+    bed[n + k] = gy;
+    bed[2 * n + k] = phi;
+  }
 }
 
 __global__ void swe2d_ctrl_init_kernel(zb_ctrl* ctrl, int phase, double t0) {
@@ -1889,6 +1963,13 @@ static LsqTable<T> make_lsq(double dx, double dy) {
   return tab;
 }
 
+// the scheme whose interior body reads prepared bed slopes: float32, order 2,
+// eta reconstruction, HLL with hydrostatic reconstruction
+static bool bed_scheme(const zb_swe2d_cfg* c) {
+  return c->dtype == ZB_F32 && c->order == 2 && c->recon == ZB_RECON_ETA &&
+         c->riemann == ZB_RIEMANN_HLL_HR;
+}
+
 template <typename T>
 static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta,
                                 double dt_stage = -1.0) {
@@ -1925,6 +2006,7 @@ static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta
   p.inv4dy = (T)(1.0 / (4.0 * c->dy));
   p.fast_i0 = p.fast_i1 = p.fast_j0 = p.fast_j1 = 0;
   p.strip_full = 0;
+  p.bed = (std::is_same<T, float>::value && bed_scheme(c)) ? (const T*)c->bed : nullptr;
   return p;
 }
 
@@ -2042,9 +2124,23 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
         b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
     ZB_CUDA_TRY(cudaGetLastError());
     if (ni > 0) {
-      swe2d_strip_kernel<T, RECON, RIEMANN, M, 2><<<(ni + wpb - 1) / wpb, STRIP_NT, 0, st>>>(
-          b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
-      ZB_CUDA_TRY(cudaGetLastError());
+      // the interior items read the prepared bed planes when there are some
+      constexpr bool BEDK = std::is_same<T, float>::value && RECON == ZB_RECON_ETA &&
+                            RIEMANN == ZB_RIEMANN_HLL_HR;
+      bool done = false;
+      if constexpr (BEDK) {
+        if (pf.bed) {
+          swe2d_strip_kernel<T, RECON, RIEMANN, M, 3><<<(ni + wpb - 1) / wpb, STRIP_NT, 0, st>>>(
+              b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
+          ZB_CUDA_TRY(cudaGetLastError());
+          done = true;
+        }
+      }
+      if (!done) {
+        swe2d_strip_kernel<T, RECON, RIEMANN, M, 2><<<(ni + wpb - 1) / wpb, STRIP_NT, 0, st>>>(
+            b, h_, qx_, qy_, h0_, qx0_, qy0_, ho_, qxo_, qyo_, ctrl, phase, pf);
+        ZB_CUDA_TRY(cudaGetLastError());
+      }
     }
     ZB_CUDA_TRY(cudaEventRecord(side->join, side->s));
     ZB_CUDA_TRY(cudaStreamWaitEvent(st, side->join, 0));
@@ -2312,6 +2408,22 @@ size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg) {
   return 3 * (size_t)cfg->nx * cfg->ny * es + 256;
 }
 
+size_t zb_swe2d_bed_bytes(const zb_swe2d_cfg* cfg) {
+  if (!valid_cfg(cfg) || !bed_scheme(cfg)) return 0;
+  return 3 * (size_t)cfg->nx * cfg->ny * sizeof(float);
+}
+
+int zb_swe2d_bed_prepare(const zb_swe2d_cfg* cfg, const void* Q, void* bed, size_t bed_bytes,
+                         zb_stream_t stream) {
+  if (!valid_cfg(cfg) || !bed_scheme(cfg) || !Q || !bed) return ZB_E_ARG;
+  if (bed_bytes < zb_swe2d_bed_bytes(cfg) || ((uintptr_t)bed & 3u)) return ZB_E_ARG;
+  const SweParams<float> p = make_params<float>(cfg, 0.0, 1.0);
+  const size_t n = (size_t)cfg->nx * cfg->ny;
+  const int grid = (int)std::min<size_t>((n + NT - 1) / NT, (size_t)148 * 16);
+  swe2d_bed_kernel<<<grid, NT, 0, (cudaStream_t)stream>>>((const float*)Q, (float*)bed, p);
+  return zb_launch_check();
+}
+
 int zb_swe2d_init(const zb_swe2d_cfg* cfg, const void* Q, zb_ctrl* ctrl, int phase,
                   double t0, zb_stream_t stream) {
   if (!valid_cfg(cfg) || !Q || !ctrl || phase < 0 || phase > 2) return ZB_E_ARG;
@@ -2536,6 +2648,7 @@ int zb_ens_prepare_tuned(const zb_swe2d_cfg* common, const zb_ens_instance* inst
     std::vector<int4> items(1), strips, estrips, cstrips;
     for (int i = 0; i < n_inst; ++i) {
       zb_swe2d_cfg c = *common;
+      c.bed = nullptr;   // instances read their own b; no prepared bed planes
       c.nx = inst[i].nx;
       c.ny = inst[i].ny;
       c.dx = inst[i].dx;

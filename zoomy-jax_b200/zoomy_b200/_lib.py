@@ -46,7 +46,7 @@ class ZbSwe2dCfg(C.Structure):
                 ("implicit_source", C.c_int32), ("dim_factor", C.c_int32),
                 ("cfl", C.c_double), ("dt_max", C.c_double),
                 ("t_end", C.c_double), ("degree", C.c_int32),
-                ("dtype", C.c_int32)]
+                ("dtype", C.c_int32), ("bed", C.c_void_p)]
 
 
 class ZbTriCfg(C.Structure):
@@ -120,6 +120,8 @@ SIGNATURES = [
     ("zb_swe2d_init", C.c_int, [_CFG, _P, _P, C.c_int, C.c_double, _P]),
     ("zb_swe2d_dt", C.c_int, [_CFG, _P, _P, C.c_double, _P]),
     ("zb_swe2d_step", C.c_int, [_CFG, _P, _P, C.c_size_t, _P, C.c_int, _P]),
+    ("zb_swe2d_bed_bytes", C.c_size_t, [_CFG]),
+    ("zb_swe2d_bed_prepare", C.c_int, [_CFG, _P, _P, C.c_size_t, _P]),
     ("zb_swe2d_step_part", C.c_int, [_CFG, _P, _P, C.c_size_t, _P, C.c_int, C.c_int, _P]),
     ("zb_swe2d_step_noalloc", C.c_int, [_CFG, _P, _P, C.c_int, _P]),
     ("zb_swe2d_stage", C.c_int, [_CFG, _P, _P, _P, C.c_double, C.c_double,
