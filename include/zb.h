@@ -366,9 +366,11 @@ typedef struct zb_smoother {
 } zb_smoother;
 
 /* Convolution engine of the U-Net's forward and data-gradient passes:
- * 1 = tcgen05 implicit GEMM (bf16 operands, float32 accumulation; default),
- * 0 = CUDA-core direct convolution (float32 operands).  Returns the previous
- * setting (process-wide; any other value only queries). */
+ * 1 = tcgen05 implicit GEMM (bf16 operands, float32 accumulation; default;
+ * zb_smoother_apply's activations in a chunked bf16 layout, 8 channels per
+ * 16 bytes), 2 = the same GEMM staging float32 planar activations everywhere
+ * (the same bits as 1), 0 = CUDA-core direct convolution (float32 operands).
+ * Returns the previous setting (process-wide; any other value only queries). */
 int zb_unet_conv_impl(int impl);
 
 /* Error word of the tensor-core kernels: non-zero when a bounded wait timed

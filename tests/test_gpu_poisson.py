@@ -201,10 +201,12 @@ def _batch(B, n, seed):
     return r, cx, cy
 
 
-@pytest.fixture(params=[1, 0], ids=["tcgen05", "cuda_core"])
+@pytest.fixture(params=[1, 2, 0], ids=["tcgen05", "tcgen05_planar", "cuda_core"])
 def conv_impl(request):
-    """Run a U-Net test on the tensor-core engine (bf16 operands) and on the
-    CUDA-core engine (float32 operands); the oracle mirrors the rounding."""
+    """Run a U-Net test on the tensor-core engine (bf16 operands; the
+    smoother application through the chunked bf16 layout, or with the float32
+    planar staging everywhere) and on the CUDA-core engine (float32
+    operands); the oracle mirrors the rounding."""
     lib = L.load()
     prev = lib.zb_unet_conv_impl(request.param)
     lib.zb_unet_status(1)
@@ -234,7 +236,7 @@ def test_unet_forward_and_gradients_match_oracle(c1, c2, conv_impl):
     y = tr.forward(rg, cxg, cyg, dx).cpu().numpy().astype(np.float64)
     Ws, bs = _oracle_weights(sm)
     r64, cx64, cy64 = r.astype(np.float64), cx.astype(np.float64), cy.astype(np.float64)
-    q = conv_impl == 1
+    q = conv_impl in (1, 2)
     yo, _ = OU.forward(Ws, bs, r64, cx64, cy64, dx, sm.cmax, bf16_inputs=q)
     assert rel_l2(y, yo) <= (1e-3 if q else 1e-4)
     loss = float(tr.loss_and_grad(rg, cxg, cyg, dx).item())
@@ -262,7 +264,7 @@ def test_unet_energy_loss_gradients_match_oracle(conv_impl):
     rg, cxg, cyg, eg = (torch.as_tensor(a, device=DEV) for a in (r, cx, cy, e))
     loss = float(tr.loss_and_grad(rg, cxg, cyg, dx, target=eg).item())
     Ws, bs = _oracle_weights(sm)
-    q = conv_impl == 1
+    q = conv_impl in (1, 2)
     lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r.astype(np.float64), cx.astype(np.float64),
                                      cy.astype(np.float64), dx, sm.cmax, bf16_inputs=q,
                                      target=e.astype(np.float64))
@@ -292,8 +294,43 @@ def test_smoother_apply_matches_oracle(conv_impl):
     cx32, cy32 = cx.astype(np.float32).astype(np.float64), cy.astype(np.float32).astype(np.float64)
     f32, x32 = f.astype(np.float32).astype(np.float64), x.astype(np.float32).astype(np.float64)
     ref = OU.smoother_apply(Ws, bs, f32, x32, cx32, cy32, dx, sm.cmax,
-                            bf16_inputs=conv_impl == 1)
+                            bf16_inputs=conv_impl in (1, 2))
     assert rel_l2(out.reshape(nx, ny).astype(np.float64), ref) <= (1e-3 if conv_impl else 1e-4)
+
+
+@pytest.mark.parametrize("c1,c2", [(8, 16), (24, 48)])
+@pytest.mark.parametrize("nx,ny", [(256, 256), (100, 132)])
+def test_chunked_layout_smoother_is_bitwise_the_planar_one(c1, c2, nx, ny):
+    """The smoother application through the chunked bf16 activations
+    (conv3x3_cb8: 16-byte staging copies, two M tiles per CTA, pool(e2)
+    written by e2's epilogue) against the planar float32 staging
+    (conv3x3_tc), bit for bit, on a square grid and on one whose sides are
+    not multiples of the 16-pixel region."""
+    lib = L.load()
+    sm = LearnedSmoother(c1, c2, seed=31)
+    sm.w.mul_(3.0)
+    sm.b.normal_(0.0, 0.1, generator=torch.Generator(device=DEV).manual_seed(2))
+    sm.refresh()
+    rng = np.random.default_rng(41)
+    h = rng.uniform(0.05, 2.5, (nx, ny))
+    cx, cy = OP.face_coefficients(h)
+    f = rng.standard_normal((nx, ny))
+    x = rng.standard_normal((nx, ny)) * 1e-3
+    g32 = lambda a: gpu(a, torch.float32)  # noqa: E731
+    outs = []
+    prev = lib.zb_unet_conv_impl(1)
+    try:
+        for impl in (1, 2):
+            lib.zb_unet_conv_impl(impl)
+            lib.zb_unet_status(1)
+            outs.append(sm.apply(nx, ny, g32(f), g32(cx), g32(cy), 1.0 / nx, x=g32(x)).clone())
+            torch.cuda.synchronize()
+            assert lib.zb_unet_status(1) == 0
+    finally:
+        lib.zb_unet_conv_impl(prev)
+    assert torch.isfinite(outs[0]).all()
+    assert torch.equal(outs[0].view(torch.int32), outs[1].view(torch.int32)), \
+        (outs[0] - outs[1]).abs().max().item()
 
 
 def test_adam_step_matches_formula():

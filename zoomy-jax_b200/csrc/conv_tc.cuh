@@ -275,5 +275,222 @@ conv3x3_tc(const float* __restrict__ inA, int cin_a, const float* __restrict__ i
   }
 }
 
+// ── the chunked bf16 activation layout (inference) ──────────────────────────
+// An activation of C channels (C a multiple of 8) on B images H x W is stored
+// as C / 8 chunks, chunk-major: byte ((chunk * B + b) * H * W + y * W + x) * 16
+// holds channels 8 chunk .. 8 chunk + 7 of pixel (b, y, x) as bf16.  A pixel's
+// chunk is then one 16-byte core-matrix row of the MMA's A operand, and a row
+// of pixels is contiguous, so a tile's halo is staged with coalesced 16-byte
+// cp.async copies (zero-filled outside the image) instead of per-thread
+// float32 gathers; the producing layer writes it in its epilogue.  Values are
+// the float32 activations rounded to bf16 once (the rounding the planar
+// kernel applies when it stages them), so a network run through this layout
+// gives the same bits as through conv3x3_tc.
+constexpr int CBX = 16, CBY = 16;            // output region: two 8 x 16 M tiles
+constexpr int CHX = CBX + 2, CHY = CBY + 2;  // halo region
+constexpr int CHP = CHX * CHY;               // 324 halo pixels
+
+__host__ __device__ inline size_t cb8_smem_bytes(int cinp, int coutp) {
+  return (size_t)cinp * CHP * 2 + (size_t)9 * cinp * coutp * 2 + 64;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+
+// Output forms of conv3x3_cb8.
+enum { CB_OUT_CHUNKED = 0, CB_OUT_F32 = 1 };
+
+// out = act(bias + conv3x3(in)) with in = [A (chA chunks; mode_a SRC_DIRECT
+// at H x W or SRC_UP: the nearest 2x upsampling of an H/2 x W/2 field), then
+// B (chB chunks at H x W)], cin real channels (the rest of the chunks and the
+// padding to 16 read as zeros).  out_form CB_OUT_CHUNKED: out holds cout / 8
+// chunks; pool (may be null) also receives the 2x2 average of the float32
+// activation (H/2 x W/2 chunks, the average of conv3x3_tc's SRC_POOL loader,
+// in its summation order).  CB_OUT_F32: out is float32 planes [co][b][y][x].
+// H and W even.
+__global__ void __launch_bounds__(TC_THREADS)
+conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __restrict__ inB,
+            int chB, int cin, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
+            void* __restrict__ out, uint4* __restrict__ pool, int cout, int out_form, int B,
+            int H, int W, int act, int tmem_cols, unsigned* err) {
+  extern __shared__ __align__(128) unsigned char tc_sm[];
+  const int cinp = pad16(cin), coutp = pad16(cout);
+  const int nch = cinp / 8;
+  unsigned char* sA = tc_sm;
+  unsigned char* sB = tc_sm + (size_t)cinp * CHP * 2;
+  unsigned long long* mbar = (unsigned long long*)(sB + (size_t)9 * cinp * coutp * 2);
+  uint32_t* tmem_slot = (uint32_t*)(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // weights: [tap][chunk][n][8] bf16, zero outside (cout, cin)
+  for (int e = tid; e < 9 * nch * coutp; e += TC_THREADS) {
+    const int n = e % coutp;
+    const int rest = e / coutp;
+    const int ch = rest % nch, tap = rest / nch;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int ci = ch * 8 + k;
+      v[k] = (n < cout && ci < cin) ? w[((size_t)n * cin + ci) * 9 + tap] : __float2bfloat16(0.0f);
+    }
+    *(uint4*)(sB + ((size_t)(tap * nch + ch) * coutp + n) * 16) = *(const uint4*)v;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :
+                 : "r"(smem_u32(tmem_slot)), "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t mbar_a = smem_u32(mbar);
+  const uint32_t sA_a = smem_u32(sA), sB_a = smem_u32(sB);
+  const uint32_t idesc = tc_idesc(coutp);
+  const size_t npix = (size_t)B * H * W;
+  const int H2 = H >> 1, W2 = W >> 1;
+  const size_t npix2 = (size_t)B * H2 * W2;
+  const int rx = (W + CBX - 1) / CBX, ry = (H + CBY - 1) / CBY;
+  const int nreg = rx * ry * B;
+  uint32_t parity = 0;
+  bool failed = false;
+  for (int t = blockIdx.x; t < nreg; t += gridDim.x) {
+    const int b = t / (rx * ry);
+    const int rr = t - b * rx * ry;
+    const int x0 = (rr % rx) * CBX, y0 = (rr / rx) * CBY;
+    const size_t img = (size_t)b * H * W;
+    // halo region: one 16-byte copy per (chunk, halo pixel); zero outside the
+    // image and for the padding chunks
+    for (int e = tid; e < nch * CHP; e += TC_THREADS) {
+      const int ch = e / CHP, q = e - ch * CHP;
+      const int yy = y0 - 1 + q / CHX, xx = x0 - 1 + q % CHX;
+      const bool inside = yy >= 0 && yy < H && xx >= 0 && xx < W;
+      const uint4* src = inA;
+      uint32_t bytes = 0;
+      if (inside && ch < chA) {
+        src = mode_a == SRC_UP
+                  ? inA + ((size_t)ch * B + b) * H2 * W2 + (size_t)(yy >> 1) * W2 + (xx >> 1)
+                  : inA + ((size_t)ch * B + b) * H * W + (size_t)yy * W + xx;
+        bytes = 16;
+      } else if (inside && ch < chA + chB) {
+        src = inB + ((size_t)(ch - chA) * B + b) * H * W + (size_t)yy * W + xx;
+        bytes = 16;
+      }
+      cp_async16(sA_a + (uint32_t)(ch * CHP + q) * 16, src, bytes);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // make the copies visible to the tensor core's async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      // M tile i: pixels x0 + 8 i .. x0 + 8 i + 7 of the region's 16 rows,
+      // accumulator columns [i coutp, (i + 1) coutp)
+      for (int i = 0; i < 2; ++i) {
+        uint32_t acc = 0;
+        for (int tap = 0; tap < 9; ++tap) {
+          const int dy = tap / 3, dx = tap % 3;
+          for (int g = 0; g < cinp / 16; ++g) {
+            const uint32_t a = sA_a + (uint32_t)(2 * g) * (CHP * 16) +
+                               (uint32_t)(dy * CHX + dx + 8 * i) * 16;
+            const uint32_t bb = sB_a + (uint32_t)((tap * nch + 2 * g) * coutp) * 16;
+            tc_mma(tmem + (uint32_t)(i * coutp), tc_desc(a, CHP * 16, CHX * 16),
+                   tc_desc(bb, coutp * 16, 128), idesc, acc);
+            acc = 1;
+          }
+        }
+      }
+      tc_commit(mbar_a);
+    }
+    bool done = false;
+    for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it) {
+      if (mbar_try_wait(mbar_a, parity)) { done = true; break; }
+    }
+    parity ^= 1u;
+    if (__syncthreads_or(done ? 0 : 1)) {
+      failed = true;
+      if (err && tid == 0) atomicExch(err, 1u);
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: warp w owns accumulator rows 32w .. 32w+31 of both M tiles
+    const int m = warp * 32 + lane;
+    for (int i = 0; i < 2; ++i) {
+      const int x = x0 + 8 * i + (m % 8), y = y0 + m / 8;
+      const bool store = x < W && y < H;
+      // the 2x2 block's top-left lane (even x, even y) writes the pooled pixel
+      const bool pstore = store && ((m & 1) == 0) && (((m >> 3) & 1) == 0);
+      for (int c0 = 0; c0 < coutp; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(i * coutp + c0), v);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int co = c0 + k;
+          float s = v[k] + ((bias && co < cout) ? bias[co] : 0.0f);
+          if (act) s = tanhf(s);
+          v[k] = s;
+        }
+        if (out_form == CB_OUT_F32) {
+#pragma unroll
+          for (int k = 0; k < 16; ++k)
+            if (store && c0 + k < cout)
+              ((float*)out)[(size_t)(c0 + k) * npix + img + (size_t)y * W + x] = v[k];
+          continue;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int chunk = c0 / 8 + h;
+          if (chunk * 8 >= cout) continue;   // uniform
+          __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) o[k] = __float2bfloat16_rn(v[8 * h + k]);
+          if (store)
+            ((uint4*)out)[((size_t)chunk * B + b) * H * W + (size_t)y * W + x] = *(const uint4*)o;
+          if (pool) {
+            __align__(16) __nv_bfloat16 pv[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              const float a0 = v[8 * h + k];
+              const float a1 = __shfl_down_sync(0xffffffffu, a0, 1);
+              const float a2 = __shfl_down_sync(0xffffffffu, a0, 8);
+              const float a3 = __shfl_down_sync(0xffffffffu, a0, 9);
+              pv[k] = __float2bfloat16_rn(0.25f * (((a0 + a1) + a2) + a3));
+            }
+            if (pstore)
+              pool[((size_t)chunk * B + b) * H2 * W2 + (size_t)(y >> 1) * W2 + (x >> 1)] =
+                  *(const uint4*)pv;
+          }
+        }
+      }
+    }
+    // TMEM reads and shared-memory reads of this region complete before the next
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (failed) {
+    for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it)
+      if (mbar_try_wait(mbar_a, parity ^ 1u)) break;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(tmem_cols)
+                 : "memory");
+  }
+}
+
 }  // namespace unet
 }  // namespace zb

@@ -286,6 +286,25 @@ __global__ void features_kernel(const float* __restrict__ r, const float* __rest
   }
 }
 
+// the same two input channels as one chunk of the chunked bf16 layout
+// (channels 2..7 zero), each rounded as the planar kernel rounds them
+__global__ void features_cb8_kernel(const float* __restrict__ r, const float* __restrict__ s,
+                                    const float* __restrict__ cx, const float* __restrict__ cy,
+                                    int B, int H, int W, float inv_cmax, uint4* __restrict__ in) {
+  const size_t npix = (size_t)H * W, n = (size_t)B * npix;
+  for (size_t k = blockIdx.x * (size_t)NT + threadIdx.x; k < n; k += (size_t)gridDim.x * NT) {
+    const int b = (int)(k / npix);
+    const size_t p = k - (size_t)b * npix;
+    const int i = (int)(p / W), j = (int)(p - (size_t)i * W);
+    __align__(16) __nv_bfloat16 v[8];
+    v[0] = __float2bfloat16_rn(r[k] / s[b]);
+    v[1] = __float2bfloat16_rn(cell_c(cx, cy, b, H, W, i, j) * inv_cmax);
+#pragma unroll
+    for (int c = 2; c < 8; ++c) v[c] = __float2bfloat16_rn(0.0f);
+    in[k] = *(const uint4*)v;
+  }
+}
+
 // y = x_in + s dx^2 / c * out   (x_in may be null; y may alias x_in)
 __global__ void scale_out_kernel(const float* __restrict__ out, const float* __restrict__ s,
                                  const float* __restrict__ cx, const float* __restrict__ cy,
@@ -460,9 +479,13 @@ static bool valid_channels(int c1, int c2) {
          (c1 == 24 && c2 == 48);
 }
 
-// which convolution runs the forward and data-gradient passes: the tcgen05
-// implicit GEMM (bf16 operands, the default) or the CUDA-core direct
-// convolution (float32 operands, kept as the exactness reference)
+// which convolution runs the forward and data-gradient passes: 0 = the
+// CUDA-core direct convolution (float32 operands, kept as the exactness
+// reference); 1 (default) = the tcgen05 implicit GEMM (bf16 operands), the
+// smoother application's forward through the chunked bf16 layout
+// (conv3x3_cb8) and training through the float32 planar staging
+// (conv3x3_tc); 2 = the tcgen05 GEMM with the planar staging everywhere (the
+// same bits as 1)
 static int g_conv_impl = 1;
 static __device__ unsigned g_unet_err;
 
@@ -519,10 +542,53 @@ static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin
   return zb_launch_check();
 }
 
+// conv3x3_cb8 over B images H x W (see conv_tc.cuh); resident CTAs are capped
+// so that their TMEM columns (two M tiles of coutp each) fit in 512
+static int conv_cb8_launch(const uint4* inA, int chA, int mode_a, const uint4* inB, int chB,
+                           int cin, const __nv_bfloat16* w, const float* bias, void* out,
+                           uint4* pool, int cout, int out_form, int B, int H, int W, int act,
+                           cudaStream_t st) {
+  const int cinp = pad16(cin), coutp = pad16(cout);
+  if (2 * coutp > 256 || cinp > 256 || chA + chB > cinp / 8) return ZB_E_UNSUPPORTED;
+  int cols = 32;
+  while (cols < 2 * coutp) cols *= 2;
+  static std::atomic<int> sms[64];
+  static std::atomic<bool> attr[64];
+  int dev = 0;
+  ZB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return ZB_E_CUDA;
+  if (!sms[dev].load()) {
+    int v = 0;
+    ZB_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    sms[dev].store(v);
+  }
+  if (!attr[dev].load()) {
+    ZB_CUDA_TRY(cudaFuncSetAttribute(conv3x3_cb8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024));
+    attr[dev].store(true);
+  }
+  const int smem_sm = 228 * 1024, per_cta_reserved = 1024;
+  const int by_tmem = 512 / cols, by_threads = 2048 / TC_THREADS;
+  size_t smem = cb8_smem_bytes(cinp, coutp);
+  if (by_tmem < by_threads) {
+    const size_t floor_bytes = (size_t)(smem_sm / (by_tmem + 1) - per_cta_reserved + 16);
+    smem = std::max(smem, floor_bytes);
+  }
+  if (smem > 227 * 1024) return ZB_E_UNSUPPORTED;
+  const int fit = std::min(by_threads, (int)(smem_sm / (smem + per_cta_reserved)));
+  const long long nreg = (long long)((W + CBX - 1) / CBX) * ((H + CBY - 1) / CBY) * B;
+  const int grid = (int)std::max<long long>(
+      1, std::min<long long>(nreg, (long long)sms[dev] * std::max(1, fit)));
+  conv3x3_cb8<<<grid, TC_THREADS, smem, st>>>(inA, chA, mode_a, inB, chB, cin, w, bias, out,
+                                              pool, cout, out_form, B, H, W, act, cols,
+                                              unet_err_word());
+  return zb_launch_check();
+}
+
 static int conv(const float* inA, int cin_a, const float* inB, int cin,
                 const __nv_bfloat16* w, const float* bias, float* out, int cout, int B, int H,
                 int W, int act, cudaStream_t st, int mode_a = SRC_DIRECT) {
-  if (g_conv_impl == 1)
+  if (g_conv_impl >= 1)
     return conv_tc_launch(inA, cin_a, inB, cin, w, bias, out, cout, B, H, W, act, mode_a, st);
   dim3 grid((W + TS - 1) / TS, (H + TS - 1) / TS, B);
   switch (cout) {
@@ -611,6 +677,46 @@ static int forward(const Net& n, const Acts& a, const __nv_bfloat16* w, const fl
   return zb_launch_check();
 }
 
+// Inference forward in the chunked bf16 layout (conv3x3_cb8), the same bits as
+// forward(): the activations live where the float32 ones would (the chunked
+// tensors take fewer bytes); e2's epilogue also writes pool(e2), o1 reads
+// up(m2) through its loader.  The network output goes to a.out (float32).
+struct ActsCB8 {
+  uint4 *in, *e1, *e2, *e2p, *m1, *m2, *o1;
+};
+
+static bool acts_cb8(const Net& n, const Acts& a, int B, int H, int W, ActsCB8* c) {
+  const size_t N0 = (size_t)B * H * W, N1 = (size_t)B * (H / 2) * (W / 2);
+  uint4* p = (uint4*)a.in;
+  c->in = p; p += N0;
+  c->e1 = p; p += (size_t)(n.c1 / 8) * N0;
+  c->e2 = p; p += (size_t)(n.c1 / 8) * N0;
+  c->e2p = p; p += (size_t)(n.c1 / 8) * N1;
+  c->m1 = p; p += (size_t)(n.c2 / 8) * N1;
+  c->m2 = p; p += (size_t)(n.c2 / 8) * N1;
+  c->o1 = p; p += (size_t)(n.c1 / 8) * N0;
+  return (const void*)p <= (const void*)a.out && (((uintptr_t)a.in) & 15u) == 0;
+}
+
+static int forward_cb8(const Net& n, const Acts& a, const ActsCB8& c, const __nv_bfloat16* w,
+                       const float* b, int B, int H, int W, cudaStream_t st) {
+  const int H1 = H / 2, W1 = W / 2, k1 = n.c1 / 8, k2 = n.c2 / 8;
+  int rc;
+  if ((rc = conv_cb8_launch(c.in, 1, SRC_DIRECT, nullptr, 0, 2, w + n.off_w[0], b + n.off_b[0],
+                            c.e1, nullptr, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH, st))) return rc;
+  if ((rc = conv_cb8_launch(c.e1, k1, SRC_DIRECT, nullptr, 0, n.c1, w + n.off_w[1], b + n.off_b[1],
+                            c.e2, c.e2p, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH, st))) return rc;
+  if ((rc = conv_cb8_launch(c.e2p, k1, SRC_DIRECT, nullptr, 0, n.c1, w + n.off_w[2], b + n.off_b[2],
+                            c.m1, nullptr, n.c2, CB_OUT_CHUNKED, B, H1, W1, ACT_TANH, st))) return rc;
+  if ((rc = conv_cb8_launch(c.m1, k2, SRC_DIRECT, nullptr, 0, n.c2, w + n.off_w[3], b + n.off_b[3],
+                            c.m2, nullptr, n.c2, CB_OUT_CHUNKED, B, H1, W1, ACT_TANH, st))) return rc;
+  if ((rc = conv_cb8_launch(c.m2, k2, SRC_UP, c.e2, k1, n.c2 + n.c1, w + n.off_w[4], b + n.off_b[4],
+                            c.o1, nullptr, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH, st))) return rc;
+  if ((rc = conv_cb8_launch(c.o1, k1, SRC_DIRECT, nullptr, 0, n.c1, w + n.off_w[5], b + n.off_b[5],
+                            a.out, nullptr, 1, CB_OUT_F32, B, H, W, ACT_NONE, st))) return rc;
+  return zb_launch_check();
+}
+
 // data gradient through conv layer l: din (cin channels) from dout (cout)
 static int data_grad(const Net& n, int l, const __nv_bfloat16* w, __nv_bfloat16* wflip,
                      const float* dout, float* din, int B, int H, int W, cudaStream_t st) {
@@ -629,7 +735,7 @@ extern "C" {
 
 int zb_unet_conv_impl(int impl) {
   const int prev = g_conv_impl;
-  if (impl == 0 || impl == 1) g_conv_impl = impl;
+  if (impl == 0 || impl == 1 || impl == 2) g_conv_impl = impl;
   return prev;
 }
 
@@ -674,9 +780,17 @@ int zb_smoother_apply(const zb_smoother* smo, const float* f, const float* x_in,
   const size_t N0 = (size_t)nx * ny;
   patch_residual<<<gridn(N0), NT, 0, st>>>(f, x_in, cx, cy, 1, nx, ny, idx2, r_scratch);
   rms(r_scratch, 1, N0, a.part, a.s, st);
-  features_kernel<<<gridn(N0), NT, 0, st>>>(r_scratch, a.s, cx, cy, 1, nx, ny,
-                                            1.0f / smo->cmax, a.in);
-  int rc = forward(n, a, (const __nv_bfloat16*)smo->w, smo->b, 1, nx, ny, st);
+  int rc;
+  ActsCB8 c;
+  if (g_conv_impl == 1 && acts_cb8(n, a, 1, nx, ny, &c)) {
+    features_cb8_kernel<<<gridn(N0), NT, 0, st>>>(r_scratch, a.s, cx, cy, 1, nx, ny,
+                                                  1.0f / smo->cmax, c.in);
+    rc = forward_cb8(n, a, c, (const __nv_bfloat16*)smo->w, smo->b, 1, nx, ny, st);
+  } else {
+    features_kernel<<<gridn(N0), NT, 0, st>>>(r_scratch, a.s, cx, cy, 1, nx, ny,
+                                              1.0f / smo->cmax, a.in);
+    rc = forward(n, a, (const __nv_bfloat16*)smo->w, smo->b, 1, nx, ny, st);
+  }
   if (rc) return rc;
   scale_out_kernel<<<gridn(N0), NT, 0, st>>>(a.out, a.s, cx, cy, 1, nx, ny, (float)(dx * dx),
                                              x_in, x_out);
