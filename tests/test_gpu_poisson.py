@@ -201,6 +201,16 @@ def _batch(B, n, seed):
     return r, cx, cy
 
 
+# Tolerances of the tensor-core engine against the oracle: bf16 operands
+# (mirrored by the oracle); the smoother application also takes the SFU tanh
+# (tanh.approx.f32, relative error about 2^-11, not mirrored: now and then it
+# moves an activation across a bf16 rounding boundary, one bf16 step each
+# time), training the exact one
+TC_FWD_TOL = 1e-3
+TC_GRAD_TOL = 5e-3
+TC_APPLY_TOL = 4e-3
+
+
 @pytest.fixture(params=[1, 2, 0], ids=["tcgen05", "tcgen05_planar", "cuda_core"])
 def conv_impl(request):
     """Run a U-Net test on the tensor-core engine (bf16 operands; the
@@ -238,14 +248,14 @@ def test_unet_forward_and_gradients_match_oracle(c1, c2, conv_impl):
     r64, cx64, cy64 = r.astype(np.float64), cx.astype(np.float64), cy.astype(np.float64)
     q = conv_impl in (1, 2)
     yo, _ = OU.forward(Ws, bs, r64, cx64, cy64, dx, sm.cmax, bf16_inputs=q)
-    assert rel_l2(y, yo) <= (1e-3 if q else 1e-4)
+    assert rel_l2(y, yo) <= (TC_FWD_TOL if q else 1e-4)
     loss = float(tr.loss_and_grad(rg, cxg, cyg, dx).item())
     lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r64, cx64, cy64, dx, sm.cmax, bf16_inputs=q)
-    assert abs(loss - lo) <= (1e-3 if q else 1e-4) * abs(lo)
+    assert abs(loss - lo) <= (TC_FWD_TOL if q else 1e-4) * abs(lo)
     gw = tr.g_w.cpu().numpy().astype(np.float64)
     gb = tr.g_b.cpu().numpy().astype(np.float64)
     gWs, gbs = OU.split(gw, gb, c1, c2)
-    tol = 5e-3 if q else 2e-3
+    tol = TC_GRAD_TOL if q else 2e-3
     for k in range(6):
         assert rel_l2(gWs[k], dWs[k]) <= tol, (k, rel_l2(gWs[k], dWs[k]))
         assert rel_l2(gbs[k], dbs[k]) <= tol, (k, rel_l2(gbs[k], dbs[k]))
@@ -268,10 +278,10 @@ def test_unet_energy_loss_gradients_match_oracle(conv_impl):
     lo, dWs, dbs = OU.loss_and_grads(Ws, bs, r.astype(np.float64), cx.astype(np.float64),
                                      cy.astype(np.float64), dx, sm.cmax, bf16_inputs=q,
                                      target=e.astype(np.float64))
-    assert math.isfinite(loss) and abs(loss - lo) <= (1e-3 if q else 1e-4) * abs(lo)
+    assert math.isfinite(loss) and abs(loss - lo) <= (TC_FWD_TOL if q else 1e-4) * abs(lo)
     gWs, gbs = OU.split(tr.g_w.cpu().numpy().astype(np.float64),
                         tr.g_b.cpu().numpy().astype(np.float64), c1, c2)
-    tol = 5e-3 if q else 2e-3
+    tol = TC_GRAD_TOL if q else 2e-3
     for k in range(6):
         assert rel_l2(gWs[k], dWs[k]) <= tol, (k, rel_l2(gWs[k], dWs[k]))
         assert rel_l2(gbs[k], dbs[k]) <= tol, (k, rel_l2(gbs[k], dbs[k]))
@@ -295,7 +305,7 @@ def test_smoother_apply_matches_oracle(conv_impl):
     f32, x32 = f.astype(np.float32).astype(np.float64), x.astype(np.float32).astype(np.float64)
     ref = OU.smoother_apply(Ws, bs, f32, x32, cx32, cy32, dx, sm.cmax,
                             bf16_inputs=conv_impl in (1, 2))
-    assert rel_l2(out.reshape(nx, ny).astype(np.float64), ref) <= (1e-3 if conv_impl else 1e-4)
+    assert rel_l2(out.reshape(nx, ny).astype(np.float64), ref) <= (TC_APPLY_TOL if conv_impl else 1e-4)
 
 
 @pytest.mark.parametrize("c1,c2", [(8, 16), (24, 48)])

@@ -117,6 +117,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
   return ok != 0;
 }
 
+// Activation of the tensor-core epilogues: act 0 none, 1 tanhf, 2 tanh on the
+// SFU (tanh.approx.f32), whose maximum relative error, about 2^-11 per the PTX
+// ISA, sits below the bf16 rounding every activation takes before the next
+// layer reads it.  The smoother application uses 2; training keeps 1, so its
+// gradients stay those of the exact activation.
+__device__ __forceinline__ float tanh_sfu(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
   asm volatile(
@@ -251,7 +262,8 @@ conv3x3_tc(const float* __restrict__ inA, int cin_a, const float* __restrict__ i
         const int co = c0 + i;
         if (store && co < cout) {
           float s = v[i] + (bias ? bias[co] : 0.0f);
-          if (act) s = tanhf(s);
+          if (act == 1) s = tanhf(s);
+          else if (act == 2) s = tanh_sfu(s);
           out[(size_t)co * plane + img + (size_t)y * W + x] = s;
         }
       }
@@ -310,7 +322,8 @@ enum { CB_OUT_CHUNKED = 0, CB_OUT_F32 = 1 };
 // chunks; pool (may be null) also receives the 2x2 average of the float32
 // activation (H/2 x W/2 chunks, the average of conv3x3_tc's SRC_POOL loader,
 // in its summation order).  CB_OUT_F32: out is float32 planes [co][b][y][x].
-// H and W even.
+// H and W even.  act != 0: tanh on the SFU (the inference activation, act 2
+// of conv3x3_tc).
 __global__ void __launch_bounds__(TC_THREADS)
 conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __restrict__ inB,
             int chB, int cin, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
@@ -437,9 +450,11 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
           const int co = c0 + k;
-          float s = v[k] + ((bias && co < cout) ? bias[co] : 0.0f);
-          if (act) s = tanhf(s);
-          v[k] = s;
+          if (co < cout) {   // padding columns are never stored
+            float s = v[k] + (bias ? bias[co] : 0.0f);
+            if (act) s = tanh_sfu(s);   // the inference kernel: tanh on the SFU
+            v[k] = s;
+          }
         }
         if (out_form == CB_OUT_F32) {
 #pragma unroll

@@ -41,7 +41,7 @@ constexpr int NTT = TS * TS;    // threads per conv CTA
 constexpr int CCH = 8;          // input channels per shared-memory chunk
 constexpr int NT = 256;
 
-enum { ACT_NONE = 0, ACT_TANH = 1 };
+enum { ACT_NONE = 0, ACT_TANH = 1, ACT_TANH_SFU = 2 };   // see conv_tc.cuh
 
 
 // out[co][b][y][x] = act(bias[co] + sum_ci sum_tap w[co][ci][tap] in[ci][b][y+dy][x+dx])
@@ -92,7 +92,7 @@ conv3x3_fwd(const float* __restrict__ inA, int cin_a, const float* __restrict__ 
   if (x < W && y < H) {
 #pragma unroll
     for (int co = 0; co < COUT; ++co) {
-      const float v = act == ACT_TANH ? tanhf(acc[co]) : acc[co];
+      const float v = act != ACT_NONE ? tanhf(acc[co]) : acc[co];   // exact reference
       out[(size_t)co * plane + img + (size_t)y * W + x] = v;
     }
   }
@@ -664,15 +664,15 @@ static Acts acts_split(const Net& n, void* base, int B, int H, int W, bool train
 
 // forward of the network from a.in; weights bf16, biases float32
 static int forward(const Net& n, const Acts& a, const __nv_bfloat16* w, const float* b, int B, int H,
-                   int W, cudaStream_t st) {
+                   int W, cudaStream_t st, int act = ACT_TANH) {
   const int H1 = H / 2, W1 = W / 2;
   int rc;
-  if ((rc = conv(a.in, 2, nullptr, 2, w + n.off_w[0], b + n.off_b[0], a.e1, n.c1, B, H, W, ACT_TANH, st))) return rc;
-  if ((rc = conv(a.e1, n.c1, nullptr, n.c1, w + n.off_w[1], b + n.off_b[1], a.e2, n.c1, B, H, W, ACT_TANH, st))) return rc;
+  if ((rc = conv(a.in, 2, nullptr, 2, w + n.off_w[0], b + n.off_b[0], a.e1, n.c1, B, H, W, act, st))) return rc;
+  if ((rc = conv(a.e1, n.c1, nullptr, n.c1, w + n.off_w[1], b + n.off_b[1], a.e2, n.c1, B, H, W, act, st))) return rc;
   // pool(e2) and up(m2) are read through the convolutions' loaders, never stored
-  if ((rc = conv(a.e2, n.c1, nullptr, n.c1, w + n.off_w[2], b + n.off_b[2], a.m1, n.c2, B, H1, W1, ACT_TANH, st, SRC_POOL))) return rc;
-  if ((rc = conv(a.m1, n.c2, nullptr, n.c2, w + n.off_w[3], b + n.off_b[3], a.m2, n.c2, B, H1, W1, ACT_TANH, st))) return rc;
-  if ((rc = conv(a.m2, n.c2, a.e2, n.c2 + n.c1, w + n.off_w[4], b + n.off_b[4], a.o1, n.c1, B, H, W, ACT_TANH, st, SRC_UP))) return rc;
+  if ((rc = conv(a.e2, n.c1, nullptr, n.c1, w + n.off_w[2], b + n.off_b[2], a.m1, n.c2, B, H1, W1, act, st, SRC_POOL))) return rc;
+  if ((rc = conv(a.m1, n.c2, nullptr, n.c2, w + n.off_w[3], b + n.off_b[3], a.m2, n.c2, B, H1, W1, act, st))) return rc;
+  if ((rc = conv(a.m2, n.c2, a.e2, n.c2 + n.c1, w + n.off_w[4], b + n.off_b[4], a.o1, n.c1, B, H, W, act, st, SRC_UP))) return rc;
   if ((rc = conv(a.o1, n.c1, nullptr, n.c1, w + n.off_w[5], b + n.off_b[5], a.out, 1, B, H, W, ACT_NONE, st))) return rc;
   return zb_launch_check();
 }
@@ -703,15 +703,15 @@ static int forward_cb8(const Net& n, const Acts& a, const ActsCB8& c, const __nv
   const int H1 = H / 2, W1 = W / 2, k1 = n.c1 / 8, k2 = n.c2 / 8;
   int rc;
   if ((rc = conv_cb8_launch(c.in, 1, SRC_DIRECT, nullptr, 0, 2, w + n.off_w[0], b + n.off_b[0],
-                            c.e1, nullptr, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH, st))) return rc;
+                            c.e1, nullptr, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH_SFU, st))) return rc;
   if ((rc = conv_cb8_launch(c.e1, k1, SRC_DIRECT, nullptr, 0, n.c1, w + n.off_w[1], b + n.off_b[1],
-                            c.e2, c.e2p, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH, st))) return rc;
+                            c.e2, c.e2p, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH_SFU, st))) return rc;
   if ((rc = conv_cb8_launch(c.e2p, k1, SRC_DIRECT, nullptr, 0, n.c1, w + n.off_w[2], b + n.off_b[2],
-                            c.m1, nullptr, n.c2, CB_OUT_CHUNKED, B, H1, W1, ACT_TANH, st))) return rc;
+                            c.m1, nullptr, n.c2, CB_OUT_CHUNKED, B, H1, W1, ACT_TANH_SFU, st))) return rc;
   if ((rc = conv_cb8_launch(c.m1, k2, SRC_DIRECT, nullptr, 0, n.c2, w + n.off_w[3], b + n.off_b[3],
-                            c.m2, nullptr, n.c2, CB_OUT_CHUNKED, B, H1, W1, ACT_TANH, st))) return rc;
+                            c.m2, nullptr, n.c2, CB_OUT_CHUNKED, B, H1, W1, ACT_TANH_SFU, st))) return rc;
   if ((rc = conv_cb8_launch(c.m2, k2, SRC_UP, c.e2, k1, n.c2 + n.c1, w + n.off_w[4], b + n.off_b[4],
-                            c.o1, nullptr, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH, st))) return rc;
+                            c.o1, nullptr, n.c1, CB_OUT_CHUNKED, B, H, W, ACT_TANH_SFU, st))) return rc;
   if ((rc = conv_cb8_launch(c.o1, k1, SRC_DIRECT, nullptr, 0, n.c1, w + n.off_w[5], b + n.off_b[5],
                             a.out, nullptr, 1, CB_OUT_F32, B, H, W, ACT_NONE, st))) return rc;
   return zb_launch_check();
@@ -789,7 +789,7 @@ int zb_smoother_apply(const zb_smoother* smo, const float* f, const float* x_in,
   } else {
     features_kernel<<<gridn(N0), NT, 0, st>>>(r_scratch, a.s, cx, cy, 1, nx, ny,
                                               1.0f / smo->cmax, a.in);
-    rc = forward(n, a, (const __nv_bfloat16*)smo->w, smo->b, 1, nx, ny, st);
+    rc = forward(n, a, (const __nv_bfloat16*)smo->w, smo->b, 1, nx, ny, st, ACT_TANH_SFU);
   }
   if (rc) return rc;
   scale_out_kernel<<<gridn(N0), NT, 0, st>>>(a.out, a.s, cx, cy, 1, nx, ny, (float)(dx * dx),
