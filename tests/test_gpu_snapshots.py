@@ -19,7 +19,7 @@ if not torch.cuda.is_available():
 
 import zoomy_b200 as zb  # noqa: E402
 from zoomy_b200.fvm.solver import HyperbolicSolver  # noqa: E402
-from zoomy_b200.snapshots import read_snapshots, snapshot_times  # noqa: E402
+from zoomy_b200.snapshots import read_mesh, read_settings, read_snapshots, snapshot_times  # noqa: E402
 from zoomy_b200.workloads import circular_dam_state  # noqa: E402
 
 TAGS = ("left", "right", "bottom", "top")
@@ -70,3 +70,11 @@ def test_snapshots_match_a_step_by_step_march(tmp_path):
         assert np.array_equal(got[k][2], ref[k][2]), k
     assert np.array_equal(got[n_snap - 1][1], Qf.cpu().numpy())
     assert math.isclose(solver.time, t_end, rel_tol=0, abs_tol=1e-15)
+    # the mesh and the settings written beside the snapshots
+    mesh = read_mesh(path)
+    assert np.array_equal(mesh["cell_centers"], solver.mesh.cell_centers())
+    assert mesh["shape"].tolist() == [64, 48]
+    st = read_settings(path)
+    assert st["time_end"] == t_end and st["riemann"] == "hll_hr"
+    assert st["compute_dt"]["cfl"] == 0.45 and st["output"]["snapshots"] == n_snap
+    assert st["boundary_conditions"] == ["wall"] * 4 and st["dtype"] == "float64"

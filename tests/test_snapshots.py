@@ -10,7 +10,8 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-from zoomy_b200.snapshots import SnapshotWriter, read_snapshots, snapshot_times  # noqa: E402
+from zoomy_b200.snapshots import (SnapshotWriter, read_mesh, read_settings,  # noqa: E402
+                                  read_snapshots, snapshot_times)
 
 
 def test_output_times_follow_the_reference():
@@ -58,3 +59,34 @@ def test_a_write_error_is_raised_at_close(tmp_path):
     w.save(0, 0.0, torch.zeros(4, 3))
     with pytest.raises(OSError):
         w.close()
+
+
+def test_mesh_and_settings_round_trip(tmp_path):
+    """The run's mesh arrays and settings go through the writer thread in
+    order with the snapshots; written again, they are replaced."""
+    path = str(tmp_path / "run.h5")
+    mesh = {"cell_centers": np.arange(12.0).reshape(2, 6), "shape": np.array([2, 3])}
+    with SnapshotWriter(path, fmt="npy") as w:
+        w.write_mesh(mesh)
+        w.write_settings({"time_end": 0.5, "riemann": "hll_hr", "bc": ["wall"] * 4})
+        w.save(0, 0.0, torch.zeros(4, 6))
+    got = read_mesh(path)
+    assert sorted(got) == ["cell_centers", "shape"]
+    assert np.array_equal(got["cell_centers"], mesh["cell_centers"])
+    assert read_settings(path) == {"time_end": 0.5, "riemann": "hll_hr", "bc": ["wall"] * 4}
+    with SnapshotWriter(path, fmt="npy") as w:
+        w.write_mesh({"vertices": np.zeros((3, 2))})
+        w.write_settings({"time_end": 1.0})
+    assert sorted(read_mesh(path)) == ["vertices"]
+    assert read_settings(path) == {"time_end": 1.0}
+    assert read_mesh(str(tmp_path / "none.h5")) == {} and read_settings(str(tmp_path / "x")) == {}
+
+
+def test_a_settings_error_is_raised_at_close(tmp_path):
+    w = SnapshotWriter(str(tmp_path / "run.h5"), fmt="npy")
+    w.write_settings({"fine": 1})
+    w.close()
+    w = SnapshotWriter(str(tmp_path / "run2.h5"), fmt="npy")
+    with pytest.raises(TypeError):
+        w.write_settings({"not serialisable": object()})
+    w.close()

@@ -18,6 +18,8 @@ from __future__ import annotations
 import ctypes as C
 import math
 
+import numpy as np
+
 from .. import _lib as L
 from ..mesh import CartesianMesh
 from ..timestepping import Adaptive, Constant, adaptive
@@ -409,18 +411,65 @@ class HyperbolicSolver:
         :class:`~zoomy_b200.snapshots.SnapshotWriter` (the march pays a
         device-to-device copy per snapshot).  Near an output time the
         device-resident loop queues single steps so that it stops on the same
-        step as the reference."""
+        step as the reference.  Before the first snapshot the mesh and the
+        run's settings go to the same output (``solver_jax.py:1267-1283``
+        writes them there before its loop; see :mod:`zoomy_b200.snapshots`
+        for the layout)."""
         writer = None
         if write_output:
             if self.output_path is None:
                 raise ValueError("write_output needs the solver's output_path")
             from ..snapshots import SnapshotWriter
             writer = SnapshotWriter(self.output_path)
+            writer.write_mesh(self.output_mesh())
+            writer.write_settings(self.output_settings())
         try:
             return self._march(Q, Qaux, writer, max_steps)
         finally:
             if writer is not None:
                 writer.close()
+
+    def output_mesh(self):
+        """The mesh as host arrays for the output: the cell centres ``(2, C)``
+        in cell order for every mesh; the grid shape, origin and spacing of a
+        Cartesian mesh; the vertices and triangles of a triangle mesh."""
+        m = self.mesh
+        out = {"cell_centers": np.asarray(m.cell_centers(), dtype=np.float64)}
+        if isinstance(m, CartesianMesh):
+            out["shape"] = np.array([m.nx, m.ny], dtype=np.int64)
+            out["origin"] = np.array([m.x0, m.y0], dtype=np.float64)
+            out["spacing"] = np.array([m.dx, m.dy], dtype=np.float64)
+        else:
+            out["vertices"] = np.asarray(m.vertices, dtype=np.float64)
+            out["triangles"] = np.asarray(m.triangles, dtype=np.int64)
+        return out
+
+    def output_settings(self):
+        """The run's settings as a JSON-serialisable dict: solver, time
+        stepping, scheme, boundary conditions, precision and output."""
+        cfg = self.cfg
+        cd = self.compute_dt
+        step = ({"kind": "adaptive", "cfl": cd.CFL, "dimension": cd.dimension,
+                 "degree": cd.degree} if isinstance(cd, Adaptive)
+                else {"kind": "constant", "dt": getattr(cd, "dt", None)})
+        return {
+            "solver": type(self).__name__,
+            "time_end": self.time_end,
+            "compute_dt": step,
+            "reconstruction": {"order": int(cfg.order),
+                               "variables": self.reconstruction_variables,
+                               "limiter": [k for k, v in L.LIMITER.items()
+                                           if v == cfg.limiter][0]},
+            "riemann": [k for k, v in L.RIEMANN.items() if v == cfg.riemann][0],
+            "boundary_conditions": list(self.nsm.model.bc_kinds()),
+            "mood": self.mood,
+            "eps_wet": self.eps_wet,
+            "implicit_source": self.implicit_source,
+            "manning_n": float(cfg.manning_n),
+            "dtype": self.dtype,
+            "mesh": {"kind": type(self.mesh).__name__, "cells": int(self.mesh.n_cells)},
+            "output": {"path": self.output_path, "snapshots": self.output_snapshots},
+        }
 
     def _march(self, Q, Qaux, writer, max_steps):
         from ..snapshots import snapshot_times

@@ -15,9 +15,18 @@ The file format: with ``h5py`` importable, the reference's own layout in
 default ``overwrite=True`` does); without it (this image has no HDF5 library),
 the same group paths as NumPy files: ``<root>/fields/iteration_<i>/time.npy``,
 ``Q.npy``, ``Qaux.npy`` with ``<root>`` = ``path`` minus a ``.h5`` suffix.
+
+Beside the snapshots a run writes its mesh and its settings, as the reference
+does before its time loop (``zoomy_jax/fvm/solver_jax.py:1267-1283``:
+``mesh.write_to_hdf5`` and ``io.save_settings``).  Those two writers belong to
+zoomy_core, which is not part of the reference tree, so their layouts here are
+this package's own: the mesh arrays in the group ``mesh`` (HDF5) or as
+``<root>/mesh/<name>.npy``, the settings as JSON (the file attribute
+``settings`` in HDF5, ``<root>/settings.json`` otherwise).
 """
 from __future__ import annotations
 
+import json
 import os
 import queue
 import threading
@@ -61,6 +70,29 @@ def read_snapshots(path):
                                         np.load(os.path.join(d, "Q.npy")),
                                         np.load(aux) if os.path.exists(aux) else None)
     return out
+
+
+def read_mesh(path):
+    """The mesh arrays :meth:`SnapshotWriter.write_mesh` wrote (``{}`` if none)."""
+    if _h5py is not None and os.path.isfile(path):  # pragma: no cover
+        with _h5py.File(path, "r") as f:
+            return {k: v[()] for k, v in f["mesh"].items()} if "mesh" in f else {}
+    d = os.path.join(_npy_root(path), "mesh")
+    if not os.path.isdir(d):
+        return {}
+    return {f[:-4]: np.load(os.path.join(d, f)) for f in os.listdir(d) if f.endswith(".npy")}
+
+
+def read_settings(path):
+    """The settings :meth:`SnapshotWriter.write_settings` wrote (``{}`` if none)."""
+    if _h5py is not None and os.path.isfile(path):  # pragma: no cover
+        with _h5py.File(path, "r") as f:
+            return json.loads(f.attrs["settings"]) if "settings" in f.attrs else {}
+    p = os.path.join(_npy_root(path), "settings.json")
+    if not os.path.isfile(p):
+        return {}
+    with open(p) as fh:
+        return json.load(fh)
 
 
 def _npy_root(path):
@@ -140,7 +172,18 @@ class SnapshotWriter:
             s["hq"].copy_(Q)
             if Qaux is not None:
                 s["ha"].copy_(Qaux)
-        self._todo.put((k, int(i_snapshot), float(time), Qaux is not None))
+        self._todo.put(("snapshot", k, int(i_snapshot), float(time), Qaux is not None))
+
+    def write_mesh(self, arrays):
+        """Queue the run's mesh: ``{name: host array}``, written once, in
+        order with the snapshots, by the writer thread."""
+        self._check()
+        self._todo.put(("mesh", {k: np.asarray(v) for k, v in arrays.items()}))
+
+    def write_settings(self, settings):
+        """Queue the run's settings (a JSON-serialisable dict)."""
+        self._check()
+        self._todo.put(("settings", json.dumps(settings, sort_keys=True)))
 
     # ── the writer thread ─────────────────────────────────────────────────
     def _run(self):
@@ -148,7 +191,13 @@ class SnapshotWriter:
             item = self._todo.get()
             if item is None:
                 return
-            k, i, t, has_aux = item
+            if item[0] != "snapshot":
+                try:
+                    self._write_meta(item[0], item[1])
+                except BaseException as e:  # noqa: BLE001 - handed to the caller
+                    self._error = e
+                continue
+            _, k, i, t, has_aux = item
             try:
                 s = self._slots[k]
                 if s["ev"] is not None:
@@ -184,6 +233,32 @@ class SnapshotWriter:
         np.save(os.path.join(d, "Q.npy"), q)
         if a is not None:
             np.save(os.path.join(d, "Qaux.npy"), a)
+
+    def _write_meta(self, kind, payload):
+        if self.format == "hdf5":  # pragma: no cover - needs h5py
+            with _h5py.File(self.path, "a") as f:
+                if kind == "settings":
+                    f.attrs["settings"] = payload
+                    return
+                if "mesh" in f:
+                    del f["mesh"]
+                g = f.create_group("mesh")
+                for name, a in payload.items():
+                    g.create_dataset(name, data=a)
+            return
+        root = _npy_root(self.path)
+        os.makedirs(root, exist_ok=True)
+        if kind == "settings":
+            with open(os.path.join(root, "settings.json"), "w") as fh:
+                fh.write(payload)
+            return
+        d = os.path.join(root, "mesh")
+        os.makedirs(d, exist_ok=True)
+        for f in os.listdir(d):
+            if f.endswith(".npy"):
+                os.remove(os.path.join(d, f))
+        for name, a in payload.items():
+            np.save(os.path.join(d, name + ".npy"), a)
 
     def _check(self):
         if self._error is not None:
