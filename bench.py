@@ -483,6 +483,11 @@ def run_gpu(args, rank, world, local_rank, dtype_key=None, with_e2e=True):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     Qd.copy_(host_in, non_blocking=True)
+    if solver.cfg.bed:
+        # the bed planes of the uploaded state (the solver reads them for
+        # this scheme and precision), inside the timed region
+        L.check(lib.zb_swe2d_bed_prepare(cfg, L.ptr(Qd), solver.cfg.bed,
+                                         C.c_size_t(solver._bed.numel()), sp), "bed_prepare")
     lib.zb_swe2d_init(cfg, L.ptr(Qd), ctrl, 0, 0.0, sp)
     for k in range(K):
         rc = lib.zb_swe2d_step(cfg, L.ptr(Qd), ws, wsb, ctrl, k % 3, sp)

@@ -102,10 +102,10 @@ typedef struct {
   int32_t dtype;           /* ZB_F32 / ZB_F64                              */
   /* NULL, or the planes zb_swe2d_bed_prepare wrote for the b row of every
    * state stepped with this config (device memory).  Read by the fused steps
-   * of the float32 order-2 eta / HLL-HR scheme on grids without a periodic
-   * side (ignored by every other scheme, by the stage API and by the
-   * ensemble); the results are the same bits either way.  The caller owns
-   * the promise that b has not changed since the planes were prepared. */
+   * of the order-2 eta / HLL-HR scheme on grids without a periodic side
+   * (ignored by every other scheme, by the stage API and by the ensemble);
+   * the results are the same bits either way.  The caller owns the promise
+   * that b has not changed since the planes were prepared. */
   const void* bed;
 } zb_swe2d_cfg;
 
@@ -121,10 +121,10 @@ size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg);
 size_t zb_swe2d_bed_bytes(const zb_swe2d_cfg* cfg);
 
 /* The bathymetry's interior least-squares gradient (x, y) and limiter value,
- * three float32 planes laid out like a state row, from the b row of Q.  b is
- * constant in time (the reference steps it with a zero update), so a march
- * prepares them once and the interior body of every step reads them instead
- * of re-evaluating b's slope each stage (the reference's reconstruction
+ * three planes of the config's dtype laid out like a state row, from the b
+ * row of Q.  b is constant in time (the reference steps it with a zero
+ * update), so a march prepares them once and the interior body of every step
+ * reads them instead of re-evaluating b's slope each stage (the reference's reconstruction
  * evaluates the gradient and limiter of every variable, b included, on every
  * call: zoomy_jax/fvm/reconstruction_jax.py:524-533, 695-708).  ZB_E_ARG for
  * a scheme without bed planes. */

@@ -1,13 +1,14 @@
 """Prepared bed slopes (``zb_swe2d_bed_prepare``) against the bed slope
 evaluated in every stage.
 
-The bathymetry row never changes, so the float32 eta / HLL-HR fused step can
-read b's interior gradient and limiter value from planes prepared once.  The
-prepared planes repeat the strip body's own float32 operations for b, so a
-march with them is the same march bit for bit; these tests hold that over
-fused steps on square and ragged grids, every limiter, dry cells, periodic
-sides and Manning friction, and check the planes against the float64 oracle's
-interior least-squares gradient.
+The bathymetry row never changes, so the eta / HLL-HR fused step can read
+b's interior gradient and limiter value from planes prepared once.  The
+prepared planes repeat the strip body's own operations for b (the paired
+float32 block, the scalar float64 one), so a march with them is the same
+march bit for bit; these tests hold that over fused steps on square and
+ragged grids, both precisions, every limiter, dry cells, periodic sides and
+Manning friction, and check the planes against the float64 central
+least-squares gradient.
 """
 import ctypes as C
 
@@ -29,7 +30,7 @@ def _centers(nx, ny):
     return np.stack([((i + 0.5) / nx).reshape(-1), ((j + 0.5) / ny).reshape(-1)])
 
 
-def _cfg(nx, ny, limiter="minmod", bc="wall", manning=0.0, eps_wet=1e-6):
+def _cfg(nx, ny, limiter="minmod", bc="wall", manning=0.0, eps_wet=1e-6, dtype=torch.float32):
     c = L.ZbSwe2dCfg()
     c.nx, c.ny = nx, ny
     c.x0, c.y0, c.dx, c.dy = 0.0, 0.0, 1.0 / nx, 1.0 / ny
@@ -40,7 +41,7 @@ def _cfg(nx, ny, limiter="minmod", bc="wall", manning=0.0, eps_wet=1e-6):
     c.g, c.wet_dry_eps, c.eps_wet, c.manning_n = 9.81, 1e-6, eps_wet, manning
     c.implicit_source, c.dim_factor, c.cfl = 0, 2, 0.45
     c.dt_max, c.t_end, c.degree = float("inf"), float("inf"), 0
-    c.dtype = L.ZB_F32
+    c.dtype = L.ZB_F64 if dtype == torch.float64 else L.ZB_F32
     return c
 
 
@@ -60,7 +61,7 @@ def _march(lib, cfg, Q, steps):
 
 def _prepare(lib, cfg, Q):
     nb = lib.zb_swe2d_bed_bytes(C.byref(cfg))
-    assert nb == 3 * cfg.nx * cfg.ny * 4
+    assert nb == 3 * cfg.nx * cfg.ny * (8 if cfg.dtype == L.ZB_F64 else 4)
     bed = torch.empty(nb, dtype=torch.uint8, device="cuda")
     assert lib.zb_swe2d_bed_prepare(C.byref(cfg), L.ptr(Q), L.ptr(bed), C.c_size_t(nb),
                                     L.stream_ptr()) == 0
@@ -81,17 +82,18 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64], ids=["f32", "f64"])
 @pytest.mark.parametrize("state", ["dam", "grf"])
 @pytest.mark.parametrize("case", list(CASES))
-def test_prepared_bed_march_is_bitwise_the_evaluated_one(case, state):
+def test_prepared_bed_march_is_bitwise_the_evaluated_one(case, state, dtype):
     kw = dict(CASES[case])
     nx, ny = kw.pop("nx"), kw.pop("ny")
     lib = L.load()
     xc = _centers(nx, ny)
     q = circular_dam_state(xc, seed=5) if state == "dam" else grf_dam_state(xc, seed=6)
-    Q0 = torch.as_tensor(q, dtype=torch.float32, device="cuda").contiguous()
-    cfg_a = _cfg(nx, ny, **kw)
-    cfg_b = _cfg(nx, ny, **kw)
+    Q0 = torch.as_tensor(q, dtype=dtype, device="cuda").contiguous()
+    cfg_a = _cfg(nx, ny, dtype=dtype, **kw)
+    cfg_b = _cfg(nx, ny, dtype=dtype, **kw)
     bed = _prepare(lib, cfg_b, Q0)
     cfg_b.bed = bed.data_ptr()
     Qa, Qb = Q0.clone(), Q0.clone()
@@ -106,7 +108,8 @@ def test_prepared_bed_march_is_bitwise_the_evaluated_one(case, state):
     assert ca.steps == cb.steps
     if state == "dam":
         assert ca.steps == 20
-    assert torch.equal(Qa.view(torch.int32), Qb.view(torch.int32)), \
+    bits = torch.int64 if dtype == torch.float64 else torch.int32
+    assert torch.equal(Qa.view(bits), Qb.view(bits)), \
         (Qa - Qb).abs().max().item()
     assert ca.t[20 % 3] == cb.t[20 % 3]
 

@@ -69,8 +69,8 @@ struct SweParams {
   // reach the boundary and keep the control block; no tile launch)
   int strip_full;
   // the bed's interior gradient and limiter value (planes gx, gy, phi of
-  // zb_swe2d_bed_prepare), read by the float32 eta / HLL-HR interior strip
-  // body; nullptr: evaluated from b like every other variable
+  // zb_swe2d_bed_prepare), read by the eta / HLL-HR interior strip body;
+  // nullptr: evaluated from b like every other variable
   const T* bed;
   LsqTable<T> lsq;
 };
@@ -989,10 +989,11 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
   // the pre-pass, slots [side][m - (r0 - 1)][12] of this warp (side 0: column
   // 0, side 1: column ny - 1; rows r0 - 1 .. r1)
   constexpr bool PRE = EK == 3 && PAIR;
-  // BEDT: float32 interior items read b's gradient and limiter value from the
-  // planes swe2d_bed_kernel prepared (b never changes) instead of evaluating
-  // them; the planes are laid out like the state's
-  constexpr bool BED = BEDT && PAIR && EK == 0;
+  // BEDT: interior items of the eta / HLL-HR scheme read b's gradient and
+  // limiter value from the planes swe2d_bed_kernel prepared (b never
+  // changes) instead of evaluating them; the planes are laid out like the
+  // state's
+  constexpr bool BED = BEDT && EK == 0 && RECON == ZB_RECON_ETA && RIEMANN == ZB_RIEMANN_HLL_HR;
   const T* __restrict__ bedP = p.bed;
   const size_t bed_plane = (size_t)nx * ny;
   constexpr int PROWS = SXC_MAX + 2;
@@ -1126,6 +1127,12 @@ __device__ __forceinline__ void strip_item(const T* __restrict__ bP, const T* __
       } else {
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
+        if (v == 0 && BED) {   // float64 interior items: the prepared planes
+          gxa[0] = bgx;
+          gya[0] = bgy;
+          phi[0] = bphi;
+          continue;
+        }
         const T u = R1.w(v);
         const T tc = (R0.w(v) + R1.w(v)) + R2.w(v);
         const T tl = shu(tc), tr = shd(tc);
@@ -1725,42 +1732,49 @@ swe2d_amax_kernel(const T* __restrict__ hP, const T* __restrict__ qxP,
 }
 
 // The bed's interior least-squares gradient and limiter value, one thread per
-// cell: the float32 paired slope block of strip_item for variable 0 (b), in
-// the same operations and order ((left + centre) + right sums, paired
-// difference and scaling, three-input bounds, the limiter), so the strip body
-// that reads these planes produces the same bits as the one that evaluates
-// them.  Cells on the domain boundary get zeros (the interior body never
-// reads them; boundary cells take the boundary classes).
+// cell: the slope block of strip_item for variable 0 (b) -- the float32
+// paired block, the float64 scalar one -- in the same operations and order
+// ((left + centre) + right sums, difference and scaling, three-input bounds,
+// the limiter), so the strip body that reads these planes produces the same
+// bits as the one that evaluates them.  Cells on the domain boundary get zeros
+// (the interior body never reads them; boundary cells take the boundary
+// classes).
+template <typename T>
 __global__ void __launch_bounds__(NT)
-swe2d_bed_kernel(const float* __restrict__ b, float* __restrict__ bed,
-                 const SweParams<float> p) {
+swe2d_bed_kernel(const T* __restrict__ b, T* __restrict__ bed, const SweParams<T> p) {
   const int nx = p.nx, ny = p.ny;
   const size_t n = (size_t)nx * ny;
   const bool clipmin = p.limiter != ZB_LIM_NONE && p.limiter != ZB_LIM_VENKATAKRISHNAN;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(k / (size_t)ny), j = (int)(k % (size_t)ny);
-    float gx = 0.f, gy = 0.f, phi = 0.f;
+    T gx = T(0), gy = T(0), phi = T(0);
     if (i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1) {
-      const float* rm = b + (k - ny);   // row i - 1
-      const float* rc = b + k;          // row i
-      const float* rp = b + (k + ny);   // row i + 1
-      const float u = rc[0];
-      const float sx0 = (rm[-1] + rm[0]) + rm[1];   // row sums of rows i -/+ 1
-      const float sx2 = (rp[-1] + rp[0]) + rp[1];
-      const float tl = (rm[-1] + rc[-1]) + rp[-1];  // column sums of columns j -/+ 1
-      const float tr = (rm[1] + rc[1]) + rp[1];
-      const float2 gv = mul2(sub2(f2(sx2, tr), f2(sx0, tl)), f2(p.inv6dx, p.inv6dy));
-      const float umax = fmx3(u, rp[0], fmx3(rm[0], rc[1], rc[-1]));
-      const float umin = fmn3(u, rp[0], fmn3(rm[0], rc[1], rc[-1]));
-      const float2 dd = sub2(f2(umax, umin), f2(u, u));
-      gx = gv.x;
-      gy = gv.y;
-      if (clipmin) {
-        const float2 ac = mul2(gv, f2(p.half_dx, p.half_dy));
-        phi = phi_clipmin(ac.x, ac.y, dd.x, dd.y);
+      const T* rm = b + (k - ny);   // row i - 1
+      const T* rc = b + k;          // row i
+      const T* rp = b + (k + ny);   // row i + 1
+      const T u = rc[0];
+      const T sx0 = (rm[-1] + rm[0]) + rm[1];   // row sums of rows i -/+ 1
+      const T sx2 = (rp[-1] + rp[0]) + rp[1];
+      const T tl = (rm[-1] + rc[-1]) + rp[-1];  // column sums of columns j -/+ 1
+      const T tr = (rm[1] + rc[1]) + rp[1];
+      const T umax = fmx3(u, rp[0], fmx3(rm[0], rc[1], rc[-1]));
+      const T umin = fmn3(u, rp[0], fmn3(rm[0], rc[1], rc[-1]));
+      if constexpr (std::is_same<T, float>::value) {
+        const float2 gv = mul2(sub2(f2(sx2, tr), f2(sx0, tl)), f2(p.inv6dx, p.inv6dy));
+        const float2 dd = sub2(f2(umax, umin), f2(u, u));
+        gx = gv.x;
+        gy = gv.y;
+        if (clipmin) {
+          const float2 ac = mul2(gv, f2(p.half_dx, p.half_dy));
+          phi = phi_clipmin(ac.x, ac.y, dd.x, dd.y);
+        } else {
+          phi = limiter_phi(p.limiter, gv.x, gv.y, p.half_dx, p.half_dy, dd.x, dd.y, p.vk_eps2);
+        }
       } else {
-        phi = limiter_phi(p.limiter, gv.x, gv.y, p.half_dx, p.half_dy, dd.x, dd.y, p.vk_eps2);
+        gx = (sx2 - sx0) * p.inv6dx;
+        gy = (tr - tl) * p.inv6dy;
+        phi = limiter_phi(p.limiter, gx, gy, p.half_dx, p.half_dy, umax - u, umin - u, p.vk_eps2);
       }
     }
     bed[k] = gx;
@@ -1963,11 +1977,10 @@ static LsqTable<T> make_lsq(double dx, double dy) {
   return tab;
 }
 
-// the scheme whose interior body reads prepared bed slopes: float32, order 2,
-// eta reconstruction, HLL with hydrostatic reconstruction
+// the scheme whose interior body reads prepared bed slopes: order 2, eta
+// reconstruction, HLL with hydrostatic reconstruction (float32 or float64)
 static bool bed_scheme(const zb_swe2d_cfg* c) {
-  return c->dtype == ZB_F32 && c->order == 2 && c->recon == ZB_RECON_ETA &&
-         c->riemann == ZB_RIEMANN_HLL_HR;
+  return c->order == 2 && c->recon == ZB_RECON_ETA && c->riemann == ZB_RIEMANN_HLL_HR;
 }
 
 template <typename T>
@@ -2006,7 +2019,8 @@ static SweParams<T> make_params(const zb_swe2d_cfg* c, double alpha, double beta
   p.inv4dy = (T)(1.0 / (4.0 * c->dy));
   p.fast_i0 = p.fast_i1 = p.fast_j0 = p.fast_j1 = 0;
   p.strip_full = 0;
-  p.bed = (std::is_same<T, float>::value && bed_scheme(c)) ? (const T*)c->bed : nullptr;
+  p.bed = (bed_scheme(c) && (c->dtype == ZB_F64) == std::is_same<T, double>::value)
+              ? (const T*)c->bed : nullptr;
   return p;
 }
 
@@ -2125,7 +2139,7 @@ static int run_step(const zb_swe2d_cfg* c, T* Q, T* ws, zb_ctrl* ctrl, int phase
     ZB_CUDA_TRY(cudaGetLastError());
     if (ni > 0) {
       // the interior items read the prepared bed planes when there are some
-      constexpr bool BEDK = std::is_same<T, float>::value && RECON == ZB_RECON_ETA &&
+      constexpr bool BEDK = RECON == ZB_RECON_ETA &&
                             RIEMANN == ZB_RIEMANN_HLL_HR;
       bool done = false;
       if constexpr (BEDK) {
@@ -2410,17 +2424,24 @@ size_t zb_swe2d_workspace_bytes(const zb_swe2d_cfg* cfg) {
 
 size_t zb_swe2d_bed_bytes(const zb_swe2d_cfg* cfg) {
   if (!valid_cfg(cfg) || !bed_scheme(cfg)) return 0;
-  return 3 * (size_t)cfg->nx * cfg->ny * sizeof(float);
+  return 3 * (size_t)cfg->nx * cfg->ny * (cfg->dtype == ZB_F64 ? 8 : 4);
 }
 
 int zb_swe2d_bed_prepare(const zb_swe2d_cfg* cfg, const void* Q, void* bed, size_t bed_bytes,
                          zb_stream_t stream) {
   if (!valid_cfg(cfg) || !bed_scheme(cfg) || !Q || !bed) return ZB_E_ARG;
-  if (bed_bytes < zb_swe2d_bed_bytes(cfg) || ((uintptr_t)bed & 3u)) return ZB_E_ARG;
-  const SweParams<float> p = make_params<float>(cfg, 0.0, 1.0);
+  if (bed_bytes < zb_swe2d_bed_bytes(cfg) || ((uintptr_t)bed & 7u)) return ZB_E_ARG;
   const size_t n = (size_t)cfg->nx * cfg->ny;
   const int grid = (int)std::min<size_t>((n + NT - 1) / NT, (size_t)148 * 16);
-  swe2d_bed_kernel<<<grid, NT, 0, (cudaStream_t)stream>>>((const float*)Q, (float*)bed, p);
+  if (cfg->dtype == ZB_F64) {
+    const SweParams<double> p = make_params<double>(cfg, 0.0, 1.0);
+    swe2d_bed_kernel<double><<<grid, NT, 0, (cudaStream_t)stream>>>((const double*)Q,
+                                                                     (double*)bed, p);
+  } else {
+    const SweParams<float> p = make_params<float>(cfg, 0.0, 1.0);
+    swe2d_bed_kernel<float><<<grid, NT, 0, (cudaStream_t)stream>>>((const float*)Q,
+                                                                   (float*)bed, p);
+  }
   return zb_launch_check();
 }
 

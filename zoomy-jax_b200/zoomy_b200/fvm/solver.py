@@ -114,10 +114,11 @@ class HyperbolicSolver:
     True the fused float32 eta / HLL-HR steps read the bathymetry's gradient
     and limiter value from planes prepared once per state tensor instead of
     evaluating them every stage (the same bits either way); ``"auto"`` (the
-    default) does so for the Venkatakrishnan limiter, whose b evaluation is
-    costly (0.422 -> 0.376 ms per 2048^2 step on a B200), and not for the
-    clip-min limiters, where the extra loads cost what the saved arithmetic
-    gains (0.2049 -> 0.2064 ms).  A caller that edits ``Q[0]`` through a raw
+    default) does so in float64 (0.715 -> 0.643 ms per 2048^2 minmod step on a
+    B200) and for the float32 Venkatakrishnan limiter, whose b evaluation is
+    costly (0.422 -> 0.376 ms), and not for the float32 clip-min limiters,
+    where the extra loads cost what the saved arithmetic gains (0.2068 ->
+    0.2071 ms).  A caller that edits ``Q[0]`` through a raw
     pointer instead of torch clears ``solver.cfg.bed`` or sets ``use_bed =
     False``.
     """
@@ -260,7 +261,7 @@ class HyperbolicSolver:
         b's slope (``zb_swe2d_bed_prepare``), prepared again whenever the
         state tensor is another one or was modified from torch since (b is
         never written by the steps, which go through raw pointers)."""
-        auto_off = (self.use_bed == "auto"
+        auto_off = (self.use_bed == "auto" and self.cfg.dtype != L.ZB_F64
                     and self.cfg.limiter != L.LIMITER["venkatakrishnan"])
         if not isinstance(self.be, _CartBackend) or not self.use_bed or auto_off:
             self.cfg.bed = None
