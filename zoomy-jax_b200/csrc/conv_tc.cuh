@@ -301,6 +301,13 @@ conv3x3_tc(const float* __restrict__ inA, int cin_a, const float* __restrict__ i
 constexpr int CBX = 16, CBY = 16;            // output region: two 8 x 16 M tiles
 constexpr int CHX = CBX + 2, CHY = CBY + 2;  // halo region
 constexpr int CHP = CHX * CHY;               // 324 halo pixels
+// NTH = 256 (wide layers): eight warps stage the halo, and warps w and w + 4
+// read TMEM lane quarter w of M tiles 0 and 1 in the epilogue; NTH = 128:
+// four warps, each reading its lane quarter of both tiles.  Measured, one
+// 1024^2 application: (24, 48) 0.473 ms with 128 threads everywhere, 0.448
+// with 256 everywhere, 0.440 with 256 for the layers of six or more input
+// chunks only (what the launcher takes); (8, 16) 0.249 / 0.255 / 0.247.
+constexpr int CB_WIDE_CHUNKS = 6;
 
 __host__ __device__ inline size_t cb8_smem_bytes(int cinp, int coutp) {
   return (size_t)cinp * CHP * 2 + (size_t)9 * cinp * coutp * 2 + 64;
@@ -324,7 +331,8 @@ enum { CB_OUT_CHUNKED = 0, CB_OUT_F32 = 1 };
 // in its summation order).  CB_OUT_F32: out is float32 planes [co][b][y][x].
 // H and W even.  act != 0: tanh on the SFU (the inference activation, act 2
 // of conv3x3_tc).
-__global__ void __launch_bounds__(TC_THREADS)
+template <int NTH>
+__global__ void __launch_bounds__(NTH)
 conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __restrict__ inB,
             int chB, int cin, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
             void* __restrict__ out, uint4* __restrict__ pool, int cout, int out_form, int B,
@@ -339,7 +347,7 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // weights: [tap][chunk][n][8] bf16, zero outside (cout, cin)
-  for (int e = tid; e < 9 * nch * coutp; e += TC_THREADS) {
+  for (int e = tid; e < 9 * nch * coutp; e += NTH) {
     const int n = e % coutp;
     const int rest = e / coutp;
     const int ch = rest % nch, tap = rest / nch;
@@ -383,7 +391,7 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
     const size_t img = (size_t)b * H * W;
     // halo region: one 16-byte copy per (chunk, halo pixel); zero outside the
     // image and for the padding chunks
-    for (int e = tid; e < nch * CHP; e += TC_THREADS) {
+    for (int e = tid; e < nch * CHP; e += NTH) {
       const int ch = e / CHP, q = e - ch * CHP;
       const int yy = y0 - 1 + q / CHX, xx = x0 - 1 + q % CHX;
       const bool inside = yy >= 0 && yy < H && xx >= 0 && xx < W;
@@ -437,16 +445,17 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
       break;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // epilogue: warp w owns accumulator rows 32w .. 32w+31 of both M tiles
-    const int m = warp * 32 + lane;
-    for (int i = 0; i < 2; ++i) {
+    // epilogue: warp w owns accumulator rows 32 (w % 4) .. 32 (w % 4) + 31 of
+    // M tile w / 4 (NTH = 256), or of both tiles (NTH = 128)
+    const int m = (warp & 3) * 32 + lane;
+    for (int i = (NTH == 256 ? warp >> 2 : 0); i < (NTH == 256 ? (warp >> 2) + 1 : 2); ++i) {
       const int x = x0 + 8 * i + (m % 8), y = y0 + m / 8;
       const bool store = x < W && y < H;
       // the 2x2 block's top-left lane (even x, even y) writes the pooled pixel
       const bool pstore = store && ((m & 1) == 0) && (((m >> 3) & 1) == 0);
       for (int c0 = 0; c0 < coutp; c0 += 16) {
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(i * coutp + c0), v);
+        tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(i * coutp + c0), v);
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
           const int co = c0 + k;

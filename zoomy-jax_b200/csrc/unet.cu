@@ -563,12 +563,15 @@ static int conv_cb8_launch(const uint4* inA, int chA, int mode_a, const uint4* i
     sms[dev].store(v);
   }
   if (!attr[dev].load()) {
-    ZB_CUDA_TRY(cudaFuncSetAttribute(conv3x3_cb8, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024));
+    ZB_CUDA_TRY(cudaFuncSetAttribute(conv3x3_cb8<128>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    ZB_CUDA_TRY(cudaFuncSetAttribute(conv3x3_cb8<256>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     attr[dev].store(true);
   }
+  const int nth = cinp / 8 >= CB_WIDE_CHUNKS ? 256 : 128;
   const int smem_sm = 228 * 1024, per_cta_reserved = 1024;
-  const int by_tmem = 512 / cols, by_threads = 2048 / TC_THREADS;
+  const int by_tmem = 512 / cols, by_threads = 2048 / nth;
   size_t smem = cb8_smem_bytes(cinp, coutp);
   if (by_tmem < by_threads) {
     const size_t floor_bytes = (size_t)(smem_sm / (by_tmem + 1) - per_cta_reserved + 16);
@@ -579,7 +582,12 @@ static int conv_cb8_launch(const uint4* inA, int chA, int mode_a, const uint4* i
   const long long nreg = (long long)((W + CBX - 1) / CBX) * ((H + CBY - 1) / CBY) * B;
   const int grid = (int)std::max<long long>(
       1, std::min<long long>(nreg, (long long)sms[dev] * std::max(1, fit)));
-  conv3x3_cb8<<<grid, TC_THREADS, smem, st>>>(inA, chA, mode_a, inB, chB, cin, w, bias, out,
+  if (nth == 256)
+    conv3x3_cb8<256><<<grid, 256, smem, st>>>(inA, chA, mode_a, inB, chB, cin, w, bias, out,
+                                              pool, cout, out_form, B, H, W, act, cols,
+                                              unet_err_word());
+  else
+    conv3x3_cb8<128><<<grid, 128, smem, st>>>(inA, chA, mode_a, inB, chB, cin, w, bias, out,
                                               pool, cout, out_form, B, H, W, act, cols,
                                               unet_err_word());
   return zb_launch_check();
