@@ -42,7 +42,7 @@ constexpr int DENSE_MAX_CELLS = 64;   // coarsest levels this small are solved e
 struct Level {
   int nx, ny;
   float dx;
-  long long cx, cy, dg, x, f, r;   // float offsets into the workspace
+  long long cx, cy, idg, x, f, r;   // float offsets into the workspace
   long long xo;                    // the level's V-cycle result (see mg_up_kernel)
 };
 
@@ -113,7 +113,7 @@ static Plan make_plan(const zb_poisson_cfg* c) {
     L.dx = dx;
     L.cx = f; f += (long long)(nx + 1) * ny;
     L.cy = f; f += (long long)nx * (ny + 1);
-    L.dg = f; f += (long long)nx * ny;
+    L.idg = f; f += (long long)nx * ny;
     L.x = f; f += (long long)nx * ny;
     L.f = f; f += (long long)nx * ny;
     L.r = f; f += (long long)nx * ny;
@@ -206,12 +206,14 @@ __global__ void diag_kernel64(const double* cx, const double* cy, int nx, int ny
   }
 }
 
+// the float32 levels keep the inverse of the diagonal: every smoother
+// multiplies by it
 __global__ void diag_kernel32(const float* cx, const float* cy, int nx, int ny, float idx2,
-                              float* dg) {
+                              float* idg) {
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
        k += (long long)gridDim.x * NT) {
     const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
-    dg[k] = diag_at<float>(cx, cy, nx, ny, i, j, idx2);
+    idg[k] = __frcp_rn(diag_at<float>(cx, cy, nx, ny, i, j, idx2));
   }
 }
 
@@ -437,10 +439,25 @@ __device__ __forceinline__ float apply_at(const float* x, const float* cx, const
   return (a * (xc - xe) + b * (xc - xw) + c * (xc - xn) + d * (xc - xs)) * idx2;
 }
 
-// one red-black half sweep: x_i += (f_i - (A x)_i) / d_i on cells of `color`
+// sum of c_f x_j over the in-domain neighbours (a wall's ghost -x_i belongs
+// to the diagonal): the red-black update in the form
+// x_i = (f_i + idx2 * sum) / d_i, d_i containing the ghost terms
+__device__ __forceinline__ float nbsum_at(const float* x, const float* cx, const float* cy,
+                                          int nx, int ny, int i, int j) {
+  const float a = cx[(i + 1) * ny + j], b = cx[i * ny + j];
+  const float c = cy[i * (ny + 1) + j + 1], d = cy[i * (ny + 1) + j];
+  const float xe = i + 1 < nx ? x[(i + 1) * ny + j] : 0.0f;
+  const float xw = i > 0 ? x[(i - 1) * ny + j] : 0.0f;
+  const float xn = j + 1 < ny ? x[i * ny + j + 1] : 0.0f;
+  const float xs = j > 0 ? x[i * ny + j - 1] : 0.0f;
+  return (a * xe + b * xw) + (c * xn + d * xs);
+}
+
+// one red-black half sweep: x_i = (f_i + idx2 sum_j c_ij x_j) / d_i on cells
+// of `color` (the same update as x_i += (f_i - (A x)_i) / d_i)
 __global__ void __launch_bounds__(NT)
 rbgs_kernel(float* __restrict__ x, const float* __restrict__ f, const float* __restrict__ cx,
-            const float* __restrict__ cy, const float* __restrict__ dg, int nx, int ny,
+            const float* __restrict__ cy, const float* __restrict__ idg, int nx, int ny,
             float idx2, int color) {
   const int half = (ny + 1) / 2;
   for (long long t = blockIdx.x * (long long)NT + threadIdx.x; t < (long long)nx * half;
@@ -448,9 +465,7 @@ rbgs_kernel(float* __restrict__ x, const float* __restrict__ f, const float* __r
     const int i = (int)(t / half), m = (int)(t - (long long)i * half);
     const int j = 2 * m + ((i + color) & 1);
     if (j >= ny) continue;
-    float od;
-    const float ax = apply_at(x, cx, cy, nx, ny, i, j, idx2, od);
-    x[i * ny + j] += (f[i * ny + j] - ax) / dg[i * ny + j];
+    x[i * ny + j] = (f[i * ny + j] + idx2 * nbsum_at(x, cx, cy, nx, ny, i, j)) * idg[i * ny + j];
   }
 }
 
@@ -578,7 +593,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Shared-memory image of a level's tile plus a HALO-wide ring: x, f, r, dg
+// Shared-memory image of a level's tile plus a HALO-wide ring: x, f, r, idg
 // (R x R) and the face coefficients cx ((R+1) x R), cy (R x (R+1)).  A tile
 // whose ring lies wholly inside the level (most of them) takes the EDGE-free
 // path: no domain tests and no Dirichlet ghosts.
@@ -587,7 +602,7 @@ struct Stage {
   static constexpr int R = TT + 2 * HALO;
   int i0, j0, nx, ny;
   bool interior;
-  float *x, *f, *r, *dg, *cx, *cy;
+  float *x, *f, *r, *idg, *cx, *cy;
   __device__ bool inside(int a, int b) const {
     const int gi = i0 - HALO + a, gj = j0 - HALO + b;
     return gi >= 0 && gi < nx && gj >= 0 && gj < ny;
@@ -608,6 +623,25 @@ struct Stage {
     }
     return (ea * (xc - xe) + wa * (xc - xw) + nb * (xc - xn) + sb * (xc - xs)) * idx2;
   }
+  // sum of c_f x_j over the in-domain neighbours (a wall's ghost belongs to
+  // the diagonal)
+  template <bool EDGE>
+  __device__ float nbsum(int a, int b) const {
+    const float ea = cx[(a + 1) * R + b], wa = cx[a * R + b];
+    const float nb = cy[a * (R + 1) + b + 1], sb = cy[a * (R + 1) + b];
+    float xe = x[(a + 1) * R + b], xw = x[(a - 1) * R + b];
+    float xn = x[a * R + b + 1], xs = x[a * R + b - 1];
+    if (EDGE) {
+      const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+      if (gi + 1 >= nx) xe = 0.0f;
+      if (gi <= 0) xw = 0.0f;
+      if (gj + 1 >= ny) xn = 0.0f;
+      if (gj <= 0) xs = 0.0f;
+    }
+    return (ea * xe + wa * xw) + (nb * xn + sb * xs);
+  }
+  // red-black update x_i = (f_i + idx2 sum_j c_ij x_j) / d_i (the same update
+  // as x_i += (f_i - (A x)_i) / d_i, with d_i's inverse staged)
   template <bool EDGE>
   __device__ void sweep_impl(int color, int m, float idx2) const {
     for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y) {
@@ -616,21 +650,20 @@ struct Stage {
       int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
       for (; b < R - m; b += 2 * (int)blockDim.x) {
         if (EDGE && !inside(a, b)) continue;
-        const float v = ax<EDGE>(a, b, idx2);
-        x[a * R + b] += (f[a * R + b] - v) / dg[a * R + b];
+        x[a * R + b] = (f[a * R + b] + nbsum<EDGE>(a, b) * idx2) * idg[a * R + b];
       }
     }
     __syncthreads();
   }
   // the first half-sweep of a V-cycle's way down starts from x = 0, where
-  // A x = 0 exactly: the update x += (f - A x) / dg is x = f / dg, bit for bit
+  // A x = 0 exactly: the update is x = f / d
   __device__ void sweep_from_zero(int color, int m) const {
     for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y) {
       const int gi = i0 - HALO + a;
       int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
       for (; b < R - m; b += 2 * (int)blockDim.x) {
         if (!interior && !inside(a, b)) continue;
-        x[a * R + b] = f[a * R + b] / dg[a * R + b];
+        x[a * R + b] = f[a * R + b] * idg[a * R + b];
       }
     }
     __syncthreads();
@@ -650,13 +683,13 @@ struct Stage {
 template <int HALO, int TT>
 __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny,
                                        const float* __restrict__ f, const float* __restrict__ cx,
-                                       const float* __restrict__ cy, const float* __restrict__ dg,
+                                       const float* __restrict__ cy, const float* __restrict__ idg,
                                        const float* __restrict__ x) {
   constexpr int R = Stage<HALO, TT>::R;
   Stage<HALO, TT> S;
   S.i0 = i0; S.j0 = j0; S.nx = nx; S.ny = ny;
   S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
-  S.x = sm; S.f = sm + R * R; S.r = sm + 2 * R * R; S.dg = sm + 3 * R * R;
+  S.x = sm; S.f = sm + R * R; S.r = sm + 2 * R * R; S.idg = sm + 3 * R * R;
   S.cx = sm + 4 * R * R; S.cy = S.cx + (R + 1) * R;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -667,7 +700,7 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
     const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
     const long long k = in ? (long long)gi * ny + gj : 0;
     cp_async4(S.f + e, f + k, in);
-    cp_async4(S.dg + e, dg + k, in);
+    cp_async4(S.idg + e, idg + k, in);
     if (x) cp_async4(S.x + e, x + k, in);
     else S.x[e] = 0.0f;
   }
@@ -696,7 +729,7 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
 template <int NU, int TT>
 __global__ void __launch_bounds__(FNT_MAX)
 mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
-               const float* __restrict__ cy, const float* __restrict__ dg, float* __restrict__ x,
+               const float* __restrict__ cy, const float* __restrict__ idg, float* __restrict__ x,
                float* __restrict__ fc, int nx, int ny, float idx2) {
   pdl_enter();
   extern __shared__ float fsm[];
@@ -705,7 +738,7 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, dg, nullptr);
+  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, nullptr);
   if (NU > 0) S.sweep_from_zero(0, 1);
   for (int s = 1; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
   // residual where the sweeps are final and one ring beyond the tile
@@ -739,7 +772,7 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
 template <int NU, int TT>
 __global__ void __launch_bounds__(FNT_MAX)
 mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
-             const float* __restrict__ cy, const float* __restrict__ dg,
+             const float* __restrict__ cy, const float* __restrict__ idg,
              const float* __restrict__ x, const float* __restrict__ ec, float* __restrict__ xo,
              int nx, int ny, float idx2) {
   pdl_enter();
@@ -749,7 +782,7 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, dg, x);
+  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x);
   const int nxc = nx / 2, nyc = ny / 2;
   for (int a = (int)threadIdx.y; a < R; a += (int)blockDim.y)
     for (int b = (int)threadIdx.x; b < R; b += (int)blockDim.x) {
@@ -781,15 +814,13 @@ __global__ void copy32_kernel(const float* a, float* b, long long n) {
 constexpr int CT = 1024;
 
 __device__ void cta_rbgs(float* x, const float* f, const float* cx, const float* cy,
-                         const float* dg, int nx, int ny, float idx2, int color) {
+                         const float* idg, int nx, int ny, float idx2, int color) {
   const int half = (ny + 1) / 2;
   for (int t = threadIdx.x; t < nx * half; t += CT) {
     const int i = t / half, m = t - i * half;
     const int j = 2 * m + ((i + color) & 1);
     if (j >= ny) continue;
-    float od;
-    const float ax = apply_at(x, cx, cy, nx, ny, i, j, idx2, od);
-    x[i * ny + j] += (f[i * ny + j] - ax) / dg[i * ny + j];
+    x[i * ny + j] = (f[i * ny + j] + idx2 * nbsum_at(x, cx, cy, nx, ny, i, j)) * idg[i * ny + j];
   }
   __syncthreads();
 }
@@ -797,7 +828,7 @@ __device__ void cta_rbgs(float* x, const float* f, const float* cx, const float*
 // coarsest-level solve: x = A^-1 f with the inverse built at set-up when the
 // level has <= DENSE_MAX_CELLS cells, else symmetric red-black sweep pairs
 __device__ void cta_coarsest(float* x, const float* f, const float* cx, const float* cy,
-                             const float* dg, const float* inv, int nx, int ny, float idx2,
+                             const float* idg, const float* inv, int nx, int ny, float idx2,
                              int sweeps) {
   const int n = nx * ny;
   if (inv) {
@@ -810,12 +841,12 @@ __device__ void cta_coarsest(float* x, const float* f, const float* cx, const fl
     return;
   }
   for (int s = 0; s < sweeps; ++s) {
-    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 0);
-    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 1);
+    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 0);
+    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 1);
   }
   for (int s = 0; s < sweeps; ++s) {
-    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 1);
-    cta_rbgs(x, f, cx, cy, dg, nx, ny, idx2, 0);
+    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 1);
+    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 0);
   }
 }
 
@@ -823,9 +854,9 @@ __global__ void __launch_bounds__(CT)
 coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
   pdl_enter();
   extern __shared__ float sm[];
-  // shared copies of x, f, r, cx, cy, dg for every small level
+  // shared copies of x, f, r, cx, cy, idg for every small level
   float* sx[MAXL]; float* sf[MAXL]; float* sr[MAXL];
-  float* scx[MAXL]; float* scy[MAXL]; float* sdg[MAXL];
+  float* scx[MAXL]; float* scy[MAXL]; float* sidg[MAXL];
   long long o = 0;
   for (int l = P.small0; l < P.nlev; ++l) {
     const Level& L = P.L[l];
@@ -835,7 +866,7 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     sr[l] = sm + o; o += n;
     scx[l] = sm + o; o += (L.nx + 1) * L.ny;
     scy[l] = sm + o; o += L.nx * (L.ny + 1);
-    sdg[l] = sm + o; o += n;
+    sidg[l] = sm + o; o += n;
   }
   for (int l = P.small0; l < P.nlev; ++l) {
     const Level& L = P.L[l];
@@ -843,7 +874,7 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     for (int k = threadIdx.x; k < (L.nx + 1) * L.ny; k += CT) scx[l][k] = ws_f[L.cx + k];
     for (int k = threadIdx.x; k < L.nx * (L.ny + 1); k += CT) scy[l][k] = ws_f[L.cy + k];
     for (int k = threadIdx.x; k < n; k += CT) {
-      sdg[l][k] = ws_f[L.dg + k];
+      sidg[l][k] = ws_f[L.idg + k];
       sx[l][k] = 0.0f;
       if (l == P.small0) sf[l][k] = ws_f[L.f + k];
     }
@@ -855,12 +886,12 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     const Level& L = P.L[l];
     const float idx2 = 1.0f / (L.dx * L.dx);
     if (l == P.nlev - 1) {
-      cta_coarsest(sx[l], sf[l], scx[l], scy[l], sdg[l], inv, L.nx, L.ny, idx2, coarse_sweeps);
+      cta_coarsest(sx[l], sf[l], scx[l], scy[l], sidg[l], inv, L.nx, L.ny, idx2, coarse_sweeps);
       break;
     }
     for (int s = 0; s < nu; ++s) {
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 0);
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 1);
     }
     for (int k = threadIdx.x; k < L.nx * L.ny; k += CT) {
       const int i = k / L.ny, j = k - i * L.ny;
@@ -891,8 +922,8 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     }
     __syncthreads();
     for (int s = 0; s < nu; ++s) {
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 1);
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sdg[l], L.nx, L.ny, idx2, 0);
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 1);
+      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 0);
     }
   }
   const Level& L0 = P.L[P.small0];
@@ -1059,7 +1090,7 @@ static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, 
   // the coarse level's result it prolongs from
   const dim3 grid((L.ny + TT - 1) / TT, (L.nx + TT - 1) / TT);
   const size_t sm = fused_smem(down ? 2 * nu + 2 : 2 * nu, TT);
-  const float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.dg;
+  const float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.idg;
   float* a4 = fw + L.x;
   float* a5 = fw + L.xo;
 #define ZB_FUSED(K) e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2)
@@ -1144,9 +1175,9 @@ static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, 
     for (int s = 0; s < 2 * P.coarse_sweeps; ++s) {
       const int c0 = s < P.coarse_sweeps ? 0 : 1;
       rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                      fw + L.dg, L.nx, L.ny, idx2, c0);
+                                                      fw + L.idg, L.nx, L.ny, idx2, c0);
       rbgs_kernel<<<grid_for(n / 2 + 1), NT, 0, st>>>(fw + L.x, fw + L.f, fw + L.cx, fw + L.cy,
-                                                      fw + L.dg, L.nx, L.ny, idx2, 1 - c0);
+                                                      fw + L.idg, L.nx, L.ny, idx2, 1 - c0);
     }
   }
   // fine levels on the way up: coarse correction + post-smoothing, fused
@@ -1238,7 +1269,7 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
                                                    fw + L.cy);
     }
     diag_kernel32<<<grid_for((long long)L.nx * L.ny), NT, 0, st>>>(
-        fw + L.cx, fw + L.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.dg);
+        fw + L.cx, fw + L.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.idg);
   }
   if (P.cinv >= 0) coarse_inverse_kernel<<<1, 256, 0, st>>>(P, fw);
   ZB_CUDA_TRY(cudaMemsetAsync(dw + P.scal, 0, S_COUNT * sizeof(double), st));
