@@ -42,9 +42,12 @@ class PoissonSolver:
     V-cycle preconditioner; ``precond`` is ``'none'`` (plain CG), ``'mg'``,
     ``'learned'`` (the V-cycle followed by one learned smoothing step on the
     finest level) or ``'learned_replace'`` (the U-Net in place of the finest
-    level's red-black sweeps)."""
+    level's red-black sweeps).  ``coarsest``: coarsening stops at this side;
+    the default 8 ends a power-of-two hierarchy on an 8 x 8 level solved with
+    its dense inverse (1024^2 solve 1.591 -> 1.571 ms against a 4 x 4 end,
+    the same 8 iterations)."""
 
-    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
+    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
                  device=None):
         import torch
         L.require_cuda()
@@ -224,7 +227,7 @@ class ChorinSolver(HyperbolicSolver):
     ``use_graph`` (False: drive the FCG iterations from the host)."""
 
     def __init__(self, pressure_tol=1e-8, pressure_maxit=200, time_order=1, precond="mg",
-                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
+                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
                  use_graph=True, **kw):
         super().__init__(**kw)
         if time_order not in (1, 2):
