@@ -42,12 +42,13 @@ class PoissonSolver:
     V-cycle preconditioner; ``precond`` is ``'none'`` (plain CG), ``'mg'``,
     ``'learned'`` (the V-cycle followed by one learned smoothing step on the
     finest level) or ``'learned_replace'`` (the U-Net in place of the finest
-    level's red-black sweeps).  ``coarsest``: coarsening stops at this side;
-    the default 8 ends a power-of-two hierarchy on an 8 x 8 level solved with
-    its dense inverse (1024^2 solve 1.591 -> 1.571 ms against a 4 x 4 end,
-    the same 8 iterations)."""
+    level's red-black sweeps).  ``coarsest``: coarsening stops at this side
+    (a coarsest level of at most 64 cells is solved with its dense inverse,
+    built at set-up).  An 8 x 8 end instead of the default 4 x 4 one saves
+    20 us per 1024^2 solve but its 64 x 64 inverse costs about 150 us of
+    set-up, which a Chorin step pays every step (its coefficients follow h)."""
 
-    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
+    def __init__(self, nx, ny, dx, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
                  device=None):
         import torch
         L.require_cuda()
@@ -227,7 +228,7 @@ class ChorinSolver(HyperbolicSolver):
     ``use_graph`` (False: drive the FCG iterations from the host)."""
 
     def __init__(self, pressure_tol=1e-8, pressure_maxit=200, time_order=1, precond="mg",
-                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=8,
+                 smoother=None, cmin=0.1, cmax=2.0, nu=2, coarse_sweeps=8, coarsest=4,
                  use_graph=True, **kw):
         super().__init__(**kw)
         if time_order not in (1, 2):
