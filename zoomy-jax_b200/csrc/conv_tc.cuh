@@ -22,6 +22,7 @@
 // word, skips the tile's stores, and still releases its TMEM columns.
 #pragma once
 
+#include <cuda.h>   // CUtensorMap (the type only; the encoder is fetched at run time)
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -308,9 +309,32 @@ constexpr int CHP = CHX * CHY;               // 324 halo pixels
 // with 256 everywhere, 0.440 with 256 for the layers of six or more input
 // chunks only (what the launcher takes); (8, 16) 0.249 / 0.255 / 0.247.
 constexpr int CB_WIDE_CHUNKS = 6;
+// one staged chunk: the 18 x 18 halo pixels x 16 bytes, its stride rounded up
+// to 128 bytes (the alignment of a tensor-copy destination)
+constexpr int CB_CHUNK_BYTES = CHP * 16;                            // 5184
+constexpr int CB_CHUNK_STRIDE = ((CB_CHUNK_BYTES + 127) / 128) * 128;  // 5248
 
+// staged chunks, weights, two mbarriers and the TMEM slot
 __host__ __device__ inline size_t cb8_smem_bytes(int cinp, int coutp) {
-  return (size_t)cinp * CHP * 2 + (size_t)9 * cinp * coutp * 2 + 64;
+  return (size_t)(cinp / 8) * CB_CHUNK_STRIDE + (size_t)9 * cinp * coutp * 2 + 64;
+}
+
+// TMA: a 4-D tiled tensor copy of one chunk's halo box into shared memory,
+// completing on an mbarrier (no multicast)
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1,
+                                            int c2, int c3, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5}], [%6];"
+      :
+      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+        "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
+               : "memory");
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
@@ -331,20 +355,37 @@ enum { CB_OUT_CHUNKED = 0, CB_OUT_F32 = 1 };
 // in its summation order).  CB_OUT_F32: out is float32 planes [co][b][y][x].
 // H and W even.  act != 0: tanh on the SFU (the inference activation, act 2
 // of conv3x3_tc).
+// Staging: the chunks read as stored (A in SRC_DIRECT mode when tma_a, B when
+// tma_b) arrive by TMA, one 4-D box (8 channels x 18 x 18 pixels x 1 image
+// chunk) per chunk on the maps tm_a / tm_b (out-of-image pixels are filled
+// with zeros by the copy), issued by one thread and completed on an mbarrier;
+// the upsampled chunks of SRC_UP keep 16-byte cp.async copies (their address
+// map is not a box); the padding chunks are zeroed once.  Staged chunk ch sits
+// at ch * CB_CHUNK_STRIDE from the start of dynamic shared memory; a CTA whose
+// dynamic shared memory does not start on 128 bytes (the alignment a tensor
+// copy's destination needs) stages everything by cp.async instead.  (Aligning
+// the area at run time, 128 bytes more per CTA, measured 5-8 % slower.)
 template <int NTH>
 __global__ void __launch_bounds__(NTH)
 conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __restrict__ inB,
             int chB, int cin, const __nv_bfloat16* __restrict__ w, const float* __restrict__ bias,
             void* __restrict__ out, uint4* __restrict__ pool, int cout, int out_form, int B,
-            int H, int W, int act, int tmem_cols, unsigned* err) {
-  extern __shared__ __align__(128) unsigned char tc_sm[];
+            int H, int W, int act, int tmem_cols, unsigned* err,
+            const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+            int tma_a_req, int tma_b_req) {
+  extern __shared__ __align__(1024) unsigned char tc_sm[];
   const int cinp = pad16(cin), coutp = pad16(cout);
   const int nch = cinp / 8;
-  unsigned char* sA = tc_sm;
-  unsigned char* sB = tc_sm + (size_t)cinp * CHP * 2;
+  unsigned char* sA = tc_sm;   // staged chunks
+  unsigned char* sB = sA + (size_t)nch * CB_CHUNK_STRIDE;
+  const bool tma_aligned = (smem_u32(tc_sm) & 127u) == 0u;
+  const int tma_a = tma_a_req && tma_aligned, tma_b = tma_b_req && tma_aligned;
   unsigned long long* mbar = (unsigned long long*)(sB + (size_t)9 * cinp * coutp * 2);
-  uint32_t* tmem_slot = (uint32_t*)(mbar + 1);
+  uint32_t* tmem_slot = (uint32_t*)(mbar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the padding chunks past A and B read as zeros; nothing writes them again
+  for (int e = tid; e < (nch - chA - chB) * (CB_CHUNK_STRIDE / 16); e += NTH)
+    ((uint4*)(sA + (size_t)(chA + chB) * CB_CHUNK_STRIDE))[e] = make_uint4(0u, 0u, 0u, 0u);
 
   // weights: [tap][chunk][n][8] bf16, zero outside (cout, cin)
   for (int e = tid; e < 9 * nch * coutp; e += NTH) {
@@ -368,6 +409,7 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -375,23 +417,39 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t mbar_a = smem_u32(mbar);
+  const uint32_t mbar_t = smem_u32(mbar + 1);   // the TMA copies of a region
   const uint32_t sA_a = smem_u32(sA), sB_a = smem_u32(sB);
   const uint32_t idesc = tc_idesc(coutp);
   const size_t npix = (size_t)B * H * W;
   const int H2 = H >> 1, W2 = W >> 1;
-  const size_t npix2 = (size_t)B * H2 * W2;
   const int rx = (W + CBX - 1) / CBX, ry = (H + CBY - 1) / CBY;
   const int nreg = rx * ry * B;
-  uint32_t parity = 0;
+  const int ntma = (tma_a ? chA : 0) + (tma_b ? chB : 0);
+  uint32_t parity = 0, tparity = 0;
   bool failed = false;
-  for (int t = blockIdx.x; t < nreg; t += gridDim.x) {
+  // issue the staging of region t: the box-shaped chunks by TMA (the box
+  // starts one pixel up and left of the region; the innermost coordinate, the
+  // channel, is always 0), the rest by 16-byte cp.async copies (zero outside
+  // the image), as one cp.async group
+  auto issue_stage = [&](int t) {
     const int b = t / (rx * ry);
     const int rr = t - b * rx * ry;
     const int x0 = (rr % rx) * CBX, y0 = (rr / rx) * CBY;
-    const size_t img = (size_t)b * H * W;
-    // halo region: one 16-byte copy per (chunk, halo pixel); zero outside the
-    // image and for the padding chunks
-    for (int e = tid; e < nch * CHP; e += NTH) {
+    if (tid == 0 && ntma > 0) {
+      mbar_expect_tx(mbar_t, (uint32_t)ntma * CB_CHUNK_BYTES);
+      if (tma_a)
+        for (int ch = 0; ch < chA; ++ch)
+          tma_load_4d(sA_a + (uint32_t)ch * CB_CHUNK_STRIDE, &tm_a, 0, x0 - 1, y0 - 1,
+                      ch * B + b, mbar_t);
+      if (tma_b)
+        for (int ch = 0; ch < chB; ++ch)
+          tma_load_4d(sA_a + (uint32_t)(chA + ch) * CB_CHUNK_STRIDE, &tm_b, 0, x0 - 1, y0 - 1,
+                      ch * B + b, mbar_t);
+    }
+    // the rest: one 16-byte cp.async copy per (chunk, halo pixel), zero
+    // outside the image
+    const int cp_lo = tma_a ? chA : 0, cp_hi = chA + (tma_b ? 0 : chB);
+    for (int e = cp_lo * CHP + tid; e < cp_hi * CHP; e += NTH) {
       const int ch = e / CHP, q = e - ch * CHP;
       const int yy = y0 - 1 + q / CHX, xx = x0 - 1 + q % CHX;
       const bool inside = yy >= 0 && yy < H && xx >= 0 && xx < W;
@@ -406,11 +464,38 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
         src = inB + ((size_t)(ch - chA) * B + b) * H * W + (size_t)yy * W + xx;
         bytes = 16;
       }
-      cp_async16(sA_a + (uint32_t)(ch * CHP + q) * 16, src, bytes);
+      cp_async16(sA_a + (uint32_t)ch * CB_CHUNK_STRIDE + (uint32_t)q * 16, src, bytes);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // with TMA copies the next region's staging is issued as soon as this
+  // region's MMAs have read the chunks, so it lands during the epilogue;
+  // layers staged by cp.async alone (a fallback) stage at the top of each
+  // region.  Measured, one 1024^2 application against the cp.async staging
+  // at the top of each region: (24, 48) 0.443 -> 0.423 ms, (8, 16) 0.248 ->
+  // 0.244 ms.
+  const bool early = ntma > 0;
+  if (early && (int)blockIdx.x < nreg) issue_stage(blockIdx.x);
+  for (int t = blockIdx.x; t < nreg; t += gridDim.x) {
+    const int b = t / (rx * ry);
+    const int rr = t - b * rx * ry;
+    const int x0 = (rr % rx) * CBX, y0 = (rr / rx) * CBY;
+    const size_t img = (size_t)b * H * W;
+    if (!early) issue_stage(t);
+    // region t's copies
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // make the copies visible to the tensor core's async proxy
+    if (ntma > 0) {
+      bool landed = false;
+      for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it)
+        if (mbar_try_wait(mbar_t, tparity)) { landed = true; break; }
+      tparity ^= 1u;
+      if (__syncthreads_or(landed ? 0 : 1)) {
+        failed = true;
+        if (err && tid == 0) atomicExch(err, 1u);
+        break;
+      }
+    }
+    // make the cp.async copies visible to the tensor core's async proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -423,10 +508,10 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
         for (int tap = 0; tap < 9; ++tap) {
           const int dy = tap / 3, dx = tap % 3;
           for (int g = 0; g < cinp / 16; ++g) {
-            const uint32_t a = sA_a + (uint32_t)(2 * g) * (CHP * 16) +
+            const uint32_t a = sA_a + (uint32_t)(2 * g) * CB_CHUNK_STRIDE +
                                (uint32_t)(dy * CHX + dx + 8 * i) * 16;
             const uint32_t bb = sB_a + (uint32_t)((tap * nch + 2 * g) * coutp) * 16;
-            tc_mma(tmem + (uint32_t)(i * coutp), tc_desc(a, CHP * 16, CHX * 16),
+            tc_mma(tmem + (uint32_t)(i * coutp), tc_desc(a, CB_CHUNK_STRIDE, CHX * 16),
                    tc_desc(bb, coutp * 16, 128), idesc, acc);
             acc = 1;
           }
@@ -445,6 +530,9 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
       break;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // the MMAs have read the staged chunks: the next region's copies land
+    // while this region's epilogue runs
+    if (early && t + (int)gridDim.x < nreg) issue_stage(t + gridDim.x);
     // epilogue: warp w owns accumulator rows 32 (w % 4) .. 32 (w % 4) + 31 of
     // M tile w / 4 (NTH = 256), or of both tiles (NTH = 128)
     const int m = (warp & 3) * 32 + lane;
@@ -503,7 +591,14 @@ conv3x3_cb8(const uint4* __restrict__ inA, int chA, int mode_a, const uint4* __r
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (failed) {
+    // give copies and MMAs still in flight a bounded chance to land before
+    // the shared memory and the TMEM columns are released (a phase that
+    // already completed returns at once)
+    if (ntma > 0)
+      for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it)
+        if (mbar_try_wait(mbar_t, tparity ^ 1u)) break;
     for (unsigned it = 0; it < TC_SPIN_LIMIT; ++it)
       if (mbar_try_wait(mbar_a, parity ^ 1u)) break;
   }

@@ -25,6 +25,7 @@
 // shared memory, one thread per output pixel with all output channels in
 // registers.  Zero padding at image borders.
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <cstring>
 #include <algorithm>
@@ -542,6 +543,39 @@ static int conv_tc_launch(const float* inA, int cin_a, const float* inB, int cin
   return zb_launch_check();
 }
 
+// cuTensorMapEncodeTiled from the driver, fetched once through the runtime
+// (no link against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static std::atomic<void*> fn{nullptr};
+  void* f = fn.load();
+  if (!f) {
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
+                                         &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f)
+      return nullptr;
+    fn.store(f);
+  }
+  return (PFN_cuTensorMapEncodeTiled_v12000)f;
+}
+
+// The halo-box map of a chunked activation: dimensions (8 channels, W, H,
+// chunks x B) with byte strides (16, 16 W, 16 H W), box (8, 18, 18, 1); pixels
+// outside the image read as zeros.  The base is 16-byte aligned and every
+// stride a multiple of 16, as the encoder requires.
+static bool cb8_map(CUtensorMap* m, const uint4* base, int nchunks, int B, int H, int W) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc || !base || ((uintptr_t)base & 15u)) return false;
+  const cuuint64_t dims[4] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)nchunks * B};
+  const cuuint64_t strides[3] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16};
+  const cuuint32_t box[4] = {8, (cuuint32_t)CHX, (cuuint32_t)CHY, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)base, dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 // conv3x3_cb8 over B images H x W (see conv_tc.cuh); resident CTAs are capped
 // so that their TMEM columns (two M tiles of coutp each) fit in 512
 static int conv_cb8_launch(const uint4* inA, int chA, int mode_a, const uint4* inB, int chB,
@@ -582,14 +616,21 @@ static int conv_cb8_launch(const uint4* inA, int chA, int mode_a, const uint4* i
   const long long nreg = (long long)((W + CBX - 1) / CBX) * ((H + CBY - 1) / CBY) * B;
   const int grid = (int)std::max<long long>(
       1, std::min<long long>(nreg, (long long)sms[dev] * std::max(1, fit)));
+  // tensor maps of the sources read as stored (the upsampled source, and one
+  // whose map cannot be encoded, stay on the cp.async copies)
+  CUtensorMap tm_a, tm_b;
+  std::memset(&tm_a, 0, sizeof(tm_a));
+  std::memset(&tm_b, 0, sizeof(tm_b));
+  const int tma_a = (mode_a == SRC_DIRECT && chA > 0 && cb8_map(&tm_a, inA, chA, B, H, W)) ? 1 : 0;
+  const int tma_b = (chB > 0 && cb8_map(&tm_b, inB, chB, B, H, W)) ? 1 : 0;
   if (nth == 256)
     conv3x3_cb8<256><<<grid, 256, smem, st>>>(inA, chA, mode_a, inB, chB, cin, w, bias, out,
                                               pool, cout, out_form, B, H, W, act, cols,
-                                              unet_err_word());
+                                              unet_err_word(), tm_a, tm_b, tma_a, tma_b);
   else
     conv3x3_cb8<128><<<grid, 128, smem, st>>>(inA, chA, mode_a, inB, chB, cin, w, bias, out,
                                               pool, cout, out_form, B, H, W, act, cols,
-                                              unet_err_word());
+                                              unet_err_word(), tm_a, tm_b, tma_a, tma_b);
   return zb_launch_check();
 }
 
