@@ -106,18 +106,21 @@ static Plan make_plan(const zb_poisson_cfg* c) {
   long long f = 0;
   int l = 0;
   P.small0 = -1;
+  // every float array starts on 16 bytes (the fused kernels stage rows with
+  // 16-byte copies)
+  auto al4 = [](long long v) { return (v + 3) & ~3LL; };
   while (l < MAXL) {
     Level& L = P.L[l];
     L.nx = nx;
     L.ny = ny;
     L.dx = dx;
-    L.cx = f; f += (long long)(nx + 1) * ny;
-    L.cy = f; f += (long long)nx * (ny + 1);
-    L.idg = f; f += (long long)nx * ny;
-    L.x = f; f += (long long)nx * ny;
-    L.f = f; f += (long long)nx * ny;
-    L.r = f; f += (long long)nx * ny;
-    L.xo = f; f += (long long)nx * ny;
+    L.cx = f; f = al4(f + (long long)(nx + 1) * ny);
+    L.cy = f; f = al4(f + (long long)nx * (ny + 1));
+    L.idg = f; f = al4(f + (long long)nx * ny);
+    L.x = f; f = al4(f + (long long)nx * ny);
+    L.f = f; f = al4(f + (long long)nx * ny);
+    L.r = f; f = al4(f + (long long)nx * ny);
+    L.xo = f; f = al4(f + (long long)nx * ny);
     if (P.small0 < 0 && nx <= SMALL && ny <= SMALL) P.small0 = l;
     ++l;
     if (nx <= c->coarsest || ny <= c->coarsest || (nx & 1) || (ny & 1)) break;
@@ -577,9 +580,18 @@ constexpr int FT = 32;            // tile side of the levels with a tile for eve
 constexpr int FTS = 16;           // tile side of the smaller levels
 constexpr int FNT_MAX = 1024;
 
+// Staged layout of a tile with its ring: R = tile + 2 halo rows; the arrays
+// x, f, r, idg (R rows) and cx (R + 1 rows) keep PAD leading columns so that
+// every staged row starts on a 16-byte boundary of the level's row (its first
+// column j0 - halo - PAD is a multiple of 4) and a row stride RS, a multiple
+// of 4 floats; cy (R rows of R + 1) stays unpadded.
+__host__ __device__ constexpr int stage_pad(int halo) { return (4 - halo % 4) % 4; }
+__host__ __device__ constexpr int stage_rs(int halo, int tile) {
+  return ((tile + 2 * halo + stage_pad(halo) + 3) / 4) * 4;
+}
 __host__ __device__ inline size_t fused_smem(int halo, int tile) {
-  const int R = tile + 2 * halo;
-  return (size_t)(4 * R * R + 2 * (R + 1) * R) * sizeof(float);
+  const int R = tile + 2 * halo, RS = stage_rs(halo, tile);
+  return (size_t)(4 * R * RS + (R + 1) * RS + R * (R + 1)) * sizeof(float);
 }
 
 // 4-byte asynchronous global -> shared copy; src_bytes 0 writes a zero
@@ -587,6 +599,13 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src),
                "r"(valid ? 4 : 0)
+               : "memory");
+}
+// 16-byte version (four floats of a row; both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16f(float* dst, const float* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 16 : 0)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
@@ -600,6 +619,10 @@ __device__ __forceinline__ void cp_async_wait_all() {
 template <int HALO, int TT>
 struct Stage {
   static constexpr int R = TT + 2 * HALO;
+  static constexpr int PAD = stage_pad(HALO);
+  static constexpr int RS = stage_rs(HALO, TT);
+  // staged element (a, b) of x, f, r, idg (a in [0, R)) or cx (a in [0, R])
+  __device__ static constexpr int at(int a, int b) { return a * RS + b + PAD; }
   int i0, j0, nx, ny;
   bool interior;
   float *x, *f, *r, *idg, *cx, *cy;
@@ -609,11 +632,11 @@ struct Stage {
   }
   template <bool EDGE>
   __device__ float ax(int a, int b, float idx2) const {
-    const float xc = x[a * R + b];
-    const float ea = cx[(a + 1) * R + b], wa = cx[a * R + b];
+    const float xc = x[at(a, b)];
+    const float ea = cx[at(a + 1, b)], wa = cx[at(a, b)];
     const float nb = cy[a * (R + 1) + b + 1], sb = cy[a * (R + 1) + b];
-    float xe = x[(a + 1) * R + b], xw = x[(a - 1) * R + b];
-    float xn = x[a * R + b + 1], xs = x[a * R + b - 1];
+    float xe = x[at(a + 1, b)], xw = x[at(a - 1, b)];
+    float xn = x[at(a, b + 1)], xs = x[at(a, b - 1)];
     if (EDGE) {
       const int gi = i0 - HALO + a, gj = j0 - HALO + b;
       if (gi + 1 >= nx) xe = -xc;
@@ -627,10 +650,10 @@ struct Stage {
   // the diagonal)
   template <bool EDGE>
   __device__ float nbsum(int a, int b) const {
-    const float ea = cx[(a + 1) * R + b], wa = cx[a * R + b];
+    const float ea = cx[at(a + 1, b)], wa = cx[at(a, b)];
     const float nb = cy[a * (R + 1) + b + 1], sb = cy[a * (R + 1) + b];
-    float xe = x[(a + 1) * R + b], xw = x[(a - 1) * R + b];
-    float xn = x[a * R + b + 1], xs = x[a * R + b - 1];
+    float xe = x[at(a + 1, b)], xw = x[at(a - 1, b)];
+    float xn = x[at(a, b + 1)], xs = x[at(a, b - 1)];
     if (EDGE) {
       const int gi = i0 - HALO + a, gj = j0 - HALO + b;
       if (gi + 1 >= nx) xe = 0.0f;
@@ -650,7 +673,7 @@ struct Stage {
       int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
       for (; b < R - m; b += 2 * (int)blockDim.x) {
         if (EDGE && !inside(a, b)) continue;
-        x[a * R + b] = (f[a * R + b] + nbsum<EDGE>(a, b) * idx2) * idg[a * R + b];
+        x[at(a, b)] = (f[at(a, b)] + nbsum<EDGE>(a, b) * idx2) * idg[at(a, b)];
       }
     }
     __syncthreads();
@@ -663,7 +686,7 @@ struct Stage {
       int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
       for (; b < R - m; b += 2 * (int)blockDim.x) {
         if (!interior && !inside(a, b)) continue;
-        x[a * R + b] = f[a * R + b] * idg[a * R + b];
+        x[at(a, b)] = f[at(a, b)] * idg[at(a, b)];
       }
     }
     __syncthreads();
@@ -675,8 +698,8 @@ struct Stage {
     else sweep_impl<true>(color, m, idx2);
   }
   __device__ float residual(int a, int b, float idx2) const {
-    if (interior) return f[a * R + b] - ax<false>(a, b, idx2);
-    return inside(a, b) ? f[a * R + b] - ax<true>(a, b, idx2) : 0.0f;
+    if (interior) return f[at(a, b)] - ax<false>(a, b, idx2);
+    return inside(a, b) ? f[at(a, b)] - ax<true>(a, b, idx2) : 0.0f;
   }
 };
 
@@ -684,39 +707,61 @@ template <int HALO, int TT>
 __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny,
                                        const float* __restrict__ f, const float* __restrict__ cx,
                                        const float* __restrict__ cy, const float* __restrict__ idg,
-                                       const float* __restrict__ x) {
-  constexpr int R = Stage<HALO, TT>::R;
-  Stage<HALO, TT> S;
+                                       const float* __restrict__ x, int vec) {
+  using St = Stage<HALO, TT>;
+  constexpr int R = St::R, RS = St::RS, PAD = St::PAD;
+  St S;
   S.i0 = i0; S.j0 = j0; S.nx = nx; S.ny = ny;
   S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
-  S.x = sm; S.f = sm + R * R; S.r = sm + 2 * R * R; S.idg = sm + 3 * R * R;
-  S.cx = sm + 4 * R * R; S.cy = S.cx + (R + 1) * R;
+  S.x = sm; S.f = sm + R * RS; S.r = sm + 2 * R * RS; S.idg = sm + 3 * R * RS;
+  S.cx = sm + 4 * R * RS; S.cy = S.cx + (R + 1) * RS;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   // every copy is issued before any is waited for
-  for (int e = tid; e < R * R; e += nt) {
-    const int a = e / R, b = e - (e / R) * R;
-    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
-    const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
-    const long long k = in ? (long long)gi * ny + gj : 0;
-    cp_async4(S.f + e, f + k, in);
-    cp_async4(S.idg + e, idg + k, in);
-    if (x) cp_async4(S.x + e, x + k, in);
-    else S.x[e] = 0.0f;
-  }
-  for (int e = tid; e < (R + 1) * R; e += nt) {
-    {
+  if (vec) {
+    // rows as 16-byte chunks from column gs = j0 - HALO - PAD (a multiple of
+    // 4, like ny): a chunk lies wholly inside the level or wholly outside it
+    constexpr int NC = RS / 4;
+    const int gs = j0 - HALO - PAD;
+    for (int e = tid; e < R * NC; e += nt) {
+      const int a = e / NC, c = e - a * NC;
+      const int gi = i0 - HALO + a, gc = gs + 4 * c;
+      const bool in = gi >= 0 && gi < nx && gc >= 0 && gc < ny;
+      const long long k = in ? (long long)gi * ny + gc : 0;
+      cp_async16f(S.f + a * RS + 4 * c, f + k, in);
+      cp_async16f(S.idg + a * RS + 4 * c, idg + k, in);
+      if (x) cp_async16f(S.x + a * RS + 4 * c, x + k, in);
+      else *(float4*)(S.x + a * RS + 4 * c) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int e = tid; e < (R + 1) * NC; e += nt) {
+      const int a = e / NC, c = e - a * NC;
+      const int gi = i0 - HALO + a, gc = gs + 4 * c;
+      const bool in = gi >= 0 && gi <= nx && gc >= 0 && gc < ny;
+      cp_async16f(S.cx + a * RS + 4 * c, cx + (in ? (long long)gi * ny + gc : 0), in);
+    }
+  } else {
+    for (int e = tid; e < R * R; e += nt) {
+      const int a = e / R, b = e - (e / R) * R;
+      const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+      const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+      const long long k = in ? (long long)gi * ny + gj : 0;
+      cp_async4(S.f + St::at(a, b), f + k, in);
+      cp_async4(S.idg + St::at(a, b), idg + k, in);
+      if (x) cp_async4(S.x + St::at(a, b), x + k, in);
+      else S.x[St::at(a, b)] = 0.0f;
+    }
+    for (int e = tid; e < (R + 1) * R; e += nt) {
       const int a = e / R, b = e - (e / R) * R;
       const int gi = i0 - HALO + a, gj = j0 - HALO + b;
       const bool in = gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
-      cp_async4(S.cx + e, cx + (in ? (long long)gi * ny + gj : 0), in);
+      cp_async4(S.cx + St::at(a, b), cx + (in ? (long long)gi * ny + gj : 0), in);
     }
-    {
-      const int a = e / (R + 1), b = e - (e / (R + 1)) * (R + 1);
-      const int gi = i0 - HALO + a, gj = j0 - HALO + b;
-      const bool in = gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
-      cp_async4(S.cy + e, cy + (in ? (long long)gi * (ny + 1) + gj : 0), in);
-    }
+  }
+  for (int e = tid; e < R * (R + 1); e += nt) {
+    const int a = e / (R + 1), b = e - (e / (R + 1)) * (R + 1);
+    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
+    const bool in = gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
+    cp_async4(S.cy + e, cy + (in ? (long long)gi * (ny + 1) + gj : 0), in);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -730,7 +775,7 @@ template <int NU, int TT>
 __global__ void __launch_bounds__(FNT_MAX)
 mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
                const float* __restrict__ cy, const float* __restrict__ idg, float* __restrict__ x,
-               float* __restrict__ fc, int nx, int ny, float idx2) {
+               float* __restrict__ fc, int nx, int ny, float idx2, int vec) {
   pdl_enter();
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU + 2;
@@ -738,7 +783,7 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, nullptr);
+  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, nullptr, vec);
   if (NU > 0) S.sweep_from_zero(0, 1);
   for (int s = 1; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
   // residual where the sweeps are final and one ring beyond the tile
@@ -746,20 +791,20 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
     constexpr int m = 2 * NU + 1;
     for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y)
       for (int b = m + (int)threadIdx.x; b < R - m; b += (int)blockDim.x)
-        S.r[a * R + b] = S.residual(a, b, idx2);
+        S.r[S.at(a, b)] = S.residual(a, b, idx2);
   }
   __syncthreads();
   for (int e = tid; e < TT * TT; e += nt) {
     const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
-    if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
+    if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[S.at(HALO + ti, HALO + tj)];
   }
   const int nxc = nx / 2, nyc = ny / 2;
   for (int e = tid; e < (TT / 2) * (TT / 2); e += nt) {
     const int I = i0 / 2 + e / (TT / 2), J = j0 / 2 + e % (TT / 2);
     if (I >= nxc || J >= nyc) continue;
     fc[(long long)I * nyc + J] = restrict_at(
-        [&](int fi, int fj) { return S.r[(fi - i0 + HALO) * R + (fj - j0 + HALO)]; }, I, J, nxc,
+        [&](int fi, int fj) { return S.r[S.at(fi - i0 + HALO, fj - j0 + HALO)]; }, I, J, nxc,
         nyc);
   }
 }
@@ -774,7 +819,7 @@ __global__ void __launch_bounds__(FNT_MAX)
 mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
              const float* __restrict__ cy, const float* __restrict__ idg,
              const float* __restrict__ x, const float* __restrict__ ec, float* __restrict__ xo,
-             int nx, int ny, float idx2) {
+             int nx, int ny, float idx2, int vec) {
   pdl_enter();
   extern __shared__ float fsm[];
   constexpr int HALO = 2 * NU;
@@ -782,13 +827,13 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x);
+  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x, vec);
   const int nxc = nx / 2, nyc = ny / 2;
   for (int a = (int)threadIdx.y; a < R; a += (int)blockDim.y)
     for (int b = (int)threadIdx.x; b < R; b += (int)blockDim.x) {
       if (!S.inside(a, b)) continue;
       const int fi = i0 - HALO + a, fj = j0 - HALO + b;
-      S.x[a * R + b] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
+      S.x[S.at(a, b)] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
                                    fj, nxc, nyc);
     }
   __syncthreads();
@@ -796,7 +841,7 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   for (int e = tid; e < TT * TT; e += nt) {
     const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
-    if (gi < nx && gj < ny) xo[(long long)gi * ny + gj] = S.x[(HALO + ti) * R + HALO + tj];
+    if (gi < nx && gj < ny) xo[(long long)gi * ny + gj] = S.x[S.at(HALO + ti, HALO + tj)];
   }
 }
 
@@ -1093,10 +1138,16 @@ static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, 
   const float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.idg;
   float* a4 = fw + L.x;
   float* a5 = fw + L.xo;
-#define ZB_FUSED(K) e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2)
+  // rows staged as 16-byte chunks when every staged array is 16-byte aligned
+  // and the level's rows are a multiple of 4 floats (the plan aligns the
+  // arrays; odd-sized coarse levels take the 4-byte copies)
+  auto al16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0u; };
+  const int vec = (L.ny % 4 == 0 && al16(a0) && al16(a1) && al16(a3) && al16(a4)) ? 1 : 0;
+#define ZB_FUSED(K) \
+  e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, a4, to, L.nx, L.ny, idx2, vec)
 #define ZB_FUSED_UP(K) \
   e = pdl_launch(K, grid, blk, sm, st, a0, a1, a2, a3, (const float*)a4, (const float*)to, a5, \
-                 L.nx, L.ny, idx2)
+                 L.nx, L.ny, idx2, vec)
   cudaError_t e = cudaSuccess;
   if (down) {
     switch (nu) {
