@@ -680,22 +680,53 @@ struct Stage {
   }
   // the first half-sweep of a V-cycle's way down starts from x = 0, where
   // A x = 0 exactly: the update is x = f / d
-  __device__ void sweep_from_zero(int color, int m) const {
-    for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y) {
+  // (the cells enumerated as in sweep_flat, margin 1)
+  __device__ void sweep_from_zero(int color) const {
+    constexpr int M = 1, NR = R - 2 * M, HALF = NR / 2;
+    const int nt = (int)(blockDim.x * blockDim.y);
+    for (int e = (int)(threadIdx.y * blockDim.x + threadIdx.x); e < NR * HALF; e += nt) {
+      const int a = M + e / HALF, k = e - (e / HALF) * HALF;
       const int gi = i0 - HALO + a;
-      int b = m + (((color - gi - (j0 - HALO) - m) % 2 + 2) % 2) + 2 * (int)threadIdx.x;
-      for (; b < R - m; b += 2 * (int)blockDim.x) {
-        if (!interior && !inside(a, b)) continue;
-        x[at(a, b)] = f[at(a, b)] * idg[at(a, b)];
-      }
+      const int b = M + (((color - gi - (j0 - HALO) - M) % 2 + 2) % 2) + 2 * k;
+      if (!interior && !inside(a, b)) continue;
+      x[at(a, b)] = f[at(a, b)] * idg[at(a, b)];
     }
     __syncthreads();
   }
+  // The same half-sweep with the cells of `color` at least M cells inside
+  // the staged region enumerated as one list over all the threads (NR / 2 of
+  // them in each of the NR rows), so that no lane idles at the ends of the
+  // rows (a row of 44 cells has 22 of a colour for 32 lanes)
+  template <bool EDGE, int M>
+  __device__ void sweep_flat(int color, float idx2) const {
+    constexpr int NR = R - 2 * M, HALF = NR / 2;
+    const int nt = (int)(blockDim.x * blockDim.y);
+    for (int e = (int)(threadIdx.y * blockDim.x + threadIdx.x); e < NR * HALF; e += nt) {
+      const int a = M + e / HALF, k = e - (e / HALF) * HALF;
+      const int gi = i0 - HALO + a;
+      const int b = M + (((color - gi - (j0 - HALO) - M) % 2 + 2) % 2) + 2 * k;
+      if (EDGE && !inside(a, b)) continue;
+      x[at(a, b)] = (f[at(a, b)] + nbsum<EDGE>(a, b) * idx2) * idg[at(a, b)];
+    }
+    __syncthreads();
+  }
+  template <bool EDGE>
+  __device__ void sweep_m(int color, int m, float idx2) const {
+    switch (m) {
+#define ZB_SWEEP_M(M) \
+  case M: if constexpr (R - 2 * M >= 2) { sweep_flat<EDGE, M>(color, idx2); return; } break;
+      ZB_SWEEP_M(1) ZB_SWEEP_M(2) ZB_SWEEP_M(3) ZB_SWEEP_M(4) ZB_SWEEP_M(5)
+      ZB_SWEEP_M(6) ZB_SWEEP_M(7) ZB_SWEEP_M(8) ZB_SWEEP_M(9)
+#undef ZB_SWEEP_M
+      default: break;
+    }
+    sweep_impl<EDGE>(color, m, idx2);
+  }
   // one half-sweep over the cells of `color` at least m cells inside the
-  // staged region; rows over threadIdx.y, same-colour columns over threadIdx.x
+  // staged region
   __device__ void sweep(int color, int m, float idx2) const {
-    if (interior) sweep_impl<false>(color, m, idx2);
-    else sweep_impl<true>(color, m, idx2);
+    if (interior) sweep_m<false>(color, m, idx2);
+    else sweep_m<true>(color, m, idx2);
   }
   __device__ float residual(int a, int b, float idx2) const {
     if (interior) return f[at(a, b)] - ax<false>(a, b, idx2);
@@ -784,14 +815,16 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int nt = (int)(blockDim.x * blockDim.y);
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, nullptr, vec);
-  if (NU > 0) S.sweep_from_zero(0, 1);
+  if (NU > 0) S.sweep_from_zero(0);
   for (int s = 1; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
-  // residual where the sweeps are final and one ring beyond the tile
+  // residual where the sweeps are final and one ring beyond the tile (one
+  // list of cells over all the threads)
   {
-    constexpr int m = 2 * NU + 1;
-    for (int a = m + (int)threadIdx.y; a < R - m; a += (int)blockDim.y)
-      for (int b = m + (int)threadIdx.x; b < R - m; b += (int)blockDim.x)
-        S.r[S.at(a, b)] = S.residual(a, b, idx2);
+    constexpr int m = 2 * NU + 1, NRr = R - 2 * m;
+    for (int e = tid; e < NRr * NRr; e += nt) {
+      const int a = m + e / NRr, b = m + (e - (e / NRr) * NRr);
+      S.r[S.at(a, b)] = S.residual(a, b, idx2);
+    }
   }
   __syncthreads();
   for (int e = tid; e < TT * TT; e += nt) {
@@ -829,13 +862,13 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x, vec);
   const int nxc = nx / 2, nyc = ny / 2;
-  for (int a = (int)threadIdx.y; a < R; a += (int)blockDim.y)
-    for (int b = (int)threadIdx.x; b < R; b += (int)blockDim.x) {
-      if (!S.inside(a, b)) continue;
-      const int fi = i0 - HALO + a, fj = j0 - HALO + b;
-      S.x[S.at(a, b)] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
-                                   fj, nxc, nyc);
-    }
+  for (int e = tid; e < R * R; e += nt) {
+    const int a = e / R, b = e - (e / R) * R;
+    if (!S.inside(a, b)) continue;
+    const int fi = i0 - HALO + a, fj = j0 - HALO + b;
+    S.x[S.at(a, b)] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
+                                 fj, nxc, nyc);
+  }
   __syncthreads();
   for (int s = 0; s < 2 * NU; ++s) S.sweep(1 - (s & 1), s + 1, idx2);
   for (int e = tid; e < TT * TT; e += nt) {
