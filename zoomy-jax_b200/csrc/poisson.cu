@@ -889,42 +889,42 @@ __global__ void copy32_kernel(const float* a, float* b, long long n) {
 }
 
 // ── the one-CTA coarse V-cycle (levels small0 .. nlev-1 in shared memory) ───
+// Every level of at most 32 x 32 cells runs with one thread per cell: thread t
+// holds cell (t >> sh, t & (2^sh - 1)), 2^sh the level's row length rounded up
+// to a power of two, so no thread divides, and a red-black half-sweep gives
+// each thread one cell of the colour (rows of 2^(sh-1) threads).  A level's
+// phases synchronise only the warps that hold its cells (a named barrier per
+// level; a warp barrier for a one-warp level): the coarser levels run in a few
+// warps while the others wait at the next finer level's barrier.  Everything
+// the cycle reads (coefficients, inverse diagonals, the coarsest inverse, the
+// right-hand side) is staged by one round of asynchronous copies.  The sums are
+// the same float expressions as the level-wide kernels', so the result is the
+// same bits.
 constexpr int CT = 1024;
+constexpr int CT_MAX_LEVELS = 15;   // named barriers 1 .. 15, one per level
 
-__device__ void cta_rbgs(float* x, const float* f, const float* cx, const float* cy,
-                         const float* idg, int nx, int ny, float idx2, int color) {
-  const int half = (ny + 1) / 2;
-  for (int t = threadIdx.x; t < nx * half; t += CT) {
-    const int i = t / half, m = t - i * half;
-    const int j = 2 * m + ((i + color) & 1);
-    if (j >= ny) continue;
-    x[i * ny + j] = (f[i * ny + j] + idx2 * nbsum_at(x, cx, cy, nx, ny, i, j)) * idg[i * ny + j];
-  }
-  __syncthreads();
+struct CLevel {
+  int nx, ny, sh, act;        // act: threads holding the level's cells (multiple of 32)
+  float idx2;
+  int x, f, r, cx, cy, idg;   // float offsets into shared memory
+};
+
+__device__ __forceinline__ void level_sync(int id, int act) {
+  if (act <= 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(act) : "memory");
 }
 
-// coarsest-level solve: x = A^-1 f with the inverse built at set-up when the
-// level has <= DENSE_MAX_CELLS cells, else symmetric red-black sweep pairs
-__device__ void cta_coarsest(float* x, const float* f, const float* cx, const float* cy,
-                             const float* idg, const float* inv, int nx, int ny, float idx2,
-                             int sweeps) {
-  const int n = nx * ny;
-  if (inv) {
-    for (int k = threadIdx.x; k < n; k += CT) {
-      float v = 0.0f;
-      for (int m = 0; m < n; ++m) v += inv[k * n + m] * f[m];
-      x[k] = v;
-    }
-    __syncthreads();
-    return;
-  }
-  for (int s = 0; s < sweeps; ++s) {
-    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 0);
-    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 1);
-  }
-  for (int s = 0; s < sweeps; ++s) {
-    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 1);
-    cta_rbgs(x, f, cx, cy, idg, nx, ny, idx2, 0);
+// one half-sweep of `color` by thread t; from_zero: the level's x is zero
+// before it (the neighbour sum is then 0, and x need not be cleared)
+__device__ __forceinline__ void cl_half(float* sm, const CLevel& c, int t, int color,
+                                        bool from_zero) {
+  const int hs = c.sh > 0 ? c.sh - 1 : 0;
+  const int i = t >> hs, m = t & ((1 << hs) - 1);
+  const int j = 2 * m + ((i + color) & 1);
+  if (i < c.nx && j < c.ny) {
+    const int k = i * c.ny + j;
+    const float nb = from_zero ? 0.0f : nbsum_at(sm + c.x, sm + c.cx, sm + c.cy, c.nx, c.ny, i, j);
+    sm[c.x + k] = (sm[c.f + k] + c.idx2 * nb) * sm[c.idg + k];
   }
 }
 
@@ -932,80 +932,146 @@ __global__ void __launch_bounds__(CT)
 coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
   pdl_enter();
   extern __shared__ float sm[];
-  // shared copies of x, f, r, cx, cy, idg for every small level
-  float* sx[MAXL]; float* sf[MAXL]; float* sr[MAXL];
-  float* scx[MAXL]; float* scy[MAXL]; float* sidg[MAXL];
-  long long o = 0;
-  for (int l = P.small0; l < P.nlev; ++l) {
+  __shared__ CLevel tab[MAXL];
+  const int t = threadIdx.x;
+  const int l0 = P.small0, nl = P.nlev;
+  // shared layout, level after level: x, f, r (n each), cx, cy, idg; then the
+  // coarsest inverse with rows padded to n + 1 (no bank conflicts)
+  int inv_off = 0;
+  for (int l = l0; l < nl; ++l) {
     const Level& L = P.L[l];
     const int n = L.nx * L.ny;
-    sx[l] = sm + o; o += n;
-    sf[l] = sm + o; o += n;
-    sr[l] = sm + o; o += n;
-    scx[l] = sm + o; o += (L.nx + 1) * L.ny;
-    scy[l] = sm + o; o += L.nx * (L.ny + 1);
-    sidg[l] = sm + o; o += n;
+    if (t == l - l0) {
+      CLevel c;
+      c.nx = L.nx;
+      c.ny = L.ny;
+      int sh = 0;
+      while ((1 << sh) < L.ny) ++sh;
+      c.sh = sh;
+      c.act = ((L.nx << sh) + 31) & ~31;
+      c.idx2 = 1.0f / (L.dx * L.dx);
+      c.x = inv_off;
+      c.f = c.x + n;
+      c.r = c.f + n;
+      c.cx = c.r + n;
+      c.cy = c.cx + (L.nx + 1) * L.ny;
+      c.idg = c.cy + L.nx * (L.ny + 1);
+      tab[l] = c;
+    }
+    inv_off += 4 * n + (L.nx + 1) * L.ny + L.nx * (L.ny + 1);
   }
-  for (int l = P.small0; l < P.nlev; ++l) {
+  const Level& Lc = P.L[nl - 1];
+  const int nc = Lc.nx * Lc.ny;
+  float* sinv = sm + inv_off;
+  __syncthreads();
+  for (int l = l0; l < nl; ++l) {
     const Level& L = P.L[l];
+    const CLevel c = tab[l];
     const int n = L.nx * L.ny;
-    for (int k = threadIdx.x; k < (L.nx + 1) * L.ny; k += CT) scx[l][k] = ws_f[L.cx + k];
-    for (int k = threadIdx.x; k < L.nx * (L.ny + 1); k += CT) scy[l][k] = ws_f[L.cy + k];
-    for (int k = threadIdx.x; k < n; k += CT) {
-      sidg[l][k] = ws_f[L.idg + k];
-      sx[l][k] = 0.0f;
-      if (l == P.small0) sf[l][k] = ws_f[L.f + k];
+    for (int k = t; k < (L.nx + 1) * L.ny; k += CT) cp_async4(sm + c.cx + k, ws_f + L.cx + k, true);
+    for (int k = t; k < L.nx * (L.ny + 1); k += CT) cp_async4(sm + c.cy + k, ws_f + L.cy + k, true);
+    for (int k = t; k < n; k += CT) cp_async4(sm + c.idg + k, ws_f + L.idg + k, true);
+    if (l == l0)
+      for (int k = t; k < n; k += CT) cp_async4(sm + c.f + k, ws_f + L.f + k, true);
+  }
+  if (P.cinv >= 0)
+    for (int k = t; k < nc * nc; k += CT) {
+      const int a = k / nc, b = k - a * nc;
+      cp_async4(sinv + a * (nc + 1) + b, ws_f + P.cinv + k, true);
+    }
+  cp_async_wait_all();
+  __syncthreads();
+  // descend: pre-smoothing, residual, restriction into the next level's f
+  for (int l = l0; l < nl - 1; ++l) {
+    const CLevel c = tab[l];
+    const int id = 1 + l - l0;
+    if (t < c.act) {
+      for (int s = 0; s < nu; ++s) {
+        cl_half(sm, c, t, 0, s == 0);
+        level_sync(id, c.act);
+        cl_half(sm, c, t, 1, false);
+        level_sync(id, c.act);
+      }
+      {
+        const int i = t >> c.sh, j = t & ((1 << c.sh) - 1);
+        if (i < c.nx && j < c.ny) {
+          float od;
+          sm[c.r + i * c.ny + j] =
+              sm[c.f + i * c.ny + j] - apply_at(sm + c.x, sm + c.cx, sm + c.cy, c.nx, c.ny, i, j,
+                                                c.idx2, od);
+        }
+      }
+      level_sync(id, c.act);
+      const CLevel cc = tab[l + 1];
+      {
+        const int I = t >> cc.sh, J = t & ((1 << cc.sh) - 1);
+        if (I < cc.nx && J < cc.ny) {
+          const float* rl = sm + c.r;
+          const int nyf = c.ny;
+          sm[cc.f + I * cc.ny + J] = restrict_at(
+              [&](int fi, int fj) { return rl[fi * nyf + fj]; }, I, J, cc.nx, cc.ny);
+        }
+      }
+      level_sync(id, c.act);
+    }
+  }
+  // coarsest level: the dense inverse, else symmetric red-black sweep pairs
+  {
+    const CLevel c = tab[nl - 1];
+    const int id = nl - l0;
+    if (t < c.act) {
+      if (P.cinv >= 0) {
+        if (t < nc) {
+          float v = 0.0f;
+          for (int m = 0; m < nc; ++m) v += sinv[t * (nc + 1) + m] * sm[c.f + m];
+          sm[c.x + t] = v;
+        }
+        level_sync(id, c.act);
+      } else {
+        for (int s = 0; s < coarse_sweeps; ++s) {
+          cl_half(sm, c, t, 0, s == 0);
+          level_sync(id, c.act);
+          cl_half(sm, c, t, 1, false);
+          level_sync(id, c.act);
+        }
+        for (int s = 0; s < coarse_sweeps; ++s) {
+          cl_half(sm, c, t, 1, false);
+          level_sync(id, c.act);
+          cl_half(sm, c, t, 0, false);
+          level_sync(id, c.act);
+        }
+      }
+    }
+  }
+  // ascend: wait for the coarser level's result (its warps arrive after their
+  // own phases), coarse correction, post-smoothing
+  for (int l = nl - 2; l >= l0; --l) {
+    const CLevel c = tab[l], cc = tab[l + 1];
+    const int id = 1 + l - l0;
+    if (t < c.act) {
+      level_sync(id, c.act);
+      {
+        const int i = t >> c.sh, j = t & ((1 << c.sh) - 1);
+        if (i < c.nx && j < c.ny) {
+          const float* ecl = sm + cc.x;
+          const int nyc = cc.ny;
+          sm[c.x + i * c.ny + j] +=
+              prolong_at([&](int I, int J) { return ecl[I * nyc + J]; }, i, j, cc.nx, cc.ny);
+        }
+      }
+      level_sync(id, c.act);
+      for (int s = 0; s < nu; ++s) {
+        cl_half(sm, c, t, 1, false);
+        level_sync(id, c.act);
+        cl_half(sm, c, t, 0, false);
+        level_sync(id, c.act);
+      }
     }
   }
   __syncthreads();
-  const float* inv = P.cinv >= 0 ? ws_f + P.cinv : nullptr;
-  // descend
-  for (int l = P.small0; l < P.nlev; ++l) {
-    const Level& L = P.L[l];
-    const float idx2 = 1.0f / (L.dx * L.dx);
-    if (l == P.nlev - 1) {
-      cta_coarsest(sx[l], sf[l], scx[l], scy[l], sidg[l], inv, L.nx, L.ny, idx2, coarse_sweeps);
-      break;
-    }
-    for (int s = 0; s < nu; ++s) {
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 0);
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 1);
-    }
-    for (int k = threadIdx.x; k < L.nx * L.ny; k += CT) {
-      const int i = k / L.ny, j = k - i * L.ny;
-      float od;
-      sr[l][k] = sf[l][k] - apply_at(sx[l], scx[l], scy[l], L.nx, L.ny, i, j, idx2, od);
-    }
-    __syncthreads();
-    const Level& Lc = P.L[l + 1];
-    const float* rl = sr[l];
-    const int nyf = L.ny;
-    for (int k = threadIdx.x; k < Lc.nx * Lc.ny; k += CT) {
-      const int I = k / Lc.ny, J = k - I * Lc.ny;
-      sf[l + 1][k] = restrict_at([&](int fi, int fj) { return rl[fi * nyf + fj]; }, I, J, Lc.nx,
-                                 Lc.ny);
-    }
-    __syncthreads();
-  }
-  // ascend
-  for (int l = P.nlev - 2; l >= P.small0; --l) {
-    const Level& L = P.L[l];
-    const Level& Lc = P.L[l + 1];
-    const float idx2 = 1.0f / (L.dx * L.dx);
-    const float* ecl = sx[l + 1];
-    const int nyc = Lc.ny;
-    for (int k = threadIdx.x; k < L.nx * L.ny; k += CT) {
-      const int fi = k / L.ny, fj = k - fi * L.ny;
-      sx[l][k] += prolong_at([&](int I, int J) { return ecl[I * nyc + J]; }, fi, fj, Lc.nx, Lc.ny);
-    }
-    __syncthreads();
-    for (int s = 0; s < nu; ++s) {
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 1);
-      cta_rbgs(sx[l], sf[l], scx[l], scy[l], sidg[l], L.nx, L.ny, idx2, 0);
-    }
-  }
-  const Level& L0 = P.L[P.small0];
-  for (int k = threadIdx.x; k < L0.nx * L0.ny; k += CT) ws_f[L0.xo + k] = sx[P.small0][k];
+  const Level& L0 = P.L[l0];
+  const CLevel c0 = tab[l0];
+  for (int k = t; k < L0.nx * L0.ny; k += CT) ws_f[L0.xo + k] = sm[c0.x + k];
 }
 
 // dense inverse of the coarsest operator (float64 in-place Gauss-Jordan; the
@@ -1058,12 +1124,20 @@ __global__ void coarse_inverse_kernel(const Plan P, float* ws_f) {
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) inv[e] = (float)a[e / n][e % n];
 }
 
+// the one-CTA kernel's dynamic shared memory at most: 227 KB less its static
+// level table
+constexpr size_t COARSE_SMEM_MAX = 227 * 1024 - sizeof(CLevel) * MAXL;
+
 static size_t coarse_smem(const Plan& P) {
   size_t o = 0;
   for (int l = P.small0; l < P.nlev; ++l) {
     const Level& L = P.L[l];
     const size_t n = (size_t)L.nx * L.ny;
     o += 4 * n + (size_t)(L.nx + 1) * L.ny + (size_t)L.nx * (L.ny + 1);
+  }
+  if (P.cinv >= 0) {
+    const size_t nc = (size_t)P.L[P.nlev - 1].nx * P.L[P.nlev - 1].ny;
+    o += nc * (nc + 1);
   }
   return o * sizeof(float);
 }
@@ -1076,7 +1150,8 @@ static int enable_coarse_smem() {
   ZB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 32 && !(set_mask.load() & (1u << dev))) {
     ZB_CUDA_TRY(cudaFuncSetAttribute(coarse_vcycle_kernel,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)COARSE_SMEM_MAX));
 #define ZB_SMEM_ATTR(K) \
     ZB_CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024))
     ZB_SMEM_ATTR((mg_down_kernel<1, FT>)); ZB_SMEM_ATTR((mg_down_kernel<2, FT>));
@@ -1202,13 +1277,14 @@ static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, 
   return e == cudaSuccess ? ZB_OK : ZB_E_CUDA;
 }
 
-// 32 x 32 tiles with 32 x 8 threads when the level has two tiles for every
-// SM; else 16 x 16 tiles with 16 x 32 threads (four times the CTAs, one
-// staged row per thread and phase), so that the few CTAs of a small level
-// finish their serial phases sooner
+// 32 x 32 tiles with 32 x 8 threads when the level has a tile for every SM;
+// else 16 x 16 tiles with 16 x 32 threads (four times the CTAs, one staged row
+// per thread and phase), so that the few CTAs of a small level finish their
+// serial phases sooner.  At 512^2 (256 tiles of 32^2) the large tiles win: a
+// 16^2 tile stages 28^2 cells for nu = 2, three times its own
 static int fused(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
                  cudaStream_t st) {
-  const bool big = ((L.ny + FT - 1) / FT) * ((L.nx + FT - 1) / FT) >= 2 * 148;
+  const bool big = ((L.ny + FT - 1) / FT) * ((L.nx + FT - 1) / FT) >= 148;
   if (big) return fused_level<FT>(down, nu, L, fw, to, idx2, dim3(32, 8), st);
   return fused_level<FTS>(down, nu, L, fw, to, idx2, dim3(FTS, 32), st);
 }
@@ -1339,7 +1415,9 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
     coef_from_h<float><<<grid_for(nf), NT, 0, st>>>((const float*)h, L0.nx, L0.ny, cfg->cmin,
                                                     cfg->cmax, dw + P.cx64, dw + P.cy64,
                                                     fw + L0.cx, fw + L0.cy);
-  if (P.small0 < P.nlev && coarse_smem(P) > 227 * 1024) return ZB_E_TOO_LARGE;
+  if (P.small0 < P.nlev &&
+      (coarse_smem(P) > COARSE_SMEM_MAX || P.nlev - P.small0 > CT_MAX_LEVELS))
+    return ZB_E_TOO_LARGE;
   if (const int e = enable_coarse_smem()) return e;
   const long long n0 = (long long)L0.nx * L0.ny;
   diag_kernel64<<<grid_for(n0), NT, 0, st>>>(dw + P.cx64, dw + P.cy64, L0.nx, L0.ny,
