@@ -579,6 +579,10 @@ prolong_add_kernel(const float* __restrict__ ec, float* __restrict__ xf, int nxc
 constexpr int FT = 32;            // tile side of the levels with a tile for every SM
 constexpr int FTS = 16;           // tile side of the smaller levels
 constexpr int FNT_MAX = 1024;
+// threads of a fused level CTA (one-dimensional): 256 for the 32^2 tiles, 512
+// for the 16^2 ones; a compile-time count lets every phase's item loop have a
+// fixed trip count
+__host__ __device__ constexpr int fused_threads(int tile) { return tile == FT ? 256 : 512; }
 
 // Staged layout of a tile with its ring: R = tile + 2 halo rows; the arrays
 // x, f, r, idg (R rows) and cx (R + 1 rows) keep PAD leading columns so that
@@ -621,6 +625,7 @@ struct Stage {
   static constexpr int R = TT + 2 * HALO;
   static constexpr int PAD = stage_pad(HALO);
   static constexpr int RS = stage_rs(HALO, TT);
+  static constexpr int NTH = fused_threads(TT);
   // staged element (a, b) of x, f, r, idg (a in [0, R)) or cx (a in [0, R])
   __device__ static constexpr int at(int a, int b) { return a * RS + b + PAD; }
   int i0, j0, nx, ny;
@@ -683,8 +688,8 @@ struct Stage {
   // (the cells enumerated as in sweep_flat, margin 1)
   __device__ void sweep_from_zero(int color) const {
     constexpr int M = 1, NR = R - 2 * M, HALF = NR / 2;
-    const int nt = (int)(blockDim.x * blockDim.y);
-    for (int e = (int)(threadIdx.y * blockDim.x + threadIdx.x); e < NR * HALF; e += nt) {
+#pragma unroll
+    for (int e = (int)threadIdx.x; e < NR * HALF; e += NTH) {
       const int a = M + e / HALF, k = e - (e / HALF) * HALF;
       const int gi = i0 - HALO + a;
       const int b = M + (((color - gi - (j0 - HALO) - M) % 2 + 2) % 2) + 2 * k;
@@ -700,8 +705,8 @@ struct Stage {
   template <bool EDGE, int M>
   __device__ void sweep_flat(int color, float idx2) const {
     constexpr int NR = R - 2 * M, HALF = NR / 2;
-    const int nt = (int)(blockDim.x * blockDim.y);
-    for (int e = (int)(threadIdx.y * blockDim.x + threadIdx.x); e < NR * HALF; e += nt) {
+#pragma unroll
+    for (int e = (int)threadIdx.x; e < NR * HALF; e += NTH) {
       const int a = M + e / HALF, k = e - (e / HALF) * HALF;
       const int gi = i0 - HALO + a;
       const int b = M + (((color - gi - (j0 - HALO) - M) % 2 + 2) % 2) + 2 * k;
@@ -746,14 +751,15 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
   S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
   S.x = sm; S.f = sm + R * RS; S.r = sm + 2 * R * RS; S.idg = sm + 3 * R * RS;
   S.cx = sm + 4 * R * RS; S.cy = S.cx + (R + 1) * RS;
-  const int nt = (int)(blockDim.x * blockDim.y);
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  constexpr int nt = St::NTH;
+  const int tid = threadIdx.x;
   // every copy is issued before any is waited for
   if (vec) {
     // rows as 16-byte chunks from column gs = j0 - HALO - PAD (a multiple of
     // 4, like ny): a chunk lies wholly inside the level or wholly outside it
     constexpr int NC = RS / 4;
     const int gs = j0 - HALO - PAD;
+#pragma unroll
     for (int e = tid; e < R * NC; e += nt) {
       const int a = e / NC, c = e - a * NC;
       const int gi = i0 - HALO + a, gc = gs + 4 * c;
@@ -764,6 +770,7 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
       if (x) cp_async16f(S.x + a * RS + 4 * c, x + k, in);
       else *(float4*)(S.x + a * RS + 4 * c) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
+#pragma unroll
     for (int e = tid; e < (R + 1) * NC; e += nt) {
       const int a = e / NC, c = e - a * NC;
       const int gi = i0 - HALO + a, gc = gs + 4 * c;
@@ -771,6 +778,7 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
       cp_async16f(S.cx + a * RS + 4 * c, cx + (in ? (long long)gi * ny + gc : 0), in);
     }
   } else {
+#pragma unroll
     for (int e = tid; e < R * R; e += nt) {
       const int a = e / R, b = e - (e / R) * R;
       const int gi = i0 - HALO + a, gj = j0 - HALO + b;
@@ -781,6 +789,7 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
       if (x) cp_async4(S.x + St::at(a, b), x + k, in);
       else S.x[St::at(a, b)] = 0.0f;
     }
+#pragma unroll
     for (int e = tid; e < (R + 1) * R; e += nt) {
       const int a = e / R, b = e - (e / R) * R;
       const int gi = i0 - HALO + a, gj = j0 - HALO + b;
@@ -788,6 +797,7 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
       cp_async4(S.cx + St::at(a, b), cx + (in ? (long long)gi * ny + gj : 0), in);
     }
   }
+#pragma unroll
   for (int e = tid; e < R * (R + 1); e += nt) {
     const int a = e / (R + 1), b = e - (e / (R + 1)) * (R + 1);
     const int gi = i0 - HALO + a, gj = j0 - HALO + b;
@@ -812,8 +822,8 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   constexpr int HALO = 2 * NU + 2;
   constexpr int R = Stage<HALO, TT>::R;
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
-  const int nt = (int)(blockDim.x * blockDim.y);
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  constexpr int nt = fused_threads(TT);
+  const int tid = threadIdx.x;
   const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, nullptr, vec);
   if (NU > 0) S.sweep_from_zero(0);
   for (int s = 1; s < 2 * NU; ++s) S.sweep(s & 1, s + 1, idx2);
@@ -821,18 +831,21 @@ mg_down_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   // list of cells over all the threads)
   {
     constexpr int m = 2 * NU + 1, NRr = R - 2 * m;
+#pragma unroll
     for (int e = tid; e < NRr * NRr; e += nt) {
       const int a = m + e / NRr, b = m + (e - (e / NRr) * NRr);
       S.r[S.at(a, b)] = S.residual(a, b, idx2);
     }
   }
   __syncthreads();
+#pragma unroll
   for (int e = tid; e < TT * TT; e += nt) {
     const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
     if (gi < nx && gj < ny) x[(long long)gi * ny + gj] = S.x[S.at(HALO + ti, HALO + tj)];
   }
   const int nxc = nx / 2, nyc = ny / 2;
+#pragma unroll
   for (int e = tid; e < (TT / 2) * (TT / 2); e += nt) {
     const int I = i0 / 2 + e / (TT / 2), J = j0 / 2 + e % (TT / 2);
     if (I >= nxc || J >= nyc) continue;
@@ -858,10 +871,11 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   constexpr int HALO = 2 * NU;
   constexpr int R = Stage<HALO, TT>::R;
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
-  const int nt = (int)(blockDim.x * blockDim.y);
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  constexpr int nt = fused_threads(TT);
+  const int tid = threadIdx.x;
   const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x, vec);
   const int nxc = nx / 2, nyc = ny / 2;
+#pragma unroll
   for (int e = tid; e < R * R; e += nt) {
     const int a = e / R, b = e - (e / R) * R;
     if (!S.inside(a, b)) continue;
@@ -871,6 +885,7 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   }
   __syncthreads();
   for (int s = 0; s < 2 * NU; ++s) S.sweep(1 - (s & 1), s + 1, idx2);
+#pragma unroll
   for (int e = tid; e < TT * TT; e += nt) {
     const int ti = e / TT, tj = e % TT;
     const int gi = i0 + ti, gj = j0 + tj;
@@ -1277,16 +1292,16 @@ static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, 
   return e == cudaSuccess ? ZB_OK : ZB_E_CUDA;
 }
 
-// 32 x 32 tiles with 32 x 8 threads when the level has a tile for every SM;
-// else 16 x 16 tiles with 16 x 32 threads (four times the CTAs, one staged row
-// per thread and phase), so that the few CTAs of a small level finish their
-// serial phases sooner.  At 512^2 (256 tiles of 32^2) the large tiles win: a
+// 32 x 32 tiles with 256 threads when the level has a tile for every SM; else
+// 16 x 16 tiles with 512 threads (four times the CTAs, two threads per staged
+// cell), so that the few CTAs of a small level finish their serial phases
+// sooner.  At 512^2 (256 tiles of 32^2) the large tiles win: a
 // 16^2 tile stages 28^2 cells for nu = 2, three times its own
 static int fused(bool down, int nu, const Level& L, float* fw, float* to, float idx2,
                  cudaStream_t st) {
   const bool big = ((L.ny + FT - 1) / FT) * ((L.nx + FT - 1) / FT) >= 148;
-  if (big) return fused_level<FT>(down, nu, L, fw, to, idx2, dim3(32, 8), st);
-  return fused_level<FTS>(down, nu, L, fw, to, idx2, dim3(FTS, 32), st);
+  if (big) return fused_level<FT>(down, nu, L, fw, to, idx2, dim3(fused_threads(FT)), st);
+  return fused_level<FTS>(down, nu, L, fw, to, idx2, dim3(fused_threads(FTS)), st);
 }
 
 static int vcycle(const Plan& P, void* ws, int precond, const zb_smoother* smo, cudaStream_t st) {
