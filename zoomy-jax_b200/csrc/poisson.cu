@@ -593,6 +593,11 @@ __host__ __device__ constexpr int stage_pad(int halo) { return (4 - halo % 4) % 
 __host__ __device__ constexpr int stage_rs(int halo, int tile) {
   return ((tile + 2 * halo + stage_pad(halo) + 3) / 4) * 4;
 }
+// the up kernel's staged coarse tile (R / 2 + 2 square)
+__host__ __device__ inline size_t up_tile_smem(int halo, int tile) {
+  const int cr = (tile + 2 * halo) / 2 + 2;
+  return (size_t)cr * cr * sizeof(float);
+}
 __host__ __device__ inline size_t fused_smem(int halo, int tile) {
   const int R = tile + 2 * halo, RS = stage_rs(halo, tile);
   return (size_t)(4 * R * RS + (R + 1) * RS + R * (R + 1)) * sizeof(float);
@@ -630,7 +635,7 @@ struct Stage {
   __device__ static constexpr int at(int a, int b) { return a * RS + b + PAD; }
   int i0, j0, nx, ny;
   bool interior;
-  float *x, *f, *r, *idg, *cx, *cy;
+  float *x, *f, *r, *idg, *cx, *cy, *ec;
   __device__ bool inside(int a, int b) const {
     const int gi = i0 - HALO + a, gj = j0 - HALO + b;
     return gi >= 0 && gi < nx && gj >= 0 && gj < ny;
@@ -691,8 +696,8 @@ struct Stage {
 #pragma unroll
     for (int e = (int)threadIdx.x; e < NR * HALF; e += NTH) {
       const int a = M + e / HALF, k = e - (e / HALF) * HALF;
-      const int gi = i0 - HALO + a;
-      const int b = M + (((color - gi - (j0 - HALO) - M) % 2 + 2) % 2) + 2 * k;
+      // tile origins are even, so the colour of staged (a, b) is (a + b) % 2
+      const int b = M + ((color + a + M) & 1) + 2 * k;
       if (!interior && !inside(a, b)) continue;
       x[at(a, b)] = f[at(a, b)] * idg[at(a, b)];
     }
@@ -708,8 +713,8 @@ struct Stage {
 #pragma unroll
     for (int e = (int)threadIdx.x; e < NR * HALF; e += NTH) {
       const int a = M + e / HALF, k = e - (e / HALF) * HALF;
-      const int gi = i0 - HALO + a;
-      const int b = M + (((color - gi - (j0 - HALO) - M) % 2 + 2) % 2) + 2 * k;
+      // tile origins are even, so the colour of staged (a, b) is (a + b) % 2
+      const int b = M + ((color + a + M) & 1) + 2 * k;
       if (EDGE && !inside(a, b)) continue;
       x[at(a, b)] = (f[at(a, b)] + nbsum<EDGE>(a, b) * idx2) * idg[at(a, b)];
     }
@@ -743,7 +748,8 @@ template <int HALO, int TT>
 __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny,
                                        const float* __restrict__ f, const float* __restrict__ cx,
                                        const float* __restrict__ cy, const float* __restrict__ idg,
-                                       const float* __restrict__ x, int vec) {
+                                       const float* __restrict__ x, int vec,
+                                       const float* __restrict__ ec = nullptr) {
   using St = Stage<HALO, TT>;
   constexpr int R = St::R, RS = St::RS, PAD = St::PAD;
   St S;
@@ -751,31 +757,42 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
   S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
   S.x = sm; S.f = sm + R * RS; S.r = sm + 2 * R * RS; S.idg = sm + 3 * R * RS;
   S.cx = sm + 4 * R * RS; S.cy = S.cx + (R + 1) * RS;
+  S.ec = S.cy + R * (R + 1);
   constexpr int nt = St::NTH;
   const int tid = threadIdx.x;
   // every copy is issued before any is waited for
   if (vec) {
     // rows as 16-byte chunks from column gs = j0 - HALO - PAD (a multiple of
-    // 4, like ny): a chunk lies wholly inside the level or wholly outside it
-    constexpr int NC = RS / 4;
-    const int gs = j0 - HALO - PAD;
+    // 4, like ny): a chunk lies wholly inside the level or wholly outside it.
+    // Each thread keeps one chunk column and steps down the rows.
+    constexpr int NC = RS / 4, RSTEP = nt / NC;
+    const int c = tid % NC, a0 = tid / NC;
+    if (a0 < RSTEP) {
+      const int gc = j0 - HALO - PAD + 4 * c;
+      const bool cin = gc >= 0 && gc < ny;
+      const int gi0 = i0 - HALO + a0;
+      const long long k0 = (long long)gi0 * ny + gc;
 #pragma unroll
-    for (int e = tid; e < R * NC; e += nt) {
-      const int a = e / NC, c = e - a * NC;
-      const int gi = i0 - HALO + a, gc = gs + 4 * c;
-      const bool in = gi >= 0 && gi < nx && gc >= 0 && gc < ny;
-      const long long k = in ? (long long)gi * ny + gc : 0;
-      cp_async16f(S.f + a * RS + 4 * c, f + k, in);
-      cp_async16f(S.idg + a * RS + 4 * c, idg + k, in);
-      if (x) cp_async16f(S.x + a * RS + 4 * c, x + k, in);
-      else *(float4*)(S.x + a * RS + 4 * c) = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+      for (int it = 0; it < (R + RSTEP - 1) / RSTEP; ++it) {
+        const int a = a0 + it * RSTEP, gi = gi0 + it * RSTEP;
+        if (a < R) {
+          const bool in = cin && gi >= 0 && gi < nx;
+          const long long k = in ? k0 + (long long)it * RSTEP * ny : 0;
+          cp_async16f(S.f + a * RS + 4 * c, f + k, in);
+          cp_async16f(S.idg + a * RS + 4 * c, idg + k, in);
+          if (x) cp_async16f(S.x + a * RS + 4 * c, x + k, in);
+          else *(float4*)(S.x + a * RS + 4 * c) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
 #pragma unroll
-    for (int e = tid; e < (R + 1) * NC; e += nt) {
-      const int a = e / NC, c = e - a * NC;
-      const int gi = i0 - HALO + a, gc = gs + 4 * c;
-      const bool in = gi >= 0 && gi <= nx && gc >= 0 && gc < ny;
-      cp_async16f(S.cx + a * RS + 4 * c, cx + (in ? (long long)gi * ny + gc : 0), in);
+      for (int it = 0; it < (R + 1 + RSTEP - 1) / RSTEP; ++it) {
+        const int a = a0 + it * RSTEP, gi = gi0 + it * RSTEP;
+        if (a < R + 1) {
+          const bool in = cin && gi >= 0 && gi <= nx;
+          const long long k = in ? k0 + (long long)it * RSTEP * ny : 0;
+          cp_async16f(S.cx + a * RS + 4 * c, cx + k, in);
+        }
+      }
     }
   } else {
 #pragma unroll
@@ -797,12 +814,47 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
       cp_async4(S.cx + St::at(a, b), cx + (in ? (long long)gi * ny + gj : 0), in);
     }
   }
+  // cy: R rows of R + 1 faces, 4-byte copies (rows of ny + 1 floats do not
+  // start on 16 bytes); each thread keeps one column and steps down the rows
+  {
+    constexpr int W = R + 1, YSTEP = nt / W;
+    const int b = tid % W, a0 = tid / W;
+    if (a0 < YSTEP) {
+      const int gj = j0 - HALO + b, gi0 = i0 - HALO + a0;
+      const bool cin = gj >= 0 && gj <= ny;
+      const long long k0 = (long long)gi0 * (ny + 1) + gj;
 #pragma unroll
-  for (int e = tid; e < R * (R + 1); e += nt) {
-    const int a = e / (R + 1), b = e - (e / (R + 1)) * (R + 1);
-    const int gi = i0 - HALO + a, gj = j0 - HALO + b;
-    const bool in = gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
-    cp_async4(S.cy + e, cy + (in ? (long long)gi * (ny + 1) + gj : 0), in);
+      for (int it = 0; it < (R + YSTEP - 1) / YSTEP; ++it) {
+        const int a = a0 + it * YSTEP, gi = gi0 + it * YSTEP;
+        if (a < R) {
+          const bool in = cin && gi >= 0 && gi < nx;
+          cp_async4(S.cy + a * W + b, cy + (in ? k0 + (long long)it * YSTEP * (ny + 1) : 0), in);
+        }
+      }
+    }
+  }
+  if (ec) {
+    // the coarse level's result under the tile (coarse cells I0 - 1 ..
+    // I0 + R / 2, I0 = (i0 - HALO) / 2, and the same in y), loaded while the
+    // copies fly; a coarse index one beyond the wall holds the prolongation's
+    // odd reflection (minus the cell inside; plus it at a corner), so the
+    // correction below needs no wall tests; cells further out are never read
+    constexpr int CR = R / 2 + 2;
+    const int nxc = nx / 2, nyc = ny / 2;
+    const int I0 = (i0 - HALO) / 2 - 1, J0 = (j0 - HALO) / 2 - 1;
+#pragma unroll
+    for (int e = tid; e < CR * CR; e += nt) {
+      const int ci = I0 + e / CR, cj = J0 + e % CR;
+      float v = 0.0f;
+      if (ci >= -1 && ci <= nxc && cj >= -1 && cj <= nyc) {
+        const bool ox = ci < 0 || ci >= nxc, oy = cj < 0 || cj >= nyc;
+        const int ri = ci < 0 ? 0 : (ci >= nxc ? nxc - 1 : ci);
+        const int rj = cj < 0 ? 0 : (cj >= nyc ? nyc - 1 : cj);
+        v = ec[(long long)ri * nyc + rj];
+        if (ox != oy) v = -v;
+      }
+      S.ec[e] = v;
+    }
   }
   cp_async_wait_all();
   __syncthreads();
@@ -873,15 +925,37 @@ mg_up_kernel(const float* __restrict__ f, const float* __restrict__ cx,
   const int i0 = blockIdx.y * TT, j0 = blockIdx.x * TT;
   constexpr int nt = fused_threads(TT);
   const int tid = threadIdx.x;
-  const Stage<HALO, TT> S = stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x, vec);
-  const int nxc = nx / 2, nyc = ny / 2;
+  const Stage<HALO, TT> S =
+      stage_level<HALO, TT>(fsm, i0, j0, nx, ny, f, cx, cy, idg, x, vec, ec);
+  // coarse correction: each coarse cell under the staged region adds its
+  // prolongation to its 2 x 2 fine children -- prolong_at's weights in its
+  // order (own 9/16, x side 3/16, y side 3/16, diagonal 1/16), the wall
+  // reflection staged -- so the sums are prolong_at's bits.  Children outside
+  // the level are updated too; nothing reads them.
+  {
+    constexpr int CR = R / 2 + 2, NP = R / 2;
+    const float* T = S.ec;
 #pragma unroll
-  for (int e = tid; e < R * R; e += nt) {
-    const int a = e / R, b = e - (e / R) * R;
-    if (!S.inside(a, b)) continue;
-    const int fi = i0 - HALO + a, fj = j0 - HALO + b;
-    S.x[S.at(a, b)] += prolong_at([&](int I, int J) { return ec[(long long)I * nyc + J]; }, fi,
-                                 fj, nxc, nyc);
+    for (int e = tid; e < NP * NP; e += nt) {
+      const int p = 1 + e / NP, q = 1 + e % NP;
+      const float c0 = T[p * CR + q];
+      const float xm = T[(p - 1) * CR + q], xp = T[(p + 1) * CR + q];
+      const float ym = T[p * CR + q - 1], yp = T[p * CR + q + 1];
+      const float mm = T[(p - 1) * CR + q - 1], mp = T[(p - 1) * CR + q + 1];
+      const float pm = T[(p + 1) * CR + q - 1], pp = T[(p + 1) * CR + q + 1];
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const int di = d >> 1, dj = d & 1;
+        const float ex = di ? xp : xm, ey = dj ? yp : ym;
+        const float exy = di ? (dj ? pp : pm) : (dj ? mp : mm);
+        float v = 0.0f;
+        v += (9.0f / 16.0f) * c0;
+        v += (3.0f / 16.0f) * ex;
+        v += (3.0f / 16.0f) * ey;
+        v += (1.0f / 16.0f) * exy;
+        S.x[S.at(2 * p - 2 + di, 2 * q - 2 + dj)] += v;
+      }
+    }
   }
   __syncthreads();
   for (int s = 0; s < 2 * NU; ++s) S.sweep(1 - (s & 1), s + 1, idx2);
@@ -1257,7 +1331,7 @@ static int fused_level(bool down, int nu, const Level& L, float* fw, float* to, 
   // down: `to` = the coarse right-hand side it restricts into; up: `to` =
   // the coarse level's result it prolongs from
   const dim3 grid((L.ny + TT - 1) / TT, (L.nx + TT - 1) / TT);
-  const size_t sm = fused_smem(down ? 2 * nu + 2 : 2 * nu, TT);
+  const size_t sm = down ? fused_smem(2 * nu + 2, TT) : fused_smem(2 * nu, TT) + up_tile_smem(2 * nu, TT);
   const float *a0 = fw + L.f, *a1 = fw + L.cx, *a2 = fw + L.cy, *a3 = fw + L.idg;
   float* a4 = fw + L.x;
   float* a5 = fw + L.xo;
