@@ -162,36 +162,27 @@ __device__ __forceinline__ float* F(void* ws, const Plan& P, long long off) {
 }
 
 // ── set-up kernels ──────────────────────────────────────────────────────────
+// Level 0 in one pass over its cells, each coarser level in one pass over its
+// cells from the finer level's faces, and the levels of the one-CTA V-cycle
+// plus the coarsest inverse in one CTA: every cell evaluates its four faces
+// itself (a face shared by two cells is the same expression on the same
+// operands, so both get its bits), writes the faces it owns (west and south;
+// east and north on the last row and column) and its diagonal.
+
+// face coefficient: the harmonic mean of the two cells' depths clipped to
+// [cmin, cmax]; a side outside the grid takes the other cell's alone
 template <typename T>
-__global__ void coef_from_h(const T* __restrict__ h, int nx, int ny, double cmin, double cmax,
-                            double* cx64, double* cy64, float* cx32, float* cy32) {
-  const long long nfx = (long long)(nx + 1) * ny, nfy = (long long)nx * (ny + 1);
-  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < nfx + nfy;
-       k += (long long)gridDim.x * NT) {
-    double v;
-    if (k < nfx) {
-      const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
-      const double a = i > 0 ? fmin(fmax((double)h[(long long)(i - 1) * ny + j], cmin), cmax) : -1.0;
-      const double b = i < nx ? fmin(fmax((double)h[(long long)i * ny + j], cmin), cmax) : -1.0;
-      v = (a < 0) ? b : (b < 0 ? a : 2.0 * a * b / (a + b));
-      cx64[k] = v;
-      cx32[k] = (float)v;
-    } else {
-      const long long kk = k - nfx;
-      const int i = (int)(kk / (ny + 1)), j = (int)(kk - (long long)i * (ny + 1));
-      const double a = j > 0 ? fmin(fmax((double)h[(long long)i * ny + j - 1], cmin), cmax) : -1.0;
-      const double b = j < ny ? fmin(fmax((double)h[(long long)i * ny + j], cmin), cmax) : -1.0;
-      v = (a < 0) ? b : (b < 0 ? a : 2.0 * a * b / (a + b));
-      cy64[kk] = v;
-      cy32[kk] = (float)v;
-    }
-  }
+__device__ __forceinline__ double face_coef(const T* h, long long kl, long long kr, bool hasl,
+                                            bool hasr, double cmin, double cmax) {
+  const double a = hasl ? fmin(fmax((double)h[kl], cmin), cmax) : -1.0;
+  const double b = hasr ? fmin(fmax((double)h[kr], cmin), cmax) : -1.0;
+  return (a < 0) ? b : (b < 0 ? a : 2.0 * a * b / (a + b));
 }
 
+// diagonal of the 5-point operator from a cell's west, east, south and north
+// face coefficients (a wall face counts twice: its ghost is -x)
 template <typename T>
-__device__ __forceinline__ T diag_at(const T* cx, const T* cy, int nx, int ny, int i, int j, T idx2) {
-  const T a = cx[(long long)i * ny + j], b = cx[(long long)(i + 1) * ny + j];
-  const T c = cy[(long long)i * (ny + 1) + j], d = cy[(long long)i * (ny + 1) + j + 1];
+__device__ __forceinline__ T diag_of(T a, T b, T c, T d, int i, int j, int nx, int ny, T idx2) {
   T s = (a + b) + (c + d);
   if (i == 0) s += a;
   if (i == nx - 1) s += b;
@@ -200,42 +191,62 @@ __device__ __forceinline__ T diag_at(const T* cx, const T* cy, int nx, int ny, i
   return s * idx2;
 }
 
-__global__ void diag_kernel64(const double* cx, const double* cy, int nx, int ny, double idx2,
-                              double* dg) {
+// level 0: float64 faces and diagonal (the Krylov operator), float32 faces
+// and inverse diagonal (the finest multigrid level)
+template <typename T>
+__global__ void __launch_bounds__(NT)
+setup0_kernel(const T* __restrict__ h, int nx, int ny, double cmin, double cmax, double idx2,
+              float idx2f, double* __restrict__ cx64, double* __restrict__ cy64,
+              double* __restrict__ dg64, float* __restrict__ cx32, float* __restrict__ cy32,
+              float* __restrict__ idg32) {
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
        k += (long long)gridDim.x * NT) {
     const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
-    dg[k] = diag_at<double>(cx, cy, nx, ny, i, j, idx2);
+    const double w = face_coef(h, k - ny, k, i > 0, true, cmin, cmax);
+    const double e = face_coef(h, k, k + ny, true, i + 1 < nx, cmin, cmax);
+    const double so = face_coef(h, k - 1, k, j > 0, true, cmin, cmax);
+    const double no = face_coef(h, k, k + 1, true, j + 1 < ny, cmin, cmax);
+    const long long ky = (long long)i * (ny + 1) + j;
+    cx64[k] = w;
+    cx32[k] = (float)w;
+    cy64[ky] = so;
+    cy32[ky] = (float)so;
+    if (i == nx - 1) { cx64[k + ny] = e; cx32[k + ny] = (float)e; }
+    if (j == ny - 1) { cy64[ky + 1] = no; cy32[ky + 1] = (float)no; }
+    dg64[k] = diag_of<double>(w, e, so, no, i, j, nx, ny, idx2);
+    idg32[k] = __frcp_rn(
+        diag_of<float>((float)w, (float)e, (float)so, (float)no, i, j, nx, ny, idx2f));
   }
 }
 
-// the float32 levels keep the inverse of the diagonal: every smoother
-// multiplies by it
-__global__ void diag_kernel32(const float* cx, const float* cy, int nx, int ny, float idx2,
-                              float* idg) {
-  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nx * ny;
-       k += (long long)gridDim.x * NT) {
-    const int i = (int)(k / ny), j = (int)(k - (long long)i * ny);
-    idg[k] = __frcp_rn(diag_at<float>(cx, cy, nx, ny, i, j, idx2));
-  }
-}
-
-__global__ void coarsen_kernel(const float* cxf, const float* cyf, int nxc, int nyc, float* cxc,
-                               float* cyc) {
+// coarse cell (I, J): its faces as the means of the two fine faces they
+// cover, and its inverse diagonal
+__device__ __forceinline__ void coarsen_cell(const float* cxf, const float* cyf, int nxc, int nyc,
+                                             float idx2, float* cxc, float* cyc, float* idg,
+                                             int I, int J) {
   const int nyf = 2 * nyc;
-  const long long nfx = (long long)(nxc + 1) * nyc, nfy = (long long)nxc * (nyc + 1);
-  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < nfx + nfy;
+  const long long fw = (long long)(2 * I) * nyf + 2 * J, fe = fw + 2LL * nyf;
+  const long long fs = (long long)(2 * I) * (nyf + 1) + 2 * J, fn = fs + 2;
+  const float w = 0.5f * (cxf[fw] + cxf[fw + 1]);
+  const float e = 0.5f * (cxf[fe] + cxf[fe + 1]);
+  const float so = 0.5f * (cyf[fs] + cyf[fs + (nyf + 1)]);
+  const float no = 0.5f * (cyf[fn] + cyf[fn + (nyf + 1)]);
+  const long long k = (long long)I * nyc + J, ky = (long long)I * (nyc + 1) + J;
+  cxc[k] = w;
+  cyc[ky] = so;
+  if (I == nxc - 1) cxc[k + nyc] = e;
+  if (J == nyc - 1) cyc[ky + 1] = no;
+  idg[k] = __frcp_rn(diag_of<float>(w, e, so, no, I, J, nxc, nyc, idx2));
+}
+
+__global__ void __launch_bounds__(NT)
+coarsen_kernel(const float* __restrict__ cxf, const float* __restrict__ cyf, int nxc, int nyc,
+               float idx2, float* __restrict__ cxc, float* __restrict__ cyc,
+               float* __restrict__ idg) {
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < (long long)nxc * nyc;
        k += (long long)gridDim.x * NT) {
-    if (k < nfx) {
-      const int I = (int)(k / nyc), J = (int)(k - (long long)I * nyc);
-      const long long f0 = (long long)(2 * I) * nyf + 2 * J;
-      cxc[k] = 0.5f * (cxf[f0] + cxf[f0 + 1]);
-    } else {
-      const long long kk = k - nfx;
-      const int I = (int)(kk / (nyc + 1)), J = (int)(kk - (long long)I * (nyc + 1));
-      const long long f0 = (long long)(2 * I) * (nyf + 1) + 2 * J;
-      cyc[kk] = 0.5f * (cyf[f0] + cyf[f0 + (nyf + 1)]);
-    }
+    const int I = (int)(k / nyc), J = (int)(k - (long long)I * nyc);
+    coarsen_cell(cxf, cyf, nxc, nyc, idx2, cxc, cyc, idg, I, J);
   }
 }
 
@@ -1163,54 +1174,67 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
   for (int k = t; k < L0.nx * L0.ny; k += CT) ws_f[L0.xo + k] = sm[c0.x + k];
 }
 
-// dense inverse of the coarsest operator (float64 in-place Gauss-Jordan; the
-// operator is SPD, so no pivoting), stored as float32 for the V-cycle; one CTA
-__global__ void coarse_inverse_kernel(const Plan P, float* ws_f) {
+// The small levels' set-up in one CTA: levels l_first .. nlev - 1 coarsened
+// one after the other (coarsen_cell per coarse cell), then the dense inverse of
+// the coarsest operator (float64 in-place Gauss-Jordan; the operator is SPD, so
+// no pivoting), stored as float32 for the V-cycle
+constexpr int ST = 1024;
+__global__ void __launch_bounds__(ST) small_setup_kernel(const Plan P, float* ws_f, int l_first) {
   __shared__ double a[DENSE_MAX_CELLS][DENSE_MAX_CELLS];
   __shared__ double fcol[DENSE_MAX_CELLS];
   __shared__ double prow[DENSE_MAX_CELLS];
+  for (int l = l_first; l < P.nlev; ++l) {
+    const Level& L = P.L[l];
+    const Level& Lf = P.L[l - 1];
+    // the host's IEEE quotient, as the launches of the larger levels get it
+    const float idx2 = __fdiv_rn(1.0f, __fmul_rn(L.dx, L.dx));
+    for (int k = threadIdx.x; k < L.nx * L.ny; k += ST) {
+      const int I = k / L.ny, J = k - (k / L.ny) * L.ny;
+      coarsen_cell(ws_f + Lf.cx, ws_f + Lf.cy, L.nx, L.ny, idx2, ws_f + L.cx, ws_f + L.cy,
+                   ws_f + L.idg, I, J);
+    }
+    __syncthreads();
+  }
+  if (P.cinv < 0) return;
   const Level& L = P.L[P.nlev - 1];
   const int nx = L.nx, ny = L.ny, n = nx * ny;
   const double idx2 = 1.0 / ((double)L.dx * (double)L.dx);
   const float* cx = ws_f + L.cx;
   const float* cy = ws_f + L.cy;
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[e / n][e % n] = 0.0;
+  for (int e = threadIdx.x; e < n * n; e += ST) a[e / n][e % n] = 0.0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < nx; ++i)
-      for (int j = 0; j < ny; ++j) {
-        const int k = i * ny + j;
-        const double e = cx[(i + 1) * ny + j], w = cx[i * ny + j];
-        const double nn = cy[i * (ny + 1) + j + 1], ss = cy[i * (ny + 1) + j];
-        double d = (e + w) + (nn + ss);
-        if (i == 0) d += w;
-        if (i == nx - 1) d += e;
-        if (j == 0) d += ss;
-        if (j == ny - 1) d += nn;
-        a[k][k] = d * idx2;
-        if (i + 1 < nx) a[k][k + ny] = -e * idx2;
-        if (i > 0) a[k][k - ny] = -w * idx2;
-        if (j + 1 < ny) a[k][k + 1] = -nn * idx2;
-        if (j > 0) a[k][k - 1] = -ss * idx2;
-      }
+  // row k of the operator, one thread per row
+  for (int k = threadIdx.x; k < n; k += ST) {
+    const int i = k / ny, j = k - (k / ny) * ny;
+    const double e = cx[(i + 1) * ny + j], w = cx[i * ny + j];
+    const double nn = cy[i * (ny + 1) + j + 1], ss = cy[i * (ny + 1) + j];
+    double d = (e + w) + (nn + ss);
+    if (i == 0) d += w;
+    if (i == nx - 1) d += e;
+    if (j == 0) d += ss;
+    if (j == ny - 1) d += nn;
+    a[k][k] = d * idx2;
+    if (i + 1 < nx) a[k][k + ny] = -e * idx2;
+    if (i > 0) a[k][k - ny] = -w * idx2;
+    if (j + 1 < ny) a[k][k + 1] = -nn * idx2;
+    if (j > 0) a[k][k - 1] = -ss * idx2;
   }
   __syncthreads();
   // two phases per pivot, each only reading what the previous phase wrote:
   // (1) the scaled pivot row and the pivot column go to side arrays, (2) the
   // rank-one update writes every row
   for (int p = 0; p < n; ++p) {
-    for (int c = threadIdx.x; c < n; c += blockDim.x)
-      prow[c] = (c == p ? 1.0 : a[p][c]) / a[p][p];
-    for (int r = threadIdx.x; r < n; r += blockDim.x) fcol[r] = (r == p) ? 0.0 : a[r][p];
+    for (int c = threadIdx.x; c < n; c += ST) prow[c] = (c == p ? 1.0 : a[p][c]) / a[p][p];
+    for (int r = threadIdx.x; r < n; r += ST) fcol[r] = (r == p) ? 0.0 : a[r][p];
     __syncthreads();
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    for (int e = threadIdx.x; e < n * n; e += ST) {
       const int r = e / n, c = e % n;
       a[r][c] = (r == p) ? prow[c] : (c == p ? 0.0 : a[r][c]) - fcol[r] * prow[c];
     }
     __syncthreads();
   }
   float* inv = ws_f + P.cinv;
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) inv[e] = (float)a[e / n][e % n];
+  for (int e = threadIdx.x; e < n * n; e += ST) inv[e] = (float)a[e / n][e % n];
 }
 
 // the one-CTA kernel's dynamic shared memory at most: 227 KB less its static
@@ -1491,38 +1515,36 @@ int zb_poisson_setup(const zb_poisson_cfg* cfg, const void* h, int dtype, void* 
   if (!valid(cfg) || !h || !ws || (dtype != ZB_F32 && dtype != ZB_F64)) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
   if (wsb < (size_t)P.bytes) return ZB_E_ARG;
-  cudaStream_t st = (cudaStream_t)stream;
-  float* fw = (float*)((char*)ws + P.fbase);
-  double* dw = (double*)ws;
-  const Level& L0 = P.L[0];
-  const long long nf = (long long)(L0.nx + 1) * L0.ny + (long long)L0.nx * (L0.ny + 1);
-  if (dtype == ZB_F64)
-    coef_from_h<double><<<grid_for(nf), NT, 0, st>>>((const double*)h, L0.nx, L0.ny, cfg->cmin,
-                                                     cfg->cmax, dw + P.cx64, dw + P.cy64,
-                                                     fw + L0.cx, fw + L0.cy);
-  else
-    coef_from_h<float><<<grid_for(nf), NT, 0, st>>>((const float*)h, L0.nx, L0.ny, cfg->cmin,
-                                                    cfg->cmax, dw + P.cx64, dw + P.cy64,
-                                                    fw + L0.cx, fw + L0.cy);
   if (P.small0 < P.nlev &&
       (coarse_smem(P) > COARSE_SMEM_MAX || P.nlev - P.small0 > CT_MAX_LEVELS))
     return ZB_E_TOO_LARGE;
   if (const int e = enable_coarse_smem()) return e;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* fw = (float*)((char*)ws + P.fbase);
+  double* dw = (double*)ws;
+  const Level& L0 = P.L[0];
   const long long n0 = (long long)L0.nx * L0.ny;
-  diag_kernel64<<<grid_for(n0), NT, 0, st>>>(dw + P.cx64, dw + P.cy64, L0.nx, L0.ny,
-                                             1.0 / (cfg->dx * cfg->dx), dw + P.dg64);
-  for (int l = 0; l < P.nlev; ++l) {
+  const double idx2 = 1.0 / (cfg->dx * cfg->dx);
+  const float idx2f = 1.0f / (L0.dx * L0.dx);
+  if (dtype == ZB_F64)
+    setup0_kernel<double><<<grid_for(n0), NT, 0, st>>>(
+        (const double*)h, L0.nx, L0.ny, cfg->cmin, cfg->cmax, idx2, idx2f, dw + P.cx64,
+        dw + P.cy64, dw + P.dg64, fw + L0.cx, fw + L0.cy, fw + L0.idg);
+  else
+    setup0_kernel<float><<<grid_for(n0), NT, 0, st>>>(
+        (const float*)h, L0.nx, L0.ny, cfg->cmin, cfg->cmax, idx2, idx2f, dw + P.cx64,
+        dw + P.cy64, dw + P.dg64, fw + L0.cx, fw + L0.cy, fw + L0.idg);
+  // levels above the one-CTA part: one launch each; the rest and the
+  // coarsest inverse: one CTA
+  const int l_small = std::max(1, std::min(P.small0, P.nlev));
+  for (int l = 1; l < l_small; ++l) {
     const Level& L = P.L[l];
-    if (l > 0) {
-      const Level& Lf = P.L[l - 1];
-      const long long nfc = (long long)(L.nx + 1) * L.ny + (long long)L.nx * (L.ny + 1);
-      coarsen_kernel<<<grid_for(nfc), NT, 0, st>>>(fw + Lf.cx, fw + Lf.cy, L.nx, L.ny, fw + L.cx,
-                                                   fw + L.cy);
-    }
-    diag_kernel32<<<grid_for((long long)L.nx * L.ny), NT, 0, st>>>(
-        fw + L.cx, fw + L.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.idg);
+    const Level& Lf = P.L[l - 1];
+    coarsen_kernel<<<grid_for((long long)L.nx * L.ny), NT, 0, st>>>(
+        fw + Lf.cx, fw + Lf.cy, L.nx, L.ny, 1.0f / (L.dx * L.dx), fw + L.cx, fw + L.cy,
+        fw + L.idg);
   }
-  if (P.cinv >= 0) coarse_inverse_kernel<<<1, 256, 0, st>>>(P, fw);
+  if (l_small < P.nlev || P.cinv >= 0) small_setup_kernel<<<1, ST, 0, st>>>(P, fw, l_small);
   ZB_CUDA_TRY(cudaMemsetAsync(dw + P.scal, 0, S_COUNT * sizeof(double), st));
   return zb_launch_check();
 }
