@@ -543,17 +543,17 @@ def poisson_solve_bytes(cells, iterations, levels):
     cells: what the kernels must stream per cell.  Per FCG iteration (float64
     vectors, float64 level-0 face coefficients): q = A p with the p.q and p.r
     dots reads p, r, cx, cy and writes q (40 B); x += a p, r -= a q reads x,
-    p, r, q and writes x, r and the float32 copy of r (52 B); z = z32 with z.q
-    reads z32, q and writes z (20 B); p = z - b p reads z, p and writes p
-    (24 B); the V-cycle (float32) per level reads f, cx, cy, dg and writes x
-    and a quarter-size coarse right-hand side on the way down (21 B), reads
-    f, cx, cy, dg, x and the quarter-size correction and writes x on the way
-    up (25 B), over levels shrinking 4x (46 B x 4/3).  The start is one
-    residual (x, b, cx, cy read; r, r32 written: 44 B), one V-cycle, z = z32
-    and p = z (12 + 16 B)."""
+    p, r, q and writes x, r and the float32 copy of r (52 B); z.q reads the
+    V-cycle's float32 z and q (12 B); p = z - b p reads z (float32) and p and
+    writes p (20 B); the V-cycle (float32) per level reads f, cx, cy, dg and
+    writes x and a quarter-size coarse right-hand side on the way down (21 B),
+    reads f, cx, cy, dg, x and the quarter-size correction and writes x on the
+    way up (25 B), over levels shrinking 4x (46 B x 4/3).  The start is one
+    residual (x, b, cx, cy read; r, r32 written: 44 B), one V-cycle and p = z
+    (12 B)."""
     vcycle = 46.0 * (1.0 - 0.25 ** levels) / 0.75
-    per_it = 40 + 52 + 20 + 24 + vcycle
-    start = 44 + vcycle + 12 + 16
+    per_it = 40 + 52 + 12 + 20 + vcycle
+    start = 44 + vcycle + 12
     return int(cells * (start + iterations * per_it))
 
 

@@ -436,10 +436,11 @@ enum { ZB_PRECOND_NONE = 0, ZB_PRECOND_MG = 1, ZB_PRECOND_LEARNED = 2,
 
 size_t zb_poisson_workspace_bytes(const zb_poisson_cfg* cfg);
 
-/* Byte offsets inside the workspace: [0] r, [1] z, [2] p, [3] q (float64
- * Krylov vectors), [4] scalars (float64: b.b, r.r, p.q, p.r, z.q, alpha,
- * beta, relative residual at index 7, iteration count at 8), [5] the float32
- * result of the last V-cycle on level 0 (z = M r), [6] level-0 float32 f, [7]
+/* Byte offsets inside the workspace: [0] r, [1] -1 (z = M r is not kept in
+ * float64: [5] is z, converted exactly where it is read), [2] p, [3] q
+ * (float64 Krylov vectors), [4] scalars (float64: b.b, r.r, p.q, p.r, z.q,
+ * alpha, beta, relative residual at index 7, iteration count at 8), [5] the
+ * float32 result of the last V-cycle on level 0 (z = M r), [6] level-0 float32 f, [7]
  * number of levels, [8] first one-CTA level, [9] level-0 float32 x-face
  * coefficients, [10] y-face coefficients.  out holds 11. */
 int zb_poisson_layout(const zb_poisson_cfg* cfg, int64_t* out);

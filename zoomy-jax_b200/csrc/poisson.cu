@@ -50,7 +50,8 @@ struct Plan {
   int nlev, small0;          // number of levels, first one-CTA level
   Level L[MAXL];
   long long cx64, cy64, dg64;  // double offsets (level-0 operator)
-  long long vr, vz, vp, vq;    // double offsets (Krylov vectors)
+  long long vr, vp, vq;        // double offsets (Krylov vectors; z is the V-cycle's float32
+                               // result on level 0, converted where it is read)
   long long part;              // double offset of the reduction partials
   long long scal;              // double offset of the scalars
   long long cinv;              // float offset of the coarsest inverse (-1: none)
@@ -146,7 +147,6 @@ static Plan make_plan(const zb_poisson_cfg* c) {
   P.cy64 = d; d += (long long)c->nx * (c->ny + 1);
   P.dg64 = d; d += C;
   P.vr = d; d += C;
-  P.vz = d; d += C;
   P.vp = d; d += C;
   P.vq = d; d += C;
   P.part = d; d += 4 * RED_BLOCKS;
@@ -354,32 +354,27 @@ update_xr_kernel(double* __restrict__ x, double* __restrict__ r, const double* _
   finish_scalars(part_rr, nullptr, counter, scal, S_RR, 0, FIN_REL, red);
 }
 
-// z = (double) z32 ; partial z.q
+// partial z.q with z = (double) z32, the V-cycle's float32 result (the
+// conversion is exact, so z is never stored in float64)
 __global__ void __launch_bounds__(NT)
-z_from32_kernel(const float* __restrict__ z32, double* __restrict__ z,
-                const double* __restrict__ q, long long n, double* part_zq, unsigned* counter,
-                double* scal) {
+zq_kernel(const float* __restrict__ z32, const double* __restrict__ q, long long n,
+          double* part_zq, unsigned* counter, double* scal) {
   pdl_enter();
   __shared__ double red[NT / 32];
   double s = 0.0;
-  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT) {
-    const double v = (double)z32[k];
-    z[k] = v;
-    if (q) s += v * q[k];
-  }
-  if (part_zq) {
-    block_sum(s, red, &part_zq[blockIdx.x]);
-    finish_scalars(part_zq, nullptr, counter, scal, S_ZQ, 0, FIN_BETA, red);
-  }
+  for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
+    s += (double)z32[k] * q[k];
+  block_sum(s, red, &part_zq[blockIdx.x]);
+  finish_scalars(part_zq, nullptr, counter, scal, S_ZQ, 0, FIN_BETA, red);
 }
 
-// p = z - beta p
-__global__ void p_update_kernel(double* __restrict__ p, const double* __restrict__ z,
+// p = z - beta p, z = (double) z32
+__global__ void p_update_kernel(double* __restrict__ p, const float* __restrict__ z32,
                                 const double* scal, long long n, int first) {
   pdl_enter();
   const double b = first ? 0.0 : scal[S_BETA];
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
-    p[k] = first ? z[k] : z[k] - b * p[k];
+    p[k] = first ? (double)z32[k] : (double)z32[k] - b * p[k];
 }
 
 // loop control of the graph solve: counts the iteration and keeps the WHILE
@@ -396,13 +391,13 @@ __device__ __forceinline__ void fcg_loop_control(double* scal, cudaGraphConditio
 // p_update with the graph solve's loop control folded in (block 0, thread 0;
 // it reads S_REL, set by update_xr before the V-cycle, and writes S_ITER,
 // which p_update does not touch): one launch fewer per iteration
-__global__ void p_update_cond_kernel(double* __restrict__ p, const double* __restrict__ z,
+__global__ void p_update_cond_kernel(double* __restrict__ p, const float* __restrict__ z32,
                                      double* scal, long long n, int first,
                                      cudaGraphConditionalHandle h, double tol, int maxit) {
   pdl_enter();
   const double b = first ? 0.0 : scal[S_BETA];
   for (long long k = blockIdx.x * (long long)NT + threadIdx.x; k < n; k += (long long)gridDim.x * NT)
-    p[k] = first ? z[k] : z[k] - b * p[k];
+    p[k] = first ? (double)z32[k] : (double)z32[k] - b * p[k];
   if (blockIdx.x == 0 && threadIdx.x == 0) fcg_loop_control(scal, h, tol, maxit, first);
 }
 
@@ -1494,10 +1489,11 @@ size_t zb_poisson_workspace_bytes(const zb_poisson_cfg* cfg) {
 int zb_poisson_layout(const zb_poisson_cfg* cfg, int64_t* out) {
   if (!valid(cfg) || !out) return ZB_E_ARG;
   const Plan P = make_plan(cfg);
-  // byte offsets: r, z, p, q (float64 Krylov vectors), scalars, the V-cycle's
-  // float result on level 0 and level-0 f, number of levels, first one-CTA level
+  // byte offsets: r, (none), p, q (float64 Krylov vectors), scalars, the
+  // V-cycle's float result on level 0 (z) and level-0 f, number of levels,
+  // first one-CTA level
   out[0] = P.vr * 8;
-  out[1] = P.vz * 8;
+  out[1] = -1;   // no float64 z: [5] holds z = M r
   out[2] = P.vp * 8;
   out[3] = P.vq * 8;
   out[4] = P.scal * 8;
@@ -1633,15 +1629,13 @@ static int fcg_start_impl(const zb_poisson_cfg* cfg, void* ws, const double* b, 
                          scal));
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
-  ZB_CUDA_TRY(pdl_launch(z_from32_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
-                         (const float*)(fw + P.L[0].xo), dw + P.vz, (const double*)nullptr, n,
-                         (double*)nullptr, (unsigned*)nullptr, scal));
+  const float* z32 = fw + P.L[0].xo;
   if (lc)
     ZB_CUDA_TRY(pdl_launch(p_update_cond_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
-                           (const double*)(dw + P.vz), scal, n, 1, lc->h, lc->tol, lc->maxit));
+                           z32, scal, n, 1, lc->h, lc->tol, lc->maxit));
   else
-    ZB_CUDA_TRY(pdl_launch(p_update_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
-                           (const double*)(dw + P.vz), (const double*)scal, n, 1));
+    ZB_CUDA_TRY(pdl_launch(p_update_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp, z32,
+                           (const double*)scal, n, 1));
   return zb_launch_check();
 }
 
@@ -1672,15 +1666,15 @@ static int fcg_iterate_impl(const zb_poisson_cfg* cfg, void* ws, double* x, int 
                          part + 2 * RED_BLOCKS, fw + P.L[0].f, ctr + 2));
   int rc = vcycle(P, ws, precond, smo, st);
   if (rc) return rc;
-  ZB_CUDA_TRY(pdl_launch(z_from32_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st,
-                         (const float*)(fw + P.L[0].xo), dw + P.vz, (const double*)(dw + P.vq), n,
-                         part + 3 * RED_BLOCKS, ctr + 3, scal));
+  const float* z32 = fw + P.L[0].xo;
+  ZB_CUDA_TRY(pdl_launch(zq_kernel, dim3(RED_BLOCKS), dim3(NT), 0, st, z32,
+                         (const double*)(dw + P.vq), n, part + 3 * RED_BLOCKS, ctr + 3, scal));
   if (lc)
     ZB_CUDA_TRY(pdl_launch(p_update_cond_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
-                           (const double*)(dw + P.vz), scal, n, 0, lc->h, lc->tol, lc->maxit));
+                           z32, scal, n, 0, lc->h, lc->tol, lc->maxit));
   else
-    ZB_CUDA_TRY(pdl_launch(p_update_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp,
-                           (const double*)(dw + P.vz), (const double*)scal, n, 0));
+    ZB_CUDA_TRY(pdl_launch(p_update_kernel, dim3(grid_for(n)), dim3(NT), 0, st, dw + P.vp, z32,
+                           (const double*)scal, n, 0));
   return zb_launch_check();
 }
 
