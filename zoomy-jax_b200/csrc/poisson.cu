@@ -584,14 +584,17 @@ prolong_add_kernel(const float* __restrict__ ec, float* __restrict__ xf, int nxc
 // one-kernel-per-sweep sequence.
 constexpr int FT = 32;            // tile side of the levels with a tile for every SM
 constexpr int FTS = 16;           // tile side of the smaller levels
-constexpr int FNT_MAX = 1024;
 // threads of a fused level CTA (one-dimensional): 256 for the 32^2 tiles, 512
 // for the 16^2 ones; a compile-time count lets every phase's item loop have a
 // fixed trip count
 __host__ __device__ constexpr int fused_threads(int tile) { return tile == FT ? 256 : 512; }
+// register cap of the level kernels: 64 per thread (four 256-thread CTAs per
+// SM; capped for five CTAs, at 46-48 registers, the V-cycle ran 2 % slower)
+constexpr int FNT_MAX = 1024;
 
 // Staged layout of a tile with its ring: R = tile + 2 halo rows; the arrays
-// x, f, r, idg (R rows) and cx (R + 1 rows) keep PAD leading columns so that
+// x, f (the residual overwrites it), idg (R rows) and cx (R + 1 rows) keep PAD
+// leading columns so that
 // every staged row starts on a 16-byte boundary of the level's row (its first
 // column j0 - halo - PAD is a multiple of 4) and a row stride RS, a multiple
 // of 4 floats; cy (R rows of R + 1) stays unpadded.
@@ -606,7 +609,7 @@ __host__ __device__ inline size_t up_tile_smem(int halo, int tile) {
 }
 __host__ __device__ inline size_t fused_smem(int halo, int tile) {
   const int R = tile + 2 * halo, RS = stage_rs(halo, tile);
-  return (size_t)(4 * R * RS + (R + 1) * RS + R * (R + 1)) * sizeof(float);
+  return (size_t)(3 * R * RS + (R + 1) * RS + R * (R + 1)) * sizeof(float);
 }
 
 // 4-byte asynchronous global -> shared copy; src_bytes 0 writes a zero
@@ -627,7 +630,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Shared-memory image of a level's tile plus a HALO-wide ring: x, f, r, idg
+// Shared-memory image of a level's tile plus a HALO-wide ring: x, f (r), idg
 // (R x R) and the face coefficients cx ((R+1) x R), cy (R x (R+1)).  A tile
 // whose ring lies wholly inside the level (most of them) takes the EDGE-free
 // path: no domain tests and no Dirichlet ghosts.
@@ -637,7 +640,7 @@ struct Stage {
   static constexpr int PAD = stage_pad(HALO);
   static constexpr int RS = stage_rs(HALO, TT);
   static constexpr int NTH = fused_threads(TT);
-  // staged element (a, b) of x, f, r, idg (a in [0, R)) or cx (a in [0, R])
+  // staged element (a, b) of x, f, idg (a in [0, R)) or cx (a in [0, R])
   __device__ static constexpr int at(int a, int b) { return a * RS + b + PAD; }
   int i0, j0, nx, ny;
   bool interior;
@@ -761,8 +764,10 @@ __device__ Stage<HALO, TT> stage_level(float* sm, int i0, int j0, int nx, int ny
   St S;
   S.i0 = i0; S.j0 = j0; S.nx = nx; S.ny = ny;
   S.interior = i0 - HALO >= 0 && j0 - HALO >= 0 && i0 - HALO + R <= nx && j0 - HALO + R <= ny;
-  S.x = sm; S.f = sm + R * RS; S.r = sm + 2 * R * RS; S.idg = sm + 3 * R * RS;
-  S.cx = sm + 4 * R * RS; S.cy = S.cx + (R + 1) * RS;
+  // the residual overwrites f in place (a cell's residual reads only its own
+  // f), so r shares f's array
+  S.x = sm; S.f = sm + R * RS; S.r = S.f; S.idg = sm + 2 * R * RS;
+  S.cx = sm + 3 * R * RS; S.cy = S.cx + (R + 1) * RS;
   S.ec = S.cy + R * (R + 1);
   constexpr int nt = St::NTH;
   const int tid = threadIdx.x;
