@@ -264,7 +264,10 @@ class ChorinSolver(HyperbolicSolver):
     def _hyperbolic_stage(self, dt, time, Q):
         """One Euler step of the shallow-water predictor (plus Manning as
         RK1), ``solver_chorin_vam_jax.py:495-522``."""
-        Qn = Q.clone()
+        import torch
+        # the stage writes rows 1..3 of every cell; only b is carried over
+        Qn = torch.empty_like(Q)
+        Qn[0].copy_(Q[0])
         self._stage(self.cfg, Q, None, Qn, 0.0, 1.0, dt)
         if self.cfg.manning_n != 0.0:
             hinv = self.update_qaux(Q)[6].contiguous()
