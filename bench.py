@@ -465,11 +465,14 @@ def run_gpu(args, rank, world, local_rank, dtype_key=None, with_e2e=True):
     td = torch.float32 if dtype == "float32" else torch.float64
     host_in = torch.as_tensor(Q_host, dtype=td).contiguous().pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
-    # two pinned control-block buffers: the host checks step k's block while
-    # step k + 1 runs (every step's result is read back and checked, one step
-    # behind, as a driver that overlaps its checks with the device would)
-    ctrl_host = [torch.empty(L.CTRL_BYTES, dtype=torch.uint8).pin_memory() for _ in range(2)]
-    ctrl_ev = [torch.cuda.Event() for _ in range(2)]
+    # a ring of pinned control-block buffers: the host checks step k's block
+    # while steps k + 1 .. k + lag run (every step's result is read back and
+    # checked, lag steps behind, as a driver that overlaps its checks with the
+    # device would)
+    lag = max(1, int(args.e2e_lag))
+    ring = lag + 1
+    ctrl_host = [torch.empty(L.CTRL_BYTES, dtype=torch.uint8).pin_memory() for _ in range(ring)]
+    ctrl_ev = [torch.cuda.Event() for _ in range(ring)]
     Qd = torch.empty_like(Q)
 
     def check_ctrl(buf):
@@ -492,13 +495,14 @@ def run_gpu(args, rank, world, local_rank, dtype_key=None, with_e2e=True):
         for k in range(steps):
             rc = lib.zb_swe2d_step(cfg, L.ptr(Qd), ws, wsb, ctrl, k % 3, sp)
             L.check(rc, "zb_swe2d_step")
-            ctrl_host[k % 2].copy_(solver._ctrl, non_blocking=True)
-            ctrl_ev[k % 2].record(stream)
-            if k > 0:
-                ctrl_ev[(k - 1) % 2].synchronize()
-                check_ctrl(ctrl_host[(k - 1) % 2])
-        ctrl_ev[(steps - 1) % 2].synchronize()
-        check_ctrl(ctrl_host[(steps - 1) % 2])
+            ctrl_host[k % ring].copy_(solver._ctrl, non_blocking=True)
+            ctrl_ev[k % ring].record(stream)
+            if k >= lag:
+                ctrl_ev[(k - lag) % ring].synchronize()
+                check_ctrl(ctrl_host[(k - lag) % ring])
+        for j in range(max(0, steps - lag), steps):
+            ctrl_ev[j % ring].synchronize()
+            check_ctrl(ctrl_host[j % ring])
         host_out.copy_(Qd, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
@@ -520,9 +524,9 @@ def run_gpu(args, rank, world, local_rank, dtype_key=None, with_e2e=True):
            "d2h_bytes_per_step": L.CTRL_BYTES + state_bytes // K,
            "how": ("public C ABI (zb_swe2d_init/zb_swe2d_step) with pinned host "
                    "buffers: state upload, K steps each followed by a D2H read of the "
-                   "step's control block that the host checks while the next step runs, "
-                   "state download; after one untimed warm-up pass of W steps through the "
-                   "same pinned buffers")}
+                   f"step's control block that the host checks while the next {lag} "
+                   "step(s) run, state download; after one untimed warm-up pass of W steps "
+                   "through the same pinned buffers")}
     out["e2e"] = e2e
     return out
 
@@ -861,6 +865,9 @@ def main():
                          "captures use a smaller mesh)")
     ap.add_argument("--tri-host-prep", type=int, default=1,
                     help="also time the host mesh builder in the triangles leg (0: skip)")
+    ap.add_argument("--e2e-lag", type=int, default=2,
+                    help="steps the e2e host loop runs ahead of the control-block check "
+                         "(every step's block is still read and checked)")
     ap.add_argument("--chorin-no-graph", action="store_true",
                     help="drive the pressure iterations from the host (for profilers, which "
                          "do not list kernels inside conditional graph nodes)")
