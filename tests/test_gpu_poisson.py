@@ -80,6 +80,8 @@ def test_apply_matches_oracle(nx, ny):
     (96, 80, 1, 4),       # tiles cut by the domain edge, levels of odd tile counts
     (512, 512, 3, 8),     # mostly interior tiles (the edge-free path)
     (200, 136, 2, 8),     # coarsening stops at 25 x 17: no one-CTA level, swept coarsest
+    (7, 5, 2, 4),         # one level, solved by its dense inverse (built from level 0's faces)
+    (6, 6, 1, 2),         # every level in the one-CTA kernel, 3 x 3 coarsest
 ])
 def test_vcycle_matches_oracle(nx, ny, nu, coarsest):
     rng = np.random.default_rng(2)
