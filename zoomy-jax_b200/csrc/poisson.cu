@@ -1081,18 +1081,63 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
     }
   cp_async_wait_all();
   __syncthreads();
+  // The first level's cell of each thread keeps its operands in registers for
+  // the whole cycle (its faces, inverse diagonal and right-hand side do not
+  // change): its half-sweeps and residual then read only the neighbours' x,
+  // with nbsum_at's and apply_at's expressions in their order
+  const CLevel c0 = tab[l0];
+  const int i0c = t >> c0.sh, j0c = t & ((1 << c0.sh) - 1);
+  const bool own0 = t < c0.act && i0c < c0.nx && j0c < c0.ny;
+  const int k0c = own0 ? i0c * c0.ny + j0c : 0;
+  float ce = 0.0f, cw = 0.0f, cn = 0.0f, cs = 0.0f, f0c = 0.0f, g0c = 0.0f;
+  if (own0) {
+    ce = sm[c0.cx + (i0c + 1) * c0.ny + j0c];
+    cw = sm[c0.cx + i0c * c0.ny + j0c];
+    cn = sm[c0.cy + i0c * (c0.ny + 1) + j0c + 1];
+    cs = sm[c0.cy + i0c * (c0.ny + 1) + j0c];
+    f0c = sm[c0.f + k0c];
+    g0c = sm[c0.idg + k0c];
+  }
+  const bool hasE = i0c + 1 < c0.nx, hasW = i0c > 0, hasN = j0c + 1 < c0.ny, hasS = j0c > 0;
+  float* const x0 = sm + c0.x;
+  // half-sweep of `color` on the first level
+  auto half0 = [&](int color, bool from_zero) {
+    if (own0 && ((i0c + j0c + color) & 1) == 0) {
+      float nb = 0.0f;
+      if (!from_zero) {
+        const float xe = hasE ? x0[k0c + c0.ny] : 0.0f, xw = hasW ? x0[k0c - c0.ny] : 0.0f;
+        const float xn = hasN ? x0[k0c + 1] : 0.0f, xs = hasS ? x0[k0c - 1] : 0.0f;
+        nb = (ce * xe + cw * xw) + (cn * xn + cs * xs);
+      }
+      x0[k0c] = (f0c + c0.idx2 * nb) * g0c;
+    }
+  };
   // descend: pre-smoothing, residual, restriction into the next level's f
   for (int l = l0; l < nl - 1; ++l) {
     const CLevel c = tab[l];
     const int id = 1 + l - l0;
     if (t < c.act) {
-      for (int s = 0; s < nu; ++s) {
-        cl_half(sm, c, t, 0, s == 0);
-        level_sync(id, c.act);
-        cl_half(sm, c, t, 1, false);
-        level_sync(id, c.act);
-      }
-      {
+      if (l == l0) {
+        for (int s = 0; s < nu; ++s) {
+          half0(0, s == 0);
+          level_sync(id, c.act);
+          half0(1, false);
+          level_sync(id, c.act);
+        }
+        if (own0) {
+          const float xc = x0[k0c];
+          const float xe = hasE ? x0[k0c + c0.ny] : -xc, xw = hasW ? x0[k0c - c0.ny] : -xc;
+          const float xn = hasN ? x0[k0c + 1] : -xc, xs = hasS ? x0[k0c - 1] : -xc;
+          sm[c0.r + k0c] =
+              f0c - (ce * (xc - xe) + cw * (xc - xw) + cn * (xc - xn) + cs * (xc - xs)) * c0.idx2;
+        }
+      } else {
+        for (int s = 0; s < nu; ++s) {
+          cl_half(sm, c, t, 0, s == 0);
+          level_sync(id, c.act);
+          cl_half(sm, c, t, 1, false);
+          level_sync(id, c.act);
+        }
         const int i = t >> c.sh, j = t & ((1 << c.sh) - 1);
         if (i < c.nx && j < c.ny) {
           float od;
@@ -1161,16 +1206,17 @@ coarse_vcycle_kernel(const Plan P, float* ws_f, int nu, int coarse_sweeps) {
       }
       level_sync(id, c.act);
       for (int s = 0; s < nu; ++s) {
-        cl_half(sm, c, t, 1, false);
+        if (l == l0) half0(1, false);
+        else cl_half(sm, c, t, 1, false);
         level_sync(id, c.act);
-        cl_half(sm, c, t, 0, false);
+        if (l == l0) half0(0, false);
+        else cl_half(sm, c, t, 0, false);
         level_sync(id, c.act);
       }
     }
   }
   __syncthreads();
   const Level& L0 = P.L[l0];
-  const CLevel c0 = tab[l0];
   for (int k = t; k < L0.nx * L0.ny; k += CT) ws_f[L0.xo + k] = sm[c0.x + k];
 }
 
